@@ -1,0 +1,126 @@
+/*
+ * fdref — CPU oracle for the perturbation hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY. This library is a plain C++ restatement of the
+ * reference CPU kernel (crates/fd-kernel, crates/fd-fixed, crates/fd-samples of
+ * junovhs/fractodactyl). It is the parity checker for the CUDA route and the timed
+ * CPU baseline. Nothing in the product (the fractodactyl_b200 package and its
+ * CUDA library) links, loads or calls it; only tests/, __graft_entry__.smoke() and
+ * bench.py's CPU-baseline leg do.
+ *
+ * Parity pins (checked by tests/test_oracle_golden.py):
+ *   - FNV-1a hashes of four 8x4 .fds renders (crates/fd-kernel/src/sample.rs:715-752)
+ *   - exact escape counts of the reference's sample tests (sample.rs:965-1340)
+ *   - the frozen mpmath truth pack bench/truth/v1 (5 cases x 1024 observations)
+ *   - per-frame digests of crates/fd-kernel/fixtures/KERN-05.bundle (minor-0 frames)
+ *
+ * Build: oracle/Makefile (g++ -O2 -ffp-contract=off; no FMA contraction, as Rust).
+ */
+#ifndef FDREF_H
+#define FDREF_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Column bits, as fd-samples Column (crates/fd-samples/src/column.rs:7-24). */
+enum { FDREF_COL_CLASS = 1, FDREF_COL_NU = 2, FDREF_COL_DE = 4, FDREF_COL_NORMAL = 8 };
+
+/* Tier (crates/fd-kernel/src/view.rs:7-14); -1 = cheapest valid. */
+enum { FDREF_TIER_AUTO = -1, FDREF_TIER_F64 = 0, FDREF_TIER_FIXED = 1, FDREF_TIER_SCALED = 2 };
+
+/* View + Params (crates/fd-samples/src/header.rs:14-27, crates/fd-kernel/src/grid.rs:17-38). */
+typedef struct {
+  const char *center_re;
+  const char *center_im;
+  const char *width;
+  double rotation;
+  uint32_t nx, ny, ss;
+  uint64_t max_iter;
+  double escape_radius;
+  uint32_t columns; /* FDREF_COL_* bits; CLASS implied */
+  int32_t threads;
+  int32_t tier;
+} fdref_job;
+
+typedef struct fdref_ref fdref_ref; /* Reference orbit (reference.rs:7-10) + bits */
+typedef struct fdref_bla fdref_bla; /* Bla table (bla.rs:137-151) */
+
+/* Outcome of one sample (sample.rs:21-40): kind 0 escaped, 1 interior, 2 unresolved. */
+typedef struct {
+  int32_t kind;
+  uint64_t n;
+  double zr, zi, dr, di;
+  int64_t dexp;
+  uint64_t blocks, skipped;
+  double shift;
+} fdref_outcome;
+
+/* Work counters: Stats (grid.rs:41-49) + BlaStats (grid.rs:53-70). */
+typedef struct {
+  uint64_t reference_len;
+  uint64_t iterations;
+  uint64_t blocks, skipped, fallback_samples, closed_form_samples;
+  double shift_px; /* NaN when untracked */
+} fdref_stats;
+
+const char *fdref_last_error(void);
+
+/* Plane::new (view.rs:42-87): spacing h = h_m 2^h_e, tier, bits, centre as f64. */
+int fdref_plane(const fdref_job *job, double *h_m, int64_t *h_e, int32_t *tier,
+                uint64_t *bits, double *c_re, double *c_im);
+
+/* grid::reference (grid.rs:87-90) for the job, or an orbit from arrays. */
+fdref_ref *fdref_reference(const fdref_job *job);
+fdref_ref *fdref_reference_f64(double c_re, double c_im, uint64_t max_iter, double escape_radius);
+fdref_ref *fdref_reference_fixed(const char *re, const char *im, uint64_t bits, uint64_t max_iter);
+fdref_ref *fdref_reference_arrays(const double *re, const double *im, uint64_t len, uint32_t bits);
+uint64_t fdref_ref_len(const fdref_ref *r);
+uint32_t fdref_ref_bits(const fdref_ref *r);
+void fdref_ref_copy(const fdref_ref *r, double *re, double *im);
+int64_t fdref_ref_nucleus_period(const fdref_ref *r); /* -1 for None */
+void fdref_ref_free(fdref_ref *r);
+
+/* Bla::build_scaled (bla.rs:161-181). NULL + error on refusal. */
+fdref_bla *fdref_bla_build(const fdref_ref *r, double eps, double dc_max, int64_t dc_exp);
+uint32_t fdref_bla_levels(const fdref_bla *t);
+/* Export level-major [f64;7] blocks (a.re,a.im,b.re,b.im,r,alpha,beta), bla.rs:52-57. */
+uint64_t fdref_bla_block_count(const fdref_bla *t);
+void fdref_bla_export(const fdref_bla *t, double *blocks7, uint64_t *level_offsets);
+/* Bla::find (bla.rs:234-249): returns the step count (0 for None) and the block index. */
+uint64_t fdref_bla_find(const fdref_bla *t, uint64_t m, double d2, uint64_t budget,
+                        uint64_t *level, uint64_t *index);
+void fdref_bla_free(fdref_bla *t);
+/* grid::bla_dc_bound (grid.rs:418-427). */
+int fdref_bla_dc_bound(const fdref_job *job, double *dc, int64_t *e);
+
+/* sample::iterate (sample.rs:170-581) for one sample. extended: Binary64Exponent.
+ * has_c: absolute c for the closed-form test. nucleus: -2 = take r.nucleus_period(),
+ * -1 = None, else the period. */
+int fdref_iterate(const fdref_ref *r, const fdref_bla *bla, int extended, int derivative,
+                  int has_c, double cr, double ci, double ar, double ai, int64_t offset_exp,
+                  uint64_t max_iter, double r2, int64_t nucleus, fdref_outcome *out);
+
+/* render_with / render_bla (grid.rs:106-208, run :446-535). Caller-owned outputs of
+ * nx*ny entries; any may be NULL. ref NULL: computed (grid.rs:802-815). bla NULL: plain. */
+int fdref_render(const fdref_job *job, const fdref_ref *ref, const fdref_bla *bla,
+                 uint8_t *cls, double *nu, float *de, uint16_t *normal, uint64_t *n_out,
+                 double *z_out, double *dz_out, int64_t *dexp_out, fdref_stats *stats,
+                 char *kernel, size_t kernel_cap);
+
+/* Encode one escaped state's columns exactly as Store::put (store.rs:66-112). */
+void fdref_store_escaped(double h_m, int64_t h_e, uint32_t ss, double rotation, uint64_t n,
+                         double zr, double zi, double dr, double di, int64_t dexp,
+                         double *nu, float *de, uint16_t *normal);
+
+/* The .fds v1 bytes of a render (fd_samples::write, crates/fd-samples/src/write.rs:8-53).
+ * Returns the byte count; writes at most cap bytes (call with cap 0 to size). */
+int64_t fdref_render_fds(const fdref_job *job, const fdref_ref *ref, const fdref_bla *bla,
+                         uint8_t *buf, uint64_t cap);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

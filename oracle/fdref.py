@@ -1,0 +1,296 @@
+"""ctypes binding of the CPU oracle (liboracle.so, see fdref.h).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and bench.py's
+CPU-baseline leg, never by the product package.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+
+COL_CLASS, COL_NU, COL_DE, COL_NORMAL = 1, 2, 4, 8
+TIER = {None: -1, "auto": -1, "f64": 0, "fx": 1, "fixed": 1, "scaled": 2}
+
+
+class Job(C.Structure):
+    _fields_ = [
+        ("center_re", C.c_char_p),
+        ("center_im", C.c_char_p),
+        ("width", C.c_char_p),
+        ("rotation", C.c_double),
+        ("nx", C.c_uint32),
+        ("ny", C.c_uint32),
+        ("ss", C.c_uint32),
+        ("max_iter", C.c_uint64),
+        ("escape_radius", C.c_double),
+        ("columns", C.c_uint32),
+        ("threads", C.c_int32),
+        ("tier", C.c_int32),
+    ]
+
+
+class Outcome(C.Structure):
+    _fields_ = [
+        ("kind", C.c_int32),
+        ("n", C.c_uint64),
+        ("zr", C.c_double),
+        ("zi", C.c_double),
+        ("dr", C.c_double),
+        ("di", C.c_double),
+        ("dexp", C.c_int64),
+        ("blocks", C.c_uint64),
+        ("skipped", C.c_uint64),
+        ("shift", C.c_double),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("reference_len", C.c_uint64),
+        ("iterations", C.c_uint64),
+        ("blocks", C.c_uint64),
+        ("skipped", C.c_uint64),
+        ("fallback_samples", C.c_uint64),
+        ("closed_form_samples", C.c_uint64),
+        ("shift_px", C.c_double),
+    ]
+
+
+def build():
+    """Compile liboracle.so from the C++ restatement (make in oracle/)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = C.CDLL(LIB)
+        P, D, U64, I64, U32, I32 = C.c_void_p, C.c_double, C.c_uint64, C.c_int64, C.c_uint32, C.c_int32
+        L.fdref_last_error.restype = C.c_char_p
+        L.fdref_plane.argtypes = [C.POINTER(Job), C.POINTER(D), C.POINTER(I64), C.POINTER(I32),
+                                  C.POINTER(U64), C.POINTER(D), C.POINTER(D)]
+        L.fdref_reference.restype = P
+        L.fdref_reference.argtypes = [C.POINTER(Job)]
+        L.fdref_reference_f64.restype = P
+        L.fdref_reference_f64.argtypes = [D, D, U64, D]
+        L.fdref_reference_fixed.restype = P
+        L.fdref_reference_fixed.argtypes = [C.c_char_p, C.c_char_p, U64, U64]
+        L.fdref_reference_arrays.restype = P
+        L.fdref_reference_arrays.argtypes = [P, P, U64, U32]
+        L.fdref_ref_len.restype = U64
+        L.fdref_ref_len.argtypes = [P]
+        L.fdref_ref_bits.restype = U32
+        L.fdref_ref_bits.argtypes = [P]
+        L.fdref_ref_copy.argtypes = [P, P, P]
+        L.fdref_ref_nucleus_period.restype = I64
+        L.fdref_ref_nucleus_period.argtypes = [P]
+        L.fdref_ref_free.argtypes = [P]
+        L.fdref_bla_build.restype = P
+        L.fdref_bla_build.argtypes = [P, D, D, I64]
+        L.fdref_bla_levels.restype = U32
+        L.fdref_bla_levels.argtypes = [P]
+        L.fdref_bla_block_count.restype = U64
+        L.fdref_bla_block_count.argtypes = [P]
+        L.fdref_bla_export.argtypes = [P, P, P]
+        L.fdref_bla_find.restype = U64
+        L.fdref_bla_find.argtypes = [P, U64, D, U64, C.POINTER(U64), C.POINTER(U64)]
+        L.fdref_bla_free.argtypes = [P]
+        L.fdref_bla_dc_bound.argtypes = [C.POINTER(Job), C.POINTER(D), C.POINTER(I64)]
+        L.fdref_iterate.argtypes = [P, P, C.c_int, C.c_int, C.c_int, D, D, D, D, I64, U64, D, I64,
+                                    C.POINTER(Outcome)]
+        L.fdref_render.argtypes = [C.POINTER(Job), P, P, P, P, P, P, P, P, P, P, C.POINTER(Stats),
+                                   C.c_char_p, C.c_size_t]
+        L.fdref_store_escaped.argtypes = [D, I64, U32, D, U64, D, D, D, D, I64,
+                                          C.POINTER(D), C.POINTER(C.c_float), C.POINTER(C.c_uint16)]
+        L.fdref_render_fds.restype = I64
+        L.fdref_render_fds.argtypes = [C.POINTER(Job), P, P, P, U64]
+        _lib = L
+    return _lib
+
+
+def _err():
+    return lib().fdref_last_error().decode()
+
+
+def make_job(re, im, width, nx, ny, max_iter, rotation=0.0, ss=1, escape_radius=1e10,
+             columns=COL_NU | COL_DE | COL_NORMAL, threads=None, tier=None):
+    j = Job()
+    j._keep = [s.encode() if isinstance(s, str) else s for s in (re, im, width)]
+    j.center_re, j.center_im, j.width = j._keep
+    j.rotation = rotation
+    j.nx, j.ny, j.ss = nx, ny, ss
+    j.max_iter = max_iter
+    j.escape_radius = escape_radius
+    j.columns = columns
+    j.threads = threads or os.cpu_count() or 1
+    j.tier = TIER[tier] if not isinstance(tier, int) else tier
+    return j
+
+
+class Ref:
+    """A Reference orbit (crates/fd-kernel/src/reference.rs:7-10) held by the oracle."""
+
+    def __init__(self, handle):
+        if not handle:
+            raise ValueError(_err())
+        self.h = handle
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.fdref_ref_free(self.h)
+            self.h = None
+
+    @classmethod
+    def for_job(cls, job):
+        return cls(lib().fdref_reference(C.byref(job)))
+
+    @classmethod
+    def f64(cls, cr, ci, max_iter, escape_radius):
+        return cls(lib().fdref_reference_f64(cr, ci, max_iter, escape_radius))
+
+    @classmethod
+    def fixed(cls, re, im, bits, max_iter):
+        return cls(lib().fdref_reference_fixed(re.encode(), im.encode(), bits, max_iter))
+
+    @classmethod
+    def arrays(cls, re, im, bits):
+        re = np.ascontiguousarray(re, np.float64)
+        im = np.ascontiguousarray(im, np.float64)
+        return cls(lib().fdref_reference_arrays(re.ctypes.data, im.ctypes.data, len(re), bits))
+
+    def __len__(self):
+        return lib().fdref_ref_len(self.h)
+
+    @property
+    def bits(self):
+        return lib().fdref_ref_bits(self.h)
+
+    def arrays_(self):
+        n = len(self)
+        re, im = np.empty(n), np.empty(n)
+        lib().fdref_ref_copy(self.h, re.ctypes.data, im.ctypes.data)
+        return re, im
+
+    def nucleus_period(self):
+        p = lib().fdref_ref_nucleus_period(self.h)
+        return None if p < 0 else int(p)
+
+
+class Bla:
+    """A BLA table (crates/fd-kernel/src/bla.rs:137-151) built by the oracle."""
+
+    def __init__(self, ref, eps, dc_max, dc_exp=0):
+        self.ref = ref
+        self.h = lib().fdref_bla_build(ref.h, eps, dc_max, dc_exp)
+        if not self.h:
+            raise ValueError(_err())
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.fdref_bla_free(self.h)
+            self.h = None
+
+    @property
+    def levels(self):
+        return lib().fdref_bla_levels(self.h)
+
+    def export(self):
+        """Level-major blocks as an (N, 7) array and level offsets (levels + 1)."""
+        n = lib().fdref_bla_block_count(self.h)
+        blocks = np.zeros((n, 7))
+        offs = np.zeros(self.levels + 1, np.uint64)
+        lib().fdref_bla_export(self.h, blocks.ctypes.data, offs.ctypes.data)
+        return blocks, offs
+
+    def find(self, m, d2, budget):
+        lv, ix = C.c_uint64(), C.c_uint64()
+        n = lib().fdref_bla_find(self.h, m, d2, budget, C.byref(lv), C.byref(ix))
+        return None if n == 0 else (int(lv.value), int(ix.value), int(n))
+
+
+def plane(job):
+    hm, he, tier, bits, cr, ci = C.c_double(), C.c_int64(), C.c_int32(), C.c_uint64(), C.c_double(), C.c_double()
+    if lib().fdref_plane(C.byref(job), C.byref(hm), C.byref(he), C.byref(tier), C.byref(bits), C.byref(cr),
+                         C.byref(ci)) != 0:
+        raise ValueError(_err())
+    return dict(h_m=hm.value, h_e=he.value, tier=tier.value, bits=bits.value, c_re=cr.value, c_im=ci.value)
+
+
+def bla_dc_bound(job):
+    dc, e = C.c_double(), C.c_int64()
+    if lib().fdref_bla_dc_bound(C.byref(job), C.byref(dc), C.byref(e)) != 0:
+        raise ValueError(_err())
+    return dc.value, e.value
+
+
+def iterate(ref, bla=None, extended=False, derivative=True, c=None, ar=0.0, ai=0.0, offset_exp=0,
+            max_iter=1000, r2=1e20, nucleus=-2):
+    """One sample through sample.rs:170-581. nucleus -2: the orbit's own gate."""
+    o = Outcome()
+    rc = lib().fdref_iterate(ref.h, bla.h if bla else None, int(extended), int(derivative), c is not None,
+                             c[0] if c else 0.0, c[1] if c else 0.0, ar, ai, offset_exp, max_iter, r2,
+                             -1 if nucleus is None else nucleus, C.byref(o))
+    if rc != 0:
+        raise ValueError(_err())
+    kind = {0: "escaped", 1: "interior", 2: "unresolved"}[o.kind]
+    return dict(kind=kind, n=o.n, zr=o.zr, zi=o.zi, dr=o.dr, di=o.di, dexp=o.dexp, blocks=o.blocks,
+                skipped=o.skipped, shift=o.shift)
+
+
+def render(job, ref=None, bla=None, raw=False):
+    """render_with / render_bla: columns (and raw outcomes) as numpy arrays."""
+    n = job.nx * job.ny
+    cls = np.zeros(n, np.uint8)
+    nu = np.zeros(n, np.float64)
+    de = np.zeros(n, np.float32)
+    normal = np.zeros(n, np.uint16)
+    it = np.zeros(n, np.uint64)
+    z = np.zeros(2 * n) if raw else None
+    dz = np.zeros(2 * n) if raw else None
+    dexp = np.zeros(n, np.int64) if raw else None
+    st = Stats()
+    kernel = C.create_string_buffer(256)
+    ptr = lambda a: a.ctypes.data if a is not None else None
+    rc = lib().fdref_render(C.byref(job), ref.h if ref else None, bla.h if bla else None, ptr(cls), ptr(nu),
+                            ptr(de), ptr(normal), ptr(it), ptr(z), ptr(dz), ptr(dexp), C.byref(st), kernel, 256)
+    if rc != 0:
+        raise ValueError(_err())
+    out = dict(cls=cls, nu=nu, de=de, normal=normal, n=it, kernel=kernel.value.decode(),
+               stats=dict(reference_len=st.reference_len, iterations=st.iterations, blocks=st.blocks,
+                          skipped=st.skipped, fallback_samples=st.fallback_samples,
+                          closed_form_samples=st.closed_form_samples, shift_px=st.shift_px))
+    if raw:
+        out.update(z=z.reshape(n, 2), dz=dz.reshape(n, 2), dexp=dexp)
+    return out
+
+
+def store_escaped(h_m, h_e, ss, rotation, n, zr, zi, dr, di, dexp):
+    nu, de, nm = C.c_double(), C.c_float(), C.c_uint16()
+    lib().fdref_store_escaped(h_m, h_e, ss, rotation, n, zr, zi, dr, di, dexp, C.byref(nu), C.byref(de),
+                              C.byref(nm))
+    return nu.value, de.value, nm.value
+
+
+def render_fds(job, ref=None, bla=None):
+    size = lib().fdref_render_fds(C.byref(job), ref.h if ref else None, bla.h if bla else None, None, 0)
+    if size < 0:
+        raise ValueError(_err())
+    buf = (C.c_uint8 * size)()
+    lib().fdref_render_fds(C.byref(job), ref.h if ref else None, bla.h if bla else None, buf, size)
+    return bytes(buf)
+
+
+def fnv1a64(data):
+    h = 0xCBF29CE484222325
+    for b in data:
+        h = ((h ^ b) * 0x100000001B3) & 0xFFFFFFFFFFFFFFFF
+    return h

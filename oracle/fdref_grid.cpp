@@ -1,0 +1,522 @@
+// Oracle part 3: the grid driver (grid.rs), the column encoder (store.rs), the .fds v1
+// writer (crates/fd-samples/src/{header,write,wire}.rs) and the C API of fdref.h.
+// TEST INFRASTRUCTURE ONLY (see fdref.h).
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <thread>
+
+#include "fdref.h"
+#include "fdref_internal.hpp"
+
+namespace fdref {
+
+static const double LN_2 = 0.693147180559945309417232121458176568;
+static const double TAU = 6.28318530717958647692528676655900577;
+
+// store.rs:145-150
+static float de_px(double az, double log2z, double dr, double di, int64_t dexp, double px_m, int64_t px_e) {
+  double lnz = log2z * LN_2;
+  double base = 2.0 * az * lnz / (std::hypot(dr, di) * px_m);
+  int64_t k = -(dexp + px_e);
+  k = std::max<int64_t>(-4000, std::min<int64_t>(4000, k));
+  return (float)(base * exp2i(k / 2) * exp2i(k - k / 2));
+}
+
+// crates/fd-samples/src/samples.rs:45-48: round(atan2 * 65536/tau) as i64 as u16.
+static uint16_t angle(double x, double y) {
+  double t = std::atan2(y, x) * (65536.0 / TAU);
+  return (uint16_t)(uint64_t)f2i(std::round(t));
+}
+
+struct Columns {
+  uint8_t *cls = nullptr;
+  double *nu = nullptr;
+  float *de = nullptr;
+  uint16_t *normal = nullptr;
+  uint64_t *n = nullptr;
+  double *z = nullptr, *dz = nullptr;
+  int64_t *dexp = nullptr;
+};
+
+// store.rs:66-112 with the Bound column absent (class evidence Heuristic).
+static void put(const Plane &pl, uint32_t ss, uint32_t cols, const Outcome &o, size_t idx, Columns &c) {
+  if (c.n) c.n[idx] = o.n;
+  if (c.z) {
+    c.z[2 * idx] = o.zr;
+    c.z[2 * idx + 1] = o.zi;
+  }
+  if (c.dz) {
+    c.dz[2 * idx] = o.dr;
+    c.dz[2 * idx + 1] = o.di;
+  }
+  if (c.dexp) c.dexp[idx] = o.dexp;
+  if (o.kind != Kind::Escaped) {
+    if (c.cls) c.cls[idx] = (uint8_t)(o.kind == Kind::Unresolved ? 2 : 1);
+    return;
+  }
+  double z2 = o.zr * o.zr + o.zi * o.zi;
+  double log2z = 0.5 * std::log2(z2);
+  if (c.cls) c.cls[idx] = 0;
+  if ((cols & FDREF_COL_NU) && c.nu) c.nu[idx] = (double)o.n + 1.0 - std::log2(log2z);
+  if ((cols & FDREF_COL_DE) && c.de)
+    c.de[idx] = de_px(std::sqrt(z2), log2z, o.dr, o.di, o.dexp, pl.h_m * (double)ss, pl.h_e);
+  if ((cols & FDREF_COL_NORMAL) && c.normal) {
+    double x, y;
+    pl.to_screen(o.zr * o.dr + o.zi * o.di, o.zi * o.dr - o.zr * o.di, x, y);
+    c.normal[idx] = angle(x, y);
+  }
+}
+
+struct Stats {
+  uint64_t reference_len = 0, iterations = 0, blocks = 0, skipped = 0, fallback = 0, closed = 0;
+  double shift = 0.0;
+};
+
+// grid.rs:779-799
+static std::pair<Plane, Tier> setup(const View &v, const Params &p) {
+  if (p.ss == 0 || p.nx % p.ss != 0 || p.ny % p.ss != 0)
+    throw std::runtime_error("grid must be a whole number of pixels");
+  Plane plane = Plane::make(v, p.nx, p.ny);
+  Tier tier = p.tier ? *p.tier : plane.tier;
+  if (!plane.allows(tier)) throw std::runtime_error("tier is not valid at this depth");
+  return {plane, tier};
+}
+
+// grid.rs:802-815
+static Reference compute(const View &v, const Plane &plane, Tier tier, const Params &p) {
+  if (tier == Tier::F64) return Reference::make_f64(plane.c_re, plane.c_im, p.max_iter, p.escape_radius);
+  size_t l = limbs_for(plane.bits);
+  Reference r = Reference::from_fixed(Fixed::parse(v.center_re, l), Fixed::parse(v.center_im, l), p.max_iter);
+  r.bits = (uint32_t)plane.bits;
+  return r;
+}
+
+// grid.rs:818-823
+static uint32_t precision(const Plane &plane, Tier tier) { return tier == Tier::F64 ? 53 : (uint32_t)plane.bits; }
+
+// grid.rs:428-444
+static std::pair<double, int64_t> dc_bound(const Plane &plane, Tier tier, const Params &p) {
+  double half = std::hypot((double)p.nx / 2.0, (double)p.ny / 2.0);
+  if (tier == Tier::Scaled) return {plane.h_m * half, plane.h_e};
+  return {plane.h() * half, 0};
+}
+
+// grid.rs:378-413
+static void bla_checks(const Plane &plane, Tier tier, const Params &p, const Reference &r, const Bla &bla) {
+  if (bla.points != r.len()) throw std::runtime_error("BLA table covers another orbit length");
+  if (std::isnan(p.escape_radius) || p.escape_radius < 4.0)
+    throw std::runtime_error("escape radius is below 4: BLA needs escape radius >= 4");
+  auto [dc, e] = dc_bound(plane, tier, p);
+  bool over = e == bla.dc_exp ? dc > bla.dc_max
+                              : std::log2(dc) + (double)e > std::log2(bla.dc_max) + (double)bla.dc_exp;
+  if (std::isnan(dc) || over) throw std::runtime_error("view reaches |dc| beyond the BLA table's dc_max");
+}
+
+// grid.rs:446-535 + Job::one/one_from/fill (grid.rs:623-775), without series/mask/stripe.
+static std::string run(const View &v, const Params &p, const Reference *supplied, const Bla *bla, Columns cols,
+                       Stats &st, Reference *computed_out = nullptr) {
+  auto [plane, tier] = setup(v, p);
+  uint32_t need = precision(plane, tier);
+  Reference computed;
+  const Reference *ref = supplied;
+  if (supplied) {
+    uint32_t bits = supplied->bits;
+    if (bits != need && (tier == Tier::F64 || bits < need))
+      throw std::runtime_error("supplied reference has " + std::to_string(bits) + " bits; this view needs " +
+                               (tier == Tier::F64 ? "" : "at least ") + std::to_string(need));
+    if (supplied->len() == 0 || supplied->re.size() != supplied->im.size() || supplied->re[0] != 0.0 ||
+        supplied->im[0] != 0.0)
+      throw std::runtime_error("supplied reference orbit must start at Z_0 = 0 with equal re/im lengths");
+    plane.bits = bits;
+  } else {
+    computed = compute(v, plane, tier, p);
+    ref = &computed;
+  }
+  if (bla) bla_checks(plane, tier, p, *ref, *bla);
+  const bool D = (p.columns & (FDREF_COL_DE | FDREF_COL_NORMAL)) != 0;
+  const bool L = bla != nullptr;
+  const double h = plane.h();
+  const double r2 = p.escape_radius * p.escape_radius;
+  std::optional<size_t> nucleus = ref->nucleus_period();
+  std::atomic<uint32_t> next_row{0};
+  std::mutex mu;
+  auto worker = [&]() {
+    Stats local;
+    for (;;) {
+      uint32_t j = next_row.fetch_add(1);
+      if (j >= p.ny) break;
+      for (uint32_t i = 0; i < p.nx; ++i) {
+        double ux, uy;
+        plane.unit_offset(i, j, ux, uy);
+        Skip skip;
+        Outcome o;
+        switch (tier) {
+          case Tier::F64: {
+            double ar = ux * h, ai = uy * h;
+            o = iterate(false, D, L, *ref, bla, skip, std::make_pair(plane.c_re + ar, plane.c_im + ai), ar, ai, 0,
+                        p.max_iter, r2, nucleus);
+            break;
+          }
+          case Tier::Fixed:
+            o = iterate(false, D, L, *ref, bla, skip, std::nullopt, ux * h, uy * h, 0, p.max_iter, r2, nucleus);
+            break;
+          case Tier::Scaled:
+            o = iterate(true, D, L, *ref, bla, skip, std::nullopt, ux * plane.h_m, uy * plane.h_m, plane.h_e,
+                        p.max_iter, r2, nucleus);
+            break;
+        }
+        uint64_t spent = o.iterations(p.max_iter);
+        if (L) {
+          spent = spent - skip.skipped + skip.blocks;
+          local.blocks += skip.blocks;
+          local.skipped += skip.skipped;
+          bool closed = o.kind == Kind::Interior && o.n == 0;
+          local.closed += closed;
+          local.fallback += (skip.blocks == 0 && !closed);
+          local.shift = std::max(local.shift, skip.shift);
+        }
+        local.iterations += spent;
+        put(plane, p.ss, p.columns, o, (size_t)j * p.nx + i, cols);
+      }
+    }
+    std::lock_guard<std::mutex> g(mu);
+    st.iterations += local.iterations;
+    st.blocks += local.blocks;
+    st.skipped += local.skipped;
+    st.fallback += local.fallback;
+    st.closed += local.closed;
+    st.shift = std::max(st.shift, local.shift);
+  };
+  int threads = std::max(1, std::min<int>(p.threads, (int)p.ny));
+  std::vector<std::thread> pool;
+  for (int t = 1; t < threads; ++t) pool.emplace_back(worker);
+  worker();
+  for (auto &t : pool) t.join();
+  st.reference_len = ref->len();
+  // Output pixel = ss samples of spacing h (grid.rs:529-531).
+  if (L && D) st.shift = st.shift / (plane.h() * (double)p.ss);
+  else st.shift = NAN;
+  std::string kernel = plane.kernel(tier);
+  if (bla) kernel += " bla/1";
+  if (computed_out && !supplied) *computed_out = std::move(computed);
+  return kernel;
+}
+
+// ---------------------------------------------------------------- .fds v1
+struct Out {
+  std::vector<uint8_t> b;
+  void bytes(const void *p, size_t n) { b.insert(b.end(), (const uint8_t *)p, (const uint8_t *)p + n); }
+  void u16(uint16_t v) { bytes(&v, 2); }
+  void u32(uint32_t v) { bytes(&v, 4); }
+  void u64(uint64_t v) { bytes(&v, 8); }
+  void f64(double v) { bytes(&v, 8); }
+  void str(const std::string &s) {
+    if (s.size() > 65535) throw std::runtime_error("string longer than 65535 bytes");
+    u16((uint16_t)s.size());
+    bytes(s.data(), s.size());
+  }
+  void pad8() { b.resize((b.size() + 7) & ~(size_t)7, 0); }
+};
+
+// header.rs:62-81 + write.rs:8-53 (MAGIC/MAJOR/MINOR lib.rs:21-27).
+static std::vector<uint8_t> fds(const View &v, const Params &p, uint32_t colset, const std::string &kernel,
+                                const std::vector<uint8_t> &cls, const std::vector<double> &nu,
+                                const std::vector<float> &de, const std::vector<uint16_t> &normal) {
+  Out o;
+  o.bytes("FDSAMPLE", 8);
+  o.u16(1);
+  o.u16(1);
+  o.u32(colset);
+  o.u32(p.nx);
+  o.u32(p.ny);
+  o.u32(p.ss);
+  o.u32(0);
+  o.u64(p.max_iter);
+  o.f64(p.escape_radius);
+  o.f64(v.rotation);
+  o.str(v.center_re);
+  o.str(v.center_im);
+  o.str(v.width);
+  o.str(kernel);
+  o.pad8();
+  o.bytes(cls.data(), cls.size());
+  o.pad8();
+  if (colset & FDREF_COL_NU) {
+    o.bytes(nu.data(), nu.size() * 8);
+    o.pad8();
+  }
+  if (colset & FDREF_COL_DE) {
+    o.bytes(de.data(), de.size() * 4);
+    o.pad8();
+  }
+  if (colset & FDREF_COL_NORMAL) {
+    o.bytes(normal.data(), normal.size() * 2);
+    o.pad8();
+  }
+  return o.b;
+}
+
+}  // namespace fdref
+
+// ================================================================= C API
+using namespace fdref;
+
+struct fdref_ref {
+  Reference r;
+};
+struct fdref_bla {
+  Bla t;
+};
+
+static thread_local std::string g_error;
+
+#define FDREF_TRY(...)                \
+  try {                               \
+    __VA_ARGS__                       \
+  } catch (std::exception & e) {      \
+    g_error = e.what();               \
+  }
+
+static View to_view(const fdref_job *j) {
+  View v;
+  v.center_re = j->center_re;
+  v.center_im = j->center_im;
+  v.width = j->width;
+  v.rotation = j->rotation;
+  return v;
+}
+static Params to_params(const fdref_job *j) {
+  Params p;
+  p.nx = j->nx;
+  p.ny = j->ny;
+  p.ss = j->ss;
+  p.max_iter = j->max_iter;
+  p.escape_radius = j->escape_radius;
+  p.columns = j->columns | FDREF_COL_CLASS;
+  p.threads = j->threads;
+  if (j->tier >= 0) p.tier = (Tier)j->tier;
+  return p;
+}
+
+extern "C" {
+
+const char *fdref_last_error(void) { return g_error.c_str(); }
+
+int fdref_plane(const fdref_job *job, double *h_m, int64_t *h_e, int32_t *tier, uint64_t *bits, double *c_re,
+                double *c_im) {
+  FDREF_TRY({
+    Plane p = Plane::make(to_view(job), job->nx, job->ny);
+    *h_m = p.h_m;
+    *h_e = p.h_e;
+    *tier = (int32_t)p.tier;
+    *bits = p.bits;
+    *c_re = p.c_re;
+    *c_im = p.c_im;
+    return 0;
+  })
+  return -1;
+}
+
+fdref_ref *fdref_reference(const fdref_job *job) {
+  FDREF_TRY({
+    View v = to_view(job);
+    Params p = to_params(job);
+    auto [plane, tier] = setup(v, p);
+    auto *r = new fdref_ref{compute(v, plane, tier, p)};
+    r->r.bits = precision(plane, tier);
+    return r;
+  })
+  return nullptr;
+}
+
+fdref_ref *fdref_reference_f64(double c_re, double c_im, uint64_t max_iter, double escape_radius) {
+  return new fdref_ref{Reference::make_f64(c_re, c_im, max_iter, escape_radius)};
+}
+
+fdref_ref *fdref_reference_fixed(const char *re, const char *im, uint64_t bits, uint64_t max_iter) {
+  FDREF_TRY({
+    size_t l = limbs_for(bits);
+    auto *r = new fdref_ref{Reference::from_fixed(Fixed::parse(re, l), Fixed::parse(im, l), max_iter)};
+    r->r.bits = (uint32_t)bits;
+    return r;
+  })
+  return nullptr;
+}
+
+fdref_ref *fdref_reference_arrays(const double *re, const double *im, uint64_t len, uint32_t bits) {
+  auto *r = new fdref_ref;
+  r->r.re.assign(re, re + len);
+  r->r.im.assign(im, im + len);
+  r->r.bits = bits;
+  return r;
+}
+
+uint64_t fdref_ref_len(const fdref_ref *r) { return r->r.len(); }
+uint32_t fdref_ref_bits(const fdref_ref *r) { return r->r.bits; }
+void fdref_ref_copy(const fdref_ref *r, double *re, double *im) {
+  std::memcpy(re, r->r.re.data(), r->r.len() * 8);
+  std::memcpy(im, r->r.im.data(), r->r.len() * 8);
+}
+int64_t fdref_ref_nucleus_period(const fdref_ref *r) {
+  auto p = r->r.nucleus_period();
+  return p ? (int64_t)*p : -1;
+}
+void fdref_ref_free(fdref_ref *r) { delete r; }
+
+fdref_bla *fdref_bla_build(const fdref_ref *r, double eps, double dc_max, int64_t dc_exp) {
+  FDREF_TRY({ return new fdref_bla{Bla::build_scaled(r->r, eps, dc_max, dc_exp)}; })
+  return nullptr;
+}
+uint32_t fdref_bla_levels(const fdref_bla *t) { return (uint32_t)t->t.levels.size(); }
+uint64_t fdref_bla_block_count(const fdref_bla *t) {
+  uint64_t n = 0;
+  for (auto &l : t->t.levels) n += l.size();
+  return n;
+}
+void fdref_bla_export(const fdref_bla *t, double *blocks7, uint64_t *level_offsets) {
+  uint64_t at = 0;
+  for (size_t i = 0; i < t->t.levels.size(); ++i) {
+    if (level_offsets) level_offsets[i] = at;
+    for (auto &b : t->t.levels[i]) {
+      double v[7] = {b.ar, b.ai, b.br, b.bi, b.r, b.alpha, b.beta};
+      std::memcpy(blocks7 + 7 * at, v, sizeof v);
+      ++at;
+    }
+  }
+  if (level_offsets) level_offsets[t->t.levels.size()] = at;
+}
+uint64_t fdref_bla_find(const fdref_bla *t, uint64_t m, double d2, uint64_t budget, uint64_t *level,
+                        uint64_t *index) {
+  size_t len = 0, lv = 0, ix = 0;
+  const Block *b = t->t.find((size_t)m, d2, budget, len, &lv, &ix);
+  if (!b) return 0;
+  if (level) *level = lv;
+  if (index) *index = ix;
+  return len;
+}
+void fdref_bla_free(fdref_bla *t) { delete t; }
+
+int fdref_bla_dc_bound(const fdref_job *job, double *dc, int64_t *e) {
+  FDREF_TRY({
+    auto [plane, tier] = setup(to_view(job), to_params(job));
+    auto b = dc_bound(plane, tier, to_params(job));
+    *dc = b.first;
+    *e = b.second;
+    return 0;
+  })
+  return -1;
+}
+
+int fdref_iterate(const fdref_ref *r, const fdref_bla *bla, int extended, int derivative, int has_c, double cr,
+                  double ci, double ar, double ai, int64_t offset_exp, uint64_t max_iter, double r2,
+                  int64_t nucleus, fdref_outcome *out) {
+  FDREF_TRY({
+    std::optional<size_t> nuc;
+    if (nucleus == -2) nuc = r->r.nucleus_period();
+    else if (nucleus >= 0) nuc = (size_t)nucleus;
+    std::optional<std::pair<double, double>> c;
+    if (has_c) c = std::make_pair(cr, ci);
+    Skip skip;
+    Outcome o = iterate(extended != 0, derivative != 0, bla != nullptr, r->r, bla ? &bla->t : nullptr, skip, c, ar,
+                        ai, offset_exp, max_iter, r2, nuc);
+    out->kind = (int32_t)o.kind;
+    out->n = o.n;
+    out->zr = o.zr;
+    out->zi = o.zi;
+    out->dr = o.dr;
+    out->di = o.di;
+    out->dexp = o.dexp;
+    out->blocks = skip.blocks;
+    out->skipped = skip.skipped;
+    out->shift = skip.shift;
+    return 0;
+  })
+  return -1;
+}
+
+int fdref_render(const fdref_job *job, const fdref_ref *ref, const fdref_bla *bla, uint8_t *cls, double *nu,
+                 float *de, uint16_t *normal, uint64_t *n_out, double *z_out, double *dz_out, int64_t *dexp_out,
+                 fdref_stats *stats, char *kernel, size_t kernel_cap) {
+  FDREF_TRY({
+    Columns c;
+    c.cls = cls;
+    c.nu = nu;
+    c.de = de;
+    c.normal = normal;
+    c.n = n_out;
+    c.z = z_out;
+    c.dz = dz_out;
+    c.dexp = dexp_out;
+    Stats st;
+    std::string k = run(to_view(job), to_params(job), ref ? &ref->r : nullptr, bla ? &bla->t : nullptr, c, st);
+    if (stats) {
+      stats->reference_len = st.reference_len;
+      stats->iterations = st.iterations;
+      stats->blocks = st.blocks;
+      stats->skipped = st.skipped;
+      stats->fallback_samples = st.fallback;
+      stats->closed_form_samples = st.closed;
+      stats->shift_px = st.shift;
+    }
+    if (kernel && kernel_cap) {
+      std::strncpy(kernel, k.c_str(), kernel_cap - 1);
+      kernel[kernel_cap - 1] = 0;
+    }
+    return 0;
+  })
+  return -1;
+}
+
+void fdref_store_escaped(double h_m, int64_t h_e, uint32_t ss, double rotation, uint64_t n, double zr, double zi,
+                         double dr, double di, int64_t dexp, double *nu, float *de, uint16_t *normal) {
+  Plane pl{};
+  pl.h_m = h_m;
+  pl.h_e = h_e;
+  pl.sin = std::sin(rotation);
+  pl.cos = std::cos(rotation);
+  Outcome o;
+  o.kind = Kind::Escaped;
+  o.n = n;
+  o.zr = zr;
+  o.zi = zi;
+  o.dr = dr;
+  o.di = di;
+  o.dexp = dexp;
+  uint8_t cls;
+  Columns c;
+  c.cls = &cls;
+  c.nu = nu;
+  c.de = de;
+  c.normal = normal;
+  put(pl, ss, FDREF_COL_NU | FDREF_COL_DE | FDREF_COL_NORMAL, o, 0, c);
+}
+
+int64_t fdref_render_fds(const fdref_job *job, const fdref_ref *ref, const fdref_bla *bla, uint8_t *buf,
+                         uint64_t cap) {
+  FDREF_TRY({
+    View v = to_view(job);
+    Params p = to_params(job);
+    size_t n = (size_t)p.nx * p.ny;
+    std::vector<uint8_t> cls(n, 0);
+    std::vector<double> nu((p.columns & FDREF_COL_NU) ? n : 0, 0.0);
+    std::vector<float> de((p.columns & FDREF_COL_DE) ? n : 0, 0.0f);
+    std::vector<uint16_t> normal((p.columns & FDREF_COL_NORMAL) ? n : 0, 0);
+    Columns c;
+    c.cls = cls.data();
+    c.nu = nu.empty() ? nullptr : nu.data();
+    c.de = de.empty() ? nullptr : de.data();
+    c.normal = normal.empty() ? nullptr : normal.data();
+    Stats st;
+    std::string k = run(v, p, ref ? &ref->r : nullptr, bla ? &bla->t : nullptr, c, st);
+    std::vector<uint8_t> bytes = fds(v, p, p.columns, k, cls, nu, de, normal);
+    if (buf && cap) std::memcpy(buf, bytes.data(), std::min<uint64_t>(cap, bytes.size()));
+    return (int64_t)bytes.size();
+  })
+  return -1;
+}
+
+}  // extern "C"

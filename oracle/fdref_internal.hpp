@@ -1,0 +1,114 @@
+// Internal C++ types of the CPU oracle. TEST INFRASTRUCTURE ONLY (see fdref.h).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <functional>
+#include <optional>
+#include <string>
+#include <vector>
+
+namespace fdref {
+
+double exp2i(int64_t k);
+int64_t f2i(double f);
+int64_t biased_exp(double q);
+size_t limbs_for(uint64_t bits);
+
+struct Fixed {
+  bool neg = false;
+  std::vector<uint64_t> mag;
+  static Fixed parse(const std::string &s, size_t nlimbs);
+};
+
+struct Decimal {
+  bool neg = false;
+  std::vector<uint8_t> digits;
+  int64_t exp10 = 0;
+  static Decimal parse(const std::string &s);
+  double log2_abs() const;
+  Fixed to_fixed(size_t nlimbs) const;
+};
+
+bool frexp_limbs(bool neg, const uint64_t *mag, size_t l, double &m, int64_t &e);
+double to_f64_limbs(bool neg, const uint64_t *mag, size_t l);
+void orbit(const Fixed &cr, const Fixed &ci, uint64_t steps, double escape2,
+           const std::function<void(double, double)> &emit);
+
+enum class Tier { F64 = 0, Fixed = 1, Scaled = 2 };
+
+struct View {
+  std::string center_re, center_im, width;
+  double rotation = 0.0;
+};
+
+struct Params {
+  uint32_t nx = 0, ny = 0, ss = 1;
+  uint64_t max_iter = 0;
+  double escape_radius = 1e10;
+  uint32_t columns = 1;
+  int threads = 1;
+  std::optional<Tier> tier;
+};
+
+struct Plane {
+  double c_re, c_im, h_m;
+  int64_t h_e;
+  Tier tier;
+  uint64_t bits;
+  double cos, sin, half_x, half_y;
+  static Plane make(const View &v, uint32_t nx, uint32_t ny);
+  std::string kernel(Tier t) const;
+  bool allows(Tier t) const;
+  void unit_offset(size_t i, size_t j, double &ux, double &uy) const;
+  double h() const;
+  void to_screen(double re, double im, double &x, double &y) const;
+};
+
+struct Reference {
+  std::vector<double> re, im;
+  uint32_t bits = 53;
+  static const size_t MAX_LEN = 1u << 20;
+  static Reference make_f64(double c_re, double c_im, uint64_t max_iter, double escape_radius);
+  static Reference from_fixed(const Fixed &cr, const Fixed &ci, uint64_t max_iter);
+  std::optional<size_t> nucleus_period() const;
+  size_t len() const { return re.size(); }
+};
+
+struct Block {
+  double ar = 0, ai = 0, br = 0, bi = 0, r = 0, alpha = 0, beta = 0;
+  bool finite() const;
+};
+
+struct Bla {
+  double eps = 0, dc_max = 0;
+  int64_t dc_exp = 0;
+  uint64_t points = 0;
+  std::vector<std::vector<Block>> levels;
+  std::vector<std::vector<double>> r2;
+  static Bla build_scaled(const Reference &r, double eps, double dc_max, int64_t dc_exp);
+  const Block *find(size_t m, double d2, uint64_t budget, size_t &len, size_t *level = nullptr,
+                    size_t *index = nullptr) const;
+};
+
+enum class Kind { Escaped = 0, Interior = 1, Unresolved = 2 };
+
+struct Outcome {
+  Kind kind = Kind::Unresolved;
+  uint64_t n = 0;
+  double zr = 0, zi = 0, dr = 0, di = 0;
+  int64_t dexp = 0;
+  uint64_t iterations(uint64_t max_iter) const { return kind == Kind::Unresolved ? max_iter : n; }
+};
+
+struct Skip {
+  uint64_t blocks = 0, skipped = 0;
+  double shift = 0.0;
+};
+
+Outcome iterate(bool extended, bool D, bool L, const Reference &r, const Bla *bla, Skip &skip,
+                std::optional<std::pair<double, double>> c, double ar, double ai, int64_t offset_exp,
+                uint64_t max_iter, double r2, std::optional<size_t> nucleus);
+
+bool in_main_components(double cr, double ci);
+
+}  // namespace fdref
