@@ -1,0 +1,119 @@
+"""ctypes binding of libfdcuda.so (include/fdcuda.h, include/fdhost.h).
+
+The library is built in-tree (fractodactyl_b200/build.py). Loading fails loudly when it
+is missing: there is no CPU stand-in for the CUDA route.
+"""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libfdcuda.so")
+
+# fdc_status
+OK, DECLINED, INVALID, DEVICE_ERROR, TIMEOUT, NO_DEVICE = range(6)
+STATUS_NAMES = {0: "OK", 1: "DECLINED", 2: "INVALID", 3: "DEVICE_ERROR", 4: "TIMEOUT", 5: "NO_DEVICE"}
+# fdc_job flags
+DERIVATIVE, BLA, SHIFT, F32, DEVICE_OUT = 1, 2, 4, 8, 16
+
+
+class Job(C.Structure):
+    _fields_ = [
+        ("orbit", C.c_int32),
+        ("tier", C.c_int32),
+        ("nx", C.c_uint32),
+        ("ny", C.c_uint32),
+        ("ss", C.c_uint32),
+        ("flags", C.c_uint32),
+        ("c_re", C.c_double),
+        ("c_im", C.c_double),
+        ("h_m", C.c_double),
+        ("h_e", C.c_int64),
+        ("cos_rot", C.c_double),
+        ("sin_rot", C.c_double),
+        ("max_iter", C.c_uint64),
+        ("escape_radius", C.c_double),
+        ("nucleus_period", C.c_int64),
+        ("mask", C.c_void_p),
+        ("offsets", C.c_void_p),
+        ("first_row", C.c_uint32),
+        ("rows", C.c_uint32),
+        ("deadline_ms", C.c_double),
+    ]
+
+
+class Out(C.Structure):
+    _fields_ = [(name, C.c_void_p) for name in ("cls", "n", "nu", "de", "normal", "z", "dz", "dexp", "status")]
+
+
+class Counters(C.Structure):
+    _fields_ = [
+        ("samples", C.c_uint64),
+        ("iterations", C.c_uint64),
+        ("blocks", C.c_uint64),
+        ("skipped", C.c_uint64),
+        ("fallback_samples", C.c_uint64),
+        ("closed_form_samples", C.c_uint64),
+        ("shift", C.c_double),
+        ("kernel_ms", C.c_double),
+        ("launches", C.c_uint32),
+    ]
+
+
+class Plane(C.Structure):
+    _fields_ = [
+        ("c_re", C.c_double),
+        ("c_im", C.c_double),
+        ("h_m", C.c_double),
+        ("h_e", C.c_int64),
+        ("tier", C.c_int32),
+        ("bits", C.c_uint64),
+        ("cos_rot", C.c_double),
+        ("sin_rot", C.c_double),
+    ]
+
+
+# Every symbol the headers declare, for the export check.
+FDC_SYMBOLS = ["fdc_abi_version", "fdc_open", "fdc_close", "fdc_last_error", "fdc_upload_orbit", "fdc_free_orbit",
+               "fdc_upload_bla", "fdc_render"]
+FDH_SYMBOLS = ["fdh_last_error", "fdh_plane_new", "fdh_orbit_fixed", "fdh_orbit_f64", "fdh_nucleus_period",
+               "fdh_bla_build", "fdh_dc_bound", "fdh_nucleus"]
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(
+            "libfdcuda.so is not built (run `python -m fractodactyl_b200.build`); the CUDA route has no fallback")
+    L = C.CDLL(LIB_PATH)
+    P, D, U32, U64, I32, I64 = C.c_void_p, C.c_double, C.c_uint32, C.c_uint64, C.c_int32, C.c_int64
+    L.fdc_abi_version.restype = C.c_int
+    L.fdc_open.argtypes = [C.c_int, C.POINTER(P)]
+    L.fdc_close.argtypes = [P]
+    L.fdc_last_error.restype = C.c_char_p
+    L.fdc_last_error.argtypes = [P]
+    L.fdc_upload_orbit.argtypes = [P, P, P, U64, U32, C.POINTER(I32)]
+    L.fdc_free_orbit.argtypes = [P, I32]
+    L.fdc_upload_bla.argtypes = [P, I32, P, P, U32, D, D, I64]
+    L.fdc_render.argtypes = [P, C.POINTER(Job), C.POINTER(Out), C.POINTER(Counters)]
+    L.fdh_last_error.restype = C.c_char_p
+    L.fdh_plane_new.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, D, U32, U32, C.POINTER(Plane)]
+    L.fdh_orbit_fixed.restype = I64
+    L.fdh_orbit_fixed.argtypes = [C.c_char_p, C.c_char_p, U64, U64, P, P, U64]
+    L.fdh_orbit_f64.restype = I64
+    L.fdh_orbit_f64.argtypes = [D, D, U64, D, P, P, U64]
+    L.fdh_nucleus_period.restype = I64
+    L.fdh_nucleus_period.argtypes = [P, P, U64]
+    L.fdh_bla_build.argtypes = [P, P, U64, D, D, I64, C.c_int, P, P, C.POINTER(U32), C.POINTER(U64)]
+    L.fdh_dc_bound.argtypes = [C.POINTER(Plane), I32, U32, U32, C.POINTER(D), C.POINTER(I64)]
+    L.fdh_nucleus.argtypes = [C.c_char_p, C.c_char_p, D, U64, U64, C.c_char_p, C.c_char_p, C.c_size_t,
+                              C.POINTER(U64)]
+    _lib = L
+    return L
+
+
+def host_error():
+    return lib().fdh_last_error().decode()

@@ -1,0 +1,421 @@
+// C ABI of the CUDA perturbation route (include/fdcuda.h): contexts, orbit/BLA
+// uploads, and fdc_render, which launches the persistent perturbation kernel.
+// Built with -fmad=false (the plain form must round as the reference's Rust does).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/fdcuda.h"
+#include "perturb_f64.cuh"
+#include "route_internal.hpp"
+
+namespace {
+
+struct BlaDev {
+  double *r2 = nullptr;
+  double2 *coef = nullptr;
+  double2 *ab = nullptr;
+  uint32_t levels = 0;
+  uint32_t off[fdk::MAX_LEVELS] = {};
+  uint32_t count[fdk::MAX_LEVELS] = {};
+  double eps = 0, dc_max = 0;
+  int64_t dc_exp = 0;
+};
+
+struct OrbitDev {
+  double2 *z = nullptr;
+  uint64_t len = 0;
+  uint32_t bits = 0;
+  double z0r = 0, z0i = 0;
+  bool has_bla = false;
+  BlaDev bla;
+};
+
+// Device scratch of one context: work-queue head, counters, deadline flag.
+struct Scratch {
+  unsigned long long queue;
+  unsigned long long pad[3];
+  fdk::Counters counters;
+  uint32_t timed_out;
+  uint32_t pad2[7];
+};
+
+}  // namespace
+
+struct fdc_ctx {
+  int device = 0;
+  int sm_count = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  Scratch *scratch = nullptr;
+  std::map<int32_t, OrbitDev> orbits;
+  int32_t next_orbit = 1;
+  std::string err;
+  // staging for host outputs / inputs, grown on demand
+  void *stage = nullptr;
+  size_t stage_bytes = 0;
+  int blocks_per_sm[8] = {};
+};
+
+namespace {
+
+fdc_status fail(fdc_ctx *c, fdc_status s, const std::string &msg) {
+  if (c) c->err = msg;
+  return s;
+}
+
+#define CK(call)                                                                                  \
+  do {                                                                                            \
+    cudaError_t e_ = (call);                                                                      \
+    if (e_ != cudaSuccess)                                                                        \
+      return fail(ctx, FDC_DEVICE_ERROR, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+void free_bla(BlaDev &b) {
+  cudaFree(b.r2);
+  cudaFree(b.coef);
+  cudaFree(b.ab);
+  b = BlaDev{};
+}
+
+template <bool EXT, bool D, bool L>
+void *kernel_ptr() {
+  return (void *)fdk::perturb_kernel<EXT, D, L>;
+}
+
+void *pick_kernel(bool ext, bool d, bool l, int &variant) {
+  variant = (ext ? 4 : 0) | (d ? 2 : 0) | (l ? 1 : 0);
+  switch (variant) {
+    case 0: return kernel_ptr<false, false, false>();
+    case 1: return kernel_ptr<false, false, true>();
+    case 2: return kernel_ptr<false, true, false>();
+    case 3: return kernel_ptr<false, true, true>();
+    case 4: return kernel_ptr<true, false, false>();
+    case 5: return kernel_ptr<true, false, true>();
+    case 6: return kernel_ptr<true, true, false>();
+    default: return kernel_ptr<true, true, true>();
+  }
+}
+
+fdc_status open_resources(fdc_ctx *ctx) {
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  CK(cudaEventCreate(&ctx->ev0));
+  CK(cudaEventCreate(&ctx->ev1));
+  CK(cudaMalloc(&ctx->scratch, sizeof(Scratch)));
+  return FDC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fdc_abi_version(void) { return FDC_ABI_VERSION; }
+
+const char *fdc_last_error(const fdc_ctx *ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+fdc_status fdc_open(int device, fdc_ctx **out) {
+  if (!out) return FDC_INVALID;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) return FDC_NO_DEVICE;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major != 10) return FDC_NO_DEVICE;
+  fdc_ctx *ctx = new fdc_ctx;
+  ctx->device = device;
+  ctx->sm_count = prop.multiProcessorCount;
+  fdc_status s = open_resources(ctx);
+  if (s != FDC_OK) {
+    fdc_close(ctx);
+    return s;
+  }
+  *out = ctx;
+  return FDC_OK;
+}
+
+void fdc_close(fdc_ctx *ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto &kv : ctx->orbits) {
+    cudaFree(kv.second.z);
+    free_bla(kv.second.bla);
+  }
+  cudaFree(ctx->scratch);
+  cudaFree(ctx->stage);
+  if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+  if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+}
+
+fdc_status fdc_upload_orbit(fdc_ctx *ctx, const double *re, const double *im, uint64_t len, uint32_t bits,
+                            int32_t *orbit) {
+  if (!ctx || !re || !im || !orbit) return fail(ctx, FDC_INVALID, "null argument");
+  if (len < 2 || len > (1ull << 20)) return fail(ctx, FDC_INVALID, "orbit length must be in [2, 2^20]");
+  if (re[0] != 0.0 || im[0] != 0.0)
+    return fail(ctx, FDC_INVALID, "supplied reference orbit must start at Z_0 = 0");
+  CK(cudaSetDevice(ctx->device));
+  std::vector<double2> z(len);
+  for (uint64_t k = 0; k < len; ++k) z[k] = make_double2(re[k], im[k]);
+  OrbitDev o;
+  o.len = len;
+  o.bits = bits;
+  o.z0r = re[0];
+  o.z0i = im[0];
+  CK(cudaMalloc(&o.z, len * sizeof(double2)));
+  CK(cudaMemcpyAsync(o.z, z.data(), len * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  int32_t id = ctx->next_orbit++;
+  ctx->orbits[id] = o;
+  *orbit = id;
+  return FDC_OK;
+}
+
+fdc_status fdc_free_orbit(fdc_ctx *ctx, int32_t orbit) {
+  if (!ctx) return FDC_INVALID;
+  auto it = ctx->orbits.find(orbit);
+  if (it == ctx->orbits.end()) return fail(ctx, FDC_INVALID, "unknown orbit handle");
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  cudaFree(it->second.z);
+  free_bla(it->second.bla);
+  ctx->orbits.erase(it);
+  return FDC_OK;
+}
+
+fdc_status fdc_upload_bla(fdc_ctx *ctx, int32_t orbit, const double *blocks7, const uint64_t *level_offsets,
+                          uint32_t levels, double eps, double dc_max, int64_t dc_exp) {
+  if (!ctx) return FDC_INVALID;
+  auto it = ctx->orbits.find(orbit);
+  if (it == ctx->orbits.end()) return fail(ctx, FDC_INVALID, "unknown orbit handle");
+  OrbitDev &o = it->second;
+  // bla.rs:26-33 and Bla::new's shape/value checks (bla.rs:184-216)
+  if (!(eps > 0.0 && eps <= 1.0 / (double)(1u << 24) && dc_max > 0.0 && std::isfinite(dc_max)))
+    return fail(ctx, FDC_INVALID, "BLA needs 0 < eps <= 2^-24 and a finite dc_max > 0");
+  if (levels >= (uint32_t)fdk::MAX_LEVELS) return fail(ctx, FDC_INVALID, "too many BLA levels");
+  if (levels > 0 && (!blocks7 || !level_offsets)) return fail(ctx, FDC_INVALID, "null BLA arrays");
+  uint64_t steps = o.len >= 2 ? o.len - 2 : 0;
+  uint64_t total = 0;
+  for (uint32_t i = 0; i < levels; ++i) {
+    if (level_offsets[i] != total)
+      return fail(ctx, FDC_INVALID, "BLA level offsets must be contiguous and level-major");
+    total += steps >> (i + 1);
+  }
+  std::vector<double> r2(total);
+  std::vector<double2> coef(2 * total), ab(total);
+  for (uint64_t b = 0; b < total; ++b) {
+    const double *v = blocks7 + 7 * b;
+    for (int f = 0; f < 7; ++f)
+      if (!std::isfinite(v[f])) return fail(ctx, FDC_INVALID, "BLA level holds a non-finite value");
+    if (v[4] < 0.0) return fail(ctx, FDC_INVALID, "BLA level holds a negative radius");
+    r2[b] = v[4] * v[4];
+    coef[2 * b] = make_double2(v[0], v[1]);
+    coef[2 * b + 1] = make_double2(v[2], v[3]);
+    ab[b] = make_double2(v[5], v[6]);
+  }
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  free_bla(o.bla);
+  o.has_bla = false;
+  BlaDev &d = o.bla;
+  d.levels = levels;
+  d.eps = eps;
+  d.dc_max = dc_max;
+  d.dc_exp = dc_exp;
+  for (uint32_t i = 0; i < levels; ++i) {
+    d.off[i] = (uint32_t)level_offsets[i];
+    d.count[i] = (uint32_t)(steps >> (i + 1));
+  }
+  if (total) {
+    CK(cudaMalloc(&d.r2, total * sizeof(double)));
+    CK(cudaMalloc(&d.coef, 2 * total * sizeof(double2)));
+    CK(cudaMalloc(&d.ab, total * sizeof(double2)));
+    CK(cudaMemcpyAsync(d.r2, r2.data(), total * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d.coef, coef.data(), 2 * total * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d.ab, ab.data(), total * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
+  o.has_bla = true;
+  return FDC_OK;
+}
+
+fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counters *counters) {
+  if (!ctx || !job || !out) return fail(ctx, FDC_INVALID, "null argument");
+  auto it = ctx->orbits.find(job->orbit);
+  if (it == ctx->orbits.end()) return fail(ctx, FDC_INVALID, "unknown orbit handle");
+  const OrbitDev &o = it->second;
+  const fdc_job &j = *job;
+  if (j.nx == 0 || j.ny == 0) return fail(ctx, FDC_INVALID, "empty sample grid");
+  if (j.ss == 0 || j.nx % j.ss || j.ny % j.ss) return fail(ctx, FDC_INVALID, "grid must be a whole number of pixels");
+  if ((uint64_t)j.nx * j.ny >= (1ull << 31)) return fail(ctx, FDC_INVALID, "grid larger than 2^31 samples");
+  if (j.tier < 0 || j.tier > 2) return fail(ctx, FDC_INVALID, "unknown tier");
+  if (j.max_iter >= (1ull << 32)) return fail(ctx, FDC_INVALID, "max_iter must be below 2^32");
+  if (!(j.escape_radius > 0.0) || !std::isfinite(j.escape_radius * j.escape_radius))
+    return fail(ctx, FDC_INVALID, "escape radius must be positive and its square finite");
+  if (!(j.h_m >= 1.0 && j.h_m < 2.0)) return fail(ctx, FDC_INVALID, "h_m must lie in [1, 2)");
+  if (j.flags & FDC_F32) return fail(ctx, FDC_DECLINED, "precision form not built into this kernel set");
+  uint32_t first = j.first_row, rows = j.rows ? j.rows : j.ny - j.first_row;
+  if (first >= j.ny || rows > j.ny - first) return fail(ctx, FDC_INVALID, "row range outside the grid");
+  const bool ext = j.tier == FDC_TIER_SCALED;
+  const bool bla = (j.flags & FDC_BLA) != 0;
+  const bool deriv = (j.flags & FDC_DERIVATIVE) != 0;
+  double h = j.h_m * fdroute::exp2i(j.h_e);
+  if (bla) {
+    if (!o.has_bla) return fail(ctx, FDC_INVALID, "FDC_BLA without an uploaded BLA table");
+    // grid.rs:392-411
+    if (j.escape_radius < 4.0)
+      return fail(ctx, FDC_INVALID, "escape radius is below 4: BLA blocks may only skip iterates with |z| <= 2 (1 + 2 eps)");
+    double half = std::hypot((double)j.nx / 2.0, (double)j.ny / 2.0);
+    double dc = ext ? j.h_m * half : h * half;
+    int64_t e = ext ? j.h_e : 0;
+    bool over = e == o.bla.dc_exp ? dc > o.bla.dc_max
+                                  : std::log2(dc) + (double)e > std::log2(o.bla.dc_max) + (double)o.bla.dc_exp;
+    if (std::isnan(dc) || over) return fail(ctx, FDC_INVALID, "view reaches |dc| beyond the BLA table's dc_max");
+  }
+  CK(cudaSetDevice(ctx->device));
+  const uint64_t n_rows = (uint64_t)rows * j.nx;
+  const bool dev_out = (j.flags & FDC_DEVICE_OUT) != 0;
+
+  fdk::Params p{};
+  p.orbit = o.z;
+  p.last = (uint32_t)(o.len - 1);
+  p.z0r = o.z0r;
+  p.z0i = o.z0i;
+  if (bla) {
+    p.bla_r2 = o.bla.r2;
+    p.bla_coef = o.bla.coef;
+    p.bla_ab = o.bla.ab;
+    p.bla_levels = o.bla.levels;
+    std::memcpy(p.bla_off, o.bla.off, sizeof p.bla_off);
+    std::memcpy(p.bla_count, o.bla.count, sizeof p.bla_count);
+  }
+  p.nx = j.nx;
+  p.ny = j.ny;
+  p.first_row = first;
+  p.rows = rows;
+  p.tiles_x = (j.nx + 7) / 8;
+  p.tier = j.tier;
+  p.flags = (deriv ? fdk::F_DERIV : 0) | (bla ? fdk::F_BLA : 0) | ((j.flags & FDC_SHIFT) ? fdk::F_SHIFT : 0);
+  p.c_re = j.c_re;
+  p.c_im = j.c_im;
+  p.h = h;
+  p.h_m = j.h_m;
+  p.h_e = j.h_e;
+  p.cosr = j.cos_rot;
+  p.sinr = j.sin_rot;
+  p.half_x = (double)j.nx / 2.0;
+  p.half_y = (double)j.ny / 2.0;
+  p.max_iter = j.max_iter;
+  p.r2 = j.escape_radius * j.escape_radius;
+  p.nucleus = j.nucleus_period;
+  p.px_m = j.h_m * (double)j.ss;
+  p.px_e = j.h_e;
+  p.total = (uint64_t)p.tiles_x * ((rows + 3) / 4) * 32;
+  p.deadline_ns = j.deadline_ms > 0 ? (uint64_t)(j.deadline_ms * 1e6) : 0;
+  p.out_base = (uint64_t)first * j.nx;
+
+  // Device buffers: caller's (FDC_DEVICE_OUT) or staging for the rendered rows.
+  struct Col {
+    void *host;
+    size_t width;
+  } cols[9] = {{out->cls, 1}, {out->n, 4}, {out->nu, 8}, {out->de, 4}, {out->normal, 2},
+               {out->z, 16}, {out->dz, 16}, {out->dexp, 8}, {out->status, 1}};
+  size_t need = 0;
+  size_t offs[11];
+  for (int c = 0; c < 9; ++c) {
+    offs[c] = need;
+    if (cols[c].host && !dev_out) need += (n_rows * cols[c].width + 255) & ~(size_t)255;
+  }
+  offs[9] = need;  // mask
+  if (j.mask) need += (n_rows + 255) & ~(size_t)255;
+  offs[10] = need;  // offsets
+  if (j.offsets) need += (n_rows * 16 + 255) & ~(size_t)255;
+  if (need > ctx->stage_bytes) {
+    CK(cudaStreamSynchronize(ctx->stream));
+    cudaFree(ctx->stage);
+    ctx->stage = nullptr;
+    ctx->stage_bytes = 0;
+    CK(cudaMalloc(&ctx->stage, need));
+    ctx->stage_bytes = need;
+  }
+  char *stage = (char *)ctx->stage;
+  void *dptr[9];
+  for (int c = 0; c < 9; ++c) {
+    if (!cols[c].host) dptr[c] = nullptr;
+    else if (dev_out) dptr[c] = (char *)cols[c].host + p.out_base * cols[c].width;
+    else dptr[c] = stage + offs[c];
+  }
+  p.cls = (uint8_t *)dptr[0];
+  p.n_out = (uint32_t *)dptr[1];
+  p.nu = (double *)dptr[2];
+  p.de = (float *)dptr[3];
+  p.normal = (uint16_t *)dptr[4];
+  p.z_out = (double2 *)dptr[5];
+  p.dz_out = (double2 *)dptr[6];
+  p.dexp_out = (int64_t *)dptr[7];
+  p.status = (uint8_t *)dptr[8];
+  if (j.mask) {
+    p.mask = (const uint8_t *)(stage + offs[9]);
+    CK(cudaMemcpyAsync(stage + offs[9], j.mask + p.out_base, n_rows, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  if (j.offsets) {
+    p.offsets = (const double2 *)(stage + offs[10]);
+    CK(cudaMemcpyAsync(stage + offs[10], j.offsets + 2 * p.out_base, n_rows * 16, cudaMemcpyHostToDevice,
+                       ctx->stream));
+  }
+  // Samples that are never reached keep zeroed columns and status 0.
+  for (int c = 0; c < 9; ++c)
+    if (dptr[c]) CK(cudaMemsetAsync(dptr[c], 0, n_rows * cols[c].width, ctx->stream));
+  p.queue = &ctx->scratch->queue;
+  p.counters = &ctx->scratch->counters;
+  p.timed_out = &ctx->scratch->timed_out;
+  CK(cudaMemsetAsync(ctx->scratch, 0, sizeof(Scratch), ctx->stream));
+
+  int variant = 0;
+  void *fn = pick_kernel(ext, deriv, bla, variant);
+  if (!ctx->blocks_per_sm[variant]) {
+    int b = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, 128, 0));
+    ctx->blocks_per_sm[variant] = b > 0 ? b : 1;
+  }
+  dim3 grid(ctx->sm_count * ctx->blocks_per_sm[variant]), block(128);
+  void *args[] = {&p};
+  CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  CK(cudaLaunchKernel(fn, grid, block, args, 0, ctx->stream));
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  if (!dev_out) {
+    for (int c = 0; c < 9; ++c)
+      if (cols[c].host)
+        CK(cudaMemcpyAsync((char *)cols[c].host + p.out_base * cols[c].width, dptr[c], n_rows * cols[c].width,
+                           cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  Scratch sc;
+  CK(cudaMemcpyAsync(&sc, ctx->scratch, sizeof sc, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (counters) {
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+    counters->samples = sc.counters.samples;
+    counters->iterations = sc.counters.iterations;
+    counters->blocks = sc.counters.blocks;
+    counters->skipped = sc.counters.skipped;
+    counters->fallback_samples = sc.counters.fallback;
+    counters->closed_form_samples = sc.counters.closed;
+    double sh;
+    std::memcpy(&sh, &sc.counters.shift_bits, 8);
+    counters->shift = sh;
+    counters->kernel_ms = ms;
+    counters->launches = 1;
+  }
+  if (sc.timed_out) return fail(ctx, FDC_TIMEOUT, "deadline passed; unfinished samples have status 0");
+  return FDC_OK;
+}
+
+}  // extern "C"

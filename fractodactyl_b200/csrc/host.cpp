@@ -1,0 +1,655 @@
+// Host-side set-up of the perturbation route (include/fdhost.h): exact decimal centres,
+// the fixed-point reference orbit, the view plane, the nucleus gate, the BLA table and
+// the benchmark locations' nucleus recipe. Compiled with -ffp-contract=off so every f64
+// result rounds as the reference's Rust does.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/fdhost.h"
+#include "route_internal.hpp"
+
+using fdroute::exp2i;
+using fdroute::exponent_field;
+
+namespace {
+
+thread_local std::string g_err;
+
+typedef unsigned __int128 u128;
+
+// ------------------------------------------------------------------------------------
+// Exact decimals. Grammar of fd_fixed::Decimal::parse (crates/fd-fixed/src/decimal.rs:
+// 20-49): [+-]digits[.digits][(e|E)[+-]digits], surrounding whitespace ignored.
+struct Dec {
+  bool neg = false;
+  std::string digits;  // '0'..'9', most significant first
+  int64_t exp10 = 0;
+};
+
+Dec parse_decimal(const char *text) {
+  std::string s(text ? text : "");
+  const std::string bad = "not a decimal number: \"" + s + "\"";
+  size_t a = 0, b = s.size();
+  while (a < b && isspace((unsigned char)s[a])) ++a;
+  while (b > a && isspace((unsigned char)s[b - 1])) --b;
+  Dec d;
+  if (a < b && (s[a] == '-' || s[a] == '+')) d.neg = s[a++] == '-';
+  size_t e = s.find_first_of("eE", a);
+  size_t mant_end = e == std::string::npos || e >= b ? b : e;
+  int64_t ex = 0;
+  if (mant_end < b) {
+    size_t i = mant_end + 1;
+    bool eneg = false;
+    if (i < b && (s[i] == '+' || s[i] == '-')) eneg = s[i++] == '-';
+    if (i >= b) throw std::runtime_error(bad);
+    u128 v = 0;
+    for (; i < b; ++i) {
+      if (s[i] < '0' || s[i] > '9') throw std::runtime_error(bad);
+      v = v * 10 + (unsigned)(s[i] - '0');
+      if (v > (u128)INT64_MAX + 1) throw std::runtime_error(bad);
+    }
+    if (!eneg && v > (u128)INT64_MAX) throw std::runtime_error(bad);
+    ex = eneg ? (int64_t)(0 - (uint64_t)v) : (int64_t)v;
+  }
+  size_t frac_len = 0;
+  bool seen_dot = false;
+  for (size_t i = a; i < mant_end; ++i) {
+    char c = s[i];
+    if (c == '.' && !seen_dot) {
+      seen_dot = true;
+      continue;
+    }
+    if (c < '0' || c > '9') throw std::runtime_error(bad);
+    d.digits.push_back(c);
+    if (seen_dot) ++frac_len;
+  }
+  if (d.digits.empty()) throw std::runtime_error(bad);
+  if ((__int128)ex - (__int128)frac_len < INT64_MIN) throw std::runtime_error(bad);
+  d.exp10 = ex - (int64_t)frac_len;
+  if (d.digits.find_first_not_of('0') == std::string::npos) d.neg = false;
+  return d;
+}
+
+// log2 |d| to ~1e-15 (decimal.rs:52-59).
+double log2_abs(const Dec &d) {
+  size_t first = d.digits.find_first_not_of('0');
+  if (first == std::string::npos) return -INFINITY;
+  size_t n = d.digits.size() - first;
+  double head = 0.0;
+  for (size_t i = 0; i < n && i < 17; ++i) head = head * 10.0 + (double)(d.digits[first + i] - '0');
+  double rest = n > 17 ? (double)(n - 17) : 0.0;
+  return (std::log10(head) + rest + (double)d.exp10) * 3.321928094887362347870319429489390175864831393;
+}
+
+// ------------------------------------------------------------------------------------
+// Sign-magnitude fixed point: L little-endian u64 limbs, the top one the integer part.
+struct Fix {
+  bool neg = false;
+  std::vector<uint64_t> mag;
+};
+
+size_t limbs_for(uint64_t bits) { return 1 + (size_t)((bits + 63) / 64); }
+
+// floor(|d| 2^(64 (L-1))) (decimal.rs:62-96): the digits as a big integer, scaled by
+// 10^exp10 with the result's integer part required to fit one limb.
+Fix to_fix(const Dec &d, size_t L) {
+  std::vector<uint64_t> big{0};
+  auto mul_add = [&](uint64_t m, uint64_t add) {
+    u128 carry = add;
+    for (auto &x : big) {
+      u128 t = (u128)x * m + carry;
+      x = (uint64_t)t;
+      carry = t >> 64;
+    }
+    if (carry) big.push_back((uint64_t)carry);
+  };
+  static const uint64_t P10[20] = {1ull, 10ull, 100ull, 1000ull, 10000ull, 100000ull, 1000000ull, 10000000ull,
+                                   100000000ull, 1000000000ull, 10000000000ull, 100000000000ull,
+                                   1000000000000ull, 10000000000000ull, 100000000000000ull,
+                                   1000000000000000ull, 10000000000000000ull, 100000000000000000ull,
+                                   1000000000000000000ull, 10000000000000000000ull};
+  for (size_t at = 0; at < d.digits.size(); at += 19) {
+    size_t len = std::min<size_t>(19, d.digits.size() - at);
+    uint64_t chunk = 0;
+    for (size_t i = 0; i < len; ++i) chunk = chunk * 10 + (uint64_t)(d.digits[at + i] - '0');
+    mul_add(P10[len], chunk);
+  }
+  int64_t e = d.exp10;
+  while (e > 0) {
+    int k = (int)std::min<int64_t>(e, 19);
+    mul_add(P10[k], 0);
+    e -= k;
+    if (big.size() > 1) throw std::runtime_error("value too large for fixed point");
+  }
+  std::vector<uint64_t> v(L - 1, 0);
+  v.insert(v.end(), big.begin(), big.end());
+  while (e < 0) {
+    int k = (int)std::min<int64_t>(-e, 19);
+    u128 r = 0;
+    for (size_t i = v.size(); i-- > 0;) {
+      u128 cur = (r << 64) | v[i];
+      v[i] = (uint64_t)(cur / P10[k]);
+      r = cur % P10[k];
+    }
+    e += k;
+    if (std::all_of(v.begin(), v.end(), [](uint64_t x) { return x == 0; })) break;
+  }
+  for (size_t i = L; i < v.size(); ++i)
+    if (v[i]) throw std::runtime_error("value too large for fixed point");
+  v.resize(L);
+  Fix f;
+  f.mag = v;
+  f.neg = d.neg && std::any_of(v.begin(), v.end(), [](uint64_t x) { return x != 0; });
+  return f;
+}
+
+// (m, e) with v = m 2^e from the top three limbs, rounded as fd_fixed::frexp does
+// (crates/fd-fixed/src/lib.rs:75-83): top + next 2^-64 + third 2^-128 in f64, in that order.
+bool frexp_fix(bool neg, const uint64_t *mag, size_t L, double &m, int64_t &e) {
+  size_t k = L;
+  while (k > 0 && mag[k - 1] == 0) --k;
+  if (k == 0) return false;
+  --k;
+  double v = (double)mag[k] + (k >= 1 ? (double)mag[k - 1] : 0.0) * exp2i(-64) +
+             (k >= 2 ? (double)mag[k - 2] : 0.0) * exp2i(-128);
+  int64_t ve = exponent_field(v);
+  double mm = v * exp2i(-ve);
+  m = neg ? -mm : mm;
+  e = ve + 64 * ((int64_t)k - ((int64_t)L - 1));
+  return true;
+}
+
+// crates/fd-fixed/src/lib.rs:86-93
+double fix_to_f64(bool neg, const uint64_t *mag, size_t L) {
+  double m;
+  int64_t e;
+  if (!frexp_fix(neg, mag, L, m, e)) return 0.0;
+  if (e < -1000) return m * exp2i(e + 100) * exp2i(-100);
+  return m * exp2i(e);
+}
+
+// Magnitude arithmetic on L limbs.
+inline int mag_cmp(const uint64_t *a, const uint64_t *b, size_t L) {
+  for (size_t i = L; i-- > 0;)
+    if (a[i] != b[i]) return a[i] < b[i] ? -1 : 1;
+  return 0;
+}
+inline void mag_add(const uint64_t *a, const uint64_t *b, uint64_t *o, size_t L) {
+  u128 c = 0;
+  for (size_t i = 0; i < L; ++i) {
+    c += (u128)a[i] + b[i];
+    o[i] = (uint64_t)c;
+    c >>= 64;
+  }
+}
+inline void mag_sub(const uint64_t *a, const uint64_t *b, uint64_t *o, size_t L) {
+  uint64_t borrow = 0;
+  for (size_t i = 0; i < L; ++i) {
+    u128 t = (u128)a[i] - b[i] - borrow;
+    o[i] = (uint64_t)t;
+    borrow = (uint64_t)(t >> 64) & 1;
+  }
+}
+inline bool nonzero(const uint64_t *a, size_t L) {
+  for (size_t i = 0; i < L; ++i)
+    if (a[i]) return true;
+  return false;
+}
+// Signed sum; zero is never negative. Returns the sign of o.
+inline bool sadd(bool an, const uint64_t *a, bool bn, const uint64_t *b, uint64_t *o, size_t L) {
+  if (an == bn) {
+    mag_add(a, b, o, L);
+    return an && nonzero(o, L);
+  }
+  if (mag_cmp(a, b, L) < 0) {
+    mag_sub(b, a, o, L);
+    return bn;
+  }
+  mag_sub(a, b, o, L);
+  return an && nonzero(o, L);
+}
+
+// o = floor(a^2 / 2^(64 (L-1))): column-wise (product-scanning) square with a 192-bit
+// column accumulator, doubling the off-diagonal terms as they are added.
+void square_trunc(const uint64_t *a, uint64_t *o, size_t L, uint64_t *prod) {
+  uint64_t c0 = 0, c1 = 0, c2 = 0;  // accumulator (c2:c1:c0)
+  for (size_t k = 0; k < 2 * L - 1; ++k) {
+    size_t lo = k >= L ? k - L + 1 : 0;
+    size_t hi = k / 2;  // i <= j = k - i
+    for (size_t i = lo; i <= hi; ++i) {
+      size_t j = k - i;
+      if (j >= L) continue;
+      u128 p = (u128)a[i] * a[j];
+      uint64_t pl = (uint64_t)p, ph = (uint64_t)(p >> 64);
+      int times = i == j ? 1 : 2;
+      for (int t = 0; t < times; ++t) {
+        u128 s = (u128)c0 + pl;
+        c0 = (uint64_t)s;
+        s = (u128)c1 + ph + (uint64_t)(s >> 64);
+        c1 = (uint64_t)s;
+        c2 += (uint64_t)(s >> 64);
+      }
+    }
+    prod[k] = c0;
+    c0 = c1;
+    c1 = c2;
+    c2 = 0;
+  }
+  prod[2 * L - 1] = c0;
+  std::memcpy(o, prod + (L - 1), L * sizeof(uint64_t));
+}
+
+// Z_{n+1} = Z_n^2 + C from Z_0 = 0 in L-limb fixed point with three squarings per step
+// (x' = x^2 - y^2 + cr, y' = (x + y)^2 - x^2 - y^2 + ci, crates/fd-fixed/src/orbit.rs:
+// 14-43), each point rounded to f64 by fix_to_f64; stops after `steps` points or at the
+// first point with |Z|^2 > escape2.
+uint64_t fixed_orbit(const Fix &cr, const Fix &ci, uint64_t steps, double escape2, double *re, double *im) {
+  const size_t L = cr.mag.size();
+  std::vector<uint64_t> buf(9 * L, 0);
+  uint64_t *x = buf.data(), *y = x + L, *x2 = y + L, *y2 = x2 + L, *s = y2 + L, *s2 = s + L, *t = s2 + L;
+  std::vector<uint64_t> prod(2 * L);
+  bool xn = false, yn = false;
+  uint64_t n = 0;
+  for (; n < steps;) {
+    square_trunc(x, x2, L, prod.data());
+    square_trunc(y, y2, L, prod.data());
+    sadd(xn, x, yn, y, s, L);
+    square_trunc(s, s2, L, prod.data());
+    bool tn = sadd(false, x2, true, y2, t, L);
+    xn = sadd(tn, t, cr.neg, cr.mag.data(), x, L);
+    mag_add(x2, y2, s, L);
+    tn = sadd(false, s2, true, s, t, L);
+    yn = sadd(tn, t, ci.neg, ci.mag.data(), y, L);
+    double fx = fix_to_f64(xn, x, L), fy = fix_to_f64(yn, y, L);
+    re[n] = fx;
+    im[n] = fy;
+    ++n;
+    if (fx * fx + fy * fy > escape2) break;
+  }
+  return n;
+}
+
+// ------------------------------------------------------------------------------------
+// BLA blocks (crates/fd-kernel/src/bla.rs:35-129), stored as [f64; 7].
+struct Blk {
+  double ar, ai, br, bi, r, alpha, beta;
+};
+
+inline Blk blk_single(double zr, double zi, double eps) {  // bla.rs:72-85
+  double az = std::hypot(zr, zi);
+  double r = 2.0 * eps * az;
+  if (!(r > 0.0 && az <= 2.0)) return Blk{0, 0, 0, 0, 0, 0, 0};
+  return Blk{2.0 * zr + 0.0, 2.0 * zi + 0.0, 1.0, 0.0, r, r, 0.0};
+}
+
+inline double times_exp2(double v, int64_t e) {  // bla.rs:115-121
+  return e >= -1022 ? v * exp2i(e) : v * exp2i(-1022) * exp2i(e + 1022);
+}
+
+inline double fmin_rust(double a, double b) { return std::isnan(a) ? b : (std::isnan(b) ? a : (a < b ? a : b)); }
+
+inline Blk blk_merge(const Blk &x, const Blk &y, double c, int64_t ce) {  // bla.rs:91-112
+  if (x.r == 0.0 || y.r == 0.0) return Blk{0, 0, 0, 0, 0, 0, 0};
+  double ax = std::hypot(x.ar, x.ai), ay = std::hypot(y.ar, y.ai);
+  double ahat = ax + x.alpha;
+  double bhat = std::hypot(x.br, x.bi) + x.beta;
+  double r = fmin_rust(x.r, (y.r - times_exp2(bhat * c, ce)) / ahat);
+  Blk z;
+  z.ar = y.ar * x.ar - y.ai * x.ai + 0.0 + 0.0;
+  z.ai = y.ar * x.ai + y.ai * x.ar + 0.0 + 0.0;
+  z.br = y.ar * x.br - y.ai * x.bi + y.br + 0.0;
+  z.bi = y.ar * x.bi + y.ai * x.br + y.bi + 0.0;
+  z.r = r;
+  z.alpha = ay * x.alpha + y.alpha * ahat;
+  z.beta = ay * x.beta + y.alpha * bhat + y.beta;
+  bool fin = std::isfinite(z.ar) && std::isfinite(z.ai) && std::isfinite(z.br) && std::isfinite(z.bi) &&
+             std::isfinite(z.r) && std::isfinite(z.alpha) && std::isfinite(z.beta);
+  if (r > 0.0 && fin) return z;
+  return Blk{0, 0, 0, 0, 0, 0, 0};
+}
+
+template <class F>
+void parallel_for(uint64_t n, int threads, F f) {
+  if (threads <= 1 || n < 4096) {
+    f(0, n);
+    return;
+  }
+  std::vector<std::thread> pool;
+  uint64_t chunk = (n + threads - 1) / threads;
+  for (int t = 0; t < threads; ++t) {
+    uint64_t a = t * chunk, b = std::min<uint64_t>(n, a + chunk);
+    if (a >= b) break;
+    pool.emplace_back([=] { f(a, b); });
+  }
+  for (auto &th : pool) th.join();
+}
+
+// Fixed-point to decimal string with `digits` fraction digits (truncated).
+std::string fix_to_string(const Fix &f, size_t digits) {
+  const size_t L = f.mag.size();
+  std::string out = f.neg ? "-" : "";
+  out += std::to_string(f.mag[L - 1]);
+  out += '.';
+  std::vector<uint64_t> frac(f.mag.begin(), f.mag.end() - 1);
+  while (digits > 0) {
+    int k = (int)std::min<size_t>(digits, 19);
+    uint64_t m = 1;
+    for (int i = 0; i < k; ++i) m *= 10;
+    u128 carry = 0;
+    for (auto &x : frac) {
+      u128 t = (u128)x * m + carry;
+      x = (uint64_t)t;
+      carry = t >> 64;
+    }
+    std::string part = std::to_string((uint64_t)carry);
+    out += std::string(k - part.size(), '0') + part;
+    digits -= k;
+  }
+  return out;
+}
+
+// Floating value m 2^e (|m| in [1, 2)) with a wide exponent, for derivatives that leave
+// f64's range.
+struct Fec {
+  double re = 0, im = 0;
+  int64_t e = 0;
+};
+inline Fec fec_norm(double re, double im, int64_t e) {
+  double a = std::max(std::fabs(re), std::fabs(im));
+  if (a == 0.0) return Fec{0, 0, 0};
+  int k = std::ilogb(a);
+  return Fec{std::scalbn(re, -k), std::scalbn(im, -k), e + k};
+}
+
+// v as a fixed-point magnitude with F = 64 (L-1) fraction bits (|v| = m 2^e < 2^63).
+Fix fe_to_fix(double m, int64_t e, size_t L) {
+  Fix f;
+  f.mag.assign(L, 0);
+  if (m == 0.0) return f;
+  f.neg = m < 0;
+  int k;
+  double mm = std::frexp(std::fabs(m), &k);  // mm in [0.5, 1)
+  uint64_t bits53 = (uint64_t)std::ldexp(mm, 53);
+  int64_t shift = e + k - 53 + 64 * (int64_t)(L - 1);  // value = bits53 2^shift in units of 2^-F
+  for (int b = 0; b < 53; ++b) {
+    if (!((bits53 >> b) & 1)) continue;
+    int64_t pos = shift + b;
+    if (pos < 0 || pos >= (int64_t)(64 * L)) continue;
+    f.mag[pos / 64] |= 1ull << (pos % 64);
+  }
+  return f;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *fdh_last_error(void) { return g_err.c_str(); }
+
+int fdh_plane_new(const char *center_re, const char *center_im, const char *width, double rotation, uint32_t nx,
+                  uint32_t ny, fdh_plane *out) {
+  try {
+    // crates/fd-kernel/src/view.rs:42-87
+    if (nx == 0 || ny == 0) throw std::runtime_error("empty sample grid");
+    Dec w = parse_decimal(width);
+    double lw = log2_abs(w);
+    if (w.neg || !std::isfinite(lw)) throw std::runtime_error("view width must be positive");
+    double need = std::ceil(std::max(64.0 - lw, 64.0));
+    Fix wf = to_fix(w, limbs_for((uint64_t)need));
+    double wm;
+    int64_t we;
+    if (!frexp_fix(wf.neg, wf.mag.data(), wf.mag.size(), wm, we)) throw std::runtime_error("view width underflowed");
+    double q = wm / (double)nx;
+    int64_t qe = exponent_field(q);
+    out->h_m = q * exp2i(-qe);
+    out->h_e = we + qe;
+    auto num = [](const char *s) {
+      parse_decimal(s);
+      return std::strtod(s, nullptr);
+    };
+    out->c_re = num(center_re);
+    out->c_im = num(center_im);
+    if (!(std::isfinite(out->c_re) && std::isfinite(out->c_im))) throw std::runtime_error("view centre out of range");
+    double c_mag = std::max(std::max(std::fabs(out->c_re), std::fabs(out->c_im)), exp2i(-1022));
+    bool f64_ok = std::log2(c_mag) - 52.0 <= (double)out->h_e - 10.0 && out->h_e > -1000;
+    out->tier = f64_ok ? 0 : (out->h_e >= -900 ? 1 : 2);
+    out->bits = (uint64_t)std::max<int64_t>(128 - out->h_e, 128);
+    out->sin_rot = std::sin(rotation);
+    out->cos_rot = std::cos(rotation);
+    return 0;
+  } catch (std::exception &e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+int64_t fdh_orbit_fixed(const char *center_re, const char *center_im, uint64_t bits, uint64_t max_iter, double *re,
+                        double *im, uint64_t cap) {
+  try {
+    uint64_t steps = std::min<uint64_t>(max_iter, (1ull << 20) - 1);
+    if (cap < steps + 1) throw std::runtime_error("orbit buffers too small");
+    size_t L = limbs_for(bits);
+    Fix cr = to_fix(parse_decimal(center_re), L), ci = to_fix(parse_decimal(center_im), L);
+    re[0] = 0.0;
+    im[0] = 0.0;
+    return (int64_t)(1 + fixed_orbit(cr, ci, steps, 4294967296.0, re + 1, im + 1));
+  } catch (std::exception &e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+int64_t fdh_orbit_f64(double c_re, double c_im, uint64_t max_iter, double escape_radius, double *re, double *im,
+                      uint64_t cap) {
+  uint64_t steps = std::min<uint64_t>(max_iter, (1ull << 20) - 1);
+  if (cap < steps + 1) {
+    g_err = "orbit buffers too small";
+    return -1;
+  }
+  // reference.rs:21-48
+  double x = 0.0, y = 0.0, lim = escape_radius * escape_radius;
+  re[0] = 0.0;
+  im[0] = 0.0;
+  uint64_t n = 1;
+  for (uint64_t s = 0; s < steps; ++s) {
+    double t = x * x - y * y + c_re;
+    y = 2.0 * x * y + c_im;
+    x = t;
+    re[n] = x;
+    im[n] = y;
+    ++n;
+    if (x * x + y * y > lim) break;
+  }
+  return (int64_t)n;
+}
+
+int64_t fdh_nucleus_period(const double *re, const double *im, uint64_t len) {
+  // reference.rs:102-120
+  if (len < 2) return -1;
+  double record = std::hypot(re[1], im[1]);
+  double log_beta = 0.0;
+  for (uint64_t p = 2; p < len / 2; ++p) {
+    double previous = std::hypot(re[p - 1], im[p - 1]);
+    log_beta += 1.0 + std::log2(previous);
+    double radius = std::hypot(re[p], im[p]);
+    if (radius > 1e-140 && radius < 1e-24 && radius < record * 1e-12 && 1.0 + log_beta + std::log2(radius) < -40.0 &&
+        std::hypot(re[2 * p], im[2 * p]) <= 2.0 * radius)
+      return (int64_t)p;
+    record = fmin_rust(record, radius);
+  }
+  return -1;
+}
+
+int fdh_bla_build(const double *re, const double *im, uint64_t len, double eps, double dc_max, int64_t dc_exp,
+                  int threads, double *blocks7, uint64_t *level_offsets, uint32_t *levels, uint64_t *blocks) {
+  // bla.rs:161-216: singles over Z_1..Z_steps, pairwise merges level by level, stopping
+  // before the first level without a valid block.
+  if (!(eps > 0.0 && eps <= 1.0 / (double)(1u << 24) && dc_max > 0.0 && std::isfinite(dc_max))) {
+    g_err = "BLA needs 0 < eps <= 2^-24 and a finite dc_max > 0";
+    return -1;
+  }
+  if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+  uint64_t steps = len >= 2 ? len - 2 : 0;
+  std::vector<Blk> cur(steps / 2), next;
+  // level 1 directly from pairs of singles
+  parallel_for(steps / 2, threads, [&](uint64_t a, uint64_t b) {
+    for (uint64_t t = a; t < b; ++t)
+      cur[t] = blk_merge(blk_single(re[2 * t + 1], im[2 * t + 1], eps), blk_single(re[2 * t + 2], im[2 * t + 2], eps),
+                         dc_max, dc_exp);
+  });
+  std::vector<std::vector<Blk>> lv;
+  auto any_valid = [](const std::vector<Blk> &l) {
+    for (auto &b : l)
+      if (b.r > 0.0) return true;
+    return false;
+  };
+  while (any_valid(cur)) {
+    next.assign(cur.size() / 2, Blk{});
+    parallel_for(next.size(), threads, [&](uint64_t a, uint64_t b) {
+      for (uint64_t t = a; t < b; ++t) next[t] = blk_merge(cur[2 * t], cur[2 * t + 1], dc_max, dc_exp);
+    });
+    lv.push_back(std::move(cur));
+    cur = std::move(next);
+  }
+  uint64_t total = 0;
+  for (auto &l : lv) total += l.size();
+  *levels = (uint32_t)lv.size();
+  *blocks = total;
+  if (!blocks7) return 0;
+  uint64_t at = 0;
+  for (size_t i = 0; i < lv.size(); ++i) {
+    if (level_offsets) level_offsets[i] = at;
+    std::memcpy(blocks7 + 7 * at, lv[i].data(), lv[i].size() * sizeof(Blk));
+    at += lv[i].size();
+  }
+  if (level_offsets) level_offsets[lv.size()] = at;
+  return 0;
+}
+
+void fdh_dc_bound(const fdh_plane *plane, int32_t tier, uint32_t nx, uint32_t ny, double *dc, int64_t *e) {
+  // grid.rs:428-444
+  double half = std::hypot((double)nx / 2.0, (double)ny / 2.0);
+  if (tier == 2) {
+    *dc = plane->h_m * half;
+    *e = plane->h_e;
+  } else {
+    *dc = plane->h_m * exp2i(plane->h_e) * half;
+    *e = 0;
+  }
+}
+
+int fdh_nucleus(const char *start_re, const char *start_im, double log10_radius, uint64_t max_period, uint64_t bits,
+                char *re_out, char *im_out, size_t cap, uint64_t *period) {
+  try {
+    const size_t L = limbs_for(bits);
+    Fix cr = to_fix(parse_decimal(start_re), L), ci = to_fix(parse_decimal(start_im), L);
+    const double log2_r = log10_radius * 3.321928094887362;
+    std::vector<uint64_t> buf(8 * L), prod(2 * L);
+    uint64_t *x = buf.data(), *y = x + L, *x2 = y + L, *y2 = x2 + L, *s = y2 + L, *s2 = s + L, *t = s2 + L;
+    bool xn = false, yn = false;
+    // z as a wide-exponent complex number (shared exponent)
+    auto zfec = [&]() {
+      double mr = 0, mi = 0;
+      int64_t er = INT64_MIN / 4, ei = INT64_MIN / 4;
+      frexp_fix(xn, x, L, mr, er) || (mr = 0, true);
+      frexp_fix(yn, y, L, mi, ei) || (mi = 0, true);
+      if (mr == 0 && mi == 0) return Fec{0, 0, 0};
+      int64_t e = std::max(mr == 0 ? INT64_MIN / 4 : er, mi == 0 ? INT64_MIN / 4 : ei);
+      double a = mr == 0 ? 0.0 : std::ldexp(mr, (int)std::max<int64_t>(er - e, -2000));
+      double b = mi == 0 ? 0.0 : std::ldexp(mi, (int)std::max<int64_t>(ei - e, -2000));
+      return fec_norm(a, b, e);
+    };
+    auto log2_abs_fec = [](const Fec &v) -> double {
+      if (v.re == 0 && v.im == 0) return -(double)INFINITY;
+      return 0.5 * std::log2(v.re * v.re + v.im * v.im) + (double)v.e;
+    };
+    // dz' = 2 z dz + 1 with z, dz wide-exponent complex numbers.
+    auto dz_step = [](const Fec &z, const Fec &dz) {
+      if ((z.re == 0 && z.im == 0) || (dz.re == 0 && dz.im == 0)) return Fec{1, 0, 0};
+      Fec p = fec_norm(z.re * dz.re - z.im * dz.im, z.re * dz.im + z.im * dz.re, z.e + dz.e + 1);
+      if (p.e > 80) return p;
+      if (p.e < -80) return Fec{1, 0, 0};
+      return fec_norm(std::ldexp(p.re, (int)p.e) + 1.0, std::ldexp(p.im, (int)p.e), 0);
+    };
+    // z' = z^2 + c in fixed point (three squarings, as the reference orbit)
+    auto z_step = [&](const Fix &a, const Fix &b) {
+      square_trunc(x, x2, L, prod.data());
+      square_trunc(y, y2, L, prod.data());
+      sadd(xn, x, yn, y, s, L);
+      square_trunc(s, s2, L, prod.data());
+      bool tn = sadd(false, x2, true, y2, t, L);
+      xn = sadd(tn, t, a.neg, a.mag.data(), x, L);
+      mag_add(x2, y2, s, L);
+      tn = sadd(false, s2, true, s, t, L);
+      yn = sadd(tn, t, b.neg, b.mag.data(), y, L);
+      double fx = fix_to_f64(xn, x, L), fy = fix_to_f64(yn, y, L);
+      return fx * fx + fy * fy <= 4.0e8;
+    };
+    auto reset = [&]() {
+      std::fill(buf.begin(), buf.end(), 0);
+      xn = yn = false;
+    };
+    // Ball period (ref.py:46-52): first p with |z_p| < r |dz_p|.
+    reset();
+    Fec dz{0, 0, 0};
+    uint64_t p = 0;
+    for (uint64_t k = 1; k <= max_period; ++k) {
+      dz = dz_step(zfec(), dz);
+      if (!z_step(cr, ci)) break;
+      if (log2_abs_fec(zfec()) < log2_r + log2_abs_fec(dz)) {
+        p = k;
+        break;
+      }
+    }
+    if (p == 0) throw std::runtime_error("no ball period below the limit");
+    // Newton on z_p(c) = 0 with steps clamped to r/4 (ref.py:54-67, zone_build.rs:215-231).
+    const double log2_rmax = log2_r - 2.0;
+    bool converged = false;
+    for (int it = 0; it < 200 && !converged; ++it) {
+      reset();
+      dz = Fec{0, 0, 0};
+      for (uint64_t k = 0; k < p; ++k) {
+        dz = dz_step(zfec(), dz);
+        if (!z_step(cr, ci)) throw std::runtime_error("Newton iterate escaped");
+      }
+      Fec z = zfec();
+      if (z.re == 0 && z.im == 0) break;
+      double den = dz.re * dz.re + dz.im * dz.im;
+      Fec st = fec_norm((z.re * dz.re + z.im * dz.im) / den, (z.im * dz.re - z.re * dz.im) / den, z.e - dz.e);
+      double lmag = log2_abs_fec(st);
+      if (lmag > log2_rmax) {
+        double f = std::exp2(log2_rmax - lmag);
+        st = fec_norm(st.re * f, st.im * f, st.e);
+        lmag = log2_rmax;
+      }
+      Fix dr = fe_to_fix(st.re, st.e, L), di = fe_to_fix(st.im, st.e, L);
+      Fix nr, ni;
+      nr.mag.assign(L, 0);
+      ni.mag.assign(L, 0);
+      nr.neg = sadd(cr.neg, cr.mag.data(), !dr.neg, dr.mag.data(), nr.mag.data(), L);
+      ni.neg = sadd(ci.neg, ci.mag.data(), !di.neg, di.mag.data(), ni.mag.data(), L);
+      cr = nr;
+      ci = ni;
+      converged = lmag < -(double)(64 * (L - 1)) + 8;
+    }
+    if (!converged) throw std::runtime_error("nucleus Newton did not converge");
+    size_t digits = (size_t)std::ceil(64.0 * (double)(L - 1) * 0.30102999566398120) + 2;
+    std::string sre = fix_to_string(cr, digits), sim = fix_to_string(ci, digits);
+    if (sre.size() + 1 > cap || sim.size() + 1 > cap) throw std::runtime_error("output buffer too small");
+    std::memcpy(re_out, sre.c_str(), sre.size() + 1);
+    std::memcpy(im_out, sim.c_str(), sim.size() + 1);
+    *period = p;
+    return 0;
+  } catch (std::exception &e) {
+    g_err = e.what();
+    return -1;
+  }
+}
+
+}  // extern "C"

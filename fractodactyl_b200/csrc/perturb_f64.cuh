@@ -1,0 +1,591 @@
+// The plain (FP64) perturbation kernel: one lane per sample, persistent warps that
+// refill finished lanes from an atomic tile queue. The per-sample state machine is
+// iterate() of crates/fd-kernel/src/sample.rs:170-581 (Binary64 and Binary64Exponent,
+// number.rs:92-124), one loop iteration per call of step(), with the reference's
+// operation order. Compile with -fmad=false.
+#pragma once
+#include <cstdint>
+
+#include "fd_device.cuh"
+
+namespace fdk {
+
+constexpr int MAX_LEVELS = 40;
+
+struct Counters {
+  unsigned long long samples, iterations, blocks, skipped, fallback, closed;
+  unsigned long long shift_bits;  // max of the non-negative shift estimates, as bits
+  unsigned long long pad;
+};
+
+// Everything one launch needs; passed by value (kernel parameter space).
+struct Params {
+  const double2 *__restrict__ orbit;  // Z_0..Z_last, interleaved re/im
+  uint32_t last;
+  double z0r, z0i;
+  // BLA, level-major: r2[off + t], coef[2 (off + t)] = (a.re, a.im), (b.re, b.im), ab = (alpha, beta)
+  const double *__restrict__ bla_r2;
+  const double2 *__restrict__ bla_coef;
+  const double2 *__restrict__ bla_ab;
+  uint32_t bla_levels;
+  uint32_t bla_off[MAX_LEVELS];
+  uint32_t bla_count[MAX_LEVELS];
+  // frame
+  uint32_t nx, ny, first_row, rows, tiles_x;
+  int32_t tier;
+  uint32_t flags;
+  double c_re, c_im, h, h_m;
+  int64_t h_e;
+  double cosr, sinr, half_x, half_y;
+  uint64_t max_iter;
+  double r2;
+  int64_t nucleus;
+  double px_m;  // DE output pixel h_m * ss (store.rs:57-63)
+  int64_t px_e;
+  const uint8_t *__restrict__ mask;
+  const double2 *__restrict__ offsets;
+  // outputs (device)
+  uint8_t *cls;
+  uint32_t *n_out;
+  double *nu;
+  float *de;
+  uint16_t *normal;
+  double2 *z_out, *dz_out;
+  int64_t *dexp_out;
+  uint8_t *status;
+  // scratch: work queue and counters
+  unsigned long long *queue;
+  Counters *counters;
+  uint64_t total;        // queue slots (tiles * 32)
+  uint64_t deadline_ns;  // 0 = none
+  uint32_t *timed_out;
+  uint64_t out_base;  // outputs hold the rendered rows only: index idx - out_base
+};
+
+enum : uint32_t { F_DERIV = 1u, F_BLA = 2u, F_SHIFT = 4u };
+
+// Per-lane sample state (sample.rs:187-236).
+template <bool EXT>
+struct State {
+  double xr, xi, dr, di;
+  double fr, fi;  // z = Z[m] + delta (carried between steps on the ordinary tier)
+  double Zr, Zi;  // Z[m]
+  double ar, ai;  // sample offset (mantissa on the extended tier)
+  double dc_r, dc_i, scale, inverse;
+  double sr, si, qr, qi, qstep;
+  Multiplier mu;
+  Contraction ct;
+  double adc, shift;
+  int64_t offset_exp, delta_exp, derivative_exp;
+  int64_t nucleus;
+  uint64_t n, chk, sn, hold, blocks, skipped;
+  uint32_t m, idx;
+  int returns;
+  bool pending, predicted;
+};
+
+// Result of a finished sample (sample.rs:21-40): kind 0 escaped, 1 interior, 2 unresolved.
+struct Result {
+  int kind;
+  uint64_t n;
+  double zr, zi, dr, di;
+  int64_t dexp;
+};
+
+// One iteration of the while loop of sample.rs:237-575. Returns true when the sample
+// has an outcome (written to r).
+template <bool EXT, bool D, bool L>
+__device__ __forceinline__ bool step(const Params &p, State<EXT> &s, Result &res) {
+  if (s.n >= p.max_iter) {
+    res.kind = 2;
+    return true;
+  }
+  bool took = false;
+  if (L) {
+    if (s.nucleus < 0 || s.m != 0) {
+      // Bla::find (bla.rs:234-249) with the budget of sample.rs:246-263.
+      double d2 = EXT ? (s.xr * s.xr + s.xi * s.xi) * s.scale * s.scale : s.xr * s.xr + s.xi * s.xi;
+      uint64_t cap = s.hold > 0 ? s.sn + s.hold : (s.pending ? ~0ull : s.chk);
+      uint64_t budget = p.max_iter < cap ? p.max_iter : cap;
+      if (s.nucleus >= 0) {
+        uint64_t nc = s.n == 0 ? 1ull : (uint64_t)s.nucleus + 1;
+        budget = budget < nc ? budget : nc;
+      }
+      budget = budget > s.n ? budget - s.n : 0;
+      uint32_t k = s.m - 1u;
+      uint32_t tz = k == 0 ? 32u : (uint32_t)(__ffs((int)k) - 1);
+      uint32_t top = tz < p.bla_levels ? tz : p.bla_levels;
+      int lv = -1;
+      uint32_t at = 0;
+      for (uint32_t i = 0; i < top; ++i) {
+        if ((2ull << i) > budget) break;
+        uint32_t a = k >> (i + 1);
+        if (a >= p.bla_count[i]) break;
+        if (!(d2 < __ldg(p.bla_r2 + p.bla_off[i] + a))) break;
+        lv = (int)i;
+        at = a;
+      }
+      if (lv >= 0) {
+        took = true;
+        uint32_t b = p.bla_off[lv] + at;
+        double2 A = __ldg(p.bla_coef + 2 * b), B = __ldg(p.bla_coef + 2 * b + 1);
+        uint32_t len = 2u << lv;
+        if (s.nucleus >= 0 && s.n >= 1) s.ct.multiply(A.x, A.y);
+        if (!EXT && s.hold > 0) s.mu.multiply(A.x, A.y);
+        if (EXT) {
+          normalise(s.xr, s.xi, s.delta_exp, 0);
+          if (D) {
+            normalise(s.dr, s.di, s.derivative_exp, INT64_MAX / 4);
+            s.inverse = exp2i(-s.derivative_exp);
+          }
+          s.scale = exp2i(s.delta_exp);
+          double factor = exp2i(s.offset_exp - s.delta_exp);
+          s.dc_r = s.ar * factor;
+          s.dc_i = s.ai * factor;
+        }
+        if (D) {
+          double t = A.x * s.dr - A.y * s.di + B.x * s.inverse;
+          s.di = A.x * s.di + A.y * s.dr + B.y * s.inverse;
+          s.dr = t;
+          if (!EXT && (p.flags & F_SHIFT)) {
+            double2 ab = __ldg(p.bla_ab + b);
+            s.shift += (ab.x * sqrt(s.xr * s.xr + s.xi * s.xi) + ab.y * s.adc) / sqrt(s.dr * s.dr + s.di * s.di);
+          }
+        }
+        double t = A.x * s.xr - A.y * s.xi + B.x * s.dc_r - B.y * s.dc_i;
+        s.xi = A.x * s.xi + A.y * s.xr + B.x * s.dc_i + B.y * s.dc_r;
+        s.xr = t;
+        if (EXT) {
+          normalise(s.xr, s.xi, s.delta_exp, 0);
+          if (D) {
+            normalise(s.dr, s.di, s.derivative_exp, INT64_MAX / 4);
+            s.inverse = exp2i(-s.derivative_exp);
+          }
+          s.scale = exp2i(s.delta_exp);
+          double factor = exp2i(s.offset_exp - s.delta_exp);
+          s.dc_r = s.ar * factor;
+          s.dc_i = s.ai * factor;
+        }
+        s.m += len;
+        s.n += len;
+        s.blocks += 1;
+        s.skipped += len;
+      }
+    }
+  }
+  if (!took) {
+    double fr, fi;
+    if (EXT) {
+      fr = s.Zr + s.scale * s.xr;
+      fi = s.Zi + s.scale * s.xi;
+    } else {
+      fr = s.fr;  // == Z[m] + delta, carried from the previous iteration
+      fi = s.fi;
+    }
+    if (s.nucleus >= 0 && s.n >= 1) s.ct.multiply(2.0 * fr, 2.0 * fi);
+    if (!EXT && s.hold > 0) s.mu.multiply(2.0 * fr, 2.0 * fi);
+    if (D) {
+      double t = 2.0 * (fr * s.dr - fi * s.di) + s.inverse;
+      s.di = 2.0 * (fr * s.di + fi * s.dr);
+      s.dr = t;
+      if (EXT && rmax(fabs(s.dr), fabs(s.di)) > HI) {
+        s.dr = s.dr * LO;
+        s.di = s.di * LO;
+        s.derivative_exp += 32;
+        s.inverse = exp2i(-s.derivative_exp);
+      }
+    }
+    double wr = s.xr, wi = s.xi, zr = s.Zr, zi = s.Zi;
+    if (EXT) {  // number.rs:109-124
+      s.xr = 2.0 * (zr * wr - zi * wi) + s.scale * (wr * wr - wi * wi) + s.dc_r;
+      s.xi = 2.0 * (zr * wi + zi * wr) + s.scale * (2.0 * wr * wi) + s.dc_i;
+    } else {  // number.rs:92-107
+      s.xr = 2.0 * (zr * wr - zi * wi) + wr * wr - wi * wi + s.dc_r;
+      s.xi = 2.0 * (zr * wi + zi * wr + wr * wi) + s.dc_i;
+    }
+    s.m += 1;
+    s.n += 1;
+  }
+  double2 Z = __ldg(p.orbit + s.m);
+  s.Zr = Z.x;
+  s.Zi = Z.y;
+  double pr = EXT ? s.scale * s.xr : s.xr, pi = EXT ? s.scale * s.xi : s.xi;
+  double fr = Z.x + pr, fi = Z.y + pi;
+  double f2 = fr * fr + fi * fi;
+  if (f2 > p.r2) {
+    res.kind = 0;
+    res.n = s.n;
+    res.zr = fr;
+    res.zi = fi;
+    res.dr = s.dr;
+    res.di = s.di;
+    res.dexp = s.derivative_exp;
+    return true;
+  }
+  if (s.nucleus >= 0 && s.n == (uint64_t)s.nucleus + 1) {
+    if (s.ct.small()) {
+      res.kind = 1;
+      res.n = s.n;
+      return true;
+    }
+    s.nucleus = -1;
+  }
+  double delta2 = pr * pr + pi * pi;
+  bool rebase = EXT ? f2 <= delta2 : f2 < delta2;
+  if (rebase || s.m == p.last) {
+    if (EXT) {
+      if (f2 > SQUARE_OK) {
+        s.xr = fr;
+        s.xi = fi;
+        s.delta_exp = 0;
+      } else {
+        Cx3 t = sum2(Cx3{Z.x, Z.y, 0}, Cx3{s.xr, s.xi, s.delta_exp}, s.delta_exp);
+        s.xr = t.re;
+        s.xi = t.im;
+        s.delta_exp = t.e;
+      }
+      s.scale = exp2i(s.delta_exp);
+      s.m = 0;
+      s.Zr = p.z0r;
+      s.Zi = p.z0i;
+      if (s.scale < 1.0 / 1e270) {  // TINY, sample.rs:17
+        s.nucleus = -1;
+        if (D) {
+          Cx3 v = zero_step_dz(Cx3{s.xr, s.xi, s.delta_exp}, Cx3{s.dr, s.di, s.derivative_exp});
+          s.dr = v.re;
+          s.di = v.im;
+          s.derivative_exp = v.e;
+          s.inverse = exp2i(-s.derivative_exp);
+        }
+        Cx3 w = zero_step(Cx3{s.xr, s.xi, s.delta_exp}, Cx3{s.ar, s.ai, s.offset_exp});
+        s.xr = w.re;
+        s.xi = w.im;
+        s.delta_exp = w.e;
+        s.scale = exp2i(s.delta_exp);
+        s.m = 1;
+        s.n = s.n + 1;
+        double2 Z1 = __ldg(p.orbit + 1);
+        s.Zr = Z1.x;
+        s.Zi = Z1.y;
+      }
+      double factor = exp2i(s.offset_exp - s.delta_exp);
+      s.dc_r = s.ar * factor;
+      s.dc_i = s.ai * factor;
+    } else {
+      s.xr = fr;
+      s.xi = fi;
+      s.m = 0;
+      s.Zr = p.z0r;
+      s.Zi = p.z0i;
+    }
+  } else if (EXT) {
+    double magnitude = rmax(fabs(s.xr), fabs(s.xi));
+    int64_t k = 0;
+    if (magnitude > HI && s.delta_exp < 0)
+      k = -s.delta_exp < 32 ? -s.delta_exp : 32;
+    else if (magnitude < LO && magnitude != 0.0)
+      k = -32;
+    if (k != 0) {
+      double factor = exp2i(-k);
+      s.xr = s.xr * factor;
+      s.xi = s.xi * factor;
+      s.delta_exp = s.delta_exp + k;
+      s.scale = exp2i(s.delta_exp);
+      double f = exp2i(s.offset_exp - s.delta_exp);
+      s.dc_r = s.ar * f;
+      s.dc_i = s.ai * f;
+    }
+  }
+  if (!EXT) {
+    // The next plain step's z (sample.rs:331): Z[m] + delta with the current m, delta.
+    s.fr = s.Zr + s.xr;
+    s.fi = s.Zi + s.xi;
+  }
+  double check_r = EXT ? pr : s.xr, check_i = EXT ? pi : s.xi;
+  bool judge = check_r * check_r + check_i * check_i > RES2 * f2;
+  if (EXT) judge = judge && s.returns < 4;
+  if (!judge) {
+    if (EXT) {
+      if (s.n >= s.chk) {
+        s.sr = fr;
+        s.si = fi;
+        s.sn = s.n;
+        s.chk = s.chk * 2;
+      }
+    } else if (s.hold > 0) {
+      if (s.n >= s.sn + s.hold) {
+        s.hold = 0;
+        s.predicted = false;
+        s.pending = true;
+      }
+    } else if (s.n >= s.chk) {
+      s.pending = true;
+    }
+    return false;
+  }
+  double dist = fabs(fr - s.sr) + fabs(fi - s.si);
+  double size = fabs(s.sr) + fabs(s.si);
+  if (EXT) {
+    if (s.returns < 4 && dist < 1e-13 * size + 1e-300) {
+      if (contracting(p.orbit, p.last, s.m, check_r, check_i, s.ar * exp2i(s.offset_exp),
+                      s.ai * exp2i(s.offset_exp), s.n - s.sn)) {
+        res.kind = 2;
+        return true;
+      }
+      s.returns += 1;
+    }
+    if (s.n == s.chk || s.n > s.chk) {
+      s.sr = fr;
+      s.si = fi;
+      s.sn = s.n;
+      s.chk = s.chk * 2;
+    }
+    return false;
+  }
+  if (dist < 1e-3 * size) {
+    uint64_t period = s.n - s.sn;
+    if (s.hold == period && s.mu.below_one()) {
+      double mr, mi;
+      s.mu.value(mr, mi);
+      double gr = fr - s.sr, gi = fi - s.si;
+      double er = mr - 1.0, ei = mi;
+      double den = er * er + ei * ei;
+      double qpr = s.sr - (gr * er + gi * ei) / den;
+      double qpi = s.si - (gi * er - gr * ei) / den;
+      double tol = rmin(0.1 * sqrt(den), 1e-2) * s.qstep + 16.0 * U * size;
+      if (s.predicted && fabs(qpr - s.qr) + fabs(qpi - s.qi) <= tol) {
+        res.kind = 1;
+        res.n = s.n;
+        return true;
+      }
+      s.qr = qpr;
+      s.qi = qpi;
+      s.qstep = (fabs(gr) + fabs(gi)) / sqrt(den);
+      s.predicted = true;
+    } else {
+      s.predicted = false;
+    }
+    s.hold = period;
+    s.sr = fr;
+    s.si = fi;
+    s.sn = s.n;
+    s.pending = false;
+    s.mu.reset();
+    return false;
+  }
+  if (s.hold > 0) {
+    if (s.n < s.sn + s.hold) return false;
+    s.hold = 0;
+    s.predicted = false;
+    s.pending = true;
+  }
+  if (s.pending || s.n >= s.chk) {
+    uint64_t np = next_pow2(s.n + 1);
+    s.chk = s.chk > np ? s.chk : np;
+    s.sr = fr;
+    s.si = fi;
+    s.sn = s.n;
+    s.pending = false;
+  }
+  return false;
+}
+
+// Start sample `slot` of the tile queue (8x4-sample tiles, row-major tiles). Returns
+// false when the slot holds no sample to iterate (outside the grid, masked, or settled
+// by the closed-form main-component test, whose result is written here).
+template <bool EXT, bool D, bool L>
+__device__ __forceinline__ int init(const Params &p, uint64_t slot, State<EXT> &s, Result &res) {
+  uint64_t tile = slot >> 5;
+  uint32_t w = (uint32_t)slot & 31u;
+  uint32_t tx = (uint32_t)(tile % p.tiles_x), ty = (uint32_t)(tile / p.tiles_x);
+  uint32_t i = tx * 8 + (w & 7u), jj = ty * 4 + (w >> 3);
+  if (i >= p.nx || jj >= p.rows) return 0;
+  uint32_t j = p.first_row + jj;
+  uint32_t idx = j * p.nx + i;
+  if (p.mask && !p.mask[idx]) return 0;
+  s.idx = idx;
+  double ux, uy;
+  if (p.offsets) {
+    double2 o = p.offsets[idx];
+    ux = o.x;
+    uy = o.y;
+  } else {  // view.rs:118-122
+    double x = (double)i + 0.5 - p.half_x;
+    double y = (double)j + 0.5 - p.half_y;
+    ux = p.cosr * x + p.sinr * y;
+    uy = p.sinr * x - p.cosr * y;
+  }
+  if (EXT) {  // grid.rs:709-723
+    s.ar = ux * p.h_m;
+    s.ai = uy * p.h_m;
+    s.offset_exp = p.h_e;
+  } else {
+    s.ar = ux * p.h;
+    s.ai = uy * p.h;
+    s.offset_exp = 0;
+    if (p.tier == 0 && in_main_components(p.c_re + s.ar, p.c_im + s.ai)) {  // sample.rs:187-189
+      res.kind = 1;
+      res.n = 0;
+      return 2;
+    }
+  }
+  s.xr = 0.0;
+  s.xi = 0.0;
+  s.delta_exp = EXT ? s.offset_exp : 0;
+  s.scale = EXT ? exp2i(s.delta_exp) : 1.0;
+  s.dc_r = s.ar;
+  s.dc_i = s.ai;
+  s.dr = 0.0;
+  s.di = 0.0;
+  s.derivative_exp = 0;
+  s.inverse = 1.0;
+  s.m = 0;
+  s.n = 0;
+  s.Zr = p.z0r;
+  s.Zi = p.z0i;
+  s.fr = p.z0r + 0.0;
+  s.fi = p.z0i + 0.0;
+  s.sr = 0.0;
+  s.si = 0.0;
+  s.chk = 16;
+  s.sn = EXT ? 0 : 8;
+  s.returns = 0;
+  s.pending = false;
+  s.mu.reset();
+  s.hold = 0;
+  s.predicted = false;
+  s.qr = 0.0;
+  s.qi = 0.0;
+  s.qstep = 0.0;
+  s.adc = L ? sqrt(s.ar * s.ar + s.ai * s.ai) : 0.0;
+  s.nucleus = p.nucleus;
+  s.ct.reset();
+  s.blocks = 0;
+  s.skipped = 0;
+  s.shift = 0.0;
+  return 1;
+}
+
+// Column encoder (store.rs:66-112, Bound absent) and raw state.
+__device__ __forceinline__ void put(const Params &p, uint32_t sample, const Result &r) {
+  const uint64_t idx = sample - p.out_base;
+  if (p.status) p.status[idx] = 1;
+  if (p.n_out) p.n_out[idx] = (uint32_t)(r.kind == 2 ? p.max_iter : r.n);
+  if (r.kind != 0) {
+    if (p.cls) p.cls[idx] = (uint8_t)(r.kind == 2 ? 2 : 1);
+    return;
+  }
+  if (p.cls) p.cls[idx] = 0;
+  if (p.z_out) p.z_out[idx] = make_double2(r.zr, r.zi);
+  if (p.dz_out) p.dz_out[idx] = make_double2(r.dr, r.di);
+  if (p.dexp_out) p.dexp_out[idx] = r.dexp;
+  double z2 = r.zr * r.zr + r.zi * r.zi;
+  double log2z = 0.5 * log2(z2);
+  if (p.nu) p.nu[idx] = (double)r.n + 1.0 - log2(log2z);
+  if (p.de) {  // store.rs:145-150
+    double lnz = log2z * LN_2;
+    double base = 2.0 * sqrt(z2) * lnz / (hypot(r.dr, r.di) * p.px_m);
+    int64_t k = -(r.dexp + p.px_e);
+    k = k < -4000 ? -4000 : (k > 4000 ? 4000 : k);
+    p.de[idx] = (float)(base * exp2i(k / 2) * exp2i(k - k / 2));
+  }
+  if (p.normal) {  // samples.rs:45-48 through view.rs:132-134
+    double re = r.zr * r.dr + r.zi * r.di, im = r.zi * r.dr - r.zr * r.di;
+    double x = p.cosr * re + p.sinr * im, y = p.sinr * re - p.cosr * im;
+    double t = atan2(y, x) * (65536.0 / TAU);
+    p.normal[idx] = (uint16_t)(int64_t)round(t);
+  }
+}
+
+template <bool EXT, bool D, bool L>
+__global__ void __launch_bounds__(128) perturb_kernel(Params p) {
+  const unsigned FULL = 0xffffffffu;
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned lt = (1u << lane) - 1u;
+  State<EXT> s;
+  Result res;
+  bool active = false, exhausted = false;
+  uint64_t t0 = p.deadline_ns ? globaltimer() : 0;
+  unsigned long long n_samples = 0, iters = 0, blocks = 0, skipped = 0, fallback = 0, closed = 0;
+  double shift = 0.0;
+  auto finish = [&](uint32_t idx, const Result &r, uint64_t nblocks, uint64_t nskipped, double sh) {
+    put(p, idx, r);
+    uint64_t spent = r.kind == 2 ? p.max_iter : r.n;
+    if (L) {
+      spent = spent - nskipped + nblocks;
+      blocks += nblocks;
+      skipped += nskipped;
+      bool cf = r.kind == 1 && r.n == 0;
+      closed += cf;
+      fallback += (nblocks == 0 && !cf);
+      shift = fmax(shift, sh);
+    }
+    iters += spent;
+    n_samples += 1;
+  };
+  for (;;) {
+    unsigned need = __ballot_sync(FULL, !active);
+    while (need && !exhausted) {
+      if (p.deadline_ns) {
+        uint64_t now = 0;
+        if (lane == 0) now = globaltimer();
+        now = __shfl_sync(FULL, now, 0);
+        if (now - t0 > p.deadline_ns) {
+          exhausted = true;
+          if (lane == 0) atomicExch(p.timed_out, 1u);
+          break;
+        }
+      }
+      unsigned long long base = 0;
+      int leader = __ffs((int)need) - 1;
+      if ((int)lane == leader) base = atomicAdd(p.queue, (unsigned long long)__popc(need));
+      base = __shfl_sync(FULL, base, leader);
+      if (base >= p.total) {
+        exhausted = true;
+        break;
+      }
+      if (!active) {
+        uint64_t slot = base + __popc(need & lt);
+        if (slot < p.total) {
+          int got = init<EXT, D, L>(p, slot, s, res);
+          if (got == 1) {
+            active = true;
+          } else if (got == 2) {
+            finish(s.idx, res, 0, 0, 0.0);
+          }
+        }
+      }
+      need = __ballot_sync(FULL, !active);
+    }
+    if (!__any_sync(FULL, active)) break;
+    if (active) {
+      if (step<EXT, D, L>(p, s, res)) {
+        finish(s.idx, res, s.blocks, s.skipped, s.shift);
+        active = false;
+      }
+    }
+  }
+  // warp reduction of the counters, one atomic per warp
+  for (int o = 16; o > 0; o >>= 1) {
+    n_samples += __shfl_down_sync(FULL, n_samples, o);
+    iters += __shfl_down_sync(FULL, iters, o);
+    blocks += __shfl_down_sync(FULL, blocks, o);
+    skipped += __shfl_down_sync(FULL, skipped, o);
+    fallback += __shfl_down_sync(FULL, fallback, o);
+    closed += __shfl_down_sync(FULL, closed, o);
+    shift = fmax(shift, __shfl_down_sync(FULL, shift, o));
+  }
+  if (lane == 0) {
+    atomicAdd(&p.counters->samples, n_samples);
+    atomicAdd(&p.counters->iterations, iters);
+    if (L) {
+      atomicAdd(&p.counters->blocks, blocks);
+      atomicAdd(&p.counters->skipped, skipped);
+      atomicAdd(&p.counters->fallback, fallback);
+      atomicAdd(&p.counters->closed, closed);
+      if (shift > 0.0 && !isnan(shift)) atomicMax(&p.counters->shift_bits, (unsigned long long)__double_as_longlong(shift));
+    }
+  }
+}
+
+}  // namespace fdk

@@ -1,0 +1,454 @@
+"""The `--gpu-perturb cuda` route: fractodactyl's sample API over the CUDA library.
+
+Mirrors the names, argument meaning and refusals of junovhs/fractodactyl's host side for
+this path: View / Params (crates/fd-samples/src/header.rs:14-27, crates/fd-kernel/src/
+grid.rs:17-38), Plane (view.rs:42-128), Reference (reference.rs), Bla (bla.rs), and the
+route entry points perturb_gpu::{enabled, render, render_bla} (crates/fd-cli/src/
+perturb_gpu/frame.rs:62-84), whose CUDA counterpart keeps every sample the device
+finishes (its results are the CPU kernel's) instead of admitting only guarded escapes.
+Frames the route declines raise Declined: the caller restarts them on the CPU from n = 0
+(frame.rs:357-368), as the reference's route does.
+"""
+import ctypes as C
+import dataclasses
+import os
+import sys
+import time
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import lib
+
+EPS = 2.0 ** -50          # exact-mode BLA tolerance (crates/fd-cli/src/orbit.rs:16)
+EPS_MAX = 2.0 ** -41      # largest eps whose blocks never cover a judged iterate (bla.rs:17)
+FILM_EPS = 2.0 ** -26     # film-mode tolerance (orbit.rs:22)
+MAX_LEN = 1 << 20         # reference.rs:16
+COLUMNS = ("class", "nu", "de", "normal")
+TIERS = {"f64": 0, "fx": 1, "fixed": 1, "scaled": 2}
+TIER_NAMES = {0: "F64", 1: "Fixed", 2: "Scaled"}
+
+
+class Declined(RuntimeError):
+    """The route does not take this frame; render it on the CPU from n = 0."""
+
+
+class RouteError(RuntimeError):
+    pass
+
+
+def enabled(value: Optional[str]) -> bool:
+    """perturb_gpu::enabled (frame.rs:62-68) with the `cuda` and `cuda-bla` routes added."""
+    v = "off" if value is None else value
+    if v == "off":
+        return False
+    if v in ("on", "bla", "cuda", "cuda-bla"):
+        return True
+    raise ValueError(f"--gpu-perturb: expected on, bla, cuda, cuda-bla or off, got {v!r}")
+
+
+@dataclasses.dataclass
+class View:
+    center_re: str
+    center_im: str
+    width: str
+    rotation: float = 0.0
+
+
+@dataclasses.dataclass
+class Params:
+    nx: int
+    ny: int
+    ss: int = 1
+    max_iter: int = 100_000
+    escape_radius: float = 1e10
+    columns: tuple = ("nu", "de", "normal")
+    threads: int = 0
+    tier: Optional[str] = None
+
+    def needs_derivative(self):
+        return "de" in self.columns or "normal" in self.columns
+
+
+@dataclasses.dataclass
+class Plane:
+    c_re: float
+    c_im: float
+    h_m: float
+    h_e: int
+    tier: int
+    bits: int
+    cos_rot: float
+    sin_rot: float
+
+    @classmethod
+    def new(cls, view: View, nx: int, ny: int) -> "Plane":
+        p = _lib.Plane()
+        if lib().fdh_plane_new(view.center_re.encode(), view.center_im.encode(), view.width.encode(),
+                               float(view.rotation), nx, ny, C.byref(p)) != 0:
+            raise ValueError(_lib.host_error())
+        return cls(p.c_re, p.c_im, p.h_m, p.h_e, p.tier, p.bits, p.cos_rot, p.sin_rot)
+
+    def kernel(self, tier: int) -> str:
+        """view.rs:90-96."""
+        return {0: "pert-f64/1", 1: f"pert-fx/1 bits={self.bits}", 2: f"pert-fx-scaled/1 bits={self.bits}"}[tier]
+
+    def allows(self, tier: int) -> bool:
+        return tier == 2 or (tier == 1 and self.tier != 2) or (tier == 0 and self.tier == 0)
+
+    def h(self) -> float:
+        return self.h_m * 2.0 ** self.h_e if self.h_e > -1074 else 0.0
+
+    def _c(self):
+        return _lib.Plane(self.c_re, self.c_im, self.h_m, self.h_e, self.tier, self.bits, self.cos_rot,
+                          self.sin_rot)
+
+
+@dataclasses.dataclass
+class Reference:
+    """Reference orbit Z_0..Z_{len-1} as f64 SoA, with its working precision in bits."""
+    re: np.ndarray
+    im: np.ndarray
+    bits: int = 53
+
+    def __len__(self):
+        return len(self.re)
+
+    @classmethod
+    def from_fixed(cls, center_re: str, center_im: str, bits: int, max_iter: int) -> "Reference":
+        cap = min(max_iter, MAX_LEN - 1) + 1
+        re, im = np.empty(cap), np.empty(cap)
+        n = lib().fdh_orbit_fixed(center_re.encode(), center_im.encode(), bits, max_iter, re.ctypes.data,
+                                  im.ctypes.data, cap)
+        if n < 0:
+            raise ValueError(_lib.host_error())
+        return cls(re[:n].copy(), im[:n].copy(), bits)
+
+    @classmethod
+    def new(cls, c_re: float, c_im: float, max_iter: int, escape_radius: float) -> "Reference":
+        cap = min(max_iter, MAX_LEN - 1) + 1
+        re, im = np.empty(cap), np.empty(cap)
+        n = lib().fdh_orbit_f64(c_re, c_im, max_iter, escape_radius, re.ctypes.data, im.ctypes.data, cap)
+        if n < 0:
+            raise ValueError(_lib.host_error())
+        return cls(re[:n].copy(), im[:n].copy(), 53)
+
+    def nucleus_period(self) -> Optional[int]:
+        re, im = np.ascontiguousarray(self.re), np.ascontiguousarray(self.im)
+        p = lib().fdh_nucleus_period(re.ctypes.data, im.ctypes.data, len(re))
+        return None if p < 0 else int(p)
+
+
+@dataclasses.dataclass
+class Bla:
+    """A BLA table in its export form: level-major [f64; 7] blocks (bla.rs:52-57)."""
+    blocks: np.ndarray  # (n, 7)
+    level_offsets: np.ndarray  # levels + 1
+    eps: float
+    dc_max: float
+    dc_exp: int
+    points: int
+
+    @property
+    def levels(self):
+        return len(self.level_offsets) - 1
+
+    @classmethod
+    def build_scaled(cls, r: Reference, eps: float, dc_max: float, dc_exp: int = 0, threads: int = 0) -> "Bla":
+        re, im = np.ascontiguousarray(r.re), np.ascontiguousarray(r.im)
+        levels, blocks = C.c_uint32(), C.c_uint64()
+        L = lib()
+        if L.fdh_bla_build(re.ctypes.data, im.ctypes.data, len(re), eps, dc_max, dc_exp, threads, None, None,
+                           C.byref(levels), C.byref(blocks)) != 0:
+            raise ValueError(_lib.host_error())
+        b = np.zeros((blocks.value, 7))
+        offs = np.zeros(levels.value + 1, np.uint64)
+        L.fdh_bla_build(re.ctypes.data, im.ctypes.data, len(re), eps, dc_max, dc_exp, threads, b.ctypes.data,
+                        offs.ctypes.data, C.byref(levels), C.byref(blocks))
+        return cls(b, offs, eps, dc_max, dc_exp, len(re))
+
+
+@dataclasses.dataclass
+class Header:
+    """crates/fd-samples/src/header.rs:29-45."""
+    columns: tuple
+    nx: int
+    ny: int
+    ss: int
+    max_iter: int
+    escape_radius: float
+    view: View
+    kernel: str
+    minor: int = 1
+
+
+@dataclasses.dataclass
+class Samples:
+    cls: np.ndarray
+    nu: Optional[np.ndarray] = None
+    de: Optional[np.ndarray] = None
+    normal: Optional[np.ndarray] = None
+    n: Optional[np.ndarray] = None
+    z: Optional[np.ndarray] = None
+    dz: Optional[np.ndarray] = None
+    dexp: Optional[np.ndarray] = None
+    status: Optional[np.ndarray] = None
+
+
+@dataclasses.dataclass
+class Stats:
+    reference_len: int = 0
+    reference_seconds: float = 0.0
+    iterations: int = 0
+
+
+@dataclasses.dataclass
+class BlaStats:
+    blocks: int = 0
+    skipped: int = 0
+    fallback_samples: int = 0
+    closed_form_samples: int = 0
+    shift_px: Optional[float] = None
+
+
+@dataclasses.dataclass
+class RouteReport:
+    """The counters frame.rs:350-353 prints, plus device time and launch count."""
+    device: str = ""
+    accepted: int = 0
+    fallback: int = 0
+    gpu_seconds: float = 0.0
+    kernel_ms: float = 0.0
+    launches: int = 0
+    table_seconds: float = 0.0
+    table_blocks: int = 0
+    total_seconds: float = 0.0
+
+    def line(self, st: Stats, bs: Optional[BlaStats]):
+        eff = st.iterations - (bs.blocks - bs.skipped if bs else 0)
+        extra = f" gpu_blocks={bs.blocks} gpu_skipped={bs.skipped}" if bs else ""
+        return (f"fd gpu-perturb: device={self.device!r} accepted={self.accepted} fallback={self.fallback} "
+                f"guard=0 unfinished={self.fallback} invalid=0 gpu_seconds={self.gpu_seconds:.6f} "
+                f"kernel_ms={self.kernel_ms:.3f} total_seconds={self.total_seconds:.6f} restart=zero"
+                f"{extra} effective_iterations={eff}")
+
+
+def _check(status, dev, what):
+    if status == _lib.DECLINED:
+        raise Declined(f"{what}: {lib().fdc_last_error(dev.h).decode()}")
+    if status != _lib.OK and status != _lib.TIMEOUT:
+        raise RouteError(f"{what}: {_lib.STATUS_NAMES.get(status, status)}: {lib().fdc_last_error(dev.h).decode()}")
+
+
+class Device:
+    """One fdc_ctx on one GPU (a context per thread; it owns one CUDA stream)."""
+
+    def __init__(self, index: int = 0):
+        self.h = C.c_void_p()
+        st = lib().fdc_open(index, C.byref(self.h))
+        if st != _lib.OK:
+            raise RouteError(f"fdc_open({index}): {_lib.STATUS_NAMES.get(st, st)}")
+        self.index = index
+        self._orbits = {}
+
+    def close(self):
+        if self.h:
+            lib().fdc_close(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, r: Reference, bla: Optional[Bla] = None) -> int:
+        re, im = np.ascontiguousarray(r.re), np.ascontiguousarray(r.im)
+        h = C.c_int32()
+        _check(lib().fdc_upload_orbit(self.h, re.ctypes.data, im.ctypes.data, len(re), r.bits, C.byref(h)), self,
+               "upload orbit")
+        if bla is not None:
+            b = np.ascontiguousarray(bla.blocks)
+            offs = np.ascontiguousarray(bla.level_offsets)
+            _check(lib().fdc_upload_bla(self.h, h.value, b.ctypes.data if len(b) else None,
+                                        offs.ctypes.data, bla.levels, bla.eps, bla.dc_max, bla.dc_exp), self,
+                   "upload BLA")
+        return h.value
+
+    def free(self, orbit: int):
+        lib().fdc_free_orbit(self.h, orbit)
+
+    def render_job(self, job: _lib.Job, raw=False, columns=COLUMNS, device_out=None):
+        """fdc_render into fresh host arrays (or caller device buffers)."""
+        n = job.nx * job.ny
+        out = _lib.Out()
+        arrays = {}
+        if device_out is not None:
+            for k, v in device_out.items():
+                setattr(out, k, v)
+        else:
+            want = {"cls": np.uint8, "status": np.uint8, "n": np.uint32}
+            if "nu" in columns:
+                want["nu"] = np.float64
+            if "de" in columns:
+                want["de"] = np.float32
+            if "normal" in columns:
+                want["normal"] = np.uint16
+            for k, dt in want.items():
+                arrays[k] = np.zeros(n, dt)
+            if raw:
+                arrays["z"] = np.zeros((n, 2))
+                arrays["dz"] = np.zeros((n, 2))
+                arrays["dexp"] = np.zeros(n, np.int64)
+            for k, a in arrays.items():
+                setattr(out, k, a.ctypes.data)
+        cnt = _lib.Counters()
+        st = lib().fdc_render(self.h, C.byref(job), C.byref(out), C.byref(cnt))
+        _check(st, self, "render")
+        return arrays, cnt, st
+
+
+def _setup(view: View, p: Params):
+    """grid.rs:779-799."""
+    if p.ss == 0 or p.nx % p.ss or p.ny % p.ss:
+        raise ValueError("grid must be a whole number of pixels")
+    plane = Plane.new(view, p.nx, p.ny)
+    tier = plane.tier if p.tier in (None, "auto") else TIERS[p.tier]
+    if not plane.allows(tier):
+        raise ValueError(f"{TIER_NAMES[tier]} tier is not valid at this depth (cheapest valid: "
+                         f"{TIER_NAMES[plane.tier]})")
+    return plane, tier
+
+
+def reference(view: View, p: Params):
+    """grid::reference (grid.rs:87-90, compute :802-815): the orbit and its precision."""
+    plane, tier = _setup(view, p)
+    if tier == 0:
+        return Reference.new(plane.c_re, plane.c_im, p.max_iter, p.escape_radius), 53
+    return Reference.from_fixed(view.center_re, view.center_im, plane.bits, p.max_iter), plane.bits
+
+
+def bla_dc_bound(view: View, p: Params):
+    """grid.rs:418-427."""
+    plane, tier = _setup(view, p)
+    dc, e = C.c_double(), C.c_int64()
+    lib().fdh_dc_bound(C.byref(plane._c()), tier, p.nx, p.ny, C.byref(dc), C.byref(e))
+    return dc.value, e.value
+
+
+_devices = {}
+
+
+def device(index: int = 0) -> Device:
+    d = _devices.get(index)
+    if d is None:
+        d = _devices[index] = Device(index)
+    return d
+
+
+def make_job(plane: Plane, tier: int, p: Params, orbit: int, nucleus: Optional[int], flags: int) -> _lib.Job:
+    j = _lib.Job()
+    j.orbit = orbit
+    j.tier = tier
+    j.nx, j.ny, j.ss = p.nx, p.ny, p.ss
+    j.flags = flags
+    j.c_re, j.c_im = plane.c_re, plane.c_im
+    j.h_m, j.h_e = plane.h_m, plane.h_e
+    j.cos_rot, j.sin_rot = plane.cos_rot, plane.sin_rot
+    j.max_iter = p.max_iter
+    j.escape_radius = p.escape_radius
+    j.nucleus_period = -1 if nucleus is None else nucleus
+    return j
+
+
+def render_with(view: View, p: Params, orbit=None, bla: Optional[Bla] = None, dev: Optional[Device] = None,
+                raw=False, shift=True, report: Optional[RouteReport] = None, quiet=True):
+    """fd_kernel::render_with / render_bla (grid.rs:106-208) on the CUDA route.
+
+    Returns (Header, Samples, Stats, BlaStats or None). Refusals are the reference's
+    (grid.rs:378-413, :461-475); Bound/Stripe columns are declined (frame.rs:129-144).
+    """
+    started = time.perf_counter()
+    if "bound" in p.columns or "stripe" in p.columns:
+        raise Declined("frame declined (bound/stripe); CPU restart from zero")
+    plane, tier = _setup(view, p)
+    need = 53 if tier == 0 else plane.bits
+    t = time.perf_counter()
+    if orbit is None:
+        r, bits = reference(view, p)
+    else:
+        r, bits = orbit
+        if bits != need and (tier == 0 or bits < need):
+            at_least = "" if tier == 0 else "at least "
+            raise ValueError(f"supplied reference has {bits} bits; this view needs {at_least}{need}")
+        if len(r) == 0 or len(r.re) != len(r.im) or r.re[0] != 0.0 or r.im[0] != 0.0:
+            raise ValueError("supplied reference orbit must start at Z_0 = 0 with equal re/im lengths")
+        plane.bits = bits
+    r.bits = bits
+    reference_seconds = time.perf_counter() - t
+    if bla is not None and bla.points != len(r):
+        raise ValueError(f"BLA table covers a {bla.points}-point orbit, not this {len(r)}-point one")
+    dev = dev or device(0)
+    h = dev.upload(r, bla)
+    try:
+        flags = (_lib.DERIVATIVE if p.needs_derivative() else 0) | (_lib.BLA if bla is not None else 0)
+        if bla is not None and shift and p.needs_derivative():
+            flags |= _lib.SHIFT
+        job = make_job(plane, tier, p, h, r.nucleus_period(), flags)
+        g = time.perf_counter()
+        arrays, cnt, status = dev.render_job(job, raw=raw, columns=p.columns)
+        gpu_seconds = time.perf_counter() - g
+    finally:
+        dev.free(h)
+    kernel = plane.kernel(tier) + (" bla/1" if bla is not None else "") + " gpu-perturb-cuda/1"
+    cols = ("class",) + tuple(c for c in ("nu", "de", "normal") if c in p.columns)
+    header = Header(cols, p.nx, p.ny, p.ss, p.max_iter, p.escape_radius, view, kernel)
+    s = Samples(cls=arrays["cls"], nu=arrays.get("nu"), de=arrays.get("de"), normal=arrays.get("normal"),
+                n=arrays.get("n"), z=arrays.get("z"), dz=arrays.get("dz"), dexp=arrays.get("dexp"),
+                status=arrays.get("status"))
+    stats = Stats(len(r), reference_seconds, int(cnt.iterations))
+    bstats = None
+    if bla is not None:
+        bstats = BlaStats(int(cnt.blocks), int(cnt.skipped), int(cnt.fallback_samples),
+                          int(cnt.closed_form_samples),
+                          cnt.shift / (plane.h() * p.ss) if (flags & _lib.SHIFT) else None)
+    rep = report if report is not None else RouteReport()
+    rep.device = f"cuda:{dev.index}"
+    rep.accepted = int(cnt.samples)
+    rep.fallback = p.nx * p.ny - int(cnt.samples)
+    rep.gpu_seconds = gpu_seconds
+    rep.kernel_ms = cnt.kernel_ms
+    rep.launches = cnt.launches
+    rep.table_blocks = 0 if bla is None else len(bla.blocks)
+    rep.total_seconds = time.perf_counter() - started
+    if not quiet:
+        print(rep.line(stats, bstats), file=sys.stderr)
+    if status == _lib.TIMEOUT:
+        raise Declined(f"deadline passed with {rep.fallback} samples unfinished; CPU restart from zero")
+    return header, s, stats, bstats
+
+
+def render(view: View, p: Params, orbit=None, **kw):
+    """perturb_gpu::render (frame.rs:70-76) on the CUDA route: plain perturbation."""
+    h, s, st, _ = render_with(view, p, orbit, None, **kw)
+    return h, s, st
+
+
+def render_bla(view: View, p: Params, orbit=None, eps: float = EPS, **kw):
+    """perturb_gpu::render_bla (frame.rs:78-84) on the CUDA route: the reference orbit
+    (computed unless supplied) and a BLA table built over it by the CPU builder for the
+    view's largest |dc| (control.rs:344-360), then the BLA kernel."""
+    if orbit is None:
+        orbit = reference(view, p)
+    if p.escape_radius < 4.0:
+        raise ValueError("escape radius is below 4: BLA blocks may only skip iterates with |z| <= 2 (1 + 2 eps)")
+    dc, e = bla_dc_bound(view, p)
+    t = time.perf_counter()
+    table = Bla.build_scaled(orbit[0], eps, dc, e, p.threads)
+    report = kw.pop("report", None) or RouteReport()
+    report.table_seconds = time.perf_counter() - t
+    if table.levels == 0:
+        h, s, st, _ = render_with(view, p, orbit, None, report=report, **kw)
+        return h, s, st, None
+    return render_with(view, p, orbit, table, report=report, **kw)

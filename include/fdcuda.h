@@ -1,0 +1,126 @@
+/*
+ * fdcuda.h - C ABI of the B200 (sm_100a) perturbation route for fractodactyl.
+ *
+ * The route replaces the WGSL dispatch of junovhs/fractodactyl's existing GPU route
+ * (crates/fd-cli/src/perturb_gpu/frame.rs:119-355, render_inner) with hand-written CUDA.
+ * The caller keeps the reference's host side: it owns the Reference orbit
+ * (crates/fd-kernel/src/reference.rs:7-10), the BLA table built by the CPU builder
+ * (crates/fd-kernel/src/bla.rs:161-181) and the Samples columns
+ * (crates/fd-samples/src/samples.rs:7-20). Every entry point takes plain pointers and
+ * sizes, copies what it needs into device memory owned by the context, writes into
+ * caller-owned buffers, and keeps no host pointer after it returns. No entry point
+ * aborts or throws: failures come back as an fdc_status and fdc_last_error().
+ *
+ * Threading: a context is used by one thread at a time; it owns one CUDA stream.
+ */
+#ifndef FDCUDA_H
+#define FDCUDA_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FDC_ABI_VERSION 1
+
+/* Status codes. On anything but FDC_OK the caller restarts the frame on the CPU from
+ * n = 0, as restart_after_attempt does (frame.rs:357-368). */
+typedef enum {
+  FDC_OK = 0,
+  FDC_DECLINED = 1,     /* the route does not take this job (caller renders on CPU) */
+  FDC_INVALID = 2,      /* malformed input (sizes, handles, non-finite values) */
+  FDC_DEVICE_ERROR = 3, /* a CUDA call failed; the context should be closed */
+  FDC_TIMEOUT = 4,      /* the job's deadline passed; samples not finished keep status 0 */
+  FDC_NO_DEVICE = 5     /* no usable sm_100 device */
+} fdc_status;
+
+/* Tiers (crates/fd-kernel/src/view.rs:7-14). */
+enum { FDC_TIER_F64 = 0, FDC_TIER_FIXED = 1, FDC_TIER_SCALED = 2 };
+
+/* Job flags. */
+enum {
+  FDC_DERIVATIVE = 1u << 0, /* track dz/dc (columns de/normal; sample.rs "D") */
+  FDC_BLA = 1u << 1,        /* apply the uploaded BLA table (sample.rs "L") */
+  FDC_SHIFT = 1u << 2,      /* accumulate the BLA first-order shift estimate (BlaStats.shift_px) */
+  FDC_F32 = 1u << 3,        /* precision form: FP32-mantissa floatexp deltas (not bit-exact) */
+  FDC_DEVICE_OUT = 1u << 4  /* fdc_out pointers are device pointers (no host copies) */
+};
+
+typedef struct fdc_ctx fdc_ctx;
+
+/* One frame (or a sub-range of it). Geometry follows Plane (view.rs:42-128): sample
+ * (i, j) has unit offset ux = cos x + sin y, uy = sin x - cos y with x = i + 0.5 - nx/2,
+ * y = j + 0.5 - ny/2, and dc = (ux, uy) h_m 2^h_e. */
+typedef struct {
+  int32_t orbit;          /* handle from fdc_upload_orbit */
+  int32_t tier;           /* FDC_TIER_* (the caller's resolved tier) */
+  uint32_t nx, ny, ss;    /* sample grid; ss only scales the DE pixel */
+  uint32_t flags;         /* FDC_* */
+  double c_re, c_im;      /* centre rounded to f64 (F64 tier closed-form test) */
+  double h_m;             /* spacing mantissa, 1 <= h_m < 2 */
+  int64_t h_e;            /* spacing exponent */
+  double cos_rot, sin_rot;
+  uint64_t max_iter;      /* < 2^32 */
+  double escape_radius;
+  int64_t nucleus_period; /* Reference::nucleus_period (reference.rs:102-120); -1 = None */
+  const uint8_t *mask;    /* optional, nx*ny host bytes: render only samples with mask != 0 */
+  const double *offsets;  /* optional, 2*nx*ny host doubles: per-sample (ux, uy) instead of the grid */
+  uint32_t first_row, rows; /* render rows [first_row, first_row + rows); rows 0 = all */
+  double deadline_ms;     /* stop taking new samples after this long; 0 = none */
+} fdc_job;
+
+/* Caller-owned outputs, nx*ny entries each (only rows rendered are written); any may be
+ * NULL. With FDC_DEVICE_OUT they are device pointers. */
+typedef struct {
+  uint8_t *cls;      /* Class byte: Kind | Evidence << 2 (crates/fd-samples/src/class.rs) */
+  uint32_t *n;       /* iterates (Escaped/Interior), max_iter for Unresolved */
+  double *nu;        /* n + 1 - log2(log2 |z|) (store.rs:97-99), escaped only */
+  float *de;         /* distance estimate in output pixels (store.rs:141-150) */
+  uint16_t *normal;  /* screen normal angle, turns * 65536 (store.rs:107-111) */
+  double *z;         /* 2 per sample: z at escape (raw state for the host encoder) */
+  double *dz;        /* 2 per sample: dz/dc mantissa */
+  int64_t *dexp;     /* dz/dc exponent */
+  uint8_t *status;   /* 1 = finished, 0 = not computed (mask, deadline) */
+} fdc_out;
+
+/* Work counters of one fdc_render (Stats grid.rs:41-49 + BlaStats grid.rs:53-70). */
+typedef struct {
+  uint64_t samples;         /* samples finished */
+  uint64_t iterations;      /* iterates, each applied block counted once */
+  uint64_t blocks, skipped; /* BLA blocks applied and steps they replaced */
+  uint64_t fallback_samples, closed_form_samples;
+  double shift;             /* largest shift estimate in c units (FDC_SHIFT) */
+  double kernel_ms;         /* device time of the render kernel(s) */
+  uint32_t launches;        /* kernels launched */
+} fdc_counters;
+
+/* Library / device. */
+int fdc_abi_version(void);
+fdc_status fdc_open(int device, fdc_ctx **out);
+void fdc_close(fdc_ctx *ctx);
+const char *fdc_last_error(const fdc_ctx *ctx);
+
+/* Upload a reference orbit Z_0..Z_{len-1} (SoA f64 as Reference keeps it) with the
+ * precision it was computed at (53 = f64 tier). Replaces the wgpu orbit packing of
+ * frame.rs:172-188. Z_0 must be 0; 2 <= len <= 2^20 (reference.rs:16). */
+fdc_status fdc_upload_orbit(fdc_ctx *ctx, const double *re, const double *im, uint64_t len, uint32_t bits,
+                            int32_t *orbit);
+fdc_status fdc_free_orbit(fdc_ctx *ctx, int32_t orbit);
+
+/* Upload the BLA table built over that orbit (Bla, bla.rs:137-151) in its export form:
+ * level-major blocks of [f64; 7] = a.re, a.im, b.re, b.im, r, alpha, beta (bla.rs:52-57,
+ * the fd-atlas chunk layout), level i (j = i + 1) at blocks7[7 * level_offsets[i]...],
+ * (points - 2) >> (i + 1) blocks each. Replaces pack_bla (frame.rs:86-117). */
+fdc_status fdc_upload_bla(fdc_ctx *ctx, int32_t orbit, const double *blocks7, const uint64_t *level_offsets,
+                          uint32_t levels, double eps, double dc_max, int64_t dc_exp);
+
+/* Render a job (replaces dispatch_batched, frame.rs:242-260, and the readback checks,
+ * :271-286). Results are those of the CPU kernel (sample.rs:170-581) for the plain form:
+ * class and n bit-exact, z and dz bit-exact, nu/de/normal within CUDA libm's ulps. */
+fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counters *counters);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

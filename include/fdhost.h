@@ -1,0 +1,71 @@
+/*
+ * fdhost.h - host-side set-up of the B200 perturbation route, in C++.
+ *
+ * These are the parts of junovhs/fractodactyl's path that stay on the CPU because they
+ * are serial or cheap (reference orbit in fixed point, the view's plane, the BLA table
+ * built by the CPU builder, the nucleus gate), offered behind a C ABI for callers that
+ * do not bring their own (the reference's Rust side computes them itself and calls only
+ * fdcuda.h). Results equal the reference's bit for bit: orbit points are exact integer
+ * arithmetic rounded by the same rule, BLA blocks use the same operation order.
+ * Errors: negative return, message in fdh_last_error() (per thread).
+ */
+#ifndef FDHOST_H
+#define FDHOST_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+const char *fdh_last_error(void);
+
+/* Plane::new (crates/fd-kernel/src/view.rs:42-87): sample spacing h = h_m 2^h_e, the
+ * cheapest valid tier (0 F64, 1 Fixed, 2 Scaled), fixed-point bits, centre as f64,
+ * rotation cos/sin. */
+typedef struct {
+  double c_re, c_im, h_m;
+  int64_t h_e;
+  int32_t tier;
+  uint64_t bits;
+  double cos_rot, sin_rot;
+} fdh_plane;
+int fdh_plane_new(const char *center_re, const char *center_im, const char *width, double rotation, uint32_t nx,
+                  uint32_t ny, fdh_plane *out);
+
+/* Reference orbits (crates/fd-kernel/src/reference.rs). The orbit is written into
+ * caller arrays of capacity cap (>= min(max_iter, 2^20 - 1) + 1); returns its length.
+ *   fdh_orbit_fixed: Reference::from_fixed over fd_fixed::orbit (reference.rs:85-96,
+ *                    crates/fd-fixed/src/orbit.rs:14-43) at the exact decimal centre.
+ *   fdh_orbit_f64:   Reference::new (reference.rs:21-48). */
+int64_t fdh_orbit_fixed(const char *center_re, const char *center_im, uint64_t bits, uint64_t max_iter, double *re,
+                        double *im, uint64_t cap);
+int64_t fdh_orbit_f64(double c_re, double c_im, uint64_t max_iter, double escape_radius, double *re, double *im,
+                      uint64_t cap);
+
+/* Reference::nucleus_period (reference.rs:102-120); -1 for None. */
+int64_t fdh_nucleus_period(const double *re, const double *im, uint64_t len);
+
+/* Bla::build_scaled (crates/fd-kernel/src/bla.rs:161-181) over an orbit, in the export
+ * layout fdc_upload_bla takes: level-major [f64; 7] blocks. First call with blocks7 =
+ * NULL to learn the level count and block count; level_offsets has levels + 1 entries.
+ * threads <= 0: all cores. */
+int fdh_bla_build(const double *re, const double *im, uint64_t len, double eps, double dc_max, int64_t dc_exp,
+                  int threads, double *blocks7, uint64_t *level_offsets, uint32_t *levels, uint64_t *blocks);
+
+/* grid.rs:418-444: bound m 2^e on |dc| over a view's samples for a tier. */
+void fdh_dc_bound(const fdh_plane *plane, int32_t tier, uint32_t nx, uint32_t ny, double *dc, int64_t *e);
+
+/* Nucleus recipe of the benchmark locations (no reference API; after
+ * tools/research/twolevel/ref.py:46-67 and crates/fd-cli/src/zone_build.rs:215-231):
+ * the ball period of the disc of radius 10^log10_radius around (start_re, start_im)
+ * (first p with |z_p| < r |dz_p|, up to max_period), then Newton on z_p(c) = 0 at `bits`
+ * fixed-point bits with steps clamped to r/4. Writes the nucleus as decimal strings
+ * (caller buffers of cap bytes) and its period; returns 0 on convergence. */
+int fdh_nucleus(const char *start_re, const char *start_im, double log10_radius, uint64_t max_period, uint64_t bits,
+                char *re_out, char *im_out, size_t cap, uint64_t *period);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

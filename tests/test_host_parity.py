@@ -1,0 +1,132 @@
+"""CPU tests of the route's C++ host side against the oracle, and of the C ABI's surface.
+
+The host set-up (decimal centres, fixed-point orbit, plane, BLA builder, nucleus gate)
+must equal the reference's bit for bit; the oracle stands in for the reference here.
+No test in this file touches a GPU.
+"""
+import ctypes as C
+import json
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import fdref
+import fractodactyl_b200 as fd
+from fractodactyl_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+KATS = json.load(open(os.path.join(ROOT, "tests", "golden", "kats.json")))
+
+
+def declared(header):
+    text = open(os.path.join(ROOT, "include", header)).read()
+    return sorted(set(re.findall(r"\b(fd[ch]_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True, check=True)
+    exported = set(line.split()[-1] for line in out.stdout.splitlines())
+    want = declared("fdcuda.h") + declared("fdhost.h")
+    assert want and set(want) <= exported, set(want) - exported
+    assert set(want) == set(_lib.FDC_SYMBOLS + _lib.FDH_SYMBOLS)
+
+
+def test_library_loads_and_reports_no_device_without_a_gpu():
+    L = _lib.lib()
+    assert L.fdc_abi_version() == 1
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    h = C.c_void_p()
+    assert L.fdc_open(0, C.byref(h)) == _lib.NO_DEVICE and not h
+
+
+VIEWS = [("-0.7453", "0.1127", "0.0065", 0.3), ("0", "1", "1e-20", 0.0), ("0", "1", "1e-300", 0.5),
+         ("0", "1", "1e-1000", 0.0), ("0.25", "0", "1e-3", 0.0), ("-2", "0", "1e-200", 0.0),
+         ("3e-298", "1." + "0" * 300 + "7", "1e-300", 0.0), ("-0.7436438870371587", "0.1318259042053120", "1e-12", 0.0)]
+
+
+@pytest.mark.parametrize("re_,im_,width,rot", VIEWS)
+def test_plane_equals_reference(re_, im_, width, rot):
+    a = fdref.plane(fdref.make_job(re_, im_, width, 480, 270, 100, rotation=rot))
+    b = fd.Plane.new(fd.View(re_, im_, width, rot), 480, 270)
+    assert (a["h_m"], a["h_e"], a["tier"], a["bits"], a["c_re"], a["c_im"]) == \
+        (b.h_m, b.h_e, b.tier, b.bits, b.c_re, b.c_im)
+
+
+@pytest.mark.parametrize("bad", ["", ".", "1e", "--1", "1.2.3", "0x10", "abc"])
+def test_plane_refuses_malformed_decimals(bad):
+    with pytest.raises(ValueError):
+        fd.Plane.new(fd.View(bad, "0", "1"), 8, 8)
+    with pytest.raises(ValueError):
+        fd.Plane.new(fd.View("0", "0", bad), 8, 8)
+
+
+@pytest.mark.parametrize("bits", [128, 177, 218, 471, 1130, 3456])
+def test_fixed_orbit_bit_exact(bits):
+    re_, im_ = KATS["v0"]["re"], KATS["v0"]["im"]
+    a = fdref.Ref.fixed(re_, im_, bits, 3000)
+    b = fd.Reference.from_fixed(re_, im_, bits, 3000)
+    ar, ai = a.arrays_()
+    assert len(b) == len(a)
+    assert np.array_equal(ar.view(np.uint64), b.re.view(np.uint64))
+    assert np.array_equal(ai.view(np.uint64), b.im.view(np.uint64))
+
+
+def test_fixed_orbit_escaping_and_rung():
+    rung = KATS["rung_7676"]
+    for (re_, im_, bits, n) in [("1", "1", 128, 100), ("-0.75", "0.1", 256, 5000),
+                                (rung["re"], rung["im"], 3456, 4000)]:
+        a = fdref.Ref.fixed(re_, im_, bits, n)
+        b = fd.Reference.from_fixed(re_, im_, bits, n)
+        ar, ai = a.arrays_()
+        assert np.array_equal(ar, b.re) and np.array_equal(ai, b.im)
+        assert a.nucleus_period() == b.nucleus_period()
+
+
+def test_f64_orbit_and_nucleus_gate():
+    for c in [(-0.7487, 0.0789), (0.2501, 0.0), (-1.7548776662466927, 0.0), (0.0, 1.0)]:
+        a = fdref.Ref.f64(c[0], c[1], 100_000, 1e10)
+        b = fd.Reference.new(c[0], c[1], 100_000, 1e10)
+        ar, ai = a.arrays_()
+        assert np.array_equal(ar, b.re) and np.array_equal(ai, b.im)
+        assert a.nucleus_period() == b.nucleus_period()
+
+
+@pytest.mark.parametrize("eps,dc,e", [(2.0 ** -50, 1e-25, 0), (2.0 ** -41, 2e-17, 0), (2.0 ** -50, 1.3, -1000),
+                                      (2.0 ** -26, 1e-30, 0)])
+def test_bla_table_bit_exact(eps, dc, e):
+    a = fdref.Ref.f64(-0.743643887037158, 0.131825904205312, 20_000, 1e10)
+    re_, im_ = a.arrays_()
+    ta = fdref.Bla(a, eps, dc, e)
+    tb = fd.Bla.build_scaled(fd.Reference(re_, im_, 53), eps, dc, e, threads=4)
+    ba, oa = ta.export()
+    assert np.array_equal(oa, tb.level_offsets)
+    assert np.array_equal(ba.view(np.uint64), tb.blocks.view(np.uint64))
+
+
+def test_bla_refuses_bad_eps():
+    r = fd.Reference.new(-0.7453, 0.1127, 2000, 1e10)
+    with pytest.raises(ValueError):
+        fd.Bla.build_scaled(r, 2.0 * 2.0 ** -24, 1e-20)
+    with pytest.raises(ValueError):
+        fd.Bla.build_scaled(r, 2.0 ** -50, float("inf"))
+
+
+def test_dc_bound_equals_reference():
+    for (re_, im_, width) in [("-0.7453", "0.1127", "0.0065"), ("0", "1", "1e-300")]:
+        job = fdref.make_job(re_, im_, width, 32, 32, 100)
+        assert fdref.bla_dc_bound(job) == fd.bla_dc_bound(fd.View(re_, im_, width), fd.Params(32, 32))
+
+
+def test_route_flag_and_declines():
+    assert fd.enabled(None) is False and fd.enabled("cuda") and fd.enabled("cuda-bla") and fd.enabled("bla")
+    with pytest.raises(ValueError):
+        fd.enabled("fast")
+    with pytest.raises(fd.Declined):
+        fd.render(fd.View("0", "1", "1e-3"), fd.Params(8, 8, columns=("nu", "bound")))
+    with pytest.raises(ValueError):
+        fd.route._setup(fd.View("0", "1", "1e-300"), fd.Params(8, 8, tier="f64"))
