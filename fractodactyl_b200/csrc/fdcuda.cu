@@ -263,6 +263,9 @@ fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counte
   uint32_t first = j.first_row, rows = j.rows ? j.rows : j.ny - j.first_row;
   if (first >= j.ny || rows > j.ny - first) return fail(ctx, FDC_INVALID, "row range outside the grid");
   const bool ext = j.tier == FDC_TIER_SCALED;
+  // The scaled tier's exact-range step from Z_0 continues at Z_1 (sample.rs:430-447),
+  // which needs a next point after it.
+  if (ext && o.len < 3) return fail(ctx, FDC_INVALID, "the scaled tier needs an orbit of at least 3 points");
   const bool bla = (j.flags & FDC_BLA) != 0;
   const bool deriv = (j.flags & FDC_DERIVATIVE) != 0;
   double h = j.h_m * fdroute::exp2i(j.h_e);

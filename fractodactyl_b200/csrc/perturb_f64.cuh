@@ -402,11 +402,11 @@ __device__ __forceinline__ int init(const Params &p, uint64_t slot, State<EXT> &
   if (i >= p.nx || jj >= p.rows) return 0;
   uint32_t j = p.first_row + jj;
   uint32_t idx = j * p.nx + i;
-  if (p.mask && !p.mask[idx]) return 0;
+  if (p.mask && !p.mask[idx - p.out_base]) return 0;  // inputs hold the rendered rows only
   s.idx = idx;
   double ux, uy;
   if (p.offsets) {
-    double2 o = p.offsets[idx];
+    double2 o = p.offsets[idx - p.out_base];
     ux = o.x;
     uy = o.y;
   } else {  // view.rs:118-122
