@@ -43,8 +43,9 @@ struct Columns {
 };
 
 // store.rs:66-112 with the Bound column absent (class evidence Heuristic).
-static void put(const Plane &pl, uint32_t ss, uint32_t cols, const Outcome &o, size_t idx, Columns &c) {
-  if (c.n) c.n[idx] = o.n;
+static void put(const Plane &pl, uint32_t ss, uint32_t cols, const Outcome &o, size_t idx, Columns &c,
+                uint64_t max_iter = 0) {
+  if (c.n) c.n[idx] = o.iterations(max_iter);  // Outcome::iterations (sample.rs:45-50)
   if (c.z) {
     c.z[2 * idx] = o.zr;
     c.z[2 * idx + 1] = o.zi;
@@ -180,7 +181,7 @@ static std::string run(const View &v, const Params &p, const Reference *supplied
           local.shift = std::max(local.shift, skip.shift);
         }
         local.iterations += spent;
-        put(plane, p.ss, p.columns, o, (size_t)j * p.nx + i, cols);
+        put(plane, p.ss, p.columns, o, (size_t)j * p.nx + i, cols, p.max_iter);
       }
     }
     std::lock_guard<std::mutex> g(mu);
