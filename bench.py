@@ -1,0 +1,332 @@
+"""Benchmark of the perturbation hot path on B200: effective pixel-iterations per second.
+
+One step = one full frame of the benchmark configuration (default: config 2, the seeded
+1e-100 nucleus frame, 1920x1080, 1,000,000 iterations, BLA from the CPU builder, floatexp
+deltas) rendered by the CUDA route. Effective pixel-iterations count the steps BLA blocks
+skipped: iterations - blocks + skipped (crates/fd-cli/src/render.rs:182 of the reference).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config 2|1]
+
+value: device-resident inputs (orbit + BLA table uploaded once, outputs in device
+memory), time = CUDA events around each frame's kernel on the route's stream, L2 flushed
+between frames. e2e: the public API call a user makes with host buffers (fdc_upload_orbit,
+fdc_upload_bla, fdc_render into host arrays), every step including its host<->device
+copies, wall clock. N > 1: every rank renders its own copy of the frame (weak scaling),
+time = max over ranks. --impl reference: the reference CPU kernel (this repo's C++
+restatement of it, oracle/) on the host cores over a bounded sample of the frame's rows.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "effective pixel-iter/s on 1 B200: FP32-floatexp vs FP64 plain at ≥99.9% count match"
+UNIT = "pixel-iter/s"
+
+# Algorithmic FP64 operations (multiplies, adds, subtracts, compares) per unit, counted from
+# the reference formulas (sample.rs:266-575, number.rs:92-124).
+FLOPS_PLAIN = {(False, True): 40, (False, False): 31, (True, True): 47, (True, False): 38}
+FLOPS_BLOCK = {True: 37, False: 27}
+OUT_BYTES = {"cls": 1, "n": 4, "nu": 8, "de": 4, "normal": 2, "status": 1}
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def frame_for(args):
+    from fractodactyl_b200 import locations
+    if args.config == 1:
+        return locations.config1()
+    return locations.config2(seed=args.seed)
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm = [float(r[1]) for r in rows if len(r) > 8 and r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) > 8 and r[2].strip().replace(".", "").isdigit()]
+        reasons = set()
+        for r in rows:
+            if len(r) < 9:
+                continue
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"),
+                               r[5:9]):
+                if v.strip() == "Active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def allmax(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def reference_arm(args, fr):
+    """The reference CPU kernel on the host cores over a bounded sample of the frame's rows."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import fdref
+    cores = os.cpu_count() or 1
+    p, v = fr.params, fr.view
+    cols = fdref.COL_NU * ("nu" in p.columns) | fdref.COL_DE * ("de" in p.columns) | \
+        fdref.COL_NORMAL * ("normal" in p.columns)
+    job = fdref.make_job(v.center_re, v.center_im, v.width, p.nx, p.ny, p.max_iter, rotation=v.rotation,
+                         escape_radius=p.escape_radius, columns=cols, threads=cores, tier=p.tier)
+    t = time.perf_counter()
+    ref = fdref.Ref.for_job(job)
+    bla = None
+    if fr.bla_eps is not None:
+        dc, e = fdref.bla_dc_bound(job)
+        bla = fdref.Bla(ref, fr.bla_eps, dc, e)
+    setup = time.perf_counter() - t
+
+    def sample(step):
+        job.row_first, job.row_step = (p.ny // 2) % step, step
+        t0 = time.perf_counter()
+        out = fdref.render(job, ref, bla)
+        dt = time.perf_counter() - t0
+        s = out["stats"]
+        return s["iterations"] - s["blocks"] + s["skipped"], dt, len(range(job.row_first, p.ny, step)) * p.nx
+
+    step = max(1, p.ny // 8)
+    eff, dt, n = sample(step)
+    target = min(args.cpu_seconds, 150.0 / max(1, args.steps))
+    if dt > 0:
+        step = max(1, min(p.ny, int(step * dt / target))) if dt < target else step
+    return fdref, job, ref, bla, sample, step, setup, cores
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    fr = frame_for(args)
+    fdref, job, ref, bla, sample, step, setup, cores = reference_arm(args, fr)
+    for _ in range(args.warmup):
+        pass  # the CPU kernel has no warm state worth priming; warm-up steps are not repeated work
+    effs, times, n = 0, 0.0, 0
+    for _ in range(args.steps):
+        e, dt, n = sample(step)
+        effs += e
+        times += dt
+    value = effs / times
+    rows = len(range(job.row_first, fr.params.ny, step))
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * times / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded location)", "impl": "reference",
+            "config": {"workload": fr.name, "nx": fr.params.nx, "ny": fr.params.ny,
+                       "max_iter": fr.params.max_iter, "bla_eps": fr.bla_eps, "tier": fr.params.tier or "auto",
+                       "period": fr.period, "sample_rows": rows},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{rows} of {fr.params.ny} rows (every {step}th) of the frame per step; "
+                                       f"orbit + BLA set-up {setup:.2f} s excluded"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import ctypes as C
+
+    import torch
+
+    import fractodactyl_b200 as fd
+    from fractodactyl_b200 import _lib
+
+    rank, world, local = dist_init(args.gpus)
+    fr = frame_for(args)
+    view, p = fr.view, fr.params
+    plane, tier = fd.route._setup(view, p)
+    t = time.perf_counter()
+    r, bits = fd.reference(view, p)
+    r.bits = bits
+    orbit_s = time.perf_counter() - t
+    bla = None
+    t = time.perf_counter()
+    if fr.bla_eps is not None:
+        dc, e = fd.bla_dc_bound(view, p)
+        bla = fd.Bla.build_scaled(r, fr.bla_eps, dc, e)
+        if bla.levels == 0:
+            bla = None
+    bla_s = time.perf_counter() - t
+    dev = fd.Device(local)
+    handle = dev.upload(r, bla)
+    deriv = p.needs_derivative()
+    flags = (_lib.DERIVATIVE if deriv else 0) | (_lib.BLA if bla is not None else 0)
+    nuc = r.nucleus_period()
+    n = p.nx * p.ny
+    cols = ["cls", "n", "status"] + [c for c in ("nu", "de", "normal") if c in p.columns]
+    dt = {"cls": torch.uint8, "n": torch.int32, "status": torch.uint8, "nu": torch.float64, "de": torch.float32,
+          "normal": torch.int16}
+    bufs = {c: torch.empty(n, dtype=dt[c], device=f"cuda:{local}") for c in cols}
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    job = fd.route.make_job(plane, tier, p, handle, nuc, flags | _lib.DEVICE_OUT)
+
+    def device_step():
+        arrays, cnt, st = dev.render_job(job, device_out={c: bufs[c].data_ptr() for c in cols})
+        return cnt
+
+    ext = tier == 2
+    totals = dict(it=0, blocks=0, skipped=0, ms=0.0, launches=0)
+    for _ in range(args.warmup):
+        device_step()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    for _ in range(args.steps):
+        flush.zero_()  # L2 flush between frames (outside the kernel's events)
+        torch.cuda.synchronize()  # the route's stream does not wait on torch's
+        cnt = device_step()
+        totals["it"] += cnt.iterations
+        totals["blocks"] += cnt.blocks
+        totals["skipped"] += cnt.skipped
+        totals["ms"] += cnt.kernel_ms
+        totals["launches"] += cnt.launches
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    ms_total = allmax(totals["ms"], world)
+    eff_local = totals["it"] - totals["blocks"] + totals["skipped"]
+    eff_all = eff_local * world  # every rank renders the same frame (weak scaling)
+    value = eff_all / (ms_total * 1e-3)
+
+    # roofline: FP64 operations of the dominant kernel against the measured unfused FP64 rate
+    plain_steps = totals["it"] - totals["blocks"]
+    flops = FLOPS_PLAIN[(ext, deriv)] * plain_steps + FLOPS_BLOCK[deriv] * totals["blocks"]
+    achieved = flops / (totals["ms"] * 1e-3) / 1e12
+    f64, f32 = C.c_double(), C.c_double()
+    lib = C.CDLL(_lib.LIB_PATH)
+    lib.fdk_alu_peaks.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    lib.fdk_alu_peaks(local, C.byref(f64), C.byref(f32))
+    peak = f64.value / 1e12
+
+    # e2e through the public API with host buffers: uploads (H2D), render, host columns (D2H)
+    h2d = 16 * len(r) + (56 * len(bla.blocks) if bla is not None else 0)
+    d2h = n * sum(OUT_BYTES[c] for c in cols)
+    dev.free(handle)
+    e2e_eff, e2e_s = 0, 0.0
+    for i in range(args.warmup + args.e2e_steps):
+        barrier(world)
+        t0 = time.perf_counter()
+        h2 = dev.upload(r, bla)
+        j2 = fd.route.make_job(plane, tier, p, h2, nuc, flags)
+        arrays, cnt, st = dev.render_job(j2, columns=p.columns)
+        dev.free(h2)
+        el = time.perf_counter() - t0
+        if i >= args.warmup:
+            e2e_s += el
+            e2e_eff += cnt.iterations - cnt.blocks + cnt.skipped
+    e2e_s = allmax(e2e_s, world)
+    e2e_value = e2e_eff * world / e2e_s
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        fdref, job_o, ref_o, bla_o, sample, step, setup, cores = reference_arm(args, fr)
+        eff_c, dt_c, n_c = sample(step)
+        rows = len(range(job_o.row_first, p.ny, step))
+        cpu = {"value": eff_c / dt_c, "unit": UNIT, "cores": cores, "kind": "port",
+               "sample": f"{rows} of {p.ny} rows (every {step}th) of the same frame, {dt_c:.1f} s"}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded location)",
+                "config": {"workload": fr.name, "nx": p.nx, "ny": p.ny, "max_iter": p.max_iter,
+                           "bla_eps": fr.bla_eps, "tier": {0: "f64", 1: "fixed", 2: "scaled"}[tier],
+                           "columns": list(p.columns), "period": fr.period, "reference_points": len(r),
+                           "bla_blocks": 0 if bla is None else len(bla.blocks), "l2": "flushed between steps",
+                           "form": "plain fp64 (bit-exact)", "parallelism": f"replicas x{world}"},
+                "setup_seconds": {"orbit": orbit_s, "bla": bla_s},
+                "counters": {"iterations": totals["it"] // args.steps, "blocks": totals["blocks"] // args.steps,
+                             "skipped": totals["skipped"] // args.steps},
+                "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                             "frac": achieved / peak if peak > 0 else None, "traffic": None,
+                             "peak_source": "measured live: unfused DMUL+DADD chains on all SMs (fdk_alu_peaks)"},
+                "cpu_baseline": cpu, "clocks": clk, "gpu_launches": totals["launches"],
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                        "steps": args.e2e_steps}}
+        print(json.dumps(line), flush=True)
+    dev.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--config", type=int, choices=(1, 2), default=2)
+    ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -76,7 +76,7 @@ class Plane(C.Structure):
 FDC_SYMBOLS = ["fdc_abi_version", "fdc_open", "fdc_close", "fdc_last_error", "fdc_upload_orbit", "fdc_free_orbit",
                "fdc_upload_bla", "fdc_render"]
 FDH_SYMBOLS = ["fdh_last_error", "fdh_plane_new", "fdh_orbit_fixed", "fdh_orbit_f64", "fdh_nucleus_period",
-               "fdh_bla_build", "fdh_dc_bound", "fdh_nucleus"]
+               "fdh_bla_build", "fdh_dc_bound", "fdh_location"]
 
 _lib = None
 
@@ -109,8 +109,8 @@ def lib():
     L.fdh_nucleus_period.argtypes = [P, P, U64]
     L.fdh_bla_build.argtypes = [P, P, U64, D, D, I64, C.c_int, P, P, C.POINTER(U32), C.POINTER(U64)]
     L.fdh_dc_bound.argtypes = [C.POINTER(Plane), I32, U32, U32, C.POINTER(D), C.POINTER(I64)]
-    L.fdh_nucleus.argtypes = [C.c_char_p, C.c_char_p, D, U64, U64, C.c_char_p, C.c_char_p, C.c_size_t,
-                              C.POINTER(U64)]
+    L.fdh_location.argtypes = [C.c_char_p, C.c_char_p, D, D, U64, U64, C.c_char_p, C.c_char_p, C.c_size_t,
+                               C.POINTER(U64), C.POINTER(D)]
     _lib = L
     return L
 

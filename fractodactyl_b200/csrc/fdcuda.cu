@@ -3,6 +3,7 @@
 // Built with -fmad=false (the plain form must round as the reference's Rust does).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -274,7 +275,13 @@ fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counte
     // grid.rs:392-411
     if (j.escape_radius < 4.0)
       return fail(ctx, FDC_INVALID, "escape radius is below 4: BLA blocks may only skip iterates with |z| <= 2 (1 + 2 eps)");
+    // Largest unit offset: the grid's corner (grid.rs:428-444), or the supplied offsets'.
     double half = std::hypot((double)j.nx / 2.0, (double)j.ny / 2.0);
+    if (j.offsets) {
+      half = 0.0;
+      const uint64_t lo = 2ull * first * j.nx, hi = 2ull * (first + rows) * j.nx;
+      for (uint64_t k = lo; k < hi; k += 2) half = std::max(half, std::hypot(j.offsets[k], j.offsets[k + 1]));
+    }
     double dc = ext ? j.h_m * half : h * half;
     int64_t e = ext ? j.h_e : 0;
     bool over = e == o.bla.dc_exp ? dc > o.bla.dc_max

@@ -544,107 +544,276 @@ void fdh_dc_bound(const fdh_plane *plane, int32_t tier, uint32_t nx, uint32_t ny
   }
 }
 
-int fdh_nucleus(const char *start_re, const char *start_im, double log10_radius, uint64_t max_period, uint64_t bits,
-                char *re_out, char *im_out, size_t cap, uint64_t *period) {
+namespace {
+
+// Orbit machinery of the location recipe: z in L-limb fixed point (exact z^2 + c),
+// derivatives and multipliers in wide-exponent complex floating point.
+struct Walker {
+  size_t L;
+  std::vector<uint64_t> buf, prod;
+  uint64_t *x, *y, *x2, *y2, *s, *s2, *t;
+  bool xn = false, yn = false;
+  explicit Walker(size_t l) : L(l), buf(8 * l), prod(2 * l) {
+    x = buf.data();
+    y = x + L;
+    x2 = y + L;
+    y2 = x2 + L;
+    s = y2 + L;
+    s2 = s + L;
+    t = s2 + L;
+  }
+  void reset() {
+    std::fill(buf.begin(), buf.end(), 0);
+    xn = yn = false;
+  }
+  Fec z() const {
+    double mr = 0, mi = 0;
+    int64_t er = 0, ei = 0;
+    bool hr = frexp_fix(xn, x, L, mr, er), hi = frexp_fix(yn, y, L, mi, ei);
+    if (!hr && !hi) return Fec{0, 0, 0};
+    int64_t e = !hr ? ei : (!hi ? er : std::max(er, ei));
+    double a = hr ? std::ldexp(mr, (int)std::max<int64_t>(er - e, -2000)) : 0.0;
+    double b = hi ? std::ldexp(mi, (int)std::max<int64_t>(ei - e, -2000)) : 0.0;
+    return fec_norm(a, b, e);
+  }
+  // z' = z^2 + c (three squarings); false once |z|^2 > 4e8 (escaped: the recipe's
+  // iterates never need more).
+  bool step(const Fix &a, const Fix &b) {
+    square_trunc(x, x2, L, prod.data());
+    square_trunc(y, y2, L, prod.data());
+    sadd(xn, x, yn, y, s, L);
+    square_trunc(s, s2, L, prod.data());
+    bool tn = sadd(false, x2, true, y2, t, L);
+    xn = sadd(tn, t, a.neg, a.mag.data(), x, L);
+    mag_add(x2, y2, s, L);
+    tn = sadd(false, s2, true, s, t, L);
+    yn = sadd(tn, t, b.neg, b.mag.data(), y, L);
+    double fx = fix_to_f64(xn, x, L), fy = fix_to_f64(yn, y, L);
+    return fx * fx + fy * fy <= 4.0e8;
+  }
+};
+
+inline double lg2(const Fec &v) {
+  if (v.re == 0 && v.im == 0) return -(double)INFINITY;
+  return 0.5 * std::log2(v.re * v.re + v.im * v.im) + (double)v.e;
+}
+inline Fec fmul(const Fec &a, const Fec &b) {
+  return fec_norm(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re, a.e + b.e);
+}
+inline Fec fdiv(const Fec &a, const Fec &b) {
+  double d = b.re * b.re + b.im * b.im;
+  return fec_norm((a.re * b.re + a.im * b.im) / d, (a.im * b.re - a.re * b.im) / d, a.e - b.e);
+}
+inline Fec fadd(const Fec &a, const Fec &b) {
+  if (a.re == 0 && a.im == 0) return b;
+  if (b.re == 0 && b.im == 0) return a;
+  int64_t e = std::max(a.e, b.e);
+  double sa = std::ldexp(1.0, (int)std::max<int64_t>(a.e - e, -2000));
+  double sb = std::ldexp(1.0, (int)std::max<int64_t>(b.e - e, -2000));
+  return fec_norm(a.re * sa + b.re * sb, a.im * sa + b.im * sb, e);
+}
+// dz' = 2 z dz + 1
+inline Fec dz_step(const Fec &z, const Fec &dz) { return fadd(fmul(fec_norm(2 * z.re, 2 * z.im, z.e), dz), Fec{1, 0, 0}); }
+
+Fix fec_part_to_fix(double m, int64_t e, size_t L) { return fe_to_fix(m, e, L); }
+
+// c -= step (fixed point)
+void fix_sub_step(Fix &cr, Fix &ci, const Fec &st, size_t L) {
+  Fix dr = fe_to_fix(st.re, st.e, L), di = fe_to_fix(st.im, st.e, L);
+  Fix nr, ni;
+  nr.mag.assign(L, 0);
+  ni.mag.assign(L, 0);
+  nr.neg = sadd(cr.neg, cr.mag.data(), !dr.neg, dr.mag.data(), nr.mag.data(), L);
+  ni.neg = sadd(ci.neg, ci.mag.data(), !di.neg, di.mag.data(), ni.mag.data(), L);
+  cr = nr;
+  ci = ni;
+}
+
+Fec fix_diff(const Fix &ar, const Fix &ai, const Fix &br, const Fix &bi, size_t L) {
+  std::vector<uint64_t> dr(L), di(L);
+  bool nr = sadd(ar.neg, ar.mag.data(), !br.neg, br.mag.data(), dr.data(), L);
+  bool ni = sadd(ai.neg, ai.mag.data(), !bi.neg, bi.mag.data(), di.data(), L);
+  double mr = 0, mi = 0;
+  int64_t er = 0, ei = 0;
+  bool hr = frexp_fix(nr, dr.data(), L, mr, er), hi = frexp_fix(ni, di.data(), L, mi, ei);
+  if (!hr && !hi) return Fec{0, 0, 0};
+  int64_t e = !hr ? ei : (!hi ? er : std::max(er, ei));
+  return fec_norm(hr ? std::ldexp(mr, (int)std::max<int64_t>(er - e, -2000)) : 0.0,
+                  hi ? std::ldexp(mi, (int)std::max<int64_t>(ei - e, -2000)) : 0.0, e);
+}
+
+// Newton on z_{q+r}(c) = z_q(c) (ref.py:31-43), steps clamped to 1e-3. Converged, repelling
+// (|prod 2 z_k| > 1.01 over one cycle) and not a centre (no |z_k| ~ 0) only.
+bool misiurewicz(Fix &cr, Fix &ci, int q, int r, size_t L) {
+  Walker w(L);
+  const double tol = -(double)(64 * (L - 1)) + 24;
+  for (int it = 0; it < 80; ++it) {
+    w.reset();
+    Fec dz{0, 0, 0}, dzq{0, 0, 0};
+    Fix zqr, zqi;
+    for (int n = 1; n <= q + r; ++n) {
+      dz = dz_step(w.z(), dz);
+      if (!w.step(cr, ci)) return false;
+      if (n == q) {
+        dzq = dz;
+        zqr = Fix{w.xn, std::vector<uint64_t>(w.x, w.x + L)};
+        zqi = Fix{w.yn, std::vector<uint64_t>(w.y, w.y + L)};
+      }
+    }
+    Fix zr{w.xn, std::vector<uint64_t>(w.x, w.x + L)}, zi{w.yn, std::vector<uint64_t>(w.y, w.y + L)};
+    Fec f = fix_diff(zr, zi, zqr, zqi, L);
+    Fec df = fadd(dz, fec_norm(-dzq.re, -dzq.im, dzq.e));
+    if (df.re == 0 && df.im == 0) return false;
+    if (f.re == 0 && f.im == 0) break;
+    Fec st = fdiv(f, df);
+    double l = lg2(st);
+    if (l > std::log2(1e-3)) {
+      double k = std::exp2(std::log2(1e-3) - l);
+      st = fec_norm(st.re * k, st.im * k, st.e);
+    }
+    fix_sub_step(cr, ci, st, L);
+    if (l < tol) break;
+    if (it == 79) return false;
+  }
+  // verify on one more pass
+  w.reset();
+  Fec rho{1, 0, 0};
+  double zmin = INFINITY;
+  Fix zqr, zqi;
+  for (int n = 1; n <= q + r; ++n) {
+    if (!w.step(cr, ci)) return false;
+    Fec z = w.z();
+    zmin = std::min(zmin, lg2(z));
+    if (n == q) {
+      zqr = Fix{w.xn, std::vector<uint64_t>(w.x, w.x + L)};
+      zqi = Fix{w.yn, std::vector<uint64_t>(w.y, w.y + L)};
+    }
+    if (n >= q && n < q + r) rho = fmul(rho, fec_norm(2 * z.re, 2 * z.im, z.e));
+  }
+  Fix zr{w.xn, std::vector<uint64_t>(w.x, w.x + L)}, zi{w.yn, std::vector<uint64_t>(w.y, w.y + L)};
+  double res = lg2(fix_diff(zr, zi, zqr, zqi, L));
+  return res < -(double)(64 * (L - 1)) / 2 && lg2(rho) > std::log2(1.01) && zmin > -100.0;
+}
+
+// Ball period (ref.py:46-52): first p <= max_period with |z_p| < R |dz_p|; 0 if none.
+uint64_t ball_period(const Fix &cr, const Fix &ci, double log2_R, uint64_t max_period, size_t L) {
+  Walker w(L);
+  Fec dz{0, 0, 0};
+  for (uint64_t k = 1; k <= max_period; ++k) {
+    dz = dz_step(w.z(), dz);
+    if (!w.step(cr, ci)) return 0;
+    if (lg2(w.z()) < log2_R + lg2(dz)) return k;
+  }
+  return 0;
+}
+
+// Newton on z_p(c) = 0 with steps clamped to 2^log2_max (ref.py:54-67).
+bool nucleus_newton(Fix &cr, Fix &ci, uint64_t p, double log2_max, size_t L) {
+  Walker w(L);
+  const double tol = -(double)(64 * (L - 1)) + 16;
+  for (int it = 0; it < 200; ++it) {
+    w.reset();
+    Fec dz{0, 0, 0};
+    for (uint64_t k = 0; k < p; ++k) {
+      dz = dz_step(w.z(), dz);
+      if (!w.step(cr, ci)) return false;
+    }
+    Fec z = w.z();
+    if (z.re == 0 && z.im == 0) return true;
+    Fec st = fdiv(z, dz);
+    double l = lg2(st);
+    if (l > log2_max) {
+      double k = std::exp2(log2_max - l);
+      st = fec_norm(st.re * k, st.im * k, st.e);
+    }
+    fix_sub_step(cr, ci, st, L);
+    if (l < tol) return true;
+  }
+  return false;
+}
+
+// log2 of the size estimate |1 / (beta lambda^2)| of the period-p nucleus (ref.py:69-74).
+double log2_size(const Fix &cr, const Fix &ci, uint64_t p, size_t L) {
+  Walker w(L);
+  Fec l{1, 0, 0}, b{1, 0, 0};
+  for (uint64_t k = 1; k < p; ++k) {
+    w.step(cr, ci);
+    Fec z = w.z();
+    l = fmul(fec_norm(2 * z.re, 2 * z.im, z.e), l);
+    b = fadd(b, fdiv(Fec{1, 0, 0}, l));
+  }
+  return -lg2(fmul(b, fmul(l, l)));
+}
+
+}  // namespace
+
+extern "C" int fdh_location(const char *start_re, const char *start_im, double theta, double log10_width,
+                            uint64_t bits, uint64_t max_period, char *re_out, char *im_out, size_t cap,
+                            uint64_t *period, double *log10_size_over_width) {
   try {
     const size_t L = limbs_for(bits);
-    Fix cr = to_fix(parse_decimal(start_re), L), ci = to_fix(parse_decimal(start_im), L);
-    const double log2_r = log10_radius * 3.321928094887362;
-    std::vector<uint64_t> buf(8 * L), prod(2 * L);
-    uint64_t *x = buf.data(), *y = x + L, *x2 = y + L, *y2 = x2 + L, *s = y2 + L, *s2 = s + L, *t = s2 + L;
-    bool xn = false, yn = false;
-    // z as a wide-exponent complex number (shared exponent)
-    auto zfec = [&]() {
-      double mr = 0, mi = 0;
-      int64_t er = INT64_MIN / 4, ei = INT64_MIN / 4;
-      frexp_fix(xn, x, L, mr, er) || (mr = 0, true);
-      frexp_fix(yn, y, L, mi, ei) || (mi = 0, true);
-      if (mr == 0 && mi == 0) return Fec{0, 0, 0};
-      int64_t e = std::max(mr == 0 ? INT64_MIN / 4 : er, mi == 0 ? INT64_MIN / 4 : ei);
-      double a = mr == 0 ? 0.0 : std::ldexp(mr, (int)std::max<int64_t>(er - e, -2000));
-      double b = mi == 0 ? 0.0 : std::ldexp(mi, (int)std::max<int64_t>(ei - e, -2000));
-      return fec_norm(a, b, e);
-    };
-    auto log2_abs_fec = [](const Fec &v) -> double {
-      if (v.re == 0 && v.im == 0) return -(double)INFINITY;
-      return 0.5 * std::log2(v.re * v.re + v.im * v.im) + (double)v.e;
-    };
-    // dz' = 2 z dz + 1 with z, dz wide-exponent complex numbers.
-    auto dz_step = [](const Fec &z, const Fec &dz) {
-      if ((z.re == 0 && z.im == 0) || (dz.re == 0 && dz.im == 0)) return Fec{1, 0, 0};
-      Fec p = fec_norm(z.re * dz.re - z.im * dz.im, z.re * dz.im + z.im * dz.re, z.e + dz.e + 1);
-      if (p.e > 80) return p;
-      if (p.e < -80) return Fec{1, 0, 0};
-      return fec_norm(std::ldexp(p.re, (int)p.e) + 1.0, std::ldexp(p.im, (int)p.e), 0);
-    };
-    // z' = z^2 + c in fixed point (three squarings, as the reference orbit)
-    auto z_step = [&](const Fix &a, const Fix &b) {
-      square_trunc(x, x2, L, prod.data());
-      square_trunc(y, y2, L, prod.data());
-      sadd(xn, x, yn, y, s, L);
-      square_trunc(s, s2, L, prod.data());
-      bool tn = sadd(false, x2, true, y2, t, L);
-      xn = sadd(tn, t, a.neg, a.mag.data(), x, L);
-      mag_add(x2, y2, s, L);
-      tn = sadd(false, s2, true, s, t, L);
-      yn = sadd(tn, t, b.neg, b.mag.data(), y, L);
-      double fx = fix_to_f64(xn, x, L), fy = fix_to_f64(yn, y, L);
-      return fx * fx + fy * fy <= 4.0e8;
-    };
-    auto reset = [&]() {
-      std::fill(buf.begin(), buf.end(), 0);
-      xn = yn = false;
-    };
-    // Ball period (ref.py:46-52): first p with |z_p| < r |dz_p|.
-    reset();
-    Fec dz{0, 0, 0};
-    uint64_t p = 0;
-    for (uint64_t k = 1; k <= max_period; ++k) {
-      dz = dz_step(zfec(), dz);
-      if (!z_step(cr, ci)) break;
-      if (log2_abs_fec(zfec()) < log2_r + log2_abs_fec(dz)) {
-        p = k;
-        break;
+    const double LOG2_10 = 3.321928094887362;
+    const Fix sr = to_fix(parse_decimal(start_re), L), si = to_fix(parse_decimal(start_im), L);
+    // 1. the nearest repelling Misiurewicz point of low order
+    const size_t Lm = limbs_for(192);
+    Fix s0r = to_fix(parse_decimal(start_re), Lm), s0i = to_fix(parse_decimal(start_im), Lm);
+    double best = INFINITY;
+    int bq = 0, br = 0;
+    for (int q = 3; q <= 60; ++q)
+      for (int r = 1; r <= 4; ++r) {
+        Fix mr = s0r, mi = s0i;
+        if (!misiurewicz(mr, mi, q, r, Lm)) continue;
+        double d = lg2(fix_diff(mr, mi, s0r, s0i, Lm));
+        if (d < best - 1e-9) {
+          best = d;
+          bq = q;
+          br = r;
+        }
       }
+    if (!bq) throw std::runtime_error("no repelling Misiurewicz point near the start");
+    Fix mr = sr, mi = si;
+    if (!misiurewicz(mr, mi, bq, br, L)) throw std::runtime_error("Misiurewicz refinement failed");
+    // 2. ladder nucleus near M with size ~ width / 30, bisecting log10 R (ref.py:95-117)
+    double lo = log10_width * 0.5 - 1.0, hi = log10_width * 0.95;
+    bool have = false;
+    Fix bestr, besti;
+    uint64_t bestp = 0;
+    double bests = 0;
+    for (int it = 0; it < 14; ++it) {
+      double mid = 0.5 * (lo + hi);
+      double log2_R = mid * LOG2_10;
+      // c0 = M + 0.345 R e^{i theta}
+      Fec off = fec_norm(0.345 * std::cos(theta), 0.345 * std::sin(theta), 0);
+      off.e += (int64_t)std::floor(log2_R);
+      double frac = std::exp2(log2_R - std::floor(log2_R));
+      off = fec_norm(off.re * frac, off.im * frac, off.e);
+      Fix cr = mr, ci = mi;
+      fix_sub_step(cr, ci, fec_norm(-off.re, -off.im, off.e), L);
+      uint64_t p = ball_period(cr, ci, log2_R, max_period, L);
+      if (!p || !nucleus_newton(cr, ci, p, log2_R - 2.0, L)) {
+        hi = mid;
+        continue;
+      }
+      double rel = (log2_size(cr, ci, p, L) / LOG2_10) - log10_width;  // log10 (size / W)
+      if (!have || std::fabs(rel + std::log10(30.0)) < std::fabs(bests + std::log10(30.0))) {
+        have = true;
+        bestr = cr;
+        besti = ci;
+        bestp = p;
+        bests = rel;
+      }
+      if (rel > -std::log10(30.0)) lo = mid;
+      else hi = mid;
+      if (std::fabs(rel + std::log10(30.0)) < 0.3) break;
     }
-    if (p == 0) throw std::runtime_error("no ball period below the limit");
-    // Newton on z_p(c) = 0 with steps clamped to r/4 (ref.py:54-67, zone_build.rs:215-231).
-    const double log2_rmax = log2_r - 2.0;
-    bool converged = false;
-    for (int it = 0; it < 200 && !converged; ++it) {
-      reset();
-      dz = Fec{0, 0, 0};
-      for (uint64_t k = 0; k < p; ++k) {
-        dz = dz_step(zfec(), dz);
-        if (!z_step(cr, ci)) throw std::runtime_error("Newton iterate escaped");
-      }
-      Fec z = zfec();
-      if (z.re == 0 && z.im == 0) break;
-      double den = dz.re * dz.re + dz.im * dz.im;
-      Fec st = fec_norm((z.re * dz.re + z.im * dz.im) / den, (z.im * dz.re - z.re * dz.im) / den, z.e - dz.e);
-      double lmag = log2_abs_fec(st);
-      if (lmag > log2_rmax) {
-        double f = std::exp2(log2_rmax - lmag);
-        st = fec_norm(st.re * f, st.im * f, st.e);
-        lmag = log2_rmax;
-      }
-      Fix dr = fe_to_fix(st.re, st.e, L), di = fe_to_fix(st.im, st.e, L);
-      Fix nr, ni;
-      nr.mag.assign(L, 0);
-      ni.mag.assign(L, 0);
-      nr.neg = sadd(cr.neg, cr.mag.data(), !dr.neg, dr.mag.data(), nr.mag.data(), L);
-      ni.neg = sadd(ci.neg, ci.mag.data(), !di.neg, di.mag.data(), ni.mag.data(), L);
-      cr = nr;
-      ci = ni;
-      converged = lmag < -(double)(64 * (L - 1)) + 8;
-    }
-    if (!converged) throw std::runtime_error("nucleus Newton did not converge");
+    if (!have) throw std::runtime_error("no nucleus found near the Misiurewicz point");
     size_t digits = (size_t)std::ceil(64.0 * (double)(L - 1) * 0.30102999566398120) + 2;
-    std::string sre = fix_to_string(cr, digits), sim = fix_to_string(ci, digits);
+    std::string sre = fix_to_string(bestr, digits), sim = fix_to_string(besti, digits);
     if (sre.size() + 1 > cap || sim.size() + 1 > cap) throw std::runtime_error("output buffer too small");
     std::memcpy(re_out, sre.c_str(), sre.size() + 1);
     std::memcpy(im_out, sim.c_str(), sim.size() + 1);
-    *period = p;
+    *period = bestp;
+    *log10_size_over_width = bests;
     return 0;
   } catch (std::exception &e) {
     g_err = e.what();

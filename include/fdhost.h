@@ -56,14 +56,18 @@ int fdh_bla_build(const double *re, const double *im, uint64_t len, double eps, 
 /* grid.rs:418-444: bound m 2^e on |dc| over a view's samples for a tier. */
 void fdh_dc_bound(const fdh_plane *plane, int32_t tier, uint32_t nx, uint32_t ny, double *dc, int64_t *e);
 
-/* Nucleus recipe of the benchmark locations (no reference API; after
- * tools/research/twolevel/ref.py:46-67 and crates/fd-cli/src/zone_build.rs:215-231):
- * the ball period of the disc of radius 10^log10_radius around (start_re, start_im)
- * (first p with |z_p| < r |dz_p|, up to max_period), then Newton on z_p(c) = 0 at `bits`
- * fixed-point bits with steps clamped to r/4. Writes the nucleus as decimal strings
- * (caller buffers of cap bytes) and its period; returns 0 on convergence. */
-int fdh_nucleus(const char *start_re, const char *start_im, double log10_radius, uint64_t max_period, uint64_t bits,
-                char *re_out, char *im_out, size_t cap, uint64_t *period);
+/* Location recipe of the benchmark frames (no reference API; the construction of
+ * tools/research/twolevel/ref.py:31-117 around a Misiurewicz point):
+ *   1. the repelling Misiurewicz point M(q, r), q <= 60, r <= 4, nearest the start (Newton
+ *      on z_{q+r}(c) = z_q(c) from it, ref.py:31-43);
+ *   2. the lowest-period nucleus in the disc of radius R around M + 0.345 R e^{i theta}
+ *      (ball period, ref.py:46-52; Newton clamped to R/4, :54-67), with log10 R bisected
+ *      (14 steps) until the nucleus's size estimate (:69-74) is about width/30.
+ * Fixed point at `bits` fraction bits. Writes the nucleus as decimal strings (caller
+ * buffers of cap bytes), its period and log10(size / width); returns 0 on success. */
+int fdh_location(const char *start_re, const char *start_im, double theta, double log10_width, uint64_t bits,
+                 uint64_t max_period, char *re_out, char *im_out, size_t cap, uint64_t *period,
+                 double *log10_size_over_width);
 
 #ifdef __cplusplus
 }

@@ -43,6 +43,7 @@ typedef struct {
   uint32_t columns; /* FDREF_COL_* bits; CLASS implied */
   int32_t threads;
   int32_t tier;
+  uint32_t row_first, row_step; /* render rows row_first, +row_step, ... (0, 0 = all) */
 } fdref_job;
 
 typedef struct fdref_ref fdref_ref; /* Reference orbit (reference.rs:7-10) + bits */

@@ -30,6 +30,8 @@ class Job(C.Structure):
         ("columns", C.c_uint32),
         ("threads", C.c_int32),
         ("tier", C.c_int32),
+        ("row_first", C.c_uint32),
+        ("row_step", C.c_uint32),
     ]
 
 
@@ -122,7 +124,7 @@ def _err():
 
 
 def make_job(re, im, width, nx, ny, max_iter, rotation=0.0, ss=1, escape_radius=1e10,
-             columns=COL_NU | COL_DE | COL_NORMAL, threads=None, tier=None):
+             columns=COL_NU | COL_DE | COL_NORMAL, threads=None, tier=None, row_first=0, row_step=1):
     j = Job()
     j._keep = [s.encode() if isinstance(s, str) else s for s in (re, im, width)]
     j.center_re, j.center_im, j.width = j._keep
@@ -133,6 +135,7 @@ def make_job(re, im, width, nx, ny, max_iter, rotation=0.0, ss=1, escape_radius=
     j.columns = columns
     j.threads = threads or os.cpu_count() or 1
     j.tier = TIER[tier] if not isinstance(tier, int) else tier
+    j.row_first, j.row_step = row_first, row_step
     return j
 
 

@@ -148,8 +148,9 @@ static std::string run(const View &v, const Params &p, const Reference *supplied
   auto worker = [&]() {
     Stats local;
     for (;;) {
-      uint32_t j = next_row.fetch_add(1);
-      if (j >= p.ny) break;
+      uint64_t jj = (uint64_t)p.row_first + (uint64_t)next_row.fetch_add(1) * p.row_step;
+      if (jj >= p.ny) break;
+      uint32_t j = (uint32_t)jj;
       for (uint32_t i = 0; i < p.nx; ++i) {
         double ux, uy;
         plane.unit_offset(i, j, ux, uy);
@@ -300,6 +301,8 @@ static Params to_params(const fdref_job *j) {
   p.columns = j->columns | FDREF_COL_CLASS;
   p.threads = j->threads;
   if (j->tier >= 0) p.tier = (Tier)j->tier;
+  p.row_first = j->row_first;
+  p.row_step = j->row_step ? j->row_step : 1;
   return p;
 }
 

@@ -48,6 +48,7 @@ struct Params {
   uint32_t columns = 1;
   int threads = 1;
   std::optional<Tier> tier;
+  uint32_t row_first = 0, row_step = 1;
 };
 
 struct Plane {

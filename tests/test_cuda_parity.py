@@ -150,7 +150,9 @@ def single(dev, ref_c, ar, ai, max_iter, r2, offset_exp=None, bla=None, nucleus=
         j.cos_rot, j.sin_rot = 1.0, 0.0
         j.max_iter = max_iter
         j.escape_radius = math.sqrt(r2)
-        j.nucleus_period = ref_c.nucleus_period() if nucleus == -2 else (-1 if nucleus is None else nucleus)
+        if nucleus == -2:
+            nucleus = ref_c.nucleus_period()
+        j.nucleus_period = -1 if nucleus is None else nucleus
         off = np.array([ar, ai])
         j.offsets = off.ctypes.data
         arrays, cnt, _ = dev.render_job(j, raw=True)
