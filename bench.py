@@ -43,9 +43,14 @@ def log(*a):
 
 def frame_for(args):
     from fractodactyl_b200 import locations
-    if args.config == 1:
-        return locations.config1()
-    return locations.config2(seed=args.seed)
+    fr = locations.config1() if args.config == 1 else locations.config2(seed=args.seed)
+    if args.nx or args.ny:  # smaller grid over the same view (profiling cases)
+        fr.params.nx, fr.params.ny = args.nx or fr.params.nx, args.ny or fr.params.ny
+        fr.name += f"-grid{fr.params.nx}x{fr.params.ny}"
+    if args.tier:
+        fr.params.tier = args.tier
+        fr.name += f"-{args.tier}"
+    return fr
 
 
 class Clocks:
@@ -321,6 +326,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--nx", type=int, default=0)
+    ap.add_argument("--ny", type=int, default=0)
+    ap.add_argument("--tier", choices=("fixed", "scaled"), default=None)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
