@@ -149,7 +149,7 @@ struct Contraction {
 };
 
 // sample.rs:1094-1114 for two terms.
-__device__ __noinline__ Cx3 sum2(Cx3 a, Cx3 b, int64_t zero_e) {
+static __device__ __noinline__ Cx3 sum2(Cx3 a, Cx3 b, int64_t zero_e) {
   bool have = false;
   int64_t top = 0;
   double aa = rmax(fabs(a.re), fabs(a.im));
@@ -191,7 +191,7 @@ __device__ __forceinline__ bool in_main_components(double cr, double ci) {
 }
 
 // interior.rs:16-65: does the period-step map from phase m0, delta x0, contract?
-__device__ __noinline__ bool contracting(const double2 *__restrict__ orbit, uint32_t last, uint32_t m0, double x0r,
+static __device__ __noinline__ bool contracting(const double2 *__restrict__ orbit, uint32_t last, uint32_t m0, double x0r,
                                          double x0i, double ar, double ai, uint64_t period) {
   uint32_t m = m0;
   double xr = x0r, xi = x0i, dr = 1.0, di = 0.0;

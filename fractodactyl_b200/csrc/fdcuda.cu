@@ -12,12 +12,14 @@
 #include <vector>
 
 #include "../../include/fdcuda.h"
+#include "launch.hpp"
 #include "perturb_f64.cuh"
 #include "route_internal.hpp"
 
 namespace {
 
 struct BlaDev {
+  double *fused = nullptr;  // (zr, zi, r2 of the 2-step block at m, r2 of the 4-step block at m)
   double *r2 = nullptr;
   double2 *coef = nullptr;
   double2 *ab = nullptr;
@@ -30,6 +32,7 @@ struct BlaDev {
 
 struct OrbitDev {
   double2 *z = nullptr;
+  double *z32 = nullptr;  // precision-form entries, 4 doubles per point (launch.hpp)
   uint64_t len = 0;
   uint32_t bits = 0;
   double z0r = 0, z0i = 0;
@@ -61,6 +64,7 @@ struct fdc_ctx {
   void *stage = nullptr;
   size_t stage_bytes = 0;
   int blocks_per_sm[8] = {};
+  int blocks_per_sm_f32[4] = {};
 };
 
 namespace {
@@ -78,6 +82,7 @@ fdc_status fail(fdc_ctx *c, fdc_status s, const std::string &msg) {
   } while (0)
 
 void free_bla(BlaDev &b) {
+  cudaFree(b.fused);
   cudaFree(b.r2);
   cudaFree(b.coef);
   cudaFree(b.ab);
@@ -100,6 +105,24 @@ void *pick_kernel(bool ext, bool d, bool l, int &variant) {
     case 5: return kernel_ptr<true, false, true>();
     case 6: return kernel_ptr<true, true, false>();
     default: return kernel_ptr<true, true, true>();
+  }
+}
+
+// Precision-form entries: (zr, zi) f64, (zr, zi) f32 packed in one 8-byte word (NaN where
+// |Z| < 2^-60, whose steps take the exact path), and r^2 of the 2-step block at m (or -1).
+void pack_entries32(const std::vector<double2> &z, const std::vector<double> &r2a, std::vector<double> &out) {
+  out.assign(4 * z.size(), 0.0);
+  for (size_t m = 0; m < z.size(); ++m) {
+    out[4 * m] = z[m].x;
+    out[4 * m + 1] = z[m].y;
+    float fr = (float)z[m].x, fi = (float)z[m].y;
+    if (std::fmax(std::fabs(z[m].x), std::fabs(z[m].y)) < 0x1p-60) fr = std::nanf("");
+    uint32_t a, b;
+    std::memcpy(&a, &fr, 4);
+    std::memcpy(&b, &fi, 4);
+    uint64_t w = (uint64_t)a | ((uint64_t)b << 32);
+    std::memcpy(&out[4 * m + 2], &w, 8);
+    out[4 * m + 3] = r2a.empty() ? -1.0 : r2a[m];
   }
 }
 
@@ -145,6 +168,7 @@ void fdc_close(fdc_ctx *ctx) {
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
   for (auto &kv : ctx->orbits) {
     cudaFree(kv.second.z);
+    cudaFree(kv.second.z32);
     free_bla(kv.second.bla);
   }
   cudaFree(ctx->scratch);
@@ -171,6 +195,10 @@ fdc_status fdc_upload_orbit(fdc_ctx *ctx, const double *re, const double *im, ui
   o.z0i = im[0];
   CK(cudaMalloc(&o.z, len * sizeof(double2)));
   CK(cudaMemcpyAsync(o.z, z.data(), len * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
+  std::vector<double> e32;
+  pack_entries32(z, {}, e32);
+  CK(cudaMalloc(&o.z32, e32.size() * sizeof(double)));
+  CK(cudaMemcpyAsync(o.z32, e32.data(), e32.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   int32_t id = ctx->next_orbit++;
   ctx->orbits[id] = o;
@@ -185,6 +213,7 @@ fdc_status fdc_free_orbit(fdc_ctx *ctx, int32_t orbit) {
   CK(cudaSetDevice(ctx->device));
   CK(cudaStreamSynchronize(ctx->stream));
   cudaFree(it->second.z);
+  cudaFree(it->second.z32);
   free_bla(it->second.bla);
   ctx->orbits.erase(it);
   return FDC_OK;
@@ -220,7 +249,28 @@ fdc_status fdc_upload_bla(fdc_ctx *ctx, int32_t orbit, const double *blocks7, co
     coef[2 * b + 1] = make_double2(v[2], v[3]);
     ab[b] = make_double2(v[5], v[6]);
   }
-  CK(cudaSetDevice(ctx->device));
+  // Fused stream: orbit point m with the radii of the first two levels' blocks at m.
+  std::vector<double> fused(4 * o.len, -1.0);
+  {
+    std::vector<double2> z(o.len);
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpy(z.data(), o.z, o.len * sizeof(double2), cudaMemcpyDeviceToHost));
+    for (uint64_t m = 0; m < o.len; ++m) {
+      fused[4 * m] = z[m].x;
+      fused[4 * m + 1] = z[m].y;
+    }
+    for (uint32_t i = 0; i < levels && i < 2; ++i) {
+      uint64_t cnt = steps >> (i + 1);
+      for (uint64_t t = 0; t < cnt; ++t) {
+        uint64_t m = 1 + (t << (i + 1));  // block t of level i starts at Z_m (bla.rs:131-135)
+        fused[4 * m + 2 + i] = r2[level_offsets[i] + t];
+      }
+    }
+    std::vector<double> r2a(o.len), e32;
+    for (uint64_t m = 0; m < o.len; ++m) r2a[m] = fused[4 * m + 2];
+    pack_entries32(z, r2a, e32);
+    CK(cudaMemcpy(o.z32, e32.data(), e32.size() * sizeof(double), cudaMemcpyHostToDevice));
+  }
   CK(cudaStreamSynchronize(ctx->stream));
   free_bla(o.bla);
   o.has_bla = false;
@@ -233,6 +283,8 @@ fdc_status fdc_upload_bla(fdc_ctx *ctx, int32_t orbit, const double *blocks7, co
     d.off[i] = (uint32_t)level_offsets[i];
     d.count[i] = (uint32_t)(steps >> (i + 1));
   }
+  CK(cudaMalloc(&d.fused, 4 * o.len * sizeof(double)));
+  CK(cudaMemcpyAsync(d.fused, fused.data(), 4 * o.len * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
   if (total) {
     CK(cudaMalloc(&d.r2, total * sizeof(double)));
     CK(cudaMalloc(&d.coef, 2 * total * sizeof(double2)));
@@ -240,8 +292,8 @@ fdc_status fdc_upload_bla(fdc_ctx *ctx, int32_t orbit, const double *blocks7, co
     CK(cudaMemcpyAsync(d.r2, r2.data(), total * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(d.coef, coef.data(), 2 * total * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(d.ab, ab.data(), total * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
   }
+  CK(cudaStreamSynchronize(ctx->stream));
   o.has_bla = true;
   return FDC_OK;
 }
@@ -260,7 +312,6 @@ fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counte
   if (!(j.escape_radius > 0.0) || !std::isfinite(j.escape_radius * j.escape_radius))
     return fail(ctx, FDC_INVALID, "escape radius must be positive and its square finite");
   if (!(j.h_m >= 1.0 && j.h_m < 2.0)) return fail(ctx, FDC_INVALID, "h_m must lie in [1, 2)");
-  if (j.flags & FDC_F32) return fail(ctx, FDC_DECLINED, "precision form not built into this kernel set");
   uint32_t first = j.first_row, rows = j.rows ? j.rows : j.ny - j.first_row;
   if (first >= j.ny || rows > j.ny - first) return fail(ctx, FDC_INVALID, "row range outside the grid");
   const bool ext = j.tier == FDC_TIER_SCALED;
@@ -298,6 +349,7 @@ fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counte
   p.z0r = o.z0r;
   p.z0i = o.z0i;
   if (bla) {
+    p.fused = (const double2 *)o.bla.fused;
     p.bla_r2 = o.bla.r2;
     p.bla_coef = o.bla.coef;
     p.bla_ab = o.bla.ab;
@@ -387,18 +439,22 @@ fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counte
   p.timed_out = &ctx->scratch->timed_out;
   CK(cudaMemsetAsync(ctx->scratch, 0, sizeof(Scratch), ctx->stream));
 
-  int variant = 0;
-  void *fn = pick_kernel(ext, deriv, bla, variant);
-  if (!ctx->blocks_per_sm[variant]) {
-    int b = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, 128, 0));
-    ctx->blocks_per_sm[variant] = b > 0 ? b : 1;
-  }
-  dim3 grid(ctx->sm_count * ctx->blocks_per_sm[variant]), block(128);
-  void *args[] = {&p};
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
-  CK(cudaLaunchKernel(fn, grid, block, args, 0, ctx->stream));
-  CK(cudaGetLastError());
+  if (j.flags & FDC_F32) {
+    CK(fdk::launch_f32(p, o.z32, deriv, bla, ctx->sm_count, ctx->stream, ctx->blocks_per_sm_f32));
+  } else {
+    int variant = 0;
+    void *fn = pick_kernel(ext, deriv, bla, variant);
+    if (!ctx->blocks_per_sm[variant]) {
+      int b = 0;
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, 128, 0));
+      ctx->blocks_per_sm[variant] = b > 0 ? b : 1;
+    }
+    dim3 grid(ctx->sm_count * ctx->blocks_per_sm[variant]), block(128);
+    void *args[] = {&p};
+    CK(cudaLaunchKernel(fn, grid, block, args, 0, ctx->stream));
+    CK(cudaGetLastError());
+  }
   CK(cudaEventRecord(ctx->ev1, ctx->stream));
   if (!dev_out) {
     for (int c = 0; c < 9; ++c)

@@ -1,0 +1,33 @@
+// Launcher of the precision-form kernel (compiled with fused multiply-adds).
+#include <cuda_runtime.h>
+
+#include "launch.hpp"
+#include "perturb_f32.cuh"
+
+namespace fdk {
+
+template <bool D, bool L>
+static cudaError_t launch_t(const Params &p, const Entry32 *orbit, int sm_count, cudaStream_t st, int *cache) {
+  if (*cache == 0) {
+    int b = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, perturb_f32_kernel<D, L>, 128, 0);
+    if (e != cudaSuccess) return e;
+    *cache = b > 0 ? b : 1;
+  }
+  perturb_f32_kernel<D, L><<<sm_count * *cache, 128, 0, st>>>(p, orbit);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_f32(const Params &p, const void *orbit32, bool deriv, bool bla, int sm_count, cudaStream_t st,
+                       int *blocks_per_sm) {
+  const Entry32 *o = (const Entry32 *)orbit32;
+  int v = (deriv ? 2 : 0) | (bla ? 1 : 0);
+  switch (v) {
+    case 0: return launch_t<false, false>(p, o, sm_count, st, blocks_per_sm + 0);
+    case 1: return launch_t<false, true>(p, o, sm_count, st, blocks_per_sm + 1);
+    case 2: return launch_t<true, false>(p, o, sm_count, st, blocks_per_sm + 2);
+    default: return launch_t<true, true>(p, o, sm_count, st, blocks_per_sm + 3);
+  }
+}
+
+}  // namespace fdk

@@ -1,0 +1,475 @@
+// The precision form of the perturbation kernel: the delta recurrence runs on FP32
+// mantissas with one int exponent per sample (delta = w 2^e, rescaled by 2^32 only when
+// the mantissa leaves [2^-32, 2^32]); FP64 stays on exactly four steps:
+//   1. the rebase test |Z + delta| <= |delta| (sample.rs:412-418, extended-tier rule),
+//   2. the bailout |Z + delta|^2 > R^2 and the smooth iteration's log-log (store.rs:86-99),
+//   3. the BLA validity radius comparisons |delta|^2 < r^2 (bla.rs:234-249),
+//   4. the derivative dz/dc for distance estimates (sample.rs:352-360).
+// Periodicity, the nucleus contraction and Newton's cycle prediction run in FP32.
+// Steps from an orbit point whose FP32 copy is not exact enough (|Z| < 2^-60: Z_0 and a
+// nucleus's returns) and BLA block applications use wide-exponent FP64 arithmetic.
+// Compiled with fused multiply-adds (this form is not bit-exact by design).
+#pragma once
+#include <cstdint>
+
+#include "perturb_f64.cuh"
+
+namespace fdk {
+
+// 32-byte orbit entry of the precision form: Z in f64, Z in f32 (NaN where |Z| < 2^-60),
+// the squared radius of the 2-step block starting at m (or -1).
+struct __align__(16) Entry32 {
+  double zr, zi;
+  float zr32, zi32;
+  double r2a;
+};
+
+__device__ __forceinline__ float exp2f_int(int e) {  // 2^e as f32, 0 below the normal range
+  return e < -126 ? 0.0f : (e > 127 ? __int_as_float(0x7f800000) : __int_as_float((e + 127) << 23));
+}
+
+// Multiplier / Contraction of sample.rs:600-698 on f32 mantissas with an int exponent.
+struct MulF {
+  float re, im;
+  int exp;
+  __device__ __forceinline__ void reset(float r = 1.0f) {
+    re = r;
+    im = 0.0f;
+    exp = 0;
+  }
+  __device__ __forceinline__ void multiply(float r, float i) {
+    float nr = re * r - im * i, ni = re * i + im * r;
+    re = nr;
+    im = ni;
+    float a = fmaxf(fabsf(re), fabsf(im));
+    if (!(a > 1e-18f && a < 1e18f) && a > 0.0f && isfinite(a)) {
+      int e = ilogbf(a);
+      re = scalbnf(re, -e);
+      im = scalbnf(im, -e);
+      exp += e;
+    }
+  }
+  __device__ __forceinline__ bool below(float lim) const {  // |v|^2 < lim
+    return isfinite(re) && isfinite(im) &&
+           (exp < -64 || (exp <= 64 && ((double)re * re + (double)im * im) * exp2i(2 * exp) < lim));
+  }
+};
+
+struct StateF {
+  float wr, wi;        // delta mantissa
+  float s32;           // 2^e (0 below f32's normal range)
+  float dcr, dci;      // dc 2^-e
+  float zr32, zi32;    // Z_m in f32 (NaN: take the exact step)
+  float sr, si, qr, qi, qstep;
+  int e;
+  double s64;          // 2^e in f64
+  double ar, ai;       // dc = a 2^oe
+  int oe;
+  double xr, xi;       // delta in f64 (physical), from the end of the previous iteration
+  double fr, fi;       // z = Z_m + delta in f64
+  double Zr, Zi, r2a;
+  double dr, di, inverse;
+  int64_t dexp;
+  MulF mu, ct;
+  bool ct_started;
+  uint32_t n, chk, sn, hold, m, idx, blocks, skipped;
+  int nucleus;
+  bool pending, predicted;
+};
+
+// delta = (re, im) 2^k (f64 mantissas, any k) into the f32 form, the exponent kept at or
+// above oe - 64 so that dc 2^-e stays representable.
+__device__ __forceinline__ void set_delta(StateF &s, double re, double im, int64_t k) {
+  double a = fmax(fabs(re), fabs(im));
+  int64_t e = k;
+  if (a != 0.0 && isfinite(a)) e = k + ilogb(a);
+  if (e < (int64_t)s.oe - 64) e = (int64_t)s.oe - 64;
+  int64_t sh = k - e;  // re 2^k = (re 2^sh) 2^e, 2^sh applied in two factors
+  double f1 = exp2i(sh / 2), f2 = exp2i(sh - sh / 2);
+  s.wr = (float)(re * f1 * f2);
+  s.wi = (float)(im * f1 * f2);
+  s.e = (int)e;
+  s.s32 = exp2f_int(s.e);
+  s.s64 = exp2i(s.e);
+  double g = exp2i((int64_t)s.oe - s.e);
+  s.dcr = (float)(s.ar * g);
+  s.dci = (float)(s.ai * g);
+}
+
+// Sum of two wide-exponent complex terms (as sum2, sample.rs:1094-1114).
+__device__ __forceinline__ Cx3 add3(Cx3 a, Cx3 b) { return sum2(a, b, a.e); }
+
+template <bool D, bool L>
+__device__ __forceinline__ bool step_f32(const Params &p, const Entry32 *__restrict__ orbit, StateF &s,
+                                         Result &res) {
+  if (s.n >= p.max_iter) {
+    res.kind = 2;
+    return true;
+  }
+  // speculative load of the next entry (m < last at the top of every iteration)
+  const double2 *e2 = reinterpret_cast<const double2 *>(orbit + s.m + 1);
+  double2 nz = __ldg(e2), nr = __ldg(e2 + 1);
+  bool took = false;
+  if (L && (s.nucleus < 0 || s.m != 0)) {
+    double d2 = s.xr * s.xr + s.xi * s.xi;  // FP64 radius test on the physical delta
+    uint64_t cap = s.hold > 0 ? (uint64_t)s.sn + s.hold : (s.pending ? ~0ull : (uint64_t)s.chk);
+    uint64_t budget = p.max_iter < cap ? p.max_iter : cap;
+    if (s.nucleus >= 0) {
+      uint64_t nc = s.n == 0 ? 1ull : (uint64_t)s.nucleus + 1;
+      budget = budget < nc ? budget : nc;
+    }
+    budget = budget > s.n ? budget - s.n : 0;
+    uint32_t k = s.m - 1u;
+    int lv = -1;
+    uint32_t at = 0;
+    if (budget >= 2 && d2 < s.r2a) {
+      lv = 0;
+      at = k >> 1;
+      uint32_t tz = k == 0 ? 32u : (uint32_t)(__ffs((int)k) - 1);
+      uint32_t top = tz < p.bla_levels ? tz : p.bla_levels;
+      for (uint32_t i = 1; i < top; ++i) {
+        if ((2ull << i) > budget) break;
+        uint32_t a = k >> (i + 1);
+        if (a >= p.bla_count[i]) break;
+        if (!(d2 < __ldg(p.bla_r2 + p.bla_off[i] + a))) break;
+        lv = (int)i;
+        at = a;
+      }
+    }
+    if (lv >= 0) {
+      took = true;
+      uint32_t b = p.bla_off[lv] + at;
+      double2 A = __ldg(p.bla_coef + 2 * b), B = __ldg(p.bla_coef + 2 * b + 1);
+      uint32_t len = 2u << lv;
+      if (s.nucleus >= 0 && s.n >= 1) {
+        s.ct.multiply((float)A.x, (float)A.y);
+        s.ct_started = true;
+      }
+      if (s.hold > 0) s.mu.multiply((float)A.x, (float)A.y);
+      if (D) {
+        normalise(s.dr, s.di, s.dexp, INT64_MAX / 4);
+        s.inverse = exp2i(-s.dexp);
+        double t = A.x * s.dr - A.y * s.di + B.x * s.inverse;
+        s.di = A.x * s.di + A.y * s.dr + B.y * s.inverse;
+        s.dr = t;
+        normalise(s.dr, s.di, s.dexp, INT64_MAX / 4);
+        s.inverse = exp2i(-s.dexp);
+      }
+      // delta' = A delta + B dc with wide exponents
+      double wr = s.wr, wi = s.wi;
+      Cx3 ad{A.x * wr - A.y * wi, A.x * wi + A.y * wr, s.e};
+      Cx3 bd{B.x * s.ar - B.y * s.ai, B.x * s.ai + B.y * s.ar, s.oe};
+      Cx3 d = add3(ad, bd);
+      set_delta(s, d.re, d.im, d.e);
+      s.m += len;
+      s.n += len;
+      s.blocks += 1;
+      s.skipped += len;
+    }
+  }
+  if (!took) {
+    if (s.nucleus >= 0 && s.n >= 1) {
+      s.ct.multiply((float)(2.0 * s.fr), (float)(2.0 * s.fi));
+      s.ct_started = true;
+    }
+    if (s.hold > 0) s.mu.multiply((float)(2.0 * s.fr), (float)(2.0 * s.fi));
+    if (D) {  // FP64 derivative (sample.rs:352-360)
+      double t = 2.0 * (s.fr * s.dr - s.fi * s.di) + s.inverse;
+      s.di = 2.0 * (s.fr * s.di + s.fi * s.dr);
+      s.dr = t;
+      if (fmax(fabs(s.dr), fabs(s.di)) > HI) {
+        s.dr = s.dr * LO;
+        s.di = s.di * LO;
+        s.dexp += 32;
+        s.inverse = exp2i(-s.dexp);
+      }
+    }
+    if (!isnan(s.zr32)) {
+      // FP32: w' = 2 Z w + 2^e w^2 + dc 2^-e
+      float wr = s.wr, wi = s.wi;
+      float zwr = s.zr32 * wr - s.zi32 * wi, zwi = s.zr32 * wi + s.zi32 * wr;
+      float nwr = 2.0f * zwr + s.s32 * (wr * wr - wi * wi) + s.dcr;
+      float nwi = 2.0f * zwi + s.s32 * (2.0f * wr * wi) + s.dci;
+      s.wr = nwr;
+      s.wi = nwi;
+      float mag = fmaxf(fabsf(nwr), fabsf(nwi));
+      if (mag > 4294967296.0f || (mag < 2.3283064e-10f && s.e > s.oe - 64)) set_delta(s, nwr, nwi, s.e);
+    } else {
+      // exact step at a tiny Z_m: 2 Z delta + delta^2 + dc with wide exponents
+      double wr = s.wr, wi = s.wi;
+      Cx3 zd{2.0 * (s.Zr * wr - s.Zi * wi), 2.0 * (s.Zr * wi + s.Zi * wr), s.e};
+      Cx3 dd{wr * wr - wi * wi, 2.0 * wr * wi, 2 * (int64_t)s.e};
+      Cx3 a{s.ar, s.ai, s.oe};
+      Cx3 t = add3(add3(zd, dd), a);
+      set_delta(s, t.re, t.im, t.e);
+    }
+    s.m += 1;
+    s.n += 1;
+  }
+  double2 Z = nz;
+  if (took) {
+    const double2 *e3 = reinterpret_cast<const double2 *>(orbit + s.m);
+    Z = __ldg(e3);
+    nr = __ldg(e3 + 1);
+  }
+  s.Zr = Z.x;
+  s.Zi = Z.y;
+  s.zr32 = __int_as_float((int)(__double_as_longlong(nr.x) & 0xffffffffll));
+  s.zi32 = __int_as_float((int)(__double_as_longlong(nr.x) >> 32));
+  s.r2a = nr.y;
+  // FP64: the physical delta, z, the bailout and the rebase test
+  double pr = (double)s.wr * s.s64, pi = (double)s.wi * s.s64;
+  double fr = Z.x + pr, fi = Z.y + pi;
+  double f2 = fr * fr + fi * fi;
+  if (f2 > p.r2) {
+    res.kind = 0;
+    res.n = s.n;
+    res.zr = fr;
+    res.zi = fi;
+    res.dr = s.dr;
+    res.di = s.di;
+    res.dexp = s.dexp;
+    return true;
+  }
+  if (s.nucleus >= 0 && s.n == (uint32_t)s.nucleus + 1) {
+    if (s.ct_started && s.ct.below(1e-6f)) {
+      res.kind = 1;
+      res.n = s.n;
+      return true;
+    }
+    s.nucleus = -1;
+  }
+  double delta2 = pr * pr + pi * pi;
+  if (f2 <= delta2 || s.m == p.last) {  // rebase onto Z_0 (extended-tier rule)
+    set_delta(s, fr, fi, 0);
+    s.m = 0;
+    s.Zr = p.z0r;
+    s.Zi = p.z0i;
+    s.zr32 = __int_as_float(0x7fc00000);  // Z_0 = 0: exact step
+    s.zi32 = 0.0f;
+    s.r2a = -1.0;
+    s.xr = (double)s.wr * s.s64;
+    s.xi = (double)s.wi * s.s64;
+    s.fr = s.Zr + s.xr;
+    s.fi = s.Zi + s.xi;
+  } else {
+    s.xr = pr;
+    s.xi = pi;
+    s.fr = fr;
+    s.fi = fi;
+  }
+  // periodicity in FP32 (ordinary-tier rule, sample.rs:473-574) on the rebased delta
+  bool judge = s.xr * s.xr + s.xi * s.xi > RES2 * f2;
+  if (!judge) {
+    if (s.hold > 0) {
+      if (s.n >= s.sn + s.hold) {
+        s.hold = 0;
+        s.predicted = false;
+        s.pending = true;
+      }
+    } else if (s.n >= s.chk) {
+      s.pending = true;
+    }
+    return false;
+  }
+  float gr = (float)fr, gi = (float)fi;
+  float dist = fabsf(gr - s.sr) + fabsf(gi - s.si);
+  float size = fabsf(s.sr) + fabsf(s.si);
+  if (dist < 1e-3f * size) {
+    uint32_t period = s.n - s.sn;
+    if (s.hold == period && s.mu.below(1.0f)) {
+      float sc = s.mu.exp < -60 ? 0.0f : exp2f_int(s.mu.exp < 60 ? s.mu.exp : 60);
+      float mr = s.mu.re * sc, mi = s.mu.im * sc;
+      float hr = gr - s.sr, hi = gi - s.si;
+      float er = mr - 1.0f, ei = mi;
+      float den = er * er + ei * ei;
+      float qpr = s.sr - (hr * er + hi * ei) / den;
+      float qpi = s.si - (hi * er - hr * ei) / den;
+      float tol = fminf(0.1f * sqrtf(den), 1e-2f) * s.qstep + 16.0f * 5.96e-8f * size;
+      if (s.predicted && fabsf(qpr - s.qr) + fabsf(qpi - s.qi) <= tol) {
+        res.kind = 1;
+        res.n = s.n;
+        return true;
+      }
+      s.qr = qpr;
+      s.qi = qpi;
+      s.qstep = (fabsf(hr) + fabsf(hi)) / sqrtf(den);
+      s.predicted = true;
+    } else {
+      s.predicted = false;
+    }
+    s.hold = period;
+    s.sr = gr;
+    s.si = gi;
+    s.sn = s.n;
+    s.pending = false;
+    s.mu.reset();
+    return false;
+  }
+  if (s.hold > 0) {
+    if (s.n < s.sn + s.hold) return false;
+    s.hold = 0;
+    s.predicted = false;
+    s.pending = true;
+  }
+  if (s.pending || s.n >= s.chk) {
+    uint32_t np = (uint32_t)next_pow2((uint64_t)s.n + 1);
+    s.chk = s.chk > np ? s.chk : np;
+    s.sr = gr;
+    s.si = gi;
+    s.sn = s.n;
+    s.pending = false;
+  }
+  return false;
+}
+
+template <bool D, bool L>
+__device__ __forceinline__ int init_f32(const Params &p, uint64_t slot, StateF &s, Result &res) {
+  uint64_t tile = slot >> 5;
+  uint32_t w = (uint32_t)slot & 31u;
+  uint32_t tx = (uint32_t)(tile % p.tiles_x), ty = (uint32_t)(tile / p.tiles_x);
+  uint32_t i = tx * 8 + (w & 7u), jj = ty * 4 + (w >> 3);
+  if (i >= p.nx || jj >= p.rows) return 0;
+  uint32_t j = p.first_row + jj;
+  uint32_t idx = j * p.nx + i;
+  if (p.mask && !p.mask[idx - p.out_base]) return 0;
+  s.idx = idx;
+  double ux, uy;
+  if (p.offsets) {
+    double2 o = p.offsets[idx - p.out_base];
+    ux = o.x;
+    uy = o.y;
+  } else {
+    double x = (double)i + 0.5 - p.half_x;
+    double y = (double)j + 0.5 - p.half_y;
+    ux = p.cosr * x + p.sinr * y;
+    uy = p.sinr * x - p.cosr * y;
+  }
+  if (p.tier == 2) {
+    s.ar = ux * p.h_m;
+    s.ai = uy * p.h_m;
+    s.oe = (int)p.h_e;
+  } else {
+    s.ar = ux * p.h;
+    s.ai = uy * p.h;
+    s.oe = 0;
+    if (p.tier == 0 && in_main_components(p.c_re + s.ar, p.c_im + s.ai)) {
+      res.kind = 1;
+      res.n = 0;
+      return 2;
+    }
+  }
+  set_delta(s, 0.0, 0.0, s.oe);
+  s.xr = s.xi = 0.0;
+  s.Zr = p.z0r;
+  s.Zi = p.z0i;
+  s.fr = s.Zr;
+  s.fi = s.Zi;
+  s.zr32 = __int_as_float(0x7fc00000);
+  s.zi32 = 0.0f;
+  s.r2a = -1.0;
+  s.dr = s.di = 0.0;
+  s.dexp = 0;
+  s.inverse = 1.0;
+  s.m = 0;
+  s.n = 0;
+  s.sr = s.si = 0.0f;
+  s.chk = 16;
+  s.sn = 8;
+  s.pending = false;
+  s.mu.reset();
+  s.hold = 0;
+  s.predicted = false;
+  s.qr = s.qi = s.qstep = 0.0f;
+  s.nucleus = (int)p.nucleus;
+  s.ct.reset();
+  s.ct_started = false;
+  s.blocks = 0;
+  s.skipped = 0;
+  return 1;
+}
+
+template <bool D, bool L>
+__global__ void __launch_bounds__(128) perturb_f32_kernel(Params p, const Entry32 *__restrict__ orbit) {
+  const unsigned FULL = 0xffffffffu;
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned lt = (1u << lane) - 1u;
+  StateF s;
+  Result res;
+  bool active = false, exhausted = false;
+  uint64_t t0 = p.deadline_ns ? globaltimer() : 0;
+  unsigned long long n_samples = 0, iters = 0, blocks = 0, skipped = 0, fallback = 0, closed = 0;
+  auto finish = [&](uint32_t idx, const Result &r, uint64_t nblocks, uint64_t nskipped) {
+    put(p, idx, r);
+    uint64_t spent = r.kind == 2 ? p.max_iter : r.n;
+    if (L) {
+      spent = spent - nskipped + nblocks;
+      blocks += nblocks;
+      skipped += nskipped;
+      bool cf = r.kind == 1 && r.n == 0;
+      closed += cf;
+      fallback += (nblocks == 0 && !cf);
+    }
+    iters += spent;
+    n_samples += 1;
+  };
+  for (;;) {
+    unsigned need = __ballot_sync(FULL, !active);
+    while (need && !exhausted) {
+      if (p.deadline_ns) {
+        uint64_t now = 0;
+        if (lane == 0) now = globaltimer();
+        now = __shfl_sync(FULL, now, 0);
+        if (now - t0 > p.deadline_ns) {
+          exhausted = true;
+          if (lane == 0) atomicExch(p.timed_out, 1u);
+          break;
+        }
+      }
+      unsigned long long base = 0;
+      int leader = __ffs((int)need) - 1;
+      if ((int)lane == leader) base = atomicAdd(p.queue, (unsigned long long)__popc(need));
+      base = __shfl_sync(FULL, base, leader);
+      if (base >= p.total) {
+        exhausted = true;
+        break;
+      }
+      if (!active) {
+        uint64_t slot = base + __popc(need & lt);
+        if (slot < p.total) {
+          int got = init_f32<D, L>(p, slot, s, res);
+          if (got == 1) active = true;
+          else if (got == 2) finish(s.idx, res, 0, 0);
+        }
+      }
+      need = __ballot_sync(FULL, !active);
+    }
+    if (!__any_sync(FULL, active)) break;
+    if (active) {
+      if (step_f32<D, L>(p, orbit, s, res)) {
+        finish(s.idx, res, s.blocks, s.skipped);
+        active = false;
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    n_samples += __shfl_down_sync(FULL, n_samples, o);
+    iters += __shfl_down_sync(FULL, iters, o);
+    blocks += __shfl_down_sync(FULL, blocks, o);
+    skipped += __shfl_down_sync(FULL, skipped, o);
+    fallback += __shfl_down_sync(FULL, fallback, o);
+    closed += __shfl_down_sync(FULL, closed, o);
+  }
+  if (lane == 0) {
+    atomicAdd(&p.counters->samples, n_samples);
+    atomicAdd(&p.counters->iterations, iters);
+    if (L) {
+      atomicAdd(&p.counters->blocks, blocks);
+      atomicAdd(&p.counters->skipped, skipped);
+      atomicAdd(&p.counters->fallback, fallback);
+      atomicAdd(&p.counters->closed, closed);
+    }
+  }
+}
+
+}  // namespace fdk

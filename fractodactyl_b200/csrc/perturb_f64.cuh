@@ -21,6 +21,10 @@ struct Counters {
 // Everything one launch needs; passed by value (kernel parameter space).
 struct Params {
   const double2 *__restrict__ orbit;  // Z_0..Z_last, interleaved re/im
+  // With BLA: Z_m fused with the squared radii of the level-1 and level-2 blocks (j = 1, 2)
+  // starting at m, or -1 where none starts there: 32-byte entries (zr, zi, r2a, r2b), so the
+  // first two levels of Bla::find come with the orbit point each step loads anyway.
+  const double2 *__restrict__ fused;
   uint32_t last;
   double z0r, z0i;
   // BLA, level-major: r2[off + t], coef[2 (off + t)] = (a.re, a.im), (b.re, b.im), ab = (alpha, beta)
@@ -70,6 +74,7 @@ struct State {
   double xr, xi, dr, di;
   double fr, fi;  // z = Z[m] + delta (carried between steps on the ordinary tier)
   double Zr, Zi;  // Z[m]
+  double r2a, r2b;  // radii^2 of the blocks of 2 and 4 steps starting at m (BLA kernels)
   double ar, ai;  // sample offset (mantissa on the extended tier)
   double dc_r, dc_i, scale, inverse;
   double sr, si, qr, qi, qstep;
@@ -100,6 +105,15 @@ __device__ __forceinline__ bool step(const Params &p, State<EXT> &s, Result &res
     res.kind = 2;
     return true;
   }
+  // Next orbit point, loaded before the step's arithmetic so its latency overlaps it
+  // (m < last here: a sample that reaches the last point rebases to Z_0 below).
+  double2 Zn, Rn = make_double2(-1.0, -1.0);
+  if (L) {
+    Zn = __ldg(p.fused + 2 * (s.m + 1));
+    Rn = __ldg(p.fused + 2 * (s.m + 1) + 1);
+  } else {
+    Zn = __ldg(p.orbit + s.m + 1);
+  }
   bool took = false;
   if (L) {
     if (s.nucleus < 0 || s.m != 0) {
@@ -113,17 +127,25 @@ __device__ __forceinline__ bool step(const Params &p, State<EXT> &s, Result &res
       }
       budget = budget > s.n ? budget - s.n : 0;
       uint32_t k = s.m - 1u;
-      uint32_t tz = k == 0 ? 32u : (uint32_t)(__ffs((int)k) - 1);
-      uint32_t top = tz < p.bla_levels ? tz : p.bla_levels;
       int lv = -1;
       uint32_t at = 0;
-      for (uint32_t i = 0; i < top; ++i) {
-        if ((2ull << i) > budget) break;
-        uint32_t a = k >> (i + 1);
-        if (a >= p.bla_count[i]) break;
-        if (!(d2 < __ldg(p.bla_r2 + p.bla_off[i] + a))) break;
-        lv = (int)i;
-        at = a;
+      if (budget >= 2 && d2 < s.r2a) {  // level 0: r2a is -1 unless a block starts at m
+        lv = 0;
+        at = k >> 1;
+        if (budget >= 4 && d2 < s.r2b) {  // level 1, likewise
+          lv = 1;
+          at = k >> 2;
+          uint32_t tz = k == 0 ? 32u : (uint32_t)(__ffs((int)k) - 1);
+          uint32_t top = tz < p.bla_levels ? tz : p.bla_levels;
+          for (uint32_t i = 2; i < top; ++i) {
+            if ((2ull << i) > budget) break;
+            uint32_t a = k >> (i + 1);
+            if (a >= p.bla_count[i]) break;
+            if (!(d2 < __ldg(p.bla_r2 + p.bla_off[i] + a))) break;
+            lv = (int)i;
+            at = a;
+          }
+        }
       }
       if (lv >= 0) {
         took = true;
@@ -206,7 +228,15 @@ __device__ __forceinline__ bool step(const Params &p, State<EXT> &s, Result &res
     s.m += 1;
     s.n += 1;
   }
-  double2 Z = __ldg(p.orbit + s.m);
+  double2 Z = Zn;
+  if (L) {
+    if (took) {  // a block moved m by its length
+      Z = __ldg(p.fused + 2 * s.m);
+      Rn = __ldg(p.fused + 2 * s.m + 1);
+    }
+    s.r2a = Rn.x;
+    s.r2b = Rn.y;
+  }
   s.Zr = Z.x;
   s.Zi = Z.y;
   double pr = EXT ? s.scale * s.xr : s.xr, pi = EXT ? s.scale * s.xi : s.xi;
@@ -248,6 +278,8 @@ __device__ __forceinline__ bool step(const Params &p, State<EXT> &s, Result &res
       s.m = 0;
       s.Zr = p.z0r;
       s.Zi = p.z0i;
+      s.r2a = -1.0;  // no block starts at Z_0 (bla.rs:235-236)
+      s.r2b = -1.0;
       if (s.scale < 1.0 / 1e270) {  // TINY, sample.rs:17
         s.nucleus = -1;
         if (D) {
@@ -267,6 +299,11 @@ __device__ __forceinline__ bool step(const Params &p, State<EXT> &s, Result &res
         double2 Z1 = __ldg(p.orbit + 1);
         s.Zr = Z1.x;
         s.Zi = Z1.y;
+        if (L) {
+          double2 rr = __ldg(p.fused + 3);
+          s.r2a = rr.x;
+          s.r2b = rr.y;
+        }
       }
       double factor = exp2i(s.offset_exp - s.delta_exp);
       s.dc_r = s.ar * factor;
@@ -277,6 +314,8 @@ __device__ __forceinline__ bool step(const Params &p, State<EXT> &s, Result &res
       s.m = 0;
       s.Zr = p.z0r;
       s.Zi = p.z0i;
+      s.r2a = -1.0;
+      s.r2b = -1.0;
     }
   } else if (EXT) {
     double magnitude = rmax(fabs(s.xr), fabs(s.xi));
@@ -443,6 +482,8 @@ __device__ __forceinline__ int init(const Params &p, uint64_t slot, State<EXT> &
   s.n = 0;
   s.Zr = p.z0r;
   s.Zi = p.z0i;
+  s.r2a = -1.0;
+  s.r2b = -1.0;
   s.fr = p.z0r + 0.0;
   s.fi = p.z0i + 0.0;
   s.sr = 0.0;

@@ -121,6 +121,11 @@ void fdref_store_escaped(double h_m, int64_t h_e, uint32_t ss, double rotation, 
 int64_t fdref_render_fds(const fdref_job *job, const fdref_ref *ref, const fdref_bla *bla,
                          uint8_t *buf, uint64_t cap);
 
+/* fd-fixed direct iteration at one sample's exact c = centre + (ar, ai) 2^oe: the escape
+ * count (0 if none within max_iter) and z there; ~0 on a parse error. */
+uint64_t fdref_direct(const char *cre, const char *cim, double ar, double ai, int64_t oe, uint64_t bits,
+                      uint64_t max_iter, double escape_radius, double *zr, double *zi);
+
 #ifdef __cplusplus
 }
 #endif

@@ -113,6 +113,8 @@ def lib():
                                    C.c_char_p, C.c_size_t]
         L.fdref_store_escaped.argtypes = [D, I64, U32, D, U64, D, D, D, D, I64,
                                           C.POINTER(D), C.POINTER(C.c_float), C.POINTER(C.c_uint16)]
+        L.fdref_direct.restype = U64
+        L.fdref_direct.argtypes = [C.c_char_p, C.c_char_p, D, D, I64, U64, U64, D, C.POINTER(D), C.POINTER(D)]
         L.fdref_render_fds.restype = I64
         L.fdref_render_fds.argtypes = [C.POINTER(Job), P, P, P, U64]
         _lib = L
@@ -297,3 +299,13 @@ def fnv1a64(data):
     for b in data:
         h = ((h ^ b) * 0x100000001B3) & 0xFFFFFFFFFFFFFFFF
     return h
+
+
+def direct(cre, cim, ar, ai, oe, bits, max_iter, escape_radius):
+    """fd-fixed direct iteration at the sample's exact c: (n or None, zr, zi)."""
+    zr, zi = C.c_double(), C.c_double()
+    n = lib().fdref_direct(cre.encode(), cim.encode(), ar, ai, oe, bits, max_iter, escape_radius, C.byref(zr),
+                           C.byref(zi))
+    if n == 2**64 - 1:
+        raise ValueError("direct iteration: bad centre")
+    return (None if n == 0 else int(n)), zr.value, zi.value

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstring>
 #include <stdexcept>
+#include <string>
 
 namespace fdref {
 
@@ -337,3 +338,80 @@ void orbit(const Fixed &cr, const Fixed &ci, uint64_t steps, double escape2,
 }
 
 }  // namespace fdref
+
+namespace fdref {
+
+// Exact fixed-point value of m 2^e (m a finite double) with L limbs, truncated toward zero.
+Fixed fixed_from_double(double m, int64_t e, size_t L) {
+  Fixed f;
+  f.mag.assign(L, 0);
+  if (m == 0.0) return f;
+  f.neg = m < 0;
+  int k;
+  double mm = std::frexp(std::fabs(m), &k);  // |m| = mm 2^k, mm in [0.5, 1)
+  uint64_t bits53 = (uint64_t)std::ldexp(mm, 53);
+  int64_t shift = e + k - 53 + 64 * (int64_t)(L - 1);
+  for (int b = 0; b < 53; ++b) {
+    if (!((bits53 >> b) & 1)) continue;
+    int64_t pos = shift + b;
+    if (pos < 0 || pos >= (int64_t)(64 * L)) continue;
+    f.mag[pos / 64] |= 1ull << (pos % 64);
+  }
+  return f;
+}
+
+// Direct iteration z <- z^2 + c from z = 0 at c = centre + (ar, ai) 2^oe in L-limb fixed
+// point (the fd-fixed orbit step, orbit.rs:14-43, at the sample's own c), until
+// |z|^2 > 2^32; the last steps to the escape radius in f64 (z is then far from 0, so f64
+// carries it to 1e-16 relative). Returns the escape count (0: none within max_iter).
+uint64_t direct_escape(const std::string &cre, const std::string &cim, double ar, double ai, int64_t oe,
+                       uint64_t bits, uint64_t max_iter, double r2, double &zr_out, double &zi_out) {
+  size_t L = limbs_for(bits);
+  Fixed c0r = Fixed::parse(cre, L), c0i = Fixed::parse(cim, L);
+  Fixed dr = fixed_from_double(ar, oe, L), di = fixed_from_double(ai, oe, L);
+  Fixed cr, ci;
+  cr.mag.assign(L, 0);
+  ci.mag.assign(L, 0);
+  cr.neg = limbs::add_signed(c0r.neg, c0r.mag.data(), dr.neg, dr.mag.data(), cr.mag.data(), L);
+  ci.neg = limbs::add_signed(c0i.neg, c0i.mag.data(), di.neg, di.mag.data(), ci.mag.data(), L);
+  uint64_t n = 0;
+  double fx = 0, fy = 0;
+  bool out = false;
+  orbit(cr, ci, max_iter, 4294967296.0, [&](double a, double b) {
+    ++n;
+    fx = a;
+    fy = b;
+    if (a * a + b * b > 4294967296.0) out = true;
+  });
+  if (!out) {
+    if (fx * fx + fy * fy > r2) {
+      zr_out = fx;
+      zi_out = fy;
+      return n;
+    }
+    return 0;
+  }
+  double x = fx, y = fy, c_r = to_f64_limbs(cr.neg, cr.mag.data(), L), c_i = to_f64_limbs(ci.neg, ci.mag.data(), L);
+  // the orbit stopped at the first point past 2^16 in modulus: check it, then continue
+  while (!(x * x + y * y > r2)) {
+    if (n >= max_iter) return 0;
+    double t = x * x - y * y + c_r;
+    y = 2.0 * x * y + c_i;
+    x = t;
+    ++n;
+  }
+  zr_out = x;
+  zi_out = y;
+  return n;
+}
+
+}  // namespace fdref
+
+extern "C" uint64_t fdref_direct(const char *cre, const char *cim, double ar, double ai, int64_t oe, uint64_t bits,
+                                 uint64_t max_iter, double escape_radius, double *zr, double *zi) {
+  try {
+    return fdref::direct_escape(cre, cim, ar, ai, oe, bits, max_iter, escape_radius * escape_radius, *zr, *zi);
+  } catch (...) {
+    return ~0ull;
+  }
+}

@@ -1,0 +1,116 @@
+"""The precision form (FP32-mantissa floatexp deltas, FP64 for the rebase test, the
+bailout, the BLA radii and the derivative) against the plain FP64 route and against the
+fd-fixed direct-iteration oracle on a seeded subset of samples.
+
+Acceptance, per frame: escape counts equal to the plain route's on >= 99.9% of samples
+and at most 1 iteration off elsewhere (classes equal where both escape); smooth iteration
+within 1e-6 relative where the counts agree. Against direct iteration: the reported
+mismatch rate and smooth-iteration error stay within the same bounds.
+"""
+import math
+
+import numpy as np
+import pytest
+
+import fdref
+import fractodactyl_b200 as fd
+from fractodactyl_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+COUNT_MATCH = 0.999
+NU_REL = 1e-6
+
+
+@pytest.fixture(scope="module")
+def dev():
+    d = fd.Device(0)
+    yield d
+    d.close()
+
+
+def both_forms(dev, view, p, bla_eps=None):
+    r, bits = fd.reference(view, p)
+    r.bits = bits
+    plane, tier = fd.route._setup(view, p)
+    bla = None
+    if bla_eps is not None:
+        dc, e = fd.bla_dc_bound(view, p)
+        bla = fd.Bla.build_scaled(r, bla_eps, dc, e)
+        if bla.levels == 0:
+            bla = None
+    h = dev.upload(r, bla)
+    try:
+        flags = (_lib.DERIVATIVE if p.needs_derivative() else 0) | (_lib.BLA if bla is not None else 0)
+        j = fd.route.make_job(plane, tier, p, h, r.nucleus_period(), flags)
+        plain, cp, _ = dev.render_job(j, columns=p.columns, raw=True)
+        j.flags = flags | _lib.F32
+        prec, cq, _ = dev.render_job(j, columns=p.columns, raw=True)
+    finally:
+        dev.free(h)
+    return plane, tier, plain, prec, cp, cq
+
+
+def agreement(a, b):
+    """Fractions of samples whose escape counts agree (both non-escaping counts as agreeing)
+    and agree within one iteration."""
+    n = len(a["cls"])
+    ea, eb = a["cls"] == 0, b["cls"] == 0
+    dn = np.abs(a["n"].astype(np.int64) - b["n"].astype(np.int64))
+    same = (ea == eb) & (~ea | (dn == 0))
+    off1 = (ea == eb) & (~ea | (dn <= 1))
+    return same.sum() / n, off1.sum() / n
+
+
+VIEWS = [
+    ("-0.7453", "0.1127", "0.0065", 256, 144, 20_000, None),
+    ("-0.743643887037158704752191506114774", "0.131825904205311970493132056385139", "1e-28", 256, 144, 50_000,
+     None),
+    ("0", "1", "1e-300", 256, 144, 20_000, None),
+    ("-0.7436438870371587", "0.1318259042053120", "1e-12", 240, 135, 20_000, None),
+]
+
+
+@pytest.mark.parametrize("view", VIEWS, ids=lambda v: v[2])
+@pytest.mark.parametrize("bla", [None, 2.0 ** -50])
+def test_precision_form_agrees_with_plain(dev, view, bla):
+    re_, im_, w, nx, ny, it, tier = view
+    v = fd.View(re_, im_, w)
+    p = fd.Params(nx, ny, max_iter=it, columns=("nu", "de", "normal"), tier=tier)
+    plane, tier, a, b, cp, cq = both_forms(dev, v, p, bla)
+    same, off1 = agreement(a, b)
+    print(f"{w} bla={bla}: counts equal {same:.6f}, within one {off1:.6f}")
+    assert same >= COUNT_MATCH and off1 >= 1.0 - 0.25 * (1.0 - COUNT_MATCH), (same, off1)
+    esc = (a["cls"] == 0) & (b["cls"] == 0) & (a["n"] == b["n"])
+    rel = np.abs(a["nu"][esc] - b["nu"][esc]) / np.abs(a["nu"][esc])
+    assert rel.size == 0 or rel.max() <= NU_REL
+
+
+def test_precision_form_against_direct_iteration(dev):
+    """Seeded subset of a 1e-28 frame: both forms against fd-fixed direct iteration."""
+    re_, im_ = "-0.743643887037158704752191506114774", "0.131825904205311970493132056385139"
+    v = fd.View(re_, im_, "1e-28")
+    p = fd.Params(128, 72, max_iter=50_000, columns=("nu",))
+    plane, tier, a, b, _, _ = both_forms(dev, v, p)
+    rng = np.random.default_rng(7)
+    idx = rng.choice(p.nx * p.ny, 96, replace=False)
+    h = plane.h_m * 2.0 ** plane.h_e
+    miss_a = miss_b = 0
+    worst = 0.0
+    for k in idx:
+        i, j = int(k % p.nx), int(k // p.nx)
+        x, y = i + 0.5 - p.nx / 2.0, j + 0.5 - p.ny / 2.0
+        ux, uy = plane.cos_rot * x + plane.sin_rot * y, plane.sin_rot * x - plane.cos_rot * y
+        n, zr, zi = fdref.direct(re_, im_, ux * h, uy * h, 0, plane.bits + 64, p.max_iter, p.escape_radius)
+        for arr, which in ((a, "a"), (b, "b")):
+            esc = int(arr["cls"][k]) == 0
+            ok = (n is None and not esc) or (n is not None and esc and abs(int(arr["n"][k]) - n) <= 1)
+            if not ok:
+                if which == "a":
+                    miss_a += 1
+                else:
+                    miss_b += 1
+        if n is not None and int(b["cls"][k]) == 0 and int(b["n"][k]) == n:
+            nu = n + 1 - math.log2(math.log2(math.hypot(zr, zi)))
+            worst = max(worst, abs(b["nu"][k] - nu) / nu)
+    assert miss_a == 0 and miss_b <= 1, (miss_a, miss_b)
+    assert worst <= 1e-5, worst
