@@ -24,6 +24,8 @@ import sys
 import tempfile
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -224,40 +226,61 @@ def run_ours(args):
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
     job = fd.route.make_job(plane, tier, p, handle, nuc, flags | _lib.DEVICE_OUT)
 
-    def device_step():
-        arrays, cnt, st = dev.render_job(job, device_out={c: bufs[c].data_ptr() for c in cols})
+    def device_step(extra=0):
+        j = fd.route.make_job(plane, tier, p, handle, nuc, flags | _lib.DEVICE_OUT | extra)
+        arrays, cnt, st = dev.render_job(j, device_out={c: bufs[c].data_ptr() for c in cols})
         return cnt
 
     ext = tier == 2
-    totals = dict(it=0, blocks=0, skipped=0, ms=0.0, launches=0)
-    for _ in range(args.warmup):
-        device_step()
-    torch.cuda.synchronize()
+
+    def timed(extra):
+        tot = dict(it=0, blocks=0, skipped=0, ms=0.0, launches=0)
+        for _ in range(args.warmup):
+            device_step(extra)
+        torch.cuda.synchronize()
+        barrier(world)
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            flush.zero_()  # L2 flush between frames (outside the kernel's events)
+            torch.cuda.synchronize()  # the route's stream does not wait on torch's
+            cnt = device_step(extra)
+            tot["it"] += cnt.iterations
+            tot["blocks"] += cnt.blocks
+            tot["skipped"] += cnt.skipped
+            tot["ms"] += cnt.kernel_ms
+            tot["launches"] += cnt.launches
+        torch.cuda.synchronize()
+        barrier(world)
+        snap = {c: bufs[c].cpu().numpy().copy() for c in ("cls", "n")}
+        return tot, snap
+
     clocks = Clocks(local)
     clocks.start()
-    barrier(world)
-    torch.cuda.synchronize()
-    for _ in range(args.steps):
-        flush.zero_()  # L2 flush between frames (outside the kernel's events)
-        torch.cuda.synchronize()  # the route's stream does not wait on torch's
-        cnt = device_step()
-        totals["it"] += cnt.iterations
-        totals["blocks"] += cnt.blocks
-        totals["skipped"] += cnt.skipped
-        totals["ms"] += cnt.kernel_ms
-        totals["launches"] += cnt.launches
-    torch.cuda.synchronize()
-    barrier(world)
+    forms = {}
+    for name, extra in (("fp64_plain", 0), ("fp32_floatexp", _lib.F32)):
+        if args.form != "both" and name != {"fp64": "fp64_plain", "f32": "fp32_floatexp"}[args.form]:
+            continue
+        tot, snap = timed(extra)
+        ms = allmax(tot["ms"], world)
+        eff = (tot["it"] - tot["blocks"] + tot["skipped"]) * world
+        forms[name] = dict(tot=tot, snap=snap, ms=ms, value=eff / (ms * 1e-3))
     clk = clocks.stop()
-    ms_total = allmax(totals["ms"], world)
-    eff_local = totals["it"] - totals["blocks"] + totals["skipped"]
-    eff_all = eff_local * world  # every rank renders the same frame (weak scaling)
-    value = eff_all / (ms_total * 1e-3)
+    agree = None
+    if "fp64_plain" in forms and "fp32_floatexp" in forms:
+        a, b = forms["fp64_plain"]["snap"], forms["fp32_floatexp"]["snap"]
+        ea, eb = a["cls"] == 0, b["cls"] == 0
+        dn = np.abs(a["n"].astype(np.int64) - b["n"].astype(np.int64))
+        agree = {"count_match": float(((ea == eb) & (~ea | (dn == 0))).mean()),
+                 "within_one": float(((ea == eb) & (~ea | (dn <= 1))).mean())}
+    head = "fp32_floatexp" if ("fp32_floatexp" in forms and (agree is None or agree["count_match"] >= 0.999)) \
+        else "fp64_plain"
+    totals, ms_total, value = forms[head]["tot"], forms[head]["ms"], forms[head]["value"]
 
-    # roofline: FP64 operations of the dominant kernel against the measured unfused FP64 rate
-    plain_steps = totals["it"] - totals["blocks"]
-    flops = FLOPS_PLAIN[(ext, deriv)] * plain_steps + FLOPS_BLOCK[deriv] * totals["blocks"]
-    achieved = flops / (totals["ms"] * 1e-3) / 1e12
+    # roofline of the plain (FP64-bound) form: FP64 operations against the measured unfused FP64 rate
+    rf = forms.get("fp64_plain", forms[head])["tot"]
+    plain_steps = rf["it"] - rf["blocks"]
+    flops = FLOPS_PLAIN[(ext, deriv)] * plain_steps + FLOPS_BLOCK[deriv] * rf["blocks"]
+    achieved = flops / (rf["ms"] * 1e-3) / 1e12
     f64, f32 = C.c_double(), C.c_double()
     lib = C.CDLL(_lib.LIB_PATH)
     lib.fdk_alu_peaks.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
@@ -273,7 +296,7 @@ def run_ours(args):
         barrier(world)
         t0 = time.perf_counter()
         h2 = dev.upload(r, bla)
-        j2 = fd.route.make_job(plane, tier, p, h2, nuc, flags)
+        j2 = fd.route.make_job(plane, tier, p, h2, nuc, flags | (_lib.F32 if head == "fp32_floatexp" else 0))
         arrays, cnt, st = dev.render_job(j2, columns=p.columns)
         dev.free(h2)
         el = time.perf_counter() - t0
@@ -298,14 +321,20 @@ def run_ours(args):
                            "bla_eps": fr.bla_eps, "tier": {0: "f64", 1: "fixed", 2: "scaled"}[tier],
                            "columns": list(p.columns), "period": fr.period, "reference_points": len(r),
                            "bla_blocks": 0 if bla is None else len(bla.blocks), "l2": "flushed between steps",
-                           "form": "plain fp64 (bit-exact)", "parallelism": f"replicas x{world}"},
+                           "form": head, "parallelism": f"replicas x{world}"},
+                "forms": {k: {"value": v["value"], "ms_per_step": v["ms"] / args.steps,
+                              "iterations": v["tot"]["it"] // args.steps, "blocks": v["tot"]["blocks"] // args.steps,
+                              "skipped": v["tot"]["skipped"] // args.steps} for k, v in forms.items()},
+                "fp32_vs_fp64": (forms["fp32_floatexp"]["value"] / forms["fp64_plain"]["value"]
+                                 if len(forms) == 2 else None),
+                "agreement_fp32_vs_fp64": agree,
                 "setup_seconds": {"orbit": orbit_s, "bla": bla_s},
                 "counters": {"iterations": totals["it"] // args.steps, "blocks": totals["blocks"] // args.steps,
                              "skipped": totals["skipped"] // args.steps},
                 "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                              "frac": achieved / peak if peak > 0 else None, "traffic": None,
                              "peak_source": "measured live: unfused DMUL+DADD chains on all SMs (fdk_alu_peaks)"},
-                "cpu_baseline": cpu, "clocks": clk, "gpu_launches": totals["launches"],
+                "cpu_baseline": cpu, "clocks": clk, "gpu_launches": sum(v["tot"]["launches"] for v in forms.values()),
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "steps": args.e2e_steps}}
         print(json.dumps(line), flush=True)
@@ -329,6 +358,7 @@ def main():
     ap.add_argument("--nx", type=int, default=0)
     ap.add_argument("--ny", type=int, default=0)
     ap.add_argument("--tier", choices=("fixed", "scaled"), default=None)
+    ap.add_argument("--form", choices=("both", "fp64", "f32"), default="both")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

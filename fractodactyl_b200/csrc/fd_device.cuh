@@ -34,7 +34,7 @@ __device__ __forceinline__ double rmin(double a, double b) { return fmin(a, b); 
 // floor(RN(log2 a)) for a > 0 finite: the exponent e of a, plus one when log2(a) lies
 // so close below e + 1 that round-to-nearest gives e + 1 (a just below a power of two
 // with |e + 1| > 1). d = e + 1 - log2(a) = -log2(1 - t/2), t = 2 - m, to ~1e-24.
-__device__ __forceinline__ int64_t floor_log2(double a) {
+__device__ __noinline__ static int64_t floor_log2_slow(double a) {
   int e = ilogb(a);
   double m = scalbn(a, -e);
   if (m < 2.0 - 0x1p-40) return e;
@@ -48,6 +48,15 @@ __device__ __forceinline__ int64_t floor_log2(double a) {
   // spacing of doubles on the side of T the value lies (below T for T > 0)
   double s = (T > 0 && pow2) ? scalbn(1.0, be - 53) : scalbn(1.0, be - 52);
   return d <= 0.5 * s ? T : e;
+}
+
+// The same for the common case from the bits: a normal double whose mantissa is below
+// 2 - 2^-40 has floor(RN(log2 a)) = its exponent field - 1023.
+__device__ __forceinline__ int64_t floor_log2(double a) {
+  unsigned long long b = (unsigned long long)__double_as_longlong(a);
+  int ef = (int)((b >> 52) & 0x7ff);
+  if (ef != 0 && (b & 0xFFFFFFFFFFFFFull) < (1ull << 52) - (1ull << 12)) return ef - 1023;
+  return floor_log2_slow(a);
 }
 
 // Rust `f as i64` for the finite values floor_log2's callers pass.

@@ -83,7 +83,7 @@ struct State {
   double adc, shift;
   int64_t offset_exp, delta_exp, derivative_exp;
   int64_t nucleus;
-  uint64_t n, chk, sn, hold, blocks, skipped;
+  uint32_t n, chk, sn, hold, blocks, skipped;  // n < max_iter < 2^32; chk saturates at 2^32 - 1
   uint32_t m, idx;
   int returns;
   bool pending, predicted;
@@ -119,14 +119,14 @@ __device__ __forceinline__ bool step(const Params &p, State<EXT> &s, Result &res
     if (s.nucleus < 0 || s.m != 0) {
       // Bla::find (bla.rs:234-249) with the budget of sample.rs:246-263.
       double d2 = EXT ? (s.xr * s.xr + s.xi * s.xi) * s.scale * s.scale : s.xr * s.xr + s.xi * s.xi;
-      uint64_t cap = s.hold > 0 ? s.sn + s.hold : (s.pending ? ~0ull : s.chk);
+      uint64_t cap = s.hold > 0 ? (uint64_t)s.sn + s.hold : (s.pending ? ~0ull : (uint64_t)s.chk);
       uint64_t budget = p.max_iter < cap ? p.max_iter : cap;
       if (s.nucleus >= 0) {
         uint64_t nc = s.n == 0 ? 1ull : (uint64_t)s.nucleus + 1;
         budget = budget < nc ? budget : nc;
       }
       budget = budget > s.n ? budget - s.n : 0;
-      uint32_t k = s.m - 1u;
+      uint32_t k = s.m - 1u;  // m = 0 wraps: odd, no block
       int lv = -1;
       uint32_t at = 0;
       if (budget >= 2 && d2 < s.r2a) {  // level 0: r2a is -1 unless a block starts at m
@@ -252,7 +252,7 @@ __device__ __forceinline__ bool step(const Params &p, State<EXT> &s, Result &res
     res.dexp = s.derivative_exp;
     return true;
   }
-  if (s.nucleus >= 0 && s.n == (uint64_t)s.nucleus + 1) {
+  if (s.nucleus >= 0 && (uint64_t)s.n == (uint64_t)s.nucleus + 1) {
     if (s.ct.small()) {
       res.kind = 1;
       res.n = s.n;
@@ -349,10 +349,10 @@ __device__ __forceinline__ bool step(const Params &p, State<EXT> &s, Result &res
         s.sr = fr;
         s.si = fi;
         s.sn = s.n;
-        s.chk = s.chk * 2;
+        s.chk = s.chk >= 0x80000000u ? 0xffffffffu : s.chk * 2;
       }
     } else if (s.hold > 0) {
-      if (s.n >= s.sn + s.hold) {
+      if ((uint64_t)s.n >= (uint64_t)s.sn + s.hold) {
         s.hold = 0;
         s.predicted = false;
         s.pending = true;
@@ -367,22 +367,22 @@ __device__ __forceinline__ bool step(const Params &p, State<EXT> &s, Result &res
   if (EXT) {
     if (s.returns < 4 && dist < 1e-13 * size + 1e-300) {
       if (contracting(p.orbit, p.last, s.m, check_r, check_i, s.ar * exp2i(s.offset_exp),
-                      s.ai * exp2i(s.offset_exp), s.n - s.sn)) {
+                      s.ai * exp2i(s.offset_exp), (uint64_t)(s.n - s.sn))) {
         res.kind = 2;
         return true;
       }
       s.returns += 1;
     }
-    if (s.n == s.chk || s.n > s.chk) {
+    if (s.n >= s.chk) {
       s.sr = fr;
       s.si = fi;
       s.sn = s.n;
-      s.chk = s.chk * 2;
+      s.chk = s.chk >= 0x80000000u ? 0xffffffffu : s.chk * 2;
     }
     return false;
   }
   if (dist < 1e-3 * size) {
-    uint64_t period = s.n - s.sn;
+    uint32_t period = s.n - s.sn;
     if (s.hold == period && s.mu.below_one()) {
       double mr, mi;
       s.mu.value(mr, mi);
@@ -413,14 +413,15 @@ __device__ __forceinline__ bool step(const Params &p, State<EXT> &s, Result &res
     return false;
   }
   if (s.hold > 0) {
-    if (s.n < s.sn + s.hold) return false;
+    if ((uint64_t)s.n < (uint64_t)s.sn + s.hold) return false;
     s.hold = 0;
     s.predicted = false;
     s.pending = true;
   }
   if (s.pending || s.n >= s.chk) {
-    uint64_t np = next_pow2(s.n + 1);
-    s.chk = s.chk > np ? s.chk : np;
+    uint64_t np = next_pow2((uint64_t)s.n + 1);
+    uint32_t np32 = np > 0xffffffffull ? 0xffffffffu : (uint32_t)np;
+    s.chk = s.chk > np32 ? s.chk : np32;
     s.sr = fr;
     s.si = fi;
     s.sn = s.n;
