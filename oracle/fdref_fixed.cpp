@@ -377,11 +377,12 @@ uint64_t direct_escape(const std::string &cre, const std::string &cim, double ar
   uint64_t n = 0;
   double fx = 0, fy = 0;
   bool out = false;
-  orbit(cr, ci, max_iter, 4294967296.0, [&](double a, double b) {
+  const double stop = r2 < 4294967296.0 ? r2 : 4294967296.0;
+  orbit(cr, ci, max_iter, stop, [&](double a, double b) {
     ++n;
     fx = a;
     fy = b;
-    if (a * a + b * b > 4294967296.0) out = true;
+    if (a * a + b * b > stop) out = true;
   });
   if (!out) {
     if (fx * fx + fy * fy > r2) {
