@@ -74,9 +74,9 @@ class Plane(C.Structure):
 
 # Every symbol the headers declare, for the export check.
 FDC_SYMBOLS = ["fdc_abi_version", "fdc_open", "fdc_close", "fdc_last_error", "fdc_upload_orbit", "fdc_free_orbit",
-               "fdc_upload_bla", "fdc_render"]
+               "fdc_upload_bla", "fdc_render", "fdc_batch_create", "fdc_batch_run", "fdc_batch_free"]
 FDH_SYMBOLS = ["fdh_last_error", "fdh_plane_new", "fdh_orbit_fixed", "fdh_orbit_f64", "fdh_nucleus_period",
-               "fdh_bla_build", "fdh_dc_bound", "fdh_location"]
+               "fdh_bla_build", "fdh_dc_bound", "fdh_encode", "fdh_location"]
 
 _lib = None
 
@@ -99,6 +99,9 @@ def lib():
     L.fdc_free_orbit.argtypes = [P, I32]
     L.fdc_upload_bla.argtypes = [P, I32, P, P, U32, D, D, I64]
     L.fdc_render.argtypes = [P, C.POINTER(Job), C.POINTER(Out), C.POINTER(Counters)]
+    L.fdc_batch_create.argtypes = [P, P, P, U32, C.POINTER(P)]
+    L.fdc_batch_run.argtypes = [P, P, C.POINTER(Counters), P]
+    L.fdc_batch_free.argtypes = [P, P]
     L.fdh_last_error.restype = C.c_char_p
     L.fdh_plane_new.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, D, U32, U32, C.POINTER(Plane)]
     L.fdh_orbit_fixed.restype = I64
@@ -108,6 +111,7 @@ def lib():
     L.fdh_nucleus_period.restype = I64
     L.fdh_nucleus_period.argtypes = [P, P, U64]
     L.fdh_bla_build.argtypes = [P, P, U64, D, D, I64, C.c_int, P, P, C.POINTER(U32), C.POINTER(U64)]
+    L.fdh_encode.argtypes = [C.POINTER(Plane), U32, U64, P, P, P, P, P, P, P, P, C.c_int]
     L.fdh_dc_bound.argtypes = [C.POINTER(Plane), I32, U32, U32, C.POINTER(D), C.POINTER(I64)]
     L.fdh_location.argtypes = [C.c_char_p, C.c_char_p, D, D, U64, U64, C.c_char_p, C.c_char_p, C.c_size_t,
                                C.POINTER(U64), C.POINTER(D)]

@@ -51,6 +51,8 @@ struct Scratch {
 
 }  // namespace
 
+struct fdc_batch;
+
 struct fdc_ctx {
   int device = 0;
   int sm_count = 0;
@@ -65,6 +67,28 @@ struct fdc_ctx {
   size_t stage_bytes = 0;
   int blocks_per_sm[8] = {};
   int blocks_per_sm_f32[4] = {};
+  int blocks_per_sm_batch[8] = {};
+  int blocks_per_sm_batch_f32[4] = {};
+};
+
+// A prepared batch (include/fdcuda.h): jobs grouped by kernel variant, each group's Params
+// array and slot starts in device memory, per-job counters, and a CUDA graph of the
+// whole run (clear queues and counters, one persistent launch per group).
+struct fdc_batch {
+  struct Group {
+    bool f32, ext, deriv, bla;
+    std::vector<uint32_t> order;  // original job index of each position
+    fdk::Params *jobs = nullptr;
+    unsigned long long *starts = nullptr;
+    unsigned long long total = 0;
+    uint32_t counter_base = 0;
+  };
+  std::vector<Group> groups;
+  uint32_t njobs = 0;
+  fdk::Counters *counters = nullptr;   // njobs, in group order
+  unsigned long long *queues = nullptr;  // one per group
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
 };
 
 namespace {
@@ -126,12 +150,121 @@ void pack_entries32(const std::vector<double2> &z, const std::vector<double> &r2
   }
 }
 
+void *pick_batch_kernel(bool ext, bool d, bool l, int &variant) {
+  variant = (ext ? 4 : 0) | (d ? 2 : 0) | (l ? 1 : 0);
+  switch (variant) {
+    case 0: return (void *)fdk::perturb_batch_kernel<false, false, false>;
+    case 1: return (void *)fdk::perturb_batch_kernel<false, false, true>;
+    case 2: return (void *)fdk::perturb_batch_kernel<false, true, false>;
+    case 3: return (void *)fdk::perturb_batch_kernel<false, true, true>;
+    case 4: return (void *)fdk::perturb_batch_kernel<true, false, false>;
+    case 5: return (void *)fdk::perturb_batch_kernel<true, false, true>;
+    case 6: return (void *)fdk::perturb_batch_kernel<true, true, false>;
+    default: return (void *)fdk::perturb_batch_kernel<true, true, true>;
+  }
+}
+
+void free_batch(fdc_batch *b) {
+  if (!b) return;
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  for (auto &g : b->groups) {
+    cudaFree(g.jobs);
+    cudaFree(g.starts);
+  }
+  cudaFree(b->counters);
+  cudaFree(b->queues);
+  delete b;
+}
+
 fdc_status open_resources(fdc_ctx *ctx) {
   CK(cudaSetDevice(ctx->device));
   CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
   CK(cudaEventCreate(&ctx->ev0));
   CK(cudaEventCreate(&ctx->ev1));
   CK(cudaMalloc(&ctx->scratch, sizeof(Scratch)));
+  return FDC_OK;
+}
+
+// Validate a job against its orbit (the refusals of render_bla, grid.rs:378-413) and fill
+// the per-job part of the kernel parameters (everything but outputs, queue, counters).
+fdc_status prepare(fdc_ctx *ctx, const OrbitDev &o, const fdc_job &j, fdk::Params &p, uint32_t &first,
+                   uint32_t &rows) {
+  if (j.nx == 0 || j.ny == 0) return fail(ctx, FDC_INVALID, "empty sample grid");
+  if (j.ss == 0 || j.nx % j.ss || j.ny % j.ss) return fail(ctx, FDC_INVALID, "grid must be a whole number of pixels");
+  if ((uint64_t)j.nx * j.ny >= (1ull << 31)) return fail(ctx, FDC_INVALID, "grid larger than 2^31 samples");
+  if (j.tier < 0 || j.tier > 2) return fail(ctx, FDC_INVALID, "unknown tier");
+  if (j.max_iter >= (1ull << 32)) return fail(ctx, FDC_INVALID, "max_iter must be below 2^32");
+  if (!(j.escape_radius > 0.0) || !std::isfinite(j.escape_radius * j.escape_radius))
+    return fail(ctx, FDC_INVALID, "escape radius must be positive and its square finite");
+  if (!(j.h_m >= 1.0 && j.h_m < 2.0)) return fail(ctx, FDC_INVALID, "h_m must lie in [1, 2)");
+  first = j.first_row;
+  rows = j.rows ? j.rows : j.ny - j.first_row;
+  if (first >= j.ny || rows > j.ny - first) return fail(ctx, FDC_INVALID, "row range outside the grid");
+  const bool ext = j.tier == FDC_TIER_SCALED;
+  // The scaled tier's exact-range step from Z_0 continues at Z_1 (sample.rs:430-447),
+  // which needs a next point after it.
+  if (ext && o.len < 3) return fail(ctx, FDC_INVALID, "the scaled tier needs an orbit of at least 3 points");
+  const bool bla = (j.flags & FDC_BLA) != 0;
+  const bool deriv = (j.flags & FDC_DERIVATIVE) != 0;
+  double h = j.h_m * fdroute::exp2i(j.h_e);
+  if (bla) {
+    if (!o.has_bla) return fail(ctx, FDC_INVALID, "FDC_BLA without an uploaded BLA table");
+    // grid.rs:392-411
+    if (j.escape_radius < 4.0)
+      return fail(ctx, FDC_INVALID, "escape radius is below 4: BLA blocks may only skip iterates with |z| <= 2 (1 + 2 eps)");
+    // Largest unit offset: the grid's corner (grid.rs:428-444), or the supplied offsets'.
+    double half = std::hypot((double)j.nx / 2.0, (double)j.ny / 2.0);
+    if (j.offsets) {
+      half = 0.0;
+      const uint64_t lo = 2ull * first * j.nx, hi = 2ull * (first + rows) * j.nx;
+      for (uint64_t k = lo; k < hi; k += 2) half = std::max(half, std::hypot(j.offsets[k], j.offsets[k + 1]));
+    }
+    double dc = ext ? j.h_m * half : h * half;
+    int64_t e = ext ? j.h_e : 0;
+    bool over = e == o.bla.dc_exp ? dc > o.bla.dc_max
+                                  : std::log2(dc) + (double)e > std::log2(o.bla.dc_max) + (double)o.bla.dc_exp;
+    if (std::isnan(dc) || over) return fail(ctx, FDC_INVALID, "view reaches |dc| beyond the BLA table's dc_max");
+  }
+  p.orbit = o.z;
+  p.last = (uint32_t)(o.len - 1);
+  p.z0r = o.z0r;
+  p.z0i = o.z0i;
+  if (bla) {
+    p.fused = (const double2 *)o.bla.fused;
+    p.bla_r2 = o.bla.r2;
+    p.bla_coef = o.bla.coef;
+    p.bla_ab = o.bla.ab;
+    p.bla_levels = o.bla.levels;
+    std::memcpy(p.bla_off, o.bla.off, sizeof p.bla_off);
+    std::memcpy(p.bla_count, o.bla.count, sizeof p.bla_count);
+  }
+  p.nx = j.nx;
+  p.ny = j.ny;
+  p.first_row = first;
+  p.rows = rows;
+  p.tiles_x = (j.nx + 7) / 8;
+  p.tier = j.tier;
+  p.flags = (deriv ? fdk::F_DERIV : 0) | (bla ? fdk::F_BLA : 0) | ((j.flags & FDC_SHIFT) ? fdk::F_SHIFT : 0);
+  p.c_re = j.c_re;
+  p.c_im = j.c_im;
+  p.h = h;
+  p.h_m = j.h_m;
+  p.h_e = j.h_e;
+  p.cosr = j.cos_rot;
+  p.sinr = j.sin_rot;
+  p.half_x = (double)j.nx / 2.0;
+  p.half_y = (double)j.ny / 2.0;
+  p.max_iter = j.max_iter;
+  p.r2 = j.escape_radius * j.escape_radius;
+  p.nucleus = j.nucleus_period;
+  p.px_m = j.h_m * (double)j.ss;
+  p.px_e = j.h_e;
+  p.total = (uint64_t)p.tiles_x * ((rows + 3) / 4) * 32;
+  p.deadline_ns = j.deadline_ms > 0 ? (uint64_t)(j.deadline_ms * 1e6) : 0;
+  p.out_base = (uint64_t)first * j.nx;
+
+  p.orbit32 = o.z32;
   return FDC_OK;
 }
 
@@ -304,83 +437,16 @@ fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counte
   if (it == ctx->orbits.end()) return fail(ctx, FDC_INVALID, "unknown orbit handle");
   const OrbitDev &o = it->second;
   const fdc_job &j = *job;
-  if (j.nx == 0 || j.ny == 0) return fail(ctx, FDC_INVALID, "empty sample grid");
-  if (j.ss == 0 || j.nx % j.ss || j.ny % j.ss) return fail(ctx, FDC_INVALID, "grid must be a whole number of pixels");
-  if ((uint64_t)j.nx * j.ny >= (1ull << 31)) return fail(ctx, FDC_INVALID, "grid larger than 2^31 samples");
-  if (j.tier < 0 || j.tier > 2) return fail(ctx, FDC_INVALID, "unknown tier");
-  if (j.max_iter >= (1ull << 32)) return fail(ctx, FDC_INVALID, "max_iter must be below 2^32");
-  if (!(j.escape_radius > 0.0) || !std::isfinite(j.escape_radius * j.escape_radius))
-    return fail(ctx, FDC_INVALID, "escape radius must be positive and its square finite");
-  if (!(j.h_m >= 1.0 && j.h_m < 2.0)) return fail(ctx, FDC_INVALID, "h_m must lie in [1, 2)");
-  uint32_t first = j.first_row, rows = j.rows ? j.rows : j.ny - j.first_row;
-  if (first >= j.ny || rows > j.ny - first) return fail(ctx, FDC_INVALID, "row range outside the grid");
+  fdk::Params p{};
+  uint32_t first = 0, rows = 0;
+  fdc_status ps = prepare(ctx, o, j, p, first, rows);
+  if (ps != FDC_OK) return ps;
   const bool ext = j.tier == FDC_TIER_SCALED;
-  // The scaled tier's exact-range step from Z_0 continues at Z_1 (sample.rs:430-447),
-  // which needs a next point after it.
-  if (ext && o.len < 3) return fail(ctx, FDC_INVALID, "the scaled tier needs an orbit of at least 3 points");
   const bool bla = (j.flags & FDC_BLA) != 0;
   const bool deriv = (j.flags & FDC_DERIVATIVE) != 0;
-  double h = j.h_m * fdroute::exp2i(j.h_e);
-  if (bla) {
-    if (!o.has_bla) return fail(ctx, FDC_INVALID, "FDC_BLA without an uploaded BLA table");
-    // grid.rs:392-411
-    if (j.escape_radius < 4.0)
-      return fail(ctx, FDC_INVALID, "escape radius is below 4: BLA blocks may only skip iterates with |z| <= 2 (1 + 2 eps)");
-    // Largest unit offset: the grid's corner (grid.rs:428-444), or the supplied offsets'.
-    double half = std::hypot((double)j.nx / 2.0, (double)j.ny / 2.0);
-    if (j.offsets) {
-      half = 0.0;
-      const uint64_t lo = 2ull * first * j.nx, hi = 2ull * (first + rows) * j.nx;
-      for (uint64_t k = lo; k < hi; k += 2) half = std::max(half, std::hypot(j.offsets[k], j.offsets[k + 1]));
-    }
-    double dc = ext ? j.h_m * half : h * half;
-    int64_t e = ext ? j.h_e : 0;
-    bool over = e == o.bla.dc_exp ? dc > o.bla.dc_max
-                                  : std::log2(dc) + (double)e > std::log2(o.bla.dc_max) + (double)o.bla.dc_exp;
-    if (std::isnan(dc) || over) return fail(ctx, FDC_INVALID, "view reaches |dc| beyond the BLA table's dc_max");
-  }
   CK(cudaSetDevice(ctx->device));
   const uint64_t n_rows = (uint64_t)rows * j.nx;
   const bool dev_out = (j.flags & FDC_DEVICE_OUT) != 0;
-
-  fdk::Params p{};
-  p.orbit = o.z;
-  p.last = (uint32_t)(o.len - 1);
-  p.z0r = o.z0r;
-  p.z0i = o.z0i;
-  if (bla) {
-    p.fused = (const double2 *)o.bla.fused;
-    p.bla_r2 = o.bla.r2;
-    p.bla_coef = o.bla.coef;
-    p.bla_ab = o.bla.ab;
-    p.bla_levels = o.bla.levels;
-    std::memcpy(p.bla_off, o.bla.off, sizeof p.bla_off);
-    std::memcpy(p.bla_count, o.bla.count, sizeof p.bla_count);
-  }
-  p.nx = j.nx;
-  p.ny = j.ny;
-  p.first_row = first;
-  p.rows = rows;
-  p.tiles_x = (j.nx + 7) / 8;
-  p.tier = j.tier;
-  p.flags = (deriv ? fdk::F_DERIV : 0) | (bla ? fdk::F_BLA : 0) | ((j.flags & FDC_SHIFT) ? fdk::F_SHIFT : 0);
-  p.c_re = j.c_re;
-  p.c_im = j.c_im;
-  p.h = h;
-  p.h_m = j.h_m;
-  p.h_e = j.h_e;
-  p.cosr = j.cos_rot;
-  p.sinr = j.sin_rot;
-  p.half_x = (double)j.nx / 2.0;
-  p.half_y = (double)j.ny / 2.0;
-  p.max_iter = j.max_iter;
-  p.r2 = j.escape_radius * j.escape_radius;
-  p.nucleus = j.nucleus_period;
-  p.px_m = j.h_m * (double)j.ss;
-  p.px_e = j.h_e;
-  p.total = (uint64_t)p.tiles_x * ((rows + 3) / 4) * 32;
-  p.deadline_ns = j.deadline_ms > 0 ? (uint64_t)(j.deadline_ms * 1e6) : 0;
-  p.out_base = (uint64_t)first * j.nx;
 
   // Device buffers: caller's (FDC_DEVICE_OUT) or staging for the rendered rows.
   struct Col {
@@ -482,6 +548,171 @@ fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counte
   }
   if (sc.timed_out) return fail(ctx, FDC_TIMEOUT, "deadline passed; unfinished samples have status 0");
   return FDC_OK;
+}
+
+fdc_status fdc_batch_create(fdc_ctx *ctx, const fdc_job *jobs, const fdc_out *outs, uint32_t njobs,
+                            fdc_batch **out) {
+  if (!ctx || !jobs || !outs || !out || njobs == 0) return fail(ctx, FDC_INVALID, "null argument or empty batch");
+  *out = nullptr;
+  CK(cudaSetDevice(ctx->device));
+  std::vector<fdk::Params> params(njobs);
+  std::vector<int> key(njobs);
+  for (uint32_t k = 0; k < njobs; ++k) {
+    const fdc_job &j = jobs[k];
+    auto it = ctx->orbits.find(j.orbit);
+    if (it == ctx->orbits.end()) return fail(ctx, FDC_INVALID, "job " + std::to_string(k) + ": unknown orbit handle");
+    if (!(j.flags & FDC_DEVICE_OUT)) return fail(ctx, FDC_INVALID, "batch jobs write device outputs (FDC_DEVICE_OUT)");
+    if (j.mask || j.offsets || j.deadline_ms > 0)
+      return fail(ctx, FDC_INVALID, "batch jobs take no mask, offsets or deadline");
+    uint32_t first = 0, rows = 0;
+    fdc_status st = prepare(ctx, it->second, j, params[k], first, rows);
+    if (st != FDC_OK) {
+      ctx->err = "job " + std::to_string(k) + ": " + ctx->err;
+      return st;
+    }
+    fdk::Params &p = params[k];
+    const fdc_out &o = outs[k];
+    const uint64_t b0 = p.out_base;
+    p.cls = o.cls ? o.cls + b0 : nullptr;
+    p.n_out = o.n ? o.n + b0 : nullptr;
+    p.nu = o.nu ? o.nu + b0 : nullptr;
+    p.de = o.de ? o.de + b0 : nullptr;
+    p.normal = o.normal ? o.normal + b0 : nullptr;
+    p.z_out = o.z ? (double2 *)o.z + b0 : nullptr;
+    p.dz_out = o.dz ? (double2 *)o.dz + b0 : nullptr;
+    p.dexp_out = o.dexp ? o.dexp + b0 : nullptr;
+    p.status = o.status ? o.status + b0 : nullptr;
+    key[k] = ((j.flags & FDC_F32) ? 8 : 0) | (j.tier == FDC_TIER_SCALED ? 4 : 0) |
+             ((j.flags & FDC_DERIVATIVE) ? 2 : 0) | ((j.flags & FDC_BLA) ? 1 : 0);
+  }
+  fdc_batch *b = new fdc_batch;
+  b->njobs = njobs;
+  // group by kernel variant; within a group the deepest jobs first (their samples run
+  // longest, so starting them first shortens the tail of the launch)
+  std::map<int, std::vector<uint32_t>> by;
+  for (uint32_t k = 0; k < njobs; ++k) by[key[k]].push_back(k);
+  uint32_t base = 0;
+  auto bail = [&](fdc_status st) {
+    free_batch(b);
+    return st;
+  };
+  for (auto &kv : by) {
+    fdc_batch::Group g;
+    g.f32 = kv.first & 8;
+    g.ext = kv.first & 4;
+    g.deriv = kv.first & 2;
+    g.bla = kv.first & 1;
+    g.order = kv.second;
+    std::stable_sort(g.order.begin(), g.order.end(),
+                     [&](uint32_t a, uint32_t c) { return jobs[a].h_e < jobs[c].h_e; });
+    std::vector<fdk::Params> gp;
+    std::vector<unsigned long long> starts;
+    unsigned long long total = 0;
+    for (uint32_t k : g.order) {
+      starts.push_back(total);
+      gp.push_back(params[k]);
+      total += params[k].total;
+    }
+    starts.push_back(total);
+    g.total = total;
+    g.counter_base = base;
+    base += (uint32_t)g.order.size();
+    if (cudaMalloc(&g.jobs, gp.size() * sizeof(fdk::Params)) != cudaSuccess ||
+        cudaMalloc(&g.starts, starts.size() * sizeof(unsigned long long)) != cudaSuccess) {
+      b->groups.push_back(g);
+      return bail(fail(ctx, FDC_DEVICE_ERROR, "cudaMalloc for batch jobs failed"));
+    }
+    b->groups.push_back(g);
+    if (cudaMemcpy(g.jobs, gp.data(), gp.size() * sizeof(fdk::Params), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(g.starts, starts.data(), starts.size() * sizeof(unsigned long long), cudaMemcpyHostToDevice) !=
+            cudaSuccess)
+      return bail(fail(ctx, FDC_DEVICE_ERROR, "copying batch jobs failed"));
+  }
+  if (cudaMalloc(&b->counters, njobs * sizeof(fdk::Counters)) != cudaSuccess ||
+      cudaMalloc(&b->queues, b->groups.size() * sizeof(unsigned long long)) != cudaSuccess)
+    return bail(fail(ctx, FDC_DEVICE_ERROR, "cudaMalloc for batch scratch failed"));
+  // occupancy outside the capture
+  for (auto &g : b->groups) {
+    if (g.f32) continue;
+    int variant = 0;
+    void *fn = pick_batch_kernel(g.ext, g.deriv, g.bla, variant);
+    if (!ctx->blocks_per_sm_batch[variant]) {
+      int occ = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, 128, 0) != cudaSuccess)
+        return bail(fail(ctx, FDC_DEVICE_ERROR, "occupancy query failed"));
+      ctx->blocks_per_sm_batch[variant] = occ > 0 ? occ : 1;
+    }
+  }
+  // capture one run: clear queues and counters, one persistent launch per group
+  cudaError_t e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) e = cudaMemsetAsync(b->counters, 0, njobs * sizeof(fdk::Counters), ctx->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(b->queues, 0, b->groups.size() * sizeof(unsigned long long), ctx->stream);
+  for (size_t gi = 0; gi < b->groups.size() && e == cudaSuccess; ++gi) {
+    auto &g = b->groups[gi];
+    unsigned long long *q = b->queues + gi;
+    fdk::Counters *c = b->counters + g.counter_base;
+    uint32_t n = (uint32_t)g.order.size();
+    if (g.f32) {
+      e = fdk::launch_f32_batch(g.jobs, g.starts, n, g.total, q, c, g.deriv, g.bla, ctx->sm_count, ctx->stream,
+                                ctx->blocks_per_sm_batch_f32);
+    } else {
+      int variant = 0;
+      void *fn = pick_batch_kernel(g.ext, g.deriv, g.bla, variant);
+      void *args[] = {&g.jobs, &g.starts, &n, &g.total, &q, &c};
+      e = cudaLaunchKernel(fn, dim3(ctx->sm_count * ctx->blocks_per_sm_batch[variant]), dim3(128), args, 0,
+                           ctx->stream);
+    }
+  }
+  cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &b->graph);
+  if (e == cudaSuccess) e = e2;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, b->graph, 0);
+  if (e != cudaSuccess) return bail(fail(ctx, FDC_DEVICE_ERROR, std::string("batch graph: ") + cudaGetErrorString(e)));
+  *out = b;
+  return FDC_OK;
+}
+
+fdc_status fdc_batch_run(fdc_ctx *ctx, fdc_batch *b, fdc_counters *total, fdc_counters *per_job) {
+  if (!ctx || !b) return fail(ctx, FDC_INVALID, "null argument");
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaEventRecord(ctx->ev0, ctx->stream));
+  CK(cudaGraphLaunch(b->exec, ctx->stream));
+  CK(cudaEventRecord(ctx->ev1, ctx->stream));
+  std::vector<fdk::Counters> c(b->njobs);
+  CK(cudaMemcpyAsync(c.data(), b->counters, b->njobs * sizeof(fdk::Counters), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1));
+  fdc_counters sum{};
+  for (auto &g : b->groups)
+    for (size_t pos = 0; pos < g.order.size(); ++pos) {
+      const fdk::Counters &k = c[g.counter_base + pos];
+      fdc_counters one{};
+      one.samples = k.samples;
+      one.iterations = k.iterations;
+      one.blocks = k.blocks;
+      one.skipped = k.skipped;
+      one.fallback_samples = k.fallback;
+      one.closed_form_samples = k.closed;
+      if (per_job) per_job[g.order[pos]] = one;
+      sum.samples += one.samples;
+      sum.iterations += one.iterations;
+      sum.blocks += one.blocks;
+      sum.skipped += one.skipped;
+      sum.fallback_samples += one.fallback_samples;
+      sum.closed_form_samples += one.closed_form_samples;
+    }
+  sum.kernel_ms = ms;
+  sum.launches = (uint32_t)b->groups.size();
+  if (total) *total = sum;
+  return FDC_OK;
+}
+
+void fdc_batch_free(fdc_ctx *ctx, fdc_batch *b) {
+  if (ctx) {
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+  }
+  free_batch(b);
 }
 
 }  // extern "C"

@@ -532,6 +532,39 @@ int fdh_bla_build(const double *re, const double *im, uint64_t len, double eps, 
   return 0;
 }
 
+void fdh_encode(const fdh_plane *plane, uint32_t ss, uint64_t count, const uint8_t *cls, const uint32_t *n,
+                const double *z, const double *dz, const int64_t *dexp, double *nu, float *de, uint16_t *normal,
+                int threads) {
+  const double LN_2 = 0.693147180559945309417232121458176568;
+  const double TAU = 6.28318530717958647692528676655900577;
+  const double px_m = plane->h_m * (double)ss;
+  const int64_t px_e = plane->h_e;
+  if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+  parallel_for(count, threads, [&](uint64_t a, uint64_t b) {
+    for (uint64_t k = a; k < b; ++k) {
+      if (cls[k] & 3) continue;  // escaped samples only (store.rs:67-85)
+      double zr = z[2 * k], zi = z[2 * k + 1], dr = dz[2 * k], di = dz[2 * k + 1];
+      double z2 = zr * zr + zi * zi;
+      double log2z = 0.5 * std::log2(z2);
+      if (nu) nu[k] = (double)n[k] + 1.0 - std::log2(log2z);
+      if (de) {
+        double lnz = log2z * LN_2;
+        double base = 2.0 * std::sqrt(z2) * lnz / (std::hypot(dr, di) * px_m);
+        int64_t kk = -(dexp[k] + px_e);
+        kk = std::max<int64_t>(-4000, std::min<int64_t>(4000, kk));
+        de[k] = (float)(base * exp2i(kk / 2) * exp2i(kk - kk / 2));
+      }
+      if (normal) {
+        double re = zr * dr + zi * di, im = zi * dr - zr * di;
+        double x = plane->cos_rot * re + plane->sin_rot * im, y = plane->sin_rot * re - plane->cos_rot * im;
+        double t = std::round(std::atan2(y, x) * (65536.0 / TAU));
+        int64_t v = std::isnan(t) ? 0 : (int64_t)t;
+        normal[k] = (uint16_t)(uint64_t)v;
+      }
+    }
+  });
+}
+
 void fdh_dc_bound(const fdh_plane *plane, int32_t tier, uint32_t nx, uint32_t ny, double *dc, int64_t *e) {
   // grid.rs:428-444
   double half = std::hypot((double)nx / 2.0, (double)ny / 2.0);

@@ -390,7 +390,7 @@ __device__ __forceinline__ int init_f32(const Params &p, uint64_t slot, StateF &
 }
 
 template <bool D, bool L>
-__global__ void __launch_bounds__(128) perturb_f32_kernel(Params p, const Entry32 *__restrict__ orbit) {
+__global__ void __launch_bounds__(128, FDK_MIN_BLOCKS) perturb_f32_kernel(Params p, const Entry32 *__restrict__ orbit) {
   const unsigned FULL = 0xffffffffu;
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lt = (1u << lane) - 1u;
@@ -470,6 +470,77 @@ __global__ void __launch_bounds__(128) perturb_f32_kernel(Params p, const Entry3
       atomicAdd(&p.counters->closed, closed);
     }
   }
+}
+
+}  // namespace fdk
+
+namespace fdk {
+
+// Batch form of the precision kernel (see perturb_batch_kernel).
+template <bool D, bool L>
+__global__ void __launch_bounds__(128, FDK_MIN_BLOCKS)
+    perturb_f32_batch_kernel(const Params *__restrict__ jobs, const unsigned long long *__restrict__ starts,
+                             uint32_t njobs, unsigned long long total, unsigned long long *queue, Counters *per_job) {
+  const unsigned FULL = 0xffffffffu;
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned lt = (1u << lane) - 1u;
+  StateF s;
+  Result res;
+  bool active = false, exhausted = false;
+  uint32_t job = 0, counted = 0xffffffffu;
+  LaneCounters lc;
+  lc.clear();
+  auto finish = [&](const Params &p, uint32_t idx, const Result &r, uint64_t nblocks, uint64_t nskipped) {
+    put(p, idx, r);
+    if (counted != job) {
+      if (counted != 0xffffffffu) lc.flush(per_job + counted);
+      counted = job;
+    }
+    uint64_t spent = r.kind == 2 ? p.max_iter : r.n;
+    if (L) {
+      spent = spent - nskipped + nblocks;
+      lc.blocks += nblocks;
+      lc.skipped += nskipped;
+      bool cf = r.kind == 1 && r.n == 0;
+      lc.closed += cf;
+      lc.fallback += (nblocks == 0 && !cf);
+    }
+    lc.iterations += spent;
+    lc.samples += 1;
+  };
+  for (;;) {
+    unsigned need = __ballot_sync(FULL, !active);
+    while (need && !exhausted) {
+      unsigned long long base = 0;
+      int leader = __ffs((int)need) - 1;
+      if ((int)lane == leader) base = atomicAdd(queue, (unsigned long long)__popc(need));
+      base = __shfl_sync(FULL, base, leader);
+      if (base >= total) {
+        exhausted = true;
+        break;
+      }
+      if (!active) {
+        unsigned long long slot = base + __popc(need & lt);
+        if (slot < total) {
+          job = job_of(starts, njobs, slot);
+          const Params &p = jobs[job];
+          int got = init_f32<D, L>(p, slot - __ldg(starts + job), s, res);
+          if (got == 1) active = true;
+          else if (got == 2) finish(p, s.idx, res, 0, 0);
+        }
+      }
+      need = __ballot_sync(FULL, !active);
+    }
+    if (!__any_sync(FULL, active)) break;
+    if (active) {
+      const Params &p = jobs[job];
+      if (step_f32<D, L>(p, (const Entry32 *)p.orbit32, s, res)) {
+        finish(p, s.idx, res, s.blocks, s.skipped);
+        active = false;
+      }
+    }
+  }
+  if (counted != 0xffffffffu) lc.flush(per_job + counted);
 }
 
 }  // namespace fdk

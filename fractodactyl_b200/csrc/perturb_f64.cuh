@@ -12,6 +12,12 @@ namespace fdk {
 
 constexpr int MAX_LEVELS = 40;
 
+// Resident 128-thread blocks per SM the kernels are compiled for (caps registers at
+// 65536 / (128 * FDK_MIN_BLOCKS)); chosen by measurement.
+#ifndef FDK_MIN_BLOCKS
+#define FDK_MIN_BLOCKS 1
+#endif
+
 struct Counters {
   unsigned long long samples, iterations, blocks, skipped, fallback, closed;
   unsigned long long shift_bits;  // max of the non-negative shift estimates, as bits
@@ -25,6 +31,7 @@ struct Params {
   // starting at m, or -1 where none starts there: 32-byte entries (zr, zi, r2a, r2b), so the
   // first two levels of Bla::find come with the orbit point each step loads anyway.
   const double2 *__restrict__ fused;
+  const void *orbit32;  // precision-form entries (perturb_f32.cuh), per job in batches
   uint32_t last;
   double z0r, z0i;
   // BLA, level-major: r2[off + t], coef[2 (off + t)] = (a.re, a.im), (b.re, b.im), ab = (alpha, beta)
@@ -540,7 +547,7 @@ __device__ __forceinline__ void put(const Params &p, uint32_t sample, const Resu
 }
 
 template <bool EXT, bool D, bool L>
-__global__ void __launch_bounds__(128) perturb_kernel(Params p) {
+__global__ void __launch_bounds__(128, FDK_MIN_BLOCKS) perturb_kernel(Params p) {
   const unsigned FULL = 0xffffffffu;
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lt = (1u << lane) - 1u;
@@ -628,6 +635,106 @@ __global__ void __launch_bounds__(128) perturb_kernel(Params p) {
       if (shift > 0.0 && !isnan(shift)) atomicMax(&p.counters->shift_bits, (unsigned long long)__double_as_longlong(shift));
     }
   }
+}
+
+}  // namespace fdk
+
+namespace fdk {
+
+// Batches: many jobs (frames, tiles, locations) in one persistent launch. Job j owns
+// queue slots [starts[j], starts[j+1]); a lane takes a slot, finds its job by binary
+// search, and runs the same init/step/put as the single-job kernel on that job's Params
+// (read from global memory), so results equal fdc_render's bit for bit. Counters are
+// kept per job, flushed with atomics when a lane moves to another job.
+__device__ __forceinline__ uint32_t job_of(const unsigned long long *__restrict__ starts, uint32_t njobs,
+                                           unsigned long long slot) {
+  uint32_t lo = 0, hi = njobs;  // starts[lo] <= slot < starts[hi]
+  while (hi - lo > 1) {
+    uint32_t mid = (lo + hi) >> 1;
+    if (__ldg(starts + mid) <= slot) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
+struct LaneCounters {
+  unsigned long long samples, iterations, blocks, skipped, fallback, closed;
+  __device__ __forceinline__ void clear() { samples = iterations = blocks = skipped = fallback = closed = 0; }
+  __device__ __forceinline__ void flush(Counters *c) {
+    if (samples) atomicAdd(&c->samples, samples);
+    if (iterations) atomicAdd(&c->iterations, iterations);
+    if (blocks) atomicAdd(&c->blocks, blocks);
+    if (skipped) atomicAdd(&c->skipped, skipped);
+    if (fallback) atomicAdd(&c->fallback, fallback);
+    if (closed) atomicAdd(&c->closed, closed);
+    clear();
+  }
+};
+
+template <bool EXT, bool D, bool L>
+__global__ void __launch_bounds__(128, FDK_MIN_BLOCKS)
+    perturb_batch_kernel(const Params *__restrict__ jobs, const unsigned long long *__restrict__ starts,
+                         uint32_t njobs, unsigned long long total, unsigned long long *queue, Counters *per_job) {
+  const unsigned FULL = 0xffffffffu;
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned lt = (1u << lane) - 1u;
+  State<EXT> s;
+  Result res;
+  bool active = false, exhausted = false;
+  uint32_t job = 0, counted = 0xffffffffu;
+  LaneCounters lc;
+  lc.clear();
+  auto finish = [&](const Params &p, uint32_t idx, const Result &r, uint64_t nblocks, uint64_t nskipped) {
+    put(p, idx, r);
+    if (counted != job) {
+      if (counted != 0xffffffffu) lc.flush(per_job + counted);
+      counted = job;
+    }
+    uint64_t spent = r.kind == 2 ? p.max_iter : r.n;
+    if (L) {
+      spent = spent - nskipped + nblocks;
+      lc.blocks += nblocks;
+      lc.skipped += nskipped;
+      bool cf = r.kind == 1 && r.n == 0;
+      lc.closed += cf;
+      lc.fallback += (nblocks == 0 && !cf);
+    }
+    lc.iterations += spent;
+    lc.samples += 1;
+  };
+  for (;;) {
+    unsigned need = __ballot_sync(FULL, !active);
+    while (need && !exhausted) {
+      unsigned long long base = 0;
+      int leader = __ffs((int)need) - 1;
+      if ((int)lane == leader) base = atomicAdd(queue, (unsigned long long)__popc(need));
+      base = __shfl_sync(FULL, base, leader);
+      if (base >= total) {
+        exhausted = true;
+        break;
+      }
+      if (!active) {
+        unsigned long long slot = base + __popc(need & lt);
+        if (slot < total) {
+          job = job_of(starts, njobs, slot);
+          const Params &p = jobs[job];
+          int got = init<EXT, D, L>(p, slot - __ldg(starts + job), s, res);
+          if (got == 1) active = true;
+          else if (got == 2) finish(p, s.idx, res, 0, 0);
+        }
+      }
+      need = __ballot_sync(FULL, !active);
+    }
+    if (!__any_sync(FULL, active)) break;
+    if (active) {
+      const Params &p = jobs[job];
+      if (step<EXT, D, L>(p, s, res)) {
+        finish(p, s.idx, res, s.blocks, s.skipped);
+        active = false;
+      }
+    }
+  }
+  if (counted != 0xffffffffu) lc.flush(per_job + counted);
 }
 
 }  // namespace fdk

@@ -362,8 +362,21 @@ def make_job(plane: Plane, tier: int, p: Params, orbit: int, nucleus: Optional[i
     return j
 
 
+def encode_host(plane: Plane, ss: int, s: "Samples", columns=("nu", "de", "normal"), threads: int = 0):
+    """Columns of the escaped samples from the device's raw state, on the host with the
+    host's libm (fdh_encode = Store::put, store.rs:66-112): the CPU route's bytes."""
+    n = len(s.cls)
+    s.nu = np.zeros(n) if "nu" in columns else None
+    s.de = np.zeros(n, np.float32) if "de" in columns else None
+    s.normal = np.zeros(n, np.uint16) if "normal" in columns else None
+    ptr = lambda a: None if a is None else np.ascontiguousarray(a).ctypes.data
+    lib().fdh_encode(C.byref(plane._c()), ss, n, ptr(s.cls), ptr(s.n), ptr(s.z), ptr(s.dz), ptr(s.dexp),
+                     ptr(s.nu), ptr(s.de), ptr(s.normal), threads)
+    return s
+
+
 def render_with(view: View, p: Params, orbit=None, bla: Optional[Bla] = None, dev: Optional[Device] = None,
-                raw=False, shift=True, report: Optional[RouteReport] = None, quiet=True):
+                raw=False, shift=True, report: Optional[RouteReport] = None, quiet=True, host_encode=False):
     """fd_kernel::render_with / render_bla (grid.rs:106-208) on the CUDA route.
 
     Returns (Header, Samples, Stats, BlaStats or None). Refusals are the reference's
@@ -397,7 +410,8 @@ def render_with(view: View, p: Params, orbit=None, bla: Optional[Bla] = None, de
             flags |= _lib.SHIFT
         job = make_job(plane, tier, p, h, r.nucleus_period(), flags)
         g = time.perf_counter()
-        arrays, cnt, status = dev.render_job(job, raw=raw, columns=p.columns)
+        arrays, cnt, status = dev.render_job(job, raw=raw or host_encode,
+                                             columns=() if host_encode else p.columns)
         gpu_seconds = time.perf_counter() - g
     finally:
         dev.free(h)
@@ -407,6 +421,8 @@ def render_with(view: View, p: Params, orbit=None, bla: Optional[Bla] = None, de
     s = Samples(cls=arrays["cls"], nu=arrays.get("nu"), de=arrays.get("de"), normal=arrays.get("normal"),
                 n=arrays.get("n"), z=arrays.get("z"), dz=arrays.get("dz"), dexp=arrays.get("dexp"),
                 status=arrays.get("status"))
+    if host_encode:
+        encode_host(plane, p.ss, s, p.columns, p.threads)
     stats = Stats(len(r), reference_seconds, int(cnt.iterations))
     bstats = None
     if bla is not None:

@@ -120,6 +120,19 @@ fdc_status fdc_upload_bla(fdc_ctx *ctx, int32_t orbit, const double *blocks7, co
  * class and n bit-exact, z and dz bit-exact, nu/de/normal within CUDA libm's ulps. */
 fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counters *counters);
 
+/* Batches: many jobs (the frames of a zoom film, tiles of many locations, each job with
+ * its own orbit handle, tier and device outputs) rendered by ONE persistent launch per
+ * kernel variant from a single work queue over all jobs' tiles, deepest jobs first, the
+ * whole run captured once in a CUDA graph and replayed by fdc_batch_run. Results equal
+ * fdc_render's per job. Jobs need FDC_DEVICE_OUT, no mask/offsets/deadline; orbits and
+ * tables must stay uploaded while the batch exists. per_job (optional) has njobs
+ * entries; counters->kernel_ms is the device time of the whole replay. */
+typedef struct fdc_batch fdc_batch;
+fdc_status fdc_batch_create(fdc_ctx *ctx, const fdc_job *jobs, const fdc_out *outs, uint32_t njobs,
+                            fdc_batch **batch);
+fdc_status fdc_batch_run(fdc_ctx *ctx, fdc_batch *batch, fdc_counters *counters, fdc_counters *per_job);
+void fdc_batch_free(fdc_ctx *ctx, fdc_batch *batch);
+
 #ifdef __cplusplus
 }
 #endif

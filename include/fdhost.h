@@ -56,6 +56,16 @@ int fdh_bla_build(const double *re, const double *im, uint64_t len, double eps, 
 /* grid.rs:418-444: bound m 2^e on |dc| over a view's samples for a tier. */
 void fdh_dc_bound(const fdh_plane *plane, int32_t tier, uint32_t nx, uint32_t ny, double *dc, int64_t *e);
 
+/* Store::put for the escaped samples of a render (crates/fd-kernel/src/store.rs:66-112,
+ * Bound column absent): nu = n + 1 - log2(0.5 log2 |z|^2), de in output pixels
+ * (store.rs:141-150) and the screen normal (samples.rs:45-48) from the raw state the
+ * device returns (z, dz/dc = (dr, di) 2^dexp), evaluated with the host's libm as the
+ * reference's Rust is, so the columns are the CPU route's bytes. Samples whose class byte
+ * is not escaped (0) are left untouched; any output may be NULL. threads <= 0: all cores. */
+void fdh_encode(const fdh_plane *plane, uint32_t ss, uint64_t count, const uint8_t *cls, const uint32_t *n,
+                const double *z, const double *dz, const int64_t *dexp, double *nu, float *de, uint16_t *normal,
+                int threads);
+
 /* Location recipe of the benchmark frames (no reference API; the construction of
  * tools/research/twolevel/ref.py:31-117 around a Misiurewicz point):
  *   1. the repelling Misiurewicz point M(q, r), q <= 60, r <= 4, nearest the start (Newton

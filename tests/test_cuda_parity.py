@@ -275,3 +275,16 @@ def test_invalid_inputs_are_refused_not_crashed(dev):
         assert L.fdc_render(dev.h, C.byref(j), C.byref(out), C.byref(cnt)) == _lib.INVALID
     finally:
         dev.free(oh)
+
+
+@pytest.mark.parametrize("case", KATS["fnv_views"], ids=lambda c: c["width"])
+def test_route_reproduces_reference_fds_hashes(dev, case):
+    """End to end on the product side only: host orbit (fdh_orbit_*), CUDA kernel, host
+    encoder (fdh_encode) and .fds writer give the reference's FNV-1a hashes of these renders
+    (sample.rs:715-752), once the route's own kernel-id suffix is taken off."""
+    from fractodactyl_b200 import fds
+    view = fd.View(case["re"], case["im"], case["width"], 0.3)
+    p = fd.Params(8, 4, max_iter=5000, columns=("nu", "de", "normal"))
+    h, s, st, _ = fd.render_with(view, p, dev=dev, host_encode=True)
+    h.kernel = h.kernel.replace(" gpu-perturb-cuda/1", "")
+    assert fdref.fnv1a64(fds.encode(h, s, minor=0)) == int(case["fnv"], 16)

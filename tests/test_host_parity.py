@@ -130,3 +130,19 @@ def test_route_flag_and_declines():
         fd.render(fd.View("0", "1", "1e-3"), fd.Params(8, 8, columns=("nu", "bound")))
     with pytest.raises(ValueError):
         fd.route._setup(fd.View("0", "1", "1e-300"), fd.Params(8, 8, tier="f64"))
+
+
+@pytest.mark.parametrize("case", KATS["fnv_views"], ids=lambda c: c["width"])
+def test_fds_writer_and_host_encoder_bytes(case):
+    """fds.encode over the oracle's raw outcomes encoded by fdh_encode equals the oracle's
+    own .fds bytes (header.rs:62-81, write.rs:8-53, store.rs:66-112)."""
+    from fractodactyl_b200 import fds
+    job = fdref.make_job(case["re"], case["im"], case["width"], 8, 4, 5000, rotation=0.3, threads=1)
+    want = fdref.render_fds(job)
+    o = fdref.render(job, raw=True)
+    view = fd.View(case["re"], case["im"], case["width"], 0.3)
+    plane, tier = fd.route._setup(view, fd.Params(8, 4, max_iter=5000))
+    s = fd.Samples(cls=o["cls"], n=o["n"].astype(np.uint32), z=o["z"], dz=o["dz"], dexp=o["dexp"])
+    fd.route.encode_host(plane, 1, s)
+    h = fd.Header(("class", "nu", "de", "normal"), 8, 4, 1, 5000, 1e10, view, o["kernel"])
+    assert fds.encode(h, s) == want

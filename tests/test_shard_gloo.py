@@ -1,0 +1,73 @@
+"""Frame sharding over two ranks (gloo, CPU): each rank renders its interleaved stripes
+with the oracle standing in for the per-GPU renderer, the reduction rebuilds the frame
+exactly as one render of the whole frame."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+import fdref
+
+VIEW = ("-0.7453", "0.1127", "0.0065", 48, 30, 2000)
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, world, port, q):
+    import datetime
+
+    import torch.distributed as dist
+
+    from fractodactyl_b200 import shard
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        re_, im_, w, nx, ny, it = VIEW
+        job = fdref.make_job(re_, im_, w, nx, ny, it, threads=1)
+
+        def render_masked(mask):
+            o = fdref.render(job, raw=True)  # the oracle renders everything; keep this rank's rows
+            keep = mask.astype(bool)
+            cols = {k: np.where(keep, o[k], 0) for k in ("cls", "nu", "de", "normal")}
+            cols["n"] = np.where(keep, o["n"], 0)
+            return cols, {"samples": int(keep.sum()), "iterations": int(o["n"][keep].sum())}
+
+        frame, counters = shard.render_frame(nx, ny, render_masked)
+        q.put((rank, {k: v.tolist() for k, v in frame.items()}, counters))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_rank_frame_equals_single_render():
+    world, port = 2, _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    results = [q.get(timeout=120) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    re_, im_, w, nx, ny, it = VIEW
+    o = fdref.render(fdref.make_job(re_, im_, w, nx, ny, it, threads=1), raw=True)
+    for rank, frame, counters in results:
+        assert np.array_equal(np.array(frame["cls"], np.uint8), o["cls"])
+        assert np.array_equal(np.array(frame["n"], np.uint64), o["n"])
+        assert np.array_equal(np.array(frame["nu"]), o["nu"])
+        assert np.array_equal(np.array(frame["de"], np.float32), o["de"])
+        assert np.array_equal(np.array(frame["normal"], np.uint16), o["normal"])
+        assert counters["samples"] == nx * ny and counters["iterations"] == int(o["n"].sum())
+
+
+def test_masks_partition_the_frame():
+    from fractodactyl_b200 import shard
+    for world in (1, 2, 3, 8):
+        m = sum(shard.mask_for(17, 37, r, world).astype(int) for r in range(world))
+        assert np.all(m == 1)
