@@ -61,7 +61,7 @@ def build(verbose=False, force=False):
     objs.append(host_o)
     common = [nvcc(), ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",
               "-Xptxas", "-v" if verbose else "-O3"]
-    for src, fmad in (("fdcuda.cu", "false"), ("peaks.cu", "false"), ("perturb_f32.cu", "true")):
+    for src, fmad in (("fdcuda.cu", "false"), ("peaks.cu", "false"), ("perturb_f32.cu", "true"), ("noalloc.cu", "false")):
         path = os.path.join(CSRC, src)
         if not os.path.exists(path):
             continue

@@ -133,6 +133,30 @@ fdc_status fdc_batch_create(fdc_ctx *ctx, const fdc_job *jobs, const fdc_out *ou
 fdc_status fdc_batch_run(fdc_ctx *ctx, fdc_batch *batch, fdc_counters *counters, fdc_counters *per_job);
 void fdc_batch_free(fdc_ctx *ctx, fdc_batch *batch);
 
+/* Allocation-free rendering (no counterpart in the reference). For callers that cannot
+ * allocate device memory: a render service that owns all device memory through its own
+ * pool or arena (other allocations would fragment it or break its memory budget) and
+ * hands the library buffers carved from it. It renders the plain form (FP64,
+ * no BLA, no mask or offsets) with no context, no cudaMalloc, no cudaFree and no
+ * allocating library call: the caller passes the orbit (2*len doubles, interleaved
+ * re/im, Z_0 = 0) and every output column of `out` as DEVICE pointers, and the kernel's
+ * scratch (work-queue head, counters, per-row iteration sums) lives in one fixed device
+ * array of FDC_NOALLOC_SCRATCH_BYTES, which every GPU that loads the library holds until
+ * the process exits. That fixes the row limit: a job renders at most
+ * (FDC_NOALLOC_SCRATCH_BYTES - 256) / 8 = 8160 rows per call (job->rows, or ny when 0);
+ * larger jobs are refused with FDC_INVALID and a message naming the limit. The first
+ * call on a device looks up the array's device address (once per device); make that
+ * first call before any stream capture. Every call shares the array and clears what it
+ * uses before its kernel runs: calls that overlap on the GPU (other streams, other host
+ * threads) race on it, so serialise them. row_iterations (optional, host, `rows`
+ * entries) receives the iterations spent per rendered row; counters (optional) the
+ * sample and iteration totals. Both readbacks synchronise `stream` (NULL: the default
+ * stream). Errors: the status, and a message in `error` (cap bytes, optional). */
+#define FDC_NOALLOC_SCRATCH_BYTES 65536
+fdc_status fdc_render_noalloc(int device, const double *orbit, uint64_t len, const fdc_job *job, const fdc_out *out,
+                              uint64_t *row_iterations, fdc_counters *counters, void *stream, char *error,
+                              size_t error_cap);
+
 #ifdef __cplusplus
 }
 #endif
