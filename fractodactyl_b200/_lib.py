@@ -72,10 +72,16 @@ class Plane(C.Structure):
     ]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("defer", C.c_uint32), ("blocks_per_sm", C.c_uint32), ("tile_w", C.c_uint32)]
+
+
+DEFAULT_DEFER = 0  # FDC_DEFAULT_DEFER: each kernel variant's measured default
+
 # Every symbol the headers declare, for the export check.
 FDC_SYMBOLS = ["fdc_abi_version", "fdc_open", "fdc_close", "fdc_last_error", "fdc_upload_orbit", "fdc_free_orbit",
                "fdc_upload_bla", "fdc_render", "fdc_batch_create", "fdc_batch_run", "fdc_batch_free",
-               "fdc_render_noalloc"]
+               "fdc_render_noalloc", "fdc_set_tuning", "fdc_get_tuning"]
 FDH_SYMBOLS = ["fdh_last_error", "fdh_plane_new", "fdh_orbit_fixed", "fdh_orbit_f64", "fdh_nucleus_period",
                "fdh_bla_build", "fdh_dc_bound", "fdh_encode", "fdh_location"]
 
@@ -103,6 +109,8 @@ def lib():
     L.fdc_batch_create.argtypes = [P, P, P, U32, C.POINTER(P)]
     L.fdc_batch_run.argtypes = [P, P, C.POINTER(Counters), P]
     L.fdc_batch_free.argtypes = [P, P]
+    L.fdc_set_tuning.argtypes = [P, C.POINTER(Tuning)]
+    L.fdc_get_tuning.argtypes = [P, C.POINTER(Tuning)]
     L.fdc_render_noalloc.argtypes = [C.c_int, P, U64, C.POINTER(Job), C.POINTER(Out), P, C.POINTER(Counters), P,
                                      C.c_char_p, C.c_size_t]
     L.fdh_last_error.restype = C.c_char_p

@@ -69,7 +69,22 @@ struct fdc_ctx {
   int blocks_per_sm_f32[4] = {};
   int blocks_per_sm_batch[8] = {};
   int blocks_per_sm_batch_f32[4] = {};
+  fdc_tuning tune{FDC_DEFAULT_DEFER, 0, 0};
 };
+
+// Persistent grid of a plain-form kernel: the occupancy limit, or fewer blocks per SM
+// when the tuning asks for fewer.
+// Lanes a warp gathers before applying BLA blocks (fdc_tuning.defer; 0: per variant).
+static uint32_t defer_for(const fdc_ctx *ctx, bool ext) {
+  if (ctx->tune.defer > 0) return ctx->tune.defer;
+  return ext ? 12u : 4u;
+}
+
+static int grid_blocks(const fdc_ctx *ctx, int occupancy) {
+  int b = occupancy;
+  if (ctx->tune.blocks_per_sm > 0 && (int)ctx->tune.blocks_per_sm < b) b = (int)ctx->tune.blocks_per_sm;
+  return ctx->sm_count * b;
+}
 
 // A prepared batch (include/fdcuda.h): jobs grouped by kernel variant, each group's Params
 // array and slot starts in device memory, per-job counters, and a CUDA graph of the
@@ -243,7 +258,8 @@ fdc_status prepare(fdc_ctx *ctx, const OrbitDev &o, const fdc_job &j, fdk::Param
   p.ny = j.ny;
   p.first_row = first;
   p.rows = rows;
-  p.tiles_x = (j.nx + 7) / 8;
+  p.tile_shift = ctx->tune.tile_w ? (uint32_t)__builtin_ctz(ctx->tune.tile_w) : 3u;
+  p.tiles_x = (j.nx + (1u << p.tile_shift) - 1) >> p.tile_shift;
   p.tier = j.tier;
   p.flags = (deriv ? fdk::F_DERIV : 0) | (bla ? fdk::F_BLA : 0) | ((j.flags & FDC_SHIFT) ? fdk::F_SHIFT : 0);
   p.c_re = j.c_re;
@@ -260,9 +276,11 @@ fdc_status prepare(fdc_ctx *ctx, const OrbitDev &o, const fdc_job &j, fdk::Param
   p.nucleus = j.nucleus_period;
   p.px_m = j.h_m * (double)j.ss;
   p.px_e = j.h_e;
-  p.total = (uint64_t)p.tiles_x * ((rows + 3) / 4) * 32;
+  const uint32_t tile_h = 32u >> p.tile_shift;
+  p.total = (uint64_t)p.tiles_x * ((rows + tile_h - 1) / tile_h) * 32;
   p.deadline_ns = j.deadline_ms > 0 ? (uint64_t)(j.deadline_ms * 1e6) : 0;
   p.out_base = (uint64_t)first * j.nx;
+  p.defer = defer_for(ctx, p.tier == FDC_TIER_SCALED);
 
   p.orbit32 = o.z32;
   return FDC_OK;
@@ -507,7 +525,8 @@ fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counte
 
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
   if (j.flags & FDC_F32) {
-    CK(fdk::launch_f32(p, o.z32, deriv, bla, ctx->sm_count, ctx->stream, ctx->blocks_per_sm_f32));
+    CK(fdk::launch_f32(p, o.z32, deriv, bla, ctx->sm_count, (int)ctx->tune.blocks_per_sm, ctx->stream,
+                       ctx->blocks_per_sm_f32));
   } else {
     int variant = 0;
     void *fn = pick_kernel(ext, deriv, bla, variant);
@@ -516,7 +535,7 @@ fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counte
       CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, 128, 0));
       ctx->blocks_per_sm[variant] = b > 0 ? b : 1;
     }
-    dim3 grid(ctx->sm_count * ctx->blocks_per_sm[variant]), block(128);
+    dim3 grid(grid_blocks(ctx, ctx->blocks_per_sm[variant])), block(128);
     void *args[] = {&p};
     CK(cudaLaunchKernel(fn, grid, block, args, 0, ctx->stream));
     CK(cudaGetLastError());
@@ -547,6 +566,22 @@ fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counte
     counters->launches = 1;
   }
   if (sc.timed_out) return fail(ctx, FDC_TIMEOUT, "deadline passed; unfinished samples have status 0");
+  return FDC_OK;
+}
+
+fdc_status fdc_set_tuning(fdc_ctx *ctx, const fdc_tuning *t) {
+  if (!ctx || !t) return fail(ctx, FDC_INVALID, "null argument");
+  if (t->defer > 32) return fail(ctx, FDC_INVALID, "defer must be in [0, 32]");
+  if (t->blocks_per_sm > 64) return fail(ctx, FDC_INVALID, "blocks_per_sm must be at most 64");
+  if (t->tile_w > 32 || (t->tile_w & (t->tile_w - 1)))
+    return fail(ctx, FDC_INVALID, "tile_w must be 0 or a power of two up to 32");
+  ctx->tune = *t;
+  return FDC_OK;
+}
+
+fdc_status fdc_get_tuning(const fdc_ctx *ctx, fdc_tuning *t) {
+  if (!ctx || !t) return FDC_INVALID;
+  *t = ctx->tune;
   return FDC_OK;
 }
 
@@ -653,13 +688,15 @@ fdc_status fdc_batch_create(fdc_ctx *ctx, const fdc_job *jobs, const fdc_out *ou
     fdk::Counters *c = b->counters + g.counter_base;
     uint32_t n = (uint32_t)g.order.size();
     if (g.f32) {
-      e = fdk::launch_f32_batch(g.jobs, g.starts, n, g.total, q, c, g.deriv, g.bla, ctx->sm_count, ctx->stream,
+      e = fdk::launch_f32_batch(g.jobs, g.starts, n, g.total, q, c, g.deriv, g.bla, ctx->sm_count,
+                                (int)ctx->tune.blocks_per_sm, defer_for(ctx, g.ext), ctx->stream,
                                 ctx->blocks_per_sm_batch_f32);
     } else {
       int variant = 0;
       void *fn = pick_batch_kernel(g.ext, g.deriv, g.bla, variant);
-      void *args[] = {&g.jobs, &g.starts, &n, &g.total, &q, &c};
-      e = cudaLaunchKernel(fn, dim3(ctx->sm_count * ctx->blocks_per_sm_batch[variant]), dim3(128), args, 0,
+      uint32_t defer = defer_for(ctx, g.ext);
+      void *args[] = {&g.jobs, &g.starts, &n, &g.total, &q, &c, &defer};
+      e = cudaLaunchKernel(fn, dim3(grid_blocks(ctx, ctx->blocks_per_sm_batch[variant])), dim3(128), args, 0,
                            ctx->stream);
     }
   }

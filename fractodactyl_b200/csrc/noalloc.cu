@@ -158,6 +158,7 @@ extern "C" fdc_status fdc_render_noalloc(int device, const double *orbit, uint64
   p.ny = j.ny;
   p.first_row = first;
   p.rows = rows;
+  p.tile_shift = 3;  // 8x4-sample tiles
   p.tiles_x = (j.nx + 7) / 8;
   p.tier = j.tier;
   p.flags = deriv ? fdk::F_DERIV : 0;

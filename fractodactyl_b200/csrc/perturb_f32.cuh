@@ -16,6 +16,11 @@
 
 namespace fdk {
 
+// Resident 128-thread blocks per SM the precision-form kernels are compiled for.
+#ifndef FDK_MIN_BLOCKS_F32
+#define FDK_MIN_BLOCKS_F32 5
+#endif
+
 // 32-byte orbit entry of the precision form: Z in f64, Z in f32 (NaN where |Z| < 2^-60),
 // the squared radius of the 2-step block starting at m (or -1).
 struct __align__(16) Entry32 {
@@ -65,7 +70,7 @@ struct StateF {
   double s64;          // 2^e in f64
   double ar, ai;       // dc = a 2^oe
   int oe;
-  double xr, xi;       // delta in f64 (physical), from the end of the previous iteration
+  double d2;           // |delta|^2 in f64 (physical), from the end of the previous iteration
   double fr, fi;       // z = Z_m + delta in f64
   double Zr, Zi, r2a;
   double dr, di, inverse;
@@ -73,6 +78,7 @@ struct StateF {
   MulF mu, ct;
   bool ct_started;
   uint32_t n, chk, sn, hold, m, idx, blocks, skipped;
+  uint32_t lim;  // relimit_f32()
   int nucleus;
   bool pending, predicted;
 };
@@ -99,113 +105,144 @@ __device__ __forceinline__ void set_delta(StateF &s, double re, double im, int64
 // Sum of two wide-exponent complex terms (as sum2, sample.rs:1094-1114).
 __device__ __forceinline__ Cx3 add3(Cx3 a, Cx3 b) { return sum2(a, b, a.e); }
 
+// delta = w 2^e as f64 (the physical delta of the FP64 steps): the f32 bits moved into
+// an f64 with the exponent e added, exact; subnormal, zero and non-finite w, and results
+// outside f64's normal range, take the conversion and a multiply by s64 = 2^e.
+__device__ __forceinline__ double phys(float w, int e, double s64) {
+  const uint32_t b = __float_as_uint(w);
+  const uint32_t ef = (b >> 23) & 0xffu;
+  const int E = (int)ef - 127 + e + 1023;
+  if (ef - 1u < 254u && E >= 1 && E <= 2046) {
+    const uint32_t hi = (b & 0x80000000u) | ((uint32_t)E << 20) | ((b & 0x7fffffu) >> 3);
+    return __hiloint2double((int)hi, (int)(b << 29));
+  }
+  return (double)w * s64;
+}
+
+// Bla::find's iteration limit with n left out (relimit of the plain form).
+__device__ __forceinline__ void relimit_f32(const Params &p, StateF &s) {
+  uint64_t cap = s.hold > 0 ? (uint64_t)s.sn + s.hold : (s.pending ? ~0ull : (uint64_t)s.chk);
+  uint64_t b = p.max_iter < cap ? p.max_iter : cap;
+  if (s.nucleus >= 0 && (uint64_t)s.nucleus + 1 < b) b = (uint64_t)s.nucleus + 1;
+  s.lim = (uint32_t)b;
+}
+
+// Bla::find on the FP64 |delta|^2 of the iteration's start (s.d2).
+__device__ __forceinline__ int find_block_f32(const Params &p, const StateF &s, uint32_t &at) {
+  if (!(s.nucleus < 0 || s.m != 0)) return -1;
+  const uint32_t budget = s.lim > s.n ? s.lim - s.n : 0u;
+  if (budget < 2 || !(s.d2 < s.r2a)) return -1;
+  const double d2 = s.d2;
+  const uint32_t k = s.m - 1u;
+  at = k >> 1;
+  const uint32_t tz = k == 0 ? 32u : (uint32_t)(__ffs((int)k) - 1);
+  const uint32_t top = tz < p.bla_levels ? tz : p.bla_levels;
+  constexpr uint32_t PRE = 4;  // levels 1..4
+  double r[PRE];
+  bool ok[PRE];
+#pragma unroll
+  for (uint32_t q = 0; q < PRE; ++q) {
+    const uint32_t i = 1 + q, a = k >> (i + 1);
+    ok[q] = i < top && (2u << i) <= budget && a < p.bla_count[i];
+    r[q] = ok[q] ? __ldg(p.bla_r2 + p.bla_off[i] + a) : -1.0;
+  }
+  int lv = 0;
+#pragma unroll
+  for (uint32_t q = 0; q < PRE; ++q) {
+    if (!ok[q] || !(d2 < r[q])) return lv;
+    lv = (int)(1 + q);
+    at = k >> (2 + q);
+  }
+  for (uint32_t i = 1 + PRE; i < top; ++i) {
+    if ((2ull << i) > budget) break;
+    const uint32_t a = k >> (i + 1);
+    if (a >= p.bla_count[i]) break;
+    if (!(d2 < __ldg(p.bla_r2 + p.bla_off[i] + a))) break;
+    lv = (int)i;
+    at = a;
+  }
+  return lv;
+}
+
+// delta' = A delta + B dc with wide exponents, dz' = A dz + B in FP64.
+template <bool D>
+__device__ __forceinline__ void apply_block_f32(const Params &p, StateF &s, int lv, uint32_t at) {
+  const uint32_t b = p.bla_off[lv] + at;
+  const double2 A = __ldg(p.bla_coef + 2 * b), B = __ldg(p.bla_coef + 2 * b + 1);
+  const uint32_t len = 2u << lv;
+  if (s.nucleus >= 0 && s.n >= 1) {
+    s.ct.multiply((float)A.x, (float)A.y);
+    s.ct_started = true;
+  }
+  if (s.hold > 0) s.mu.multiply((float)A.x, (float)A.y);
+  if (D) {
+    normalise(s.dr, s.di, s.dexp, INT64_MAX / 4);
+    s.inverse = exp2i(-s.dexp);
+    double t = A.x * s.dr - A.y * s.di + B.x * s.inverse;
+    s.di = A.x * s.di + A.y * s.dr + B.y * s.inverse;
+    s.dr = t;
+    normalise(s.dr, s.di, s.dexp, INT64_MAX / 4);
+    s.inverse = exp2i(-s.dexp);
+  }
+  const double wr = s.wr, wi = s.wi;
+  Cx3 ad{A.x * wr - A.y * wi, A.x * wi + A.y * wr, s.e};
+  Cx3 bd{B.x * s.ar - B.y * s.ai, B.x * s.ai + B.y * s.ar, s.oe};
+  Cx3 d = add3(ad, bd);
+  set_delta(s, d.re, d.im, d.e);
+  s.m += len;
+  s.n += len;
+  s.blocks += 1;
+  s.skipped += len;
+}
+
+// One ordinary step: FP64 derivative on z = Z_m + delta (carried in fr, fi), FP32 delta.
+template <bool D>
+__device__ __forceinline__ void plain_update_f32(StateF &s) {
+  if (s.nucleus >= 0 && s.n >= 1) {
+    s.ct.multiply((float)(2.0 * s.fr), (float)(2.0 * s.fi));
+    s.ct_started = true;
+  }
+  if (s.hold > 0) s.mu.multiply((float)(2.0 * s.fr), (float)(2.0 * s.fi));
+  if (D) {  // FP64 derivative (sample.rs:352-360)
+    double t = 2.0 * (s.fr * s.dr - s.fi * s.di) + s.inverse;
+    s.di = 2.0 * (s.fr * s.di + s.fi * s.dr);
+    s.dr = t;
+    if (fmax(fabs(s.dr), fabs(s.di)) > HI) {
+      s.dr = s.dr * LO;
+      s.di = s.di * LO;
+      s.dexp += 32;
+      s.inverse = exp2i(-s.dexp);
+    }
+  }
+  if (!isnan(s.zr32)) {
+    // FP32: w' = 2 Z w + 2^e w^2 + dc 2^-e
+    const float wr = s.wr, wi = s.wi;
+    const float zwr = s.zr32 * wr - s.zi32 * wi, zwi = s.zr32 * wi + s.zi32 * wr;
+    const float nwr = 2.0f * zwr + s.s32 * (wr * wr - wi * wi) + s.dcr;
+    const float nwi = 2.0f * zwi + s.s32 * (2.0f * wr * wi) + s.dci;
+    s.wr = nwr;
+    s.wi = nwi;
+    const float mag = fmaxf(fabsf(nwr), fabsf(nwi));
+    if (mag > 4294967296.0f || (mag < 2.3283064e-10f && s.e > s.oe - 64)) set_delta(s, nwr, nwi, s.e);
+  } else {
+    // exact step at a tiny Z_m: 2 Z delta + delta^2 + dc with wide exponents
+    const double wr = s.wr, wi = s.wi;
+    Cx3 zd{2.0 * (s.Zr * wr - s.Zi * wi), 2.0 * (s.Zr * wi + s.Zi * wr), s.e};
+    Cx3 dd{wr * wr - wi * wi, 2.0 * wr * wi, 2 * (int64_t)s.e};
+    Cx3 a{s.ar, s.ai, s.oe};
+    Cx3 t = add3(add3(zd, dd), a);
+    set_delta(s, t.re, t.im, t.e);
+  }
+  s.m += 1;
+  s.n += 1;
+}
+
+// After the update: next entry, FP64 bailout and rebase test, FP32 periodicity. nz/nr
+// hold the entry m + 1 prefetched at the iteration's start (after a plain step); after a
+// block (took) the entry at the new m is loaded here.
 template <bool D, bool L>
-__device__ __forceinline__ bool step_f32(const Params &p, const Entry32 *__restrict__ orbit, StateF &s,
-                                         Result &res) {
-  if (s.n >= p.max_iter) {
-    res.kind = 2;
-    return true;
-  }
-  // speculative load of the next entry (m < last at the top of every iteration)
-  const double2 *e2 = reinterpret_cast<const double2 *>(orbit + s.m + 1);
-  double2 nz = __ldg(e2), nr = __ldg(e2 + 1);
-  bool took = false;
-  if (L && (s.nucleus < 0 || s.m != 0)) {
-    double d2 = s.xr * s.xr + s.xi * s.xi;  // FP64 radius test on the physical delta
-    uint64_t cap = s.hold > 0 ? (uint64_t)s.sn + s.hold : (s.pending ? ~0ull : (uint64_t)s.chk);
-    uint64_t budget = p.max_iter < cap ? p.max_iter : cap;
-    if (s.nucleus >= 0) {
-      uint64_t nc = s.n == 0 ? 1ull : (uint64_t)s.nucleus + 1;
-      budget = budget < nc ? budget : nc;
-    }
-    budget = budget > s.n ? budget - s.n : 0;
-    uint32_t k = s.m - 1u;
-    int lv = -1;
-    uint32_t at = 0;
-    if (budget >= 2 && d2 < s.r2a) {
-      lv = 0;
-      at = k >> 1;
-      uint32_t tz = k == 0 ? 32u : (uint32_t)(__ffs((int)k) - 1);
-      uint32_t top = tz < p.bla_levels ? tz : p.bla_levels;
-      for (uint32_t i = 1; i < top; ++i) {
-        if ((2ull << i) > budget) break;
-        uint32_t a = k >> (i + 1);
-        if (a >= p.bla_count[i]) break;
-        if (!(d2 < __ldg(p.bla_r2 + p.bla_off[i] + a))) break;
-        lv = (int)i;
-        at = a;
-      }
-    }
-    if (lv >= 0) {
-      took = true;
-      uint32_t b = p.bla_off[lv] + at;
-      double2 A = __ldg(p.bla_coef + 2 * b), B = __ldg(p.bla_coef + 2 * b + 1);
-      uint32_t len = 2u << lv;
-      if (s.nucleus >= 0 && s.n >= 1) {
-        s.ct.multiply((float)A.x, (float)A.y);
-        s.ct_started = true;
-      }
-      if (s.hold > 0) s.mu.multiply((float)A.x, (float)A.y);
-      if (D) {
-        normalise(s.dr, s.di, s.dexp, INT64_MAX / 4);
-        s.inverse = exp2i(-s.dexp);
-        double t = A.x * s.dr - A.y * s.di + B.x * s.inverse;
-        s.di = A.x * s.di + A.y * s.dr + B.y * s.inverse;
-        s.dr = t;
-        normalise(s.dr, s.di, s.dexp, INT64_MAX / 4);
-        s.inverse = exp2i(-s.dexp);
-      }
-      // delta' = A delta + B dc with wide exponents
-      double wr = s.wr, wi = s.wi;
-      Cx3 ad{A.x * wr - A.y * wi, A.x * wi + A.y * wr, s.e};
-      Cx3 bd{B.x * s.ar - B.y * s.ai, B.x * s.ai + B.y * s.ar, s.oe};
-      Cx3 d = add3(ad, bd);
-      set_delta(s, d.re, d.im, d.e);
-      s.m += len;
-      s.n += len;
-      s.blocks += 1;
-      s.skipped += len;
-    }
-  }
-  if (!took) {
-    if (s.nucleus >= 0 && s.n >= 1) {
-      s.ct.multiply((float)(2.0 * s.fr), (float)(2.0 * s.fi));
-      s.ct_started = true;
-    }
-    if (s.hold > 0) s.mu.multiply((float)(2.0 * s.fr), (float)(2.0 * s.fi));
-    if (D) {  // FP64 derivative (sample.rs:352-360)
-      double t = 2.0 * (s.fr * s.dr - s.fi * s.di) + s.inverse;
-      s.di = 2.0 * (s.fr * s.di + s.fi * s.dr);
-      s.dr = t;
-      if (fmax(fabs(s.dr), fabs(s.di)) > HI) {
-        s.dr = s.dr * LO;
-        s.di = s.di * LO;
-        s.dexp += 32;
-        s.inverse = exp2i(-s.dexp);
-      }
-    }
-    if (!isnan(s.zr32)) {
-      // FP32: w' = 2 Z w + 2^e w^2 + dc 2^-e
-      float wr = s.wr, wi = s.wi;
-      float zwr = s.zr32 * wr - s.zi32 * wi, zwi = s.zr32 * wi + s.zi32 * wr;
-      float nwr = 2.0f * zwr + s.s32 * (wr * wr - wi * wi) + s.dcr;
-      float nwi = 2.0f * zwi + s.s32 * (2.0f * wr * wi) + s.dci;
-      s.wr = nwr;
-      s.wi = nwi;
-      float mag = fmaxf(fabsf(nwr), fabsf(nwi));
-      if (mag > 4294967296.0f || (mag < 2.3283064e-10f && s.e > s.oe - 64)) set_delta(s, nwr, nwi, s.e);
-    } else {
-      // exact step at a tiny Z_m: 2 Z delta + delta^2 + dc with wide exponents
-      double wr = s.wr, wi = s.wi;
-      Cx3 zd{2.0 * (s.Zr * wr - s.Zi * wi), 2.0 * (s.Zr * wi + s.Zi * wr), s.e};
-      Cx3 dd{wr * wr - wi * wi, 2.0 * wr * wi, 2 * (int64_t)s.e};
-      Cx3 a{s.ar, s.ai, s.oe};
-      Cx3 t = add3(add3(zd, dd), a);
-      set_delta(s, t.re, t.im, t.e);
-    }
-    s.m += 1;
-    s.n += 1;
-  }
+__device__ __forceinline__ bool post_f32(const Params &p, const Entry32 *__restrict__ orbit, StateF &s,
+                                         Result &res, bool took, double2 nz, double2 nr) {
   double2 Z = nz;
   if (took) {
     const double2 *e3 = reinterpret_cast<const double2 *>(orbit + s.m);
@@ -218,9 +255,9 @@ __device__ __forceinline__ bool step_f32(const Params &p, const Entry32 *__restr
   s.zi32 = __int_as_float((int)(__double_as_longlong(nr.x) >> 32));
   s.r2a = nr.y;
   // FP64: the physical delta, z, the bailout and the rebase test
-  double pr = (double)s.wr * s.s64, pi = (double)s.wi * s.s64;
-  double fr = Z.x + pr, fi = Z.y + pi;
-  double f2 = fr * fr + fi * fi;
+  const double pr = phys(s.wr, s.e, s.s64), pi = phys(s.wi, s.e, s.s64);
+  const double fr = Z.x + pr, fi = Z.y + pi;
+  const double f2 = fr * fr + fi * fi;
   if (f2 > p.r2) {
     res.kind = 0;
     res.n = s.n;
@@ -238,8 +275,9 @@ __device__ __forceinline__ bool step_f32(const Params &p, const Entry32 *__restr
       return true;
     }
     s.nucleus = -1;
+    relimit_f32(p, s);
   }
-  double delta2 = pr * pr + pi * pi;
+  const double delta2 = pr * pr + pi * pi;
   if (f2 <= delta2 || s.m == p.last) {  // rebase onto Z_0 (extended-tier rule)
     set_delta(s, fr, fi, 0);
     s.m = 0;
@@ -248,33 +286,34 @@ __device__ __forceinline__ bool step_f32(const Params &p, const Entry32 *__restr
     s.zr32 = __int_as_float(0x7fc00000);  // Z_0 = 0: exact step
     s.zi32 = 0.0f;
     s.r2a = -1.0;
-    s.xr = (double)s.wr * s.s64;
-    s.xi = (double)s.wi * s.s64;
-    s.fr = s.Zr + s.xr;
-    s.fi = s.Zi + s.xi;
+    const double xr = phys(s.wr, s.e, s.s64), xi = phys(s.wi, s.e, s.s64);
+    s.d2 = xr * xr + xi * xi;
+    s.fr = s.Zr + xr;
+    s.fi = s.Zi + xi;
   } else {
-    s.xr = pr;
-    s.xi = pi;
+    s.d2 = delta2;
     s.fr = fr;
     s.fi = fi;
   }
   // periodicity in FP32 (ordinary-tier rule, sample.rs:473-574) on the rebased delta
-  bool judge = s.xr * s.xr + s.xi * s.xi > RES2 * f2;
+  const bool judge = s.d2 > RES2 * f2;
   if (!judge) {
     if (s.hold > 0) {
       if (s.n >= s.sn + s.hold) {
         s.hold = 0;
         s.predicted = false;
         s.pending = true;
+        relimit_f32(p, s);
       }
     } else if (s.n >= s.chk) {
       s.pending = true;
+      relimit_f32(p, s);
     }
     return false;
   }
-  float gr = (float)fr, gi = (float)fi;
-  float dist = fabsf(gr - s.sr) + fabsf(gi - s.si);
-  float size = fabsf(s.sr) + fabsf(s.si);
+  const float gr = (float)fr, gi = (float)fi;
+  const float dist = fabsf(gr - s.sr) + fabsf(gi - s.si);
+  const float size = fabsf(s.sr) + fabsf(s.si);
   if (dist < 1e-3f * size) {
     uint32_t period = s.n - s.sn;
     if (s.hold == period && s.mu.below(1.0f)) {
@@ -304,6 +343,7 @@ __device__ __forceinline__ bool step_f32(const Params &p, const Entry32 *__restr
     s.sn = s.n;
     s.pending = false;
     s.mu.reset();
+    relimit_f32(p, s);
     return false;
   }
   if (s.hold > 0) {
@@ -320,7 +360,49 @@ __device__ __forceinline__ bool step_f32(const Params &p, const Entry32 *__restr
     s.sn = s.n;
     s.pending = false;
   }
+  relimit_f32(p, s);
   return false;
+}
+
+// One iteration of the precision form for the active lanes of a warp, with the block
+// deferral of warp_step.
+template <bool D, bool L>
+__device__ __forceinline__ bool warp_step_f32(const Params &p, const Entry32 *__restrict__ orbit, StateF &s,
+                                              Result &res, bool active, Waiting &w, uint32_t defer) {
+  bool upd = false, took = false, done = false;
+  double2 nz = make_double2(0.0, 0.0), nr = make_double2(0.0, -1.0);
+  if (active && !w.on) {
+    if (s.n >= p.max_iter) {
+      res.kind = 2;
+      done = true;
+    } else {
+      // speculative load of the next entry (m < last at the top of every iteration)
+      const double2 *e2 = reinterpret_cast<const double2 *>(orbit + s.m + 1);
+      nz = __ldg(e2);
+      nr = __ldg(e2 + 1);
+      int lv = -1;
+      if (L) lv = find_block_f32(p, s, w.at);
+      if (lv >= 0) {
+        w.on = true;
+        w.lv = lv;
+      } else {
+        plain_update_f32<D>(s);
+        upd = true;
+      }
+    }
+  }
+  if (L) {
+    const unsigned FULL = 0xffffffffu;
+    const unsigned waiting = __ballot_sync(FULL, w.on);
+    const unsigned stepping = __ballot_sync(FULL, upd);
+    if (waiting && ((uint32_t)__popc(waiting) >= defer || !stepping) && w.on) {
+      apply_block_f32<D>(p, s, w.lv, w.at);
+      w.on = false;
+      upd = took = true;
+    }
+  }
+  if (upd) done = post_f32<D, L>(p, orbit, s, res, took, nz, nr);
+  return done;
 }
 
 template <bool D, bool L>
@@ -328,7 +410,8 @@ __device__ __forceinline__ int init_f32(const Params &p, uint64_t slot, StateF &
   uint64_t tile = slot >> 5;
   uint32_t w = (uint32_t)slot & 31u;
   uint32_t tx = (uint32_t)(tile % p.tiles_x), ty = (uint32_t)(tile / p.tiles_x);
-  uint32_t i = tx * 8 + (w & 7u), jj = ty * 4 + (w >> 3);
+  uint32_t i = (tx << p.tile_shift) + (w & ((1u << p.tile_shift) - 1u));
+  uint32_t jj = ty * (32u >> p.tile_shift) + (w >> p.tile_shift);
   if (i >= p.nx || jj >= p.rows) return 0;
   uint32_t j = p.first_row + jj;
   uint32_t idx = j * p.nx + i;
@@ -360,7 +443,7 @@ __device__ __forceinline__ int init_f32(const Params &p, uint64_t slot, StateF &
     }
   }
   set_delta(s, 0.0, 0.0, s.oe);
-  s.xr = s.xi = 0.0;
+  s.d2 = 0.0;
   s.Zr = p.z0r;
   s.Zi = p.z0i;
   s.fr = s.Zr;
@@ -386,16 +469,18 @@ __device__ __forceinline__ int init_f32(const Params &p, uint64_t slot, StateF &
   s.ct_started = false;
   s.blocks = 0;
   s.skipped = 0;
+  relimit_f32(p, s);
   return 1;
 }
 
 template <bool D, bool L>
-__global__ void __launch_bounds__(128, FDK_MIN_BLOCKS) perturb_f32_kernel(Params p, const Entry32 *__restrict__ orbit) {
+__global__ void __launch_bounds__(128, FDK_MIN_BLOCKS_F32) perturb_f32_kernel(Params p, const Entry32 *__restrict__ orbit) {
   const unsigned FULL = 0xffffffffu;
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lt = (1u << lane) - 1u;
   StateF s;
   Result res;
+  Waiting w{false, -1, 0};
   bool active = false, exhausted = false;
   uint64_t t0 = p.deadline_ns ? globaltimer() : 0;
   unsigned long long n_samples = 0, iters = 0, blocks = 0, skipped = 0, fallback = 0, closed = 0;
@@ -445,11 +530,9 @@ __global__ void __launch_bounds__(128, FDK_MIN_BLOCKS) perturb_f32_kernel(Params
       need = __ballot_sync(FULL, !active);
     }
     if (!__any_sync(FULL, active)) break;
-    if (active) {
-      if (step_f32<D, L>(p, orbit, s, res)) {
-        finish(s.idx, res, s.blocks, s.skipped);
-        active = false;
-      }
+    if (warp_step_f32<D, L>(p, orbit, s, res, active, w, p.defer)) {
+      finish(s.idx, res, s.blocks, s.skipped);
+      active = false;
     }
   }
   for (int o = 16; o > 0; o >>= 1) {
@@ -478,14 +561,16 @@ namespace fdk {
 
 // Batch form of the precision kernel (see perturb_batch_kernel).
 template <bool D, bool L>
-__global__ void __launch_bounds__(128, FDK_MIN_BLOCKS)
+__global__ void __launch_bounds__(128, FDK_MIN_BLOCKS_F32)
     perturb_f32_batch_kernel(const Params *__restrict__ jobs, const unsigned long long *__restrict__ starts,
-                             uint32_t njobs, unsigned long long total, unsigned long long *queue, Counters *per_job) {
+                             uint32_t njobs, unsigned long long total, unsigned long long *queue, Counters *per_job,
+                             uint32_t defer) {
   const unsigned FULL = 0xffffffffu;
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lt = (1u << lane) - 1u;
   StateF s;
   Result res;
+  Waiting w{false, -1, 0};
   bool active = false, exhausted = false;
   uint32_t job = 0, counted = 0xffffffffu;
   LaneCounters lc;
@@ -532,12 +617,10 @@ __global__ void __launch_bounds__(128, FDK_MIN_BLOCKS)
       need = __ballot_sync(FULL, !active);
     }
     if (!__any_sync(FULL, active)) break;
-    if (active) {
-      const Params &p = jobs[job];
-      if (step_f32<D, L>(p, (const Entry32 *)p.orbit32, s, res)) {
-        finish(p, s.idx, res, s.blocks, s.skipped);
-        active = false;
-      }
+    const Params &p = jobs[job];
+    if (warp_step_f32<D, L>(p, (const Entry32 *)p.orbit32, s, res, active, w, defer)) {
+      finish(p, s.idx, res, s.blocks, s.skipped);
+      active = false;
     }
   }
   if (counted != 0xffffffffu) lc.flush(per_job + counted);

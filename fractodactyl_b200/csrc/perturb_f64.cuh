@@ -12,11 +12,19 @@ namespace fdk {
 
 constexpr int MAX_LEVELS = 40;
 
-// Resident 128-thread blocks per SM the kernels are compiled for (caps registers at
-// 65536 / (128 * FDK_MIN_BLOCKS)); chosen by measurement.
-#ifndef FDK_MIN_BLOCKS
-#define FDK_MIN_BLOCKS 1
+// Resident 128-thread blocks per SM each kernel variant is compiled for (caps registers
+// at 65536 / (128 * blocks)): floatexp-tier variants (EXT) and ordinary-tier variants;
+// chosen by measurement.
+#ifndef FDK_MIN_BLOCKS_EXT
+#define FDK_MIN_BLOCKS_EXT 4
 #endif
+#ifndef FDK_MIN_BLOCKS_FIX
+#define FDK_MIN_BLOCKS_FIX 4
+#endif
+template <bool EXT>
+struct Occupancy {
+  static constexpr int blocks = EXT ? FDK_MIN_BLOCKS_EXT : FDK_MIN_BLOCKS_FIX;
+};
 
 struct Counters {
   unsigned long long samples, iterations, blocks, skipped, fallback, closed;
@@ -43,6 +51,7 @@ struct Params {
   uint32_t bla_count[MAX_LEVELS];
   // frame
   uint32_t nx, ny, first_row, rows, tiles_x;
+  uint32_t tile_shift;  // tiles are 2^tile_shift samples wide and 32 / 2^tile_shift rows high
   int32_t tier;
   uint32_t flags;
   double c_re, c_im, h, h_m;
@@ -71,6 +80,7 @@ struct Params {
   uint64_t deadline_ns;  // 0 = none
   uint32_t *timed_out;
   uint64_t out_base;  // outputs hold the rendered rows only: index idx - out_base
+  uint32_t defer;     // BLA lanes a warp gathers before it applies their blocks (warp_step)
 };
 
 enum : uint32_t { F_DERIV = 1u, F_BLA = 2u, F_SHIFT = 4u };
@@ -91,6 +101,7 @@ struct State {
   int64_t offset_exp, delta_exp, derivative_exp;
   int64_t nucleus;
   uint32_t n, chk, sn, hold, blocks, skipped;  // n < max_iter < 2^32; chk saturates at 2^32 - 1
+  uint32_t lim;  // relimit()
   uint32_t m, idx;
   int returns;
   bool pending, predicted;
@@ -104,137 +115,149 @@ struct Result {
   int64_t dexp;
 };
 
-// One iteration of the while loop of sample.rs:237-575. Returns true when the sample
-// has an outcome (written to r).
-template <bool EXT, bool D, bool L>
-__device__ __forceinline__ bool step(const Params &p, State<EXT> &s, Result &res) {
-  if (s.n >= p.max_iter) {
-    res.kind = 2;
-    return true;
+// The iteration limit behind Bla::find's budget (sample.rs:246-263) with n left out:
+// min(max_iter, the next periodicity save point, nucleus + 1), kept in the state and
+// recomputed whenever one of its inputs (hold, sn, pending, chk, nucleus) changes, so an
+// iteration only subtracts n. The reference's n == 0 case (a budget of 1) never reaches
+// the search: with a nucleus gate, m == 0 skips the BLA. lim <= max_iter < 2^32.
+template <bool EXT>
+__device__ __forceinline__ void relimit(const Params &p, State<EXT> &s) {
+  uint64_t cap = s.hold > 0 ? (uint64_t)s.sn + s.hold : (s.pending ? ~0ull : (uint64_t)s.chk);
+  uint64_t b = p.max_iter < cap ? p.max_iter : cap;
+  if (s.nucleus >= 0 && (uint64_t)s.nucleus + 1 < b) b = (uint64_t)s.nucleus + 1;
+  s.lim = (uint32_t)b;
+}
+
+// Bla::find (bla.rs:234-249) at the top of an iteration: the level of the longest valid
+// block starting at m that fits the budget, or -1, with its index in that level in `at`.
+// The radii of the first two levels come with the orbit entry (r2a, r2b); those of the
+// next PRE levels are loaded together before the comparisons that would stop at them.
+template <bool EXT>
+__device__ __forceinline__ int find_block(const Params &p, const State<EXT> &s, uint32_t &at) {
+  if (!(s.nucleus < 0 || s.m != 0)) return -1;
+  const uint32_t budget = s.lim > s.n ? s.lim - s.n : 0u;
+  // r2a is -1 unless a block starts at m (d2 < r2a is then false whatever d2 is)
+  if (budget < 2 || !(s.r2a >= 0.0)) return -1;
+  const double d2 = EXT ? (s.xr * s.xr + s.xi * s.xi) * s.scale * s.scale : s.xr * s.xr + s.xi * s.xi;
+  if (!(d2 < s.r2a)) return -1;
+  const uint32_t k = s.m - 1u;     // m = 0 wraps: odd, no block
+  at = k >> 1;
+  if (budget < 4 || !(d2 < s.r2b)) return 0;
+  at = k >> 2;
+  const uint32_t tz = k == 0 ? 32u : (uint32_t)(__ffs((int)k) - 1);
+  const uint32_t top = tz < p.bla_levels ? tz : p.bla_levels;
+  constexpr uint32_t PRE = 4;  // levels 2..5
+  double r[PRE];
+  bool ok[PRE];
+#pragma unroll
+  for (uint32_t q = 0; q < PRE; ++q) {
+    const uint32_t i = 2 + q, a = k >> (i + 1);
+    ok[q] = i < top && (2u << i) <= budget && a < p.bla_count[i];
+    r[q] = ok[q] ? __ldg(p.bla_r2 + p.bla_off[i] + a) : -1.0;
   }
-  // Next orbit point, loaded before the step's arithmetic so its latency overlaps it
-  // (m < last here: a sample that reaches the last point rebases to Z_0 below).
-  double2 Zn, Rn = make_double2(-1.0, -1.0);
-  if (L) {
-    Zn = __ldg(p.fused + 2 * (s.m + 1));
-    Rn = __ldg(p.fused + 2 * (s.m + 1) + 1);
-  } else {
-    Zn = __ldg(p.orbit + s.m + 1);
+  int lv = 1;
+#pragma unroll
+  for (uint32_t q = 0; q < PRE; ++q) {
+    if (!ok[q] || !(d2 < r[q])) return lv;
+    lv = (int)(2 + q);
+    at = k >> (3 + q);
   }
-  bool took = false;
-  if (L) {
-    if (s.nucleus < 0 || s.m != 0) {
-      // Bla::find (bla.rs:234-249) with the budget of sample.rs:246-263.
-      double d2 = EXT ? (s.xr * s.xr + s.xi * s.xi) * s.scale * s.scale : s.xr * s.xr + s.xi * s.xi;
-      uint64_t cap = s.hold > 0 ? (uint64_t)s.sn + s.hold : (s.pending ? ~0ull : (uint64_t)s.chk);
-      uint64_t budget = p.max_iter < cap ? p.max_iter : cap;
-      if (s.nucleus >= 0) {
-        uint64_t nc = s.n == 0 ? 1ull : (uint64_t)s.nucleus + 1;
-        budget = budget < nc ? budget : nc;
-      }
-      budget = budget > s.n ? budget - s.n : 0;
-      uint32_t k = s.m - 1u;  // m = 0 wraps: odd, no block
-      int lv = -1;
-      uint32_t at = 0;
-      if (budget >= 2 && d2 < s.r2a) {  // level 0: r2a is -1 unless a block starts at m
-        lv = 0;
-        at = k >> 1;
-        if (budget >= 4 && d2 < s.r2b) {  // level 1, likewise
-          lv = 1;
-          at = k >> 2;
-          uint32_t tz = k == 0 ? 32u : (uint32_t)(__ffs((int)k) - 1);
-          uint32_t top = tz < p.bla_levels ? tz : p.bla_levels;
-          for (uint32_t i = 2; i < top; ++i) {
-            if ((2ull << i) > budget) break;
-            uint32_t a = k >> (i + 1);
-            if (a >= p.bla_count[i]) break;
-            if (!(d2 < __ldg(p.bla_r2 + p.bla_off[i] + a))) break;
-            lv = (int)i;
-            at = a;
-          }
-        }
-      }
-      if (lv >= 0) {
-        took = true;
-        uint32_t b = p.bla_off[lv] + at;
-        double2 A = __ldg(p.bla_coef + 2 * b), B = __ldg(p.bla_coef + 2 * b + 1);
-        uint32_t len = 2u << lv;
-        if (s.nucleus >= 0 && s.n >= 1) s.ct.multiply(A.x, A.y);
-        if (!EXT && s.hold > 0) s.mu.multiply(A.x, A.y);
-        if (EXT) {
-          normalise(s.xr, s.xi, s.delta_exp, 0);
-          if (D) {
-            normalise(s.dr, s.di, s.derivative_exp, INT64_MAX / 4);
-            s.inverse = exp2i(-s.derivative_exp);
-          }
-          s.scale = exp2i(s.delta_exp);
-          double factor = exp2i(s.offset_exp - s.delta_exp);
-          s.dc_r = s.ar * factor;
-          s.dc_i = s.ai * factor;
-        }
-        if (D) {
-          double t = A.x * s.dr - A.y * s.di + B.x * s.inverse;
-          s.di = A.x * s.di + A.y * s.dr + B.y * s.inverse;
-          s.dr = t;
-          if (!EXT && (p.flags & F_SHIFT)) {
-            double2 ab = __ldg(p.bla_ab + b);
-            s.shift += (ab.x * sqrt(s.xr * s.xr + s.xi * s.xi) + ab.y * s.adc) / sqrt(s.dr * s.dr + s.di * s.di);
-          }
-        }
-        double t = A.x * s.xr - A.y * s.xi + B.x * s.dc_r - B.y * s.dc_i;
-        s.xi = A.x * s.xi + A.y * s.xr + B.x * s.dc_i + B.y * s.dc_r;
-        s.xr = t;
-        if (EXT) {
-          normalise(s.xr, s.xi, s.delta_exp, 0);
-          if (D) {
-            normalise(s.dr, s.di, s.derivative_exp, INT64_MAX / 4);
-            s.inverse = exp2i(-s.derivative_exp);
-          }
-          s.scale = exp2i(s.delta_exp);
-          double factor = exp2i(s.offset_exp - s.delta_exp);
-          s.dc_r = s.ar * factor;
-          s.dc_i = s.ai * factor;
-        }
-        s.m += len;
-        s.n += len;
-        s.blocks += 1;
-        s.skipped += len;
-      }
-    }
+  for (uint32_t i = 2 + PRE; i < top; ++i) {
+    if ((2ull << i) > budget) break;
+    const uint32_t a = k >> (i + 1);
+    if (a >= p.bla_count[i]) break;
+    if (!(d2 < __ldg(p.bla_r2 + p.bla_off[i] + a))) break;
+    lv = (int)i;
+    at = a;
   }
-  if (!took) {
-    double fr, fi;
-    if (EXT) {
-      fr = s.Zr + s.scale * s.xr;
-      fi = s.Zi + s.scale * s.xi;
-    } else {
-      fr = s.fr;  // == Z[m] + delta, carried from the previous iteration
-      fi = s.fi;
-    }
-    if (s.nucleus >= 0 && s.n >= 1) s.ct.multiply(2.0 * fr, 2.0 * fi);
-    if (!EXT && s.hold > 0) s.mu.multiply(2.0 * fr, 2.0 * fi);
+  return lv;
+}
+
+// A BLA block application (sample.rs:264-315): delta' = A delta + B dc, dz' = A dz + B.
+template <bool EXT, bool D>
+__device__ __forceinline__ void apply_block(const Params &p, State<EXT> &s, int lv, uint32_t at) {
+  const uint32_t b = p.bla_off[lv] + at;
+  const double2 A = __ldg(p.bla_coef + 2 * b), B = __ldg(p.bla_coef + 2 * b + 1);
+  const uint32_t len = 2u << lv;
+  if (s.nucleus >= 0 && s.n >= 1) s.ct.multiply(A.x, A.y);
+  if (!EXT && s.hold > 0) s.mu.multiply(A.x, A.y);
+  if (EXT) {
+    normalise(s.xr, s.xi, s.delta_exp, 0);
     if (D) {
-      double t = 2.0 * (fr * s.dr - fi * s.di) + s.inverse;
-      s.di = 2.0 * (fr * s.di + fi * s.dr);
-      s.dr = t;
-      if (EXT && rmax(fabs(s.dr), fabs(s.di)) > HI) {
-        s.dr = s.dr * LO;
-        s.di = s.di * LO;
-        s.derivative_exp += 32;
-        s.inverse = exp2i(-s.derivative_exp);
-      }
+      normalise(s.dr, s.di, s.derivative_exp, INT64_MAX / 4);
+      s.inverse = exp2i(-s.derivative_exp);
     }
-    double wr = s.xr, wi = s.xi, zr = s.Zr, zi = s.Zi;
-    if (EXT) {  // number.rs:109-124
-      s.xr = 2.0 * (zr * wr - zi * wi) + s.scale * (wr * wr - wi * wi) + s.dc_r;
-      s.xi = 2.0 * (zr * wi + zi * wr) + s.scale * (2.0 * wr * wi) + s.dc_i;
-    } else {  // number.rs:92-107
-      s.xr = 2.0 * (zr * wr - zi * wi) + wr * wr - wi * wi + s.dc_r;
-      s.xi = 2.0 * (zr * wi + zi * wr + wr * wi) + s.dc_i;
-    }
-    s.m += 1;
-    s.n += 1;
+    s.scale = exp2i(s.delta_exp);
+    double factor = exp2i(s.offset_exp - s.delta_exp);
+    s.dc_r = s.ar * factor;
+    s.dc_i = s.ai * factor;
   }
+  if (D) {
+    double t = A.x * s.dr - A.y * s.di + B.x * s.inverse;
+    s.di = A.x * s.di + A.y * s.dr + B.y * s.inverse;
+    s.dr = t;
+    if (!EXT && (p.flags & F_SHIFT)) {
+      double2 ab = __ldg(p.bla_ab + b);
+      s.shift += (ab.x * sqrt(s.xr * s.xr + s.xi * s.xi) + ab.y * s.adc) / sqrt(s.dr * s.dr + s.di * s.di);
+    }
+  }
+  double t = A.x * s.xr - A.y * s.xi + B.x * s.dc_r - B.y * s.dc_i;
+  s.xi = A.x * s.xi + A.y * s.xr + B.x * s.dc_i + B.y * s.dc_r;
+  s.xr = t;
+  if (EXT) {
+    normalise(s.xr, s.xi, s.delta_exp, 0);
+    if (D) {
+      normalise(s.dr, s.di, s.derivative_exp, INT64_MAX / 4);
+      s.inverse = exp2i(-s.derivative_exp);
+    }
+    s.scale = exp2i(s.delta_exp);
+    double factor = exp2i(s.offset_exp - s.delta_exp);
+    s.dc_r = s.ar * factor;
+    s.dc_i = s.ai * factor;
+  }
+  s.m += len;
+  s.n += len;
+  s.blocks += 1;
+  s.skipped += len;
+}
+
+// One ordinary step (sample.rs:331-380; number.rs:92-124): z = Z[m] + delta is carried
+// from the end of the previous iteration in (fr, fi).
+template <bool EXT, bool D>
+__device__ __forceinline__ void plain_update(State<EXT> &s) {
+  const double fr = s.fr, fi = s.fi;
+  if (s.nucleus >= 0 && s.n >= 1) s.ct.multiply(2.0 * fr, 2.0 * fi);
+  if (!EXT && s.hold > 0) s.mu.multiply(2.0 * fr, 2.0 * fi);
+  if (D) {
+    double t = 2.0 * (fr * s.dr - fi * s.di) + s.inverse;
+    s.di = 2.0 * (fr * s.di + fi * s.dr);
+    s.dr = t;
+    if (EXT && rmax(fabs(s.dr), fabs(s.di)) > HI) {
+      s.dr = s.dr * LO;
+      s.di = s.di * LO;
+      s.derivative_exp += 32;
+      s.inverse = exp2i(-s.derivative_exp);
+    }
+  }
+  const double wr = s.xr, wi = s.xi, zr = s.Zr, zi = s.Zi;
+  if (EXT) {  // number.rs:109-124
+    s.xr = 2.0 * (zr * wr - zi * wi) + s.scale * (wr * wr - wi * wi) + s.dc_r;
+    s.xi = 2.0 * (zr * wi + zi * wr) + s.scale * (2.0 * wr * wi) + s.dc_i;
+  } else {  // number.rs:92-107
+    s.xr = 2.0 * (zr * wr - zi * wi) + wr * wr - wi * wi + s.dc_r;
+    s.xi = 2.0 * (zr * wi + zi * wr + wr * wi) + s.dc_i;
+  }
+  s.m += 1;
+  s.n += 1;
+}
+
+// The rest of the iteration after the update (sample.rs:381-575): the next orbit point,
+// bailout, nucleus gate, rebase, rescaling and periodicity. Zn/Rn hold the prefetched
+// entry m + 1 of the iteration's start, right after a plain step; after a block (took)
+// the entry at the new m is loaded here. Returns true when the sample has an outcome.
+template <bool EXT, bool D, bool L>
+__device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res, bool took, double2 Zn,
+                                     double2 Rn) {
   double2 Z = Zn;
   if (L) {
     if (took) {  // a block moved m by its length
@@ -266,10 +289,15 @@ __device__ __forceinline__ bool step(const Params &p, State<EXT> &s, Result &res
       return true;
     }
     s.nucleus = -1;
+    relimit(p, s);
   }
   double delta2 = pr * pr + pi * pi;
   bool rebase = EXT ? f2 <= delta2 : f2 < delta2;
+  // z of the next iteration, Z[m] + delta with the final m and delta: (fr, fi) unless the
+  // delta or its scale changes below
+  bool moved = false;
   if (rebase || s.m == p.last) {
+    moved = true;
     if (EXT) {
       if (f2 > SQUARE_OK) {
         s.xr = fr;
@@ -289,6 +317,7 @@ __device__ __forceinline__ bool step(const Params &p, State<EXT> &s, Result &res
       s.r2b = -1.0;
       if (s.scale < 1.0 / 1e270) {  // TINY, sample.rs:17
         s.nucleus = -1;
+        relimit(p, s);
         if (D) {
           Cx3 v = zero_step_dz(Cx3{s.xr, s.xi, s.delta_exp}, Cx3{s.dr, s.di, s.derivative_exp});
           s.dr = v.re;
@@ -332,6 +361,7 @@ __device__ __forceinline__ bool step(const Params &p, State<EXT> &s, Result &res
     else if (magnitude < LO && magnitude != 0.0)
       k = -32;
     if (k != 0) {
+      moved = true;
       double factor = exp2i(-k);
       s.xr = s.xr * factor;
       s.xi = s.xi * factor;
@@ -342,10 +372,12 @@ __device__ __forceinline__ bool step(const Params &p, State<EXT> &s, Result &res
       s.dc_i = s.ai * f;
     }
   }
-  if (!EXT) {
-    // The next plain step's z (sample.rs:331): Z[m] + delta with the current m, delta.
-    s.fr = s.Zr + s.xr;
-    s.fi = s.Zi + s.xi;
+  if (moved) {  // the next iteration's z (sample.rs:331; number.rs:113 on the extended tier)
+    s.fr = EXT ? s.Zr + s.scale * s.xr : s.Zr + s.xr;
+    s.fi = EXT ? s.Zi + s.scale * s.xi : s.Zi + s.xi;
+  } else {  // the same expressions on the same values
+    s.fr = fr;
+    s.fi = fi;
   }
   double check_r = EXT ? pr : s.xr, check_i = EXT ? pi : s.xi;
   bool judge = check_r * check_r + check_i * check_i > RES2 * f2;
@@ -357,15 +389,18 @@ __device__ __forceinline__ bool step(const Params &p, State<EXT> &s, Result &res
         s.si = fi;
         s.sn = s.n;
         s.chk = s.chk >= 0x80000000u ? 0xffffffffu : s.chk * 2;
+        relimit(p, s);
       }
     } else if (s.hold > 0) {
       if ((uint64_t)s.n >= (uint64_t)s.sn + s.hold) {
         s.hold = 0;
         s.predicted = false;
         s.pending = true;
+        relimit(p, s);
       }
     } else if (s.n >= s.chk) {
       s.pending = true;
+      relimit(p, s);
     }
     return false;
   }
@@ -385,6 +420,7 @@ __device__ __forceinline__ bool step(const Params &p, State<EXT> &s, Result &res
       s.si = fi;
       s.sn = s.n;
       s.chk = s.chk >= 0x80000000u ? 0xffffffffu : s.chk * 2;
+      relimit(p, s);
     }
     return false;
   }
@@ -417,6 +453,7 @@ __device__ __forceinline__ bool step(const Params &p, State<EXT> &s, Result &res
     s.sn = s.n;
     s.pending = false;
     s.mu.reset();
+    relimit(p, s);
     return false;
   }
   if (s.hold > 0) {
@@ -434,10 +471,91 @@ __device__ __forceinline__ bool step(const Params &p, State<EXT> &s, Result &res
     s.sn = s.n;
     s.pending = false;
   }
+  relimit(p, s);
   return false;
 }
 
-// Start sample `slot` of the tile queue (8x4-sample tiles, row-major tiles). Returns
+// One iteration of the while loop of sample.rs:237-575 for one lane (the allocation-free
+// kernel's form). Returns true when the sample has an outcome (written to res).
+template <bool EXT, bool D, bool L>
+__device__ __forceinline__ bool step(const Params &p, State<EXT> &s, Result &res) {
+  if (s.n >= p.max_iter) {
+    res.kind = 2;
+    return true;
+  }
+  // next orbit point, loaded before the step's arithmetic so its latency overlaps it
+  // (m < last here: a sample that reaches the last point rebases to Z_0)
+  double2 Zn, Rn = make_double2(-1.0, -1.0);
+  if (L) {
+    Zn = __ldg(p.fused + 2 * (s.m + 1));
+    Rn = __ldg(p.fused + 2 * (s.m + 1) + 1);
+  } else {
+    Zn = __ldg(p.orbit + s.m + 1);
+  }
+  uint32_t at = 0;
+  const int lv = L ? find_block(p, s, at) : -1;
+  if (lv >= 0)
+    apply_block<EXT, D>(p, s, lv, at);
+  else
+    plain_update<EXT, D>(s);
+  return post<EXT, D, L>(p, s, res, lv >= 0, Zn, Rn);
+}
+
+// A lane's BLA block found but not yet applied.
+struct Waiting {
+  bool on;
+  int lv;
+  uint32_t at;
+};
+
+// One iteration for the active lanes of a warp (every lane of the warp calls it). A lane
+// whose next operation is a BLA block waits until at least `defer` lanes of the warp wait
+// or no lane steps plainly; the waiting lanes then apply their blocks together. The warp
+// runs the block path for many lanes at a time instead of for one or two lanes on
+// nearly every iteration, and each lane's own sequence of operations is unchanged.
+template <bool EXT, bool D, bool L>
+__device__ __forceinline__ bool warp_step(const Params &p, State<EXT> &s, Result &res, bool active, Waiting &w,
+                                          uint32_t defer) {
+  bool upd = false, took = false, done = false;
+  double2 Zn = make_double2(0.0, 0.0), Rn = make_double2(-1.0, -1.0);
+  if (active && !w.on) {
+    if (s.n >= p.max_iter) {
+      res.kind = 2;
+      done = true;
+    } else {
+      if (L) {
+        Zn = __ldg(p.fused + 2 * (s.m + 1));
+        Rn = __ldg(p.fused + 2 * (s.m + 1) + 1);
+      } else {
+        Zn = __ldg(p.orbit + s.m + 1);
+      }
+      int lv = -1;
+      if (L) lv = find_block(p, s, w.at);
+      if (lv >= 0) {
+        w.on = true;
+        w.lv = lv;
+      } else {
+        plain_update<EXT, D>(s);
+        upd = true;
+      }
+    }
+  }
+  if (L) {
+    const unsigned FULL = 0xffffffffu;
+    const unsigned waiting = __ballot_sync(FULL, w.on);
+    const unsigned stepping = __ballot_sync(FULL, upd);
+    if (waiting && ((uint32_t)__popc(waiting) >= defer || !stepping) && w.on) {
+      apply_block<EXT, D>(p, s, w.lv, w.at);
+      w.on = false;
+      upd = took = true;
+    }
+  }
+  if (upd) done = post<EXT, D, L>(p, s, res, took, Zn, Rn);
+  return done;
+}
+
+// Start sample `slot` of the tile queue (one warp-sized tile per 32 slots, tiles in
+// row-major order; 8x4 samples unless tuned). Returns
 // false when the slot holds no sample to iterate (outside the grid, masked, or settled
 // by the closed-form main-component test, whose result is written here).
 template <bool EXT, bool D, bool L>
@@ -445,7 +563,8 @@ __device__ __forceinline__ int init(const Params &p, uint64_t slot, State<EXT> &
   uint64_t tile = slot >> 5;
   uint32_t w = (uint32_t)slot & 31u;
   uint32_t tx = (uint32_t)(tile % p.tiles_x), ty = (uint32_t)(tile / p.tiles_x);
-  uint32_t i = tx * 8 + (w & 7u), jj = ty * 4 + (w >> 3);
+  uint32_t i = (tx << p.tile_shift) + (w & ((1u << p.tile_shift) - 1u));
+  uint32_t jj = ty * (32u >> p.tile_shift) + (w >> p.tile_shift);
   if (i >= p.nx || jj >= p.rows) return 0;
   uint32_t j = p.first_row + jj;
   uint32_t idx = j * p.nx + i;
@@ -492,8 +611,8 @@ __device__ __forceinline__ int init(const Params &p, uint64_t slot, State<EXT> &
   s.Zi = p.z0i;
   s.r2a = -1.0;
   s.r2b = -1.0;
-  s.fr = p.z0r + 0.0;
-  s.fi = p.z0i + 0.0;
+  s.fr = EXT ? p.z0r + s.scale * 0.0 : p.z0r + 0.0;  // z of the first iteration
+  s.fi = EXT ? p.z0i + s.scale * 0.0 : p.z0i + 0.0;
   s.sr = 0.0;
   s.si = 0.0;
   s.chk = 16;
@@ -512,6 +631,7 @@ __device__ __forceinline__ int init(const Params &p, uint64_t slot, State<EXT> &
   s.blocks = 0;
   s.skipped = 0;
   s.shift = 0.0;
+  relimit(p, s);
   return 1;
 }
 
@@ -547,12 +667,13 @@ __device__ __forceinline__ void put(const Params &p, uint32_t sample, const Resu
 }
 
 template <bool EXT, bool D, bool L>
-__global__ void __launch_bounds__(128, FDK_MIN_BLOCKS) perturb_kernel(Params p) {
+__global__ void __launch_bounds__(128, Occupancy<EXT>::blocks) perturb_kernel(Params p) {
   const unsigned FULL = 0xffffffffu;
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lt = (1u << lane) - 1u;
   State<EXT> s;
   Result res;
+  Waiting w{false, -1, 0};
   bool active = false, exhausted = false;
   uint64_t t0 = p.deadline_ns ? globaltimer() : 0;
   unsigned long long n_samples = 0, iters = 0, blocks = 0, skipped = 0, fallback = 0, closed = 0;
@@ -607,11 +728,9 @@ __global__ void __launch_bounds__(128, FDK_MIN_BLOCKS) perturb_kernel(Params p) 
       need = __ballot_sync(FULL, !active);
     }
     if (!__any_sync(FULL, active)) break;
-    if (active) {
-      if (step<EXT, D, L>(p, s, res)) {
-        finish(s.idx, res, s.blocks, s.skipped, s.shift);
-        active = false;
-      }
+    if (warp_step<EXT, D, L>(p, s, res, active, w, p.defer)) {
+      finish(s.idx, res, s.blocks, s.skipped, s.shift);
+      active = false;
     }
   }
   // warp reduction of the counters, one atomic per warp
@@ -672,14 +791,16 @@ struct LaneCounters {
 };
 
 template <bool EXT, bool D, bool L>
-__global__ void __launch_bounds__(128, FDK_MIN_BLOCKS)
+__global__ void __launch_bounds__(128, Occupancy<EXT>::blocks)
     perturb_batch_kernel(const Params *__restrict__ jobs, const unsigned long long *__restrict__ starts,
-                         uint32_t njobs, unsigned long long total, unsigned long long *queue, Counters *per_job) {
+                         uint32_t njobs, unsigned long long total, unsigned long long *queue, Counters *per_job,
+                         uint32_t defer) {
   const unsigned FULL = 0xffffffffu;
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lt = (1u << lane) - 1u;
   State<EXT> s;
   Result res;
+  Waiting w{false, -1, 0};
   bool active = false, exhausted = false;
   uint32_t job = 0, counted = 0xffffffffu;
   LaneCounters lc;
@@ -726,12 +847,10 @@ __global__ void __launch_bounds__(128, FDK_MIN_BLOCKS)
       need = __ballot_sync(FULL, !active);
     }
     if (!__any_sync(FULL, active)) break;
-    if (active) {
-      const Params &p = jobs[job];
-      if (step<EXT, D, L>(p, s, res)) {
-        finish(p, s.idx, res, s.blocks, s.skipped);
-        active = false;
-      }
+    const Params &p = jobs[job];
+    if (warp_step<EXT, D, L>(p, s, res, active, w, defer)) {
+      finish(p, s.idx, res, s.blocks, s.skipped);
+      active = false;
     }
   }
   if (counted != 0xffffffffu) lc.flush(per_job + counted);

@@ -308,6 +308,76 @@ class Device:
         _check(st, self, "render")
         return arrays, cnt, st
 
+    @property
+    def tuning(self) -> _lib.Tuning:
+        t = _lib.Tuning()
+        lib().fdc_get_tuning(self.h, C.byref(t))
+        return t
+
+    def tune(self, defer: Optional[int] = None, blocks_per_sm: Optional[int] = None, tile_w: Optional[int] = None):
+        """fdc_set_tuning: change the given launch settings, keep the others."""
+        t = self.tuning
+        if defer is not None:
+            t.defer = defer
+        if blocks_per_sm is not None:
+            t.blocks_per_sm = blocks_per_sm
+        if tile_w is not None:
+            t.tile_w = tile_w
+        _check(lib().fdc_set_tuning(self.h, C.byref(t)), self, "tuning")
+
+    def batch(self, jobs, columns=COLUMNS, raw=False) -> "Batch":
+        """fdc_batch_create over `jobs` (uploaded orbits; FDC_DEVICE_OUT is set here) with
+        fresh device columns per job (torch tensors on this GPU)."""
+        return Batch(self, jobs, columns, raw)
+
+
+_BATCH_DTYPES = {"cls": "uint8", "status": "uint8", "n": "int32", "nu": "float64", "de": "float32",
+                 "normal": "int16", "z": "float64", "dz": "float64", "dexp": "int64"}
+_HOST_DTYPES = {"cls": np.uint8, "status": np.uint8, "n": np.uint32, "nu": np.float64, "de": np.float32,
+                "normal": np.uint16, "z": np.float64, "dz": np.float64, "dexp": np.int64}
+
+
+class Batch:
+    """Many jobs rendered by one graph replay (fdc_batch_run): one persistent launch per
+    kernel variant over all jobs' tiles. Outputs stay on the device between runs;
+    `columns(k)` copies job k's back."""
+
+    def __init__(self, dev: Device, jobs, columns=COLUMNS, raw=False):
+        import torch
+        self.dev, self.jobs, self.h = dev, list(jobs), C.c_void_p()
+        names = ["cls", "status", "n"] + [c for c in ("nu", "de", "normal") if c in columns]
+        if raw:
+            names += ["z", "dz", "dexp"]
+        self.bufs = []
+        outs = (_lib.Out * len(self.jobs))()
+        cjobs = (_lib.Job * len(self.jobs))()
+        for k, j in enumerate(self.jobs):
+            n = j.nx * j.ny
+            b = {}
+            for name in names:
+                shape = (n, 2) if name in ("z", "dz") else (n,)
+                b[name] = torch.zeros(shape, dtype=getattr(torch, _BATCH_DTYPES[name]), device=f"cuda:{dev.index}")
+                setattr(outs[k], name, b[name].data_ptr())
+            self.bufs.append(b)
+            C.memmove(C.byref(cjobs[k]), C.byref(j), C.sizeof(_lib.Job))
+            cjobs[k].flags |= _lib.DEVICE_OUT
+        _check(lib().fdc_batch_create(dev.h, cjobs, outs, len(self.jobs), C.byref(self.h)), dev, "batch create")
+
+    def run(self):
+        """Replay the batch; returns (total counters, per-job counters)."""
+        total = _lib.Counters()
+        per = (_lib.Counters * len(self.jobs))()
+        _check(lib().fdc_batch_run(self.dev.h, self.h, C.byref(total), per), self.dev, "batch run")
+        return total, list(per)
+
+    def columns(self, k: int):
+        return {name: t.cpu().numpy().view(_HOST_DTYPES[name]) for name, t in self.bufs[k].items()}
+
+    def free(self):
+        if self.h:
+            lib().fdc_batch_free(self.dev.h, self.h)
+            self.h = C.c_void_p()
+
 
 def _setup(view: View, p: Params):
     """grid.rs:779-799."""

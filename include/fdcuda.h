@@ -120,6 +120,25 @@ fdc_status fdc_upload_bla(fdc_ctx *ctx, int32_t orbit, const double *blocks7, co
  * class and n bit-exact, z and dz bit-exact, nu/de/normal within CUDA libm's ulps. */
 fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counters *counters);
 
+/* Launch tuning (no counterpart in the reference; the reference's shader has fixed
+ * workgroups). defer: lanes of a warp whose next operation is a BLA block wait until
+ * this many lanes of the warp wait, or no lane steps plainly, and then apply their
+ * blocks together (1: at once; 0: the measured default of each kernel variant, 12 on
+ * the floatexp tier and 4 elsewhere); results do not depend on it. blocks_per_sm:
+ * resident 128-thread blocks per SM of the persistent launch, 0 for as many as fit.
+ * tile_w: width of the warp-sized tiles of samples the work queue hands out (1, 2, 4, 8,
+ * 16 or 32; the height is 32 / tile_w), 0 for 8. A context starts with all three 0;
+ * settings apply to later fdc_render calls and to batches created after them.
+ * fractodactyl_b200.tune measures and picks them. */
+#define FDC_DEFAULT_DEFER 0
+typedef struct fdc_tuning {
+  uint32_t defer;
+  uint32_t blocks_per_sm;
+  uint32_t tile_w;
+} fdc_tuning;
+fdc_status fdc_set_tuning(fdc_ctx *ctx, const fdc_tuning *tuning);
+fdc_status fdc_get_tuning(const fdc_ctx *ctx, fdc_tuning *tuning);
+
 /* Batches: many jobs (the frames of a zoom film, tiles of many locations, each job with
  * its own orbit handle, tier and device outputs) rendered by ONE persistent launch per
  * kernel variant from a single work queue over all jobs' tiles, deepest jobs first, the
