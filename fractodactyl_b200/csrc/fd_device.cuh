@@ -27,6 +27,12 @@ __device__ __forceinline__ double exp2i(int64_t k) {
   return 0.0;
 }
 
+// The same for 32-bit exponents: one range test on the common path.
+__device__ __forceinline__ double exp2i(int k) {
+  if ((unsigned)(k + 1022) <= 2045u) return __hiloint2double((k + 1023) << 20, 0);
+  return exp2i((int64_t)k);
+}
+
 // Rust f64::max / f64::min ignore a NaN operand, as fmax/fmin do.
 __device__ __forceinline__ double rmax(double a, double b) { return fmax(a, b); }
 __device__ __forceinline__ double rmin(double a, double b) { return fmin(a, b); }
@@ -51,12 +57,14 @@ __device__ __noinline__ static int64_t floor_log2_slow(double a) {
 }
 
 // The same for the common case from the bits: a normal double whose mantissa is below
-// 2 - 2^-40 has floor(RN(log2 a)) = its exponent field - 1023.
-__device__ __forceinline__ int64_t floor_log2(double a) {
-  unsigned long long b = (unsigned long long)__double_as_longlong(a);
-  int ef = (int)((b >> 52) & 0x7ff);
-  if (ef != 0 && (b & 0xFFFFFFFFFFFFFull) < (1ull << 52) - (1ull << 12)) return ef - 1023;
-  return floor_log2_slow(a);
+// 2 - 2^-40 (not all of its top 40 fraction bits set) has floor(RN(log2 a)) = its
+// exponent field - 1023. Tested on the two 32-bit halves.
+__device__ __forceinline__ int floor_log2(double a) {
+  const unsigned hi = (unsigned)__double2hiint(a), lo = (unsigned)__double2loint(a);
+  const int ef = (int)((hi >> 20) & 0x7ffu);
+  const bool top40 = (hi & 0xfffffu) == 0xfffffu && (lo & 0xfffff000u) == 0xfffff000u;
+  if (ef != 0 && !top40) return ef - 1023;
+  return (int)floor_log2_slow(a);
 }
 
 // Rust `f as i64` for the finite values floor_log2's callers pass.
@@ -65,18 +73,22 @@ struct Cx3 {
   int64_t e;
 };
 
-// sample.rs:586-595
-__device__ __forceinline__ void normalise(double &re, double &im, int64_t &e, int64_t max_e) {
+// sample.rs:586-595, for a 64-bit exponent (the derivative's) or a 32-bit one (the
+// delta's, whose range the route bounds far inside 32 bits).
+template <typename E>
+__device__ __forceinline__ void normalise(double &re, double &im, E &e, E max_e) {
   double a = rmax(fabs(re), fabs(im));
   if (a == 0.0 || !isfinite(a)) return;
-  // i64::saturating_sub; max_e is 0 or i64::MAX/4 and |e| stays far below 2^62
-  int64_t k = floor_log2(a);
-  int64_t lim = max_e - e;
-  if (lim < k) k = lim;
+  // i64::saturating_sub; max_e is 0 or i64::MAX/4 and |e| stays far below 2^62. The
+  // shift is min(floor(log2 a), max_e - e): |floor(log2 a)| <= 1075 and max_e - e stays
+  // above -2^31 for both callers' exponents, so it fits 32 bits.
+  int k = floor_log2(a);
+  const E lim = max_e - e;
+  if (lim < (E)k) k = (int)lim;
   double h = exp2i(-(k / 2)), l = exp2i(-(k - k / 2));
   re = re * h * l;
   im = im * h * l;
-  e = e + k;
+  e = e + (E)k;
 }
 
 // sample.rs:600-652

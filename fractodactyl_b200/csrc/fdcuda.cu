@@ -213,6 +213,9 @@ fdc_status prepare(fdc_ctx *ctx, const OrbitDev &o, const fdc_job &j, fdk::Param
   if (!(j.escape_radius > 0.0) || !std::isfinite(j.escape_radius * j.escape_radius))
     return fail(ctx, FDC_INVALID, "escape radius must be positive and its square finite");
   if (!(j.h_m >= 1.0 && j.h_m < 2.0)) return fail(ctx, FDC_INVALID, "h_m must lie in [1, 2)");
+  if (j.h_e < -(1ll << 30) || j.h_e > (1ll << 30)) return fail(ctx, FDC_INVALID, "h_e must lie in [-2^30, 2^30]");
+  if (j.nucleus_period < -1 || j.nucleus_period >= (1ll << 31) - 1)
+    return fail(ctx, FDC_INVALID, "nucleus_period must be -1 or in [0, 2^31 - 1)");
   first = j.first_row;
   rows = j.rows ? j.rows : j.ny - j.first_row;
   if (first >= j.ny || rows > j.ny - first) return fail(ctx, FDC_INVALID, "row range outside the grid");

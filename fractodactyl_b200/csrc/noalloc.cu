@@ -125,6 +125,10 @@ extern "C" fdc_status fdc_render_noalloc(int device, const double *orbit, uint64
   if (!(j.escape_radius > 0.0) || !std::isfinite(j.escape_radius * j.escape_radius))
     return fail(FDC_INVALID, "escape radius must be positive and its square finite", error, error_cap);
   if (!(j.h_m >= 1.0 && j.h_m < 2.0)) return fail(FDC_INVALID, "h_m must lie in [1, 2)", error, error_cap);
+  if (j.h_e < -(1ll << 30) || j.h_e > (1ll << 30))
+    return fail(FDC_INVALID, "h_e must lie in [-2^30, 2^30]", error, error_cap);
+  if (j.nucleus_period < -1 || j.nucleus_period >= (1ll << 31) - 1)
+    return fail(FDC_INVALID, "nucleus_period must be -1 or in [0, 2^31 - 1)", error, error_cap);
   uint32_t first = j.first_row, rows = j.rows ? j.rows : j.ny - j.first_row;
   if (first >= j.ny || rows > j.ny - first) return fail(FDC_INVALID, "row range outside the grid", error, error_cap);
   if (HEADER_BYTES + 8ull * rows > SCRATCH_BYTES)

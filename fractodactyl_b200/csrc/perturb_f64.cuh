@@ -57,7 +57,7 @@ struct Params {
   double c_re, c_im, h, h_m;
   int64_t h_e;
   double cosr, sinr, half_x, half_y;
-  uint64_t max_iter;
+  uint32_t max_iter;  // < 2^32 (checked by the route)
   double r2;
   int64_t nucleus;
   double px_m;  // DE output pixel h_m * ss (store.rs:57-63)
@@ -98,8 +98,9 @@ struct State {
   Multiplier mu;
   Contraction ct;
   double adc, shift;
-  int64_t offset_exp, delta_exp, derivative_exp;
-  int64_t nucleus;
+  int32_t offset_exp, delta_exp;  // |h_e| <= 2^30 (checked by the route): deltas stay within 32 bits
+  int64_t derivative_exp;
+  int32_t nucleus;               // < 2^31 - 1 (checked by the route)
   uint32_t n, chk, sn, hold, blocks, skipped;  // n < max_iter < 2^32; chk saturates at 2^32 - 1
   uint32_t lim;  // relimit()
   uint32_t m, idx;
@@ -272,7 +273,37 @@ __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res
   double pr = EXT ? s.scale * s.xr : s.xr, pi = EXT ? s.scale * s.xi : s.xi;
   double fr = Z.x + pr, fi = Z.y + pi;
   double f2 = fr * fr + fi * fi;
-  if (f2 > p.r2) {
+  {
+    // Quiet iterations (no escape, nucleus gate, rebase, rescaling or periodicity event)
+    // leave only z for the next iteration: one test of every event, then the full
+    // sequence below only when one of them may fire. Same expressions as below.
+    const double delta2 = pr * pr + pi * pi;
+    const bool rebase = EXT ? f2 <= delta2 : f2 < delta2;
+    bool quiet = !(f2 > p.r2) && !rebase && s.m != p.last && !(s.nucleus >= 0 && s.n == (uint32_t)s.nucleus + 1u);
+    if (EXT) {
+      const double magnitude = rmax(fabs(s.xr), fabs(s.xi));
+      quiet = quiet && !(magnitude > HI && s.delta_exp < 0) && !(magnitude < LO && magnitude != 0.0);
+    }
+    const double check_r = EXT ? pr : s.xr, check_i = EXT ? pi : s.xi;
+    bool judge = check_r * check_r + check_i * check_i > RES2 * f2;
+    if (EXT) judge = judge && s.returns < 4;
+    const double dist = fabs(fr - s.sr) + fabs(fi - s.si);
+    const double size = fabs(s.sr) + fabs(s.si);
+    bool calm;
+    if (EXT) {
+      calm = s.n < s.chk && !(judge && dist < 1e-13 * size + 1e-300);
+    } else {
+      const bool held = s.hold > 0 && s.n - s.sn < s.hold;  // sn <= n while hold > 0
+      calm = judge ? !(dist < 1e-3 * size) && (s.hold > 0 ? held : !(s.pending || s.n >= s.chk))
+                   : (s.hold > 0 ? held : s.n < s.chk);
+    }
+    if (__builtin_expect(quiet && calm, 1)) {
+      s.fr = fr;
+      s.fi = fi;
+      return false;
+    }
+  }
+  if (__builtin_expect(f2 > p.r2, 0)) {
     res.kind = 0;
     res.n = s.n;
     res.zr = fr;
@@ -282,7 +313,7 @@ __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res
     res.dexp = s.derivative_exp;
     return true;
   }
-  if (s.nucleus >= 0 && (uint64_t)s.n == (uint64_t)s.nucleus + 1) {
+  if (__builtin_expect(s.nucleus >= 0, 0) && s.n == (uint32_t)s.nucleus + 1u) {
     if (s.ct.small()) {
       res.kind = 1;
       res.n = s.n;
@@ -296,7 +327,7 @@ __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res
   // z of the next iteration, Z[m] + delta with the final m and delta: (fr, fi) unless the
   // delta or its scale changes below
   bool moved = false;
-  if (rebase || s.m == p.last) {
+  if (__builtin_expect(rebase || s.m == p.last, 0)) {
     moved = true;
     if (EXT) {
       if (f2 > SQUARE_OK) {
@@ -307,7 +338,7 @@ __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res
         Cx3 t = sum2(Cx3{Z.x, Z.y, 0}, Cx3{s.xr, s.xi, s.delta_exp}, s.delta_exp);
         s.xr = t.re;
         s.xi = t.im;
-        s.delta_exp = t.e;
+        s.delta_exp = (int32_t)t.e;
       }
       s.scale = exp2i(s.delta_exp);
       s.m = 0;
@@ -328,7 +359,7 @@ __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res
         Cx3 w = zero_step(Cx3{s.xr, s.xi, s.delta_exp}, Cx3{s.ar, s.ai, s.offset_exp});
         s.xr = w.re;
         s.xi = w.im;
-        s.delta_exp = w.e;
+        s.delta_exp = (int32_t)w.e;
         s.scale = exp2i(s.delta_exp);
         s.m = 1;
         s.n = s.n + 1;
@@ -355,12 +386,12 @@ __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res
     }
   } else if (EXT) {
     double magnitude = rmax(fabs(s.xr), fabs(s.xi));
-    int64_t k = 0;
+    int32_t k = 0;
     if (magnitude > HI && s.delta_exp < 0)
       k = -s.delta_exp < 32 ? -s.delta_exp : 32;
     else if (magnitude < LO && magnitude != 0.0)
       k = -32;
-    if (k != 0) {
+    if (__builtin_expect(k != 0, 0)) {
       moved = true;
       double factor = exp2i(-k);
       s.xr = s.xr * factor;
@@ -392,7 +423,7 @@ __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res
         relimit(p, s);
       }
     } else if (s.hold > 0) {
-      if ((uint64_t)s.n >= (uint64_t)s.sn + s.hold) {
+      if (s.n - s.sn >= s.hold) {  // sn <= n while hold > 0
         s.hold = 0;
         s.predicted = false;
         s.pending = true;
@@ -457,7 +488,7 @@ __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res
     return false;
   }
   if (s.hold > 0) {
-    if ((uint64_t)s.n < (uint64_t)s.sn + s.hold) return false;
+    if (s.n - s.sn < s.hold) return false;
     s.hold = 0;
     s.predicted = false;
     s.pending = true;
@@ -584,7 +615,7 @@ __device__ __forceinline__ int init(const Params &p, uint64_t slot, State<EXT> &
   if (EXT) {  // grid.rs:709-723
     s.ar = ux * p.h_m;
     s.ai = uy * p.h_m;
-    s.offset_exp = p.h_e;
+    s.offset_exp = (int32_t)p.h_e;
   } else {
     s.ar = ux * p.h;
     s.ai = uy * p.h;
@@ -626,7 +657,7 @@ __device__ __forceinline__ int init(const Params &p, uint64_t slot, State<EXT> &
   s.qi = 0.0;
   s.qstep = 0.0;
   s.adc = L ? sqrt(s.ar * s.ar + s.ai * s.ai) : 0.0;
-  s.nucleus = p.nucleus;
+  s.nucleus = (int32_t)p.nucleus;
   s.ct.reset();
   s.blocks = 0;
   s.skipped = 0;
