@@ -38,6 +38,8 @@ class Job(C.Structure):
         ("first_row", C.c_uint32),
         ("rows", C.c_uint32),
         ("deadline_ms", C.c_double),
+        ("first_col", C.c_uint32),
+        ("cols", C.c_uint32),
     ]
 
 

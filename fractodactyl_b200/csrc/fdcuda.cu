@@ -219,6 +219,8 @@ fdc_status prepare(fdc_ctx *ctx, const OrbitDev &o, const fdc_job &j, fdk::Param
   first = j.first_row;
   rows = j.rows ? j.rows : j.ny - j.first_row;
   if (first >= j.ny || rows > j.ny - first) return fail(ctx, FDC_INVALID, "row range outside the grid");
+  const uint32_t cols = j.cols ? j.cols : j.nx - j.first_col;
+  if (j.first_col >= j.nx || cols > j.nx - j.first_col) return fail(ctx, FDC_INVALID, "column range outside the grid");
   const bool ext = j.tier == FDC_TIER_SCALED;
   // The scaled tier's exact-range step from Z_0 continues at Z_1 (sample.rs:430-447),
   // which needs a next point after it.
@@ -262,7 +264,11 @@ fdc_status prepare(fdc_ctx *ctx, const OrbitDev &o, const fdc_job &j, fdk::Param
   p.first_row = first;
   p.rows = rows;
   p.tile_shift = ctx->tune.tile_w ? (uint32_t)__builtin_ctz(ctx->tune.tile_w) : 3u;
-  p.tiles_x = (j.nx + (1u << p.tile_shift) - 1) >> p.tile_shift;
+  p.first_col = j.first_col;
+  p.cols = cols;
+  p.in_pitch = cols;  // mask and offsets are staged as the window
+  p.out_pitch = j.nx;
+  p.tiles_x = (cols + (1u << p.tile_shift) - 1) >> p.tile_shift;
   p.tier = j.tier;
   p.flags = (deriv ? fdk::F_DERIV : 0) | (bla ? fdk::F_BLA : 0) | ((j.flags & FDC_SHIFT) ? fdk::F_SHIFT : 0);
   p.c_re = j.c_re;
@@ -282,7 +288,6 @@ fdc_status prepare(fdc_ctx *ctx, const OrbitDev &o, const fdc_job &j, fdk::Param
   const uint32_t tile_h = 32u >> p.tile_shift;
   p.total = (uint64_t)p.tiles_x * ((rows + tile_h - 1) / tile_h) * 32;
   p.deadline_ns = j.deadline_ms > 0 ? (uint64_t)(j.deadline_ms * 1e6) : 0;
-  p.out_base = (uint64_t)first * j.nx;
   p.defer = defer_for(ctx, p.tier == FDC_TIER_SCALED);
 
   p.orbit32 = o.z32;
@@ -466,8 +471,17 @@ fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counte
   const bool bla = (j.flags & FDC_BLA) != 0;
   const bool deriv = (j.flags & FDC_DERIVATIVE) != 0;
   CK(cudaSetDevice(ctx->device));
-  const uint64_t n_rows = (uint64_t)rows * j.nx;
+  // the window: rows x cols samples; outputs and inputs of full frame rows (pitch nx),
+  // staged as the window (pitch cols)
+  const uint64_t n_rows = (uint64_t)rows * p.cols;
   const bool dev_out = (j.flags & FDC_DEVICE_OUT) != 0;
+  const bool full = p.cols == j.nx;
+  const uint64_t origin = (uint64_t)first * j.nx + p.first_col;
+  auto window_copy = [&](void *dst, size_t dpitch, const void *src, size_t spitch, size_t width,
+                         cudaMemcpyKind kind) {
+    if (full) return cudaMemcpyAsync(dst, src, width * rows, kind, ctx->stream);
+    return cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, rows, kind, ctx->stream);
+  };
 
   // Device buffers: caller's (FDC_DEVICE_OUT) or staging for the rendered rows.
   struct Col {
@@ -497,7 +511,7 @@ fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counte
   void *dptr[9];
   for (int c = 0; c < 9; ++c) {
     if (!cols[c].host) dptr[c] = nullptr;
-    else if (dev_out) dptr[c] = (char *)cols[c].host + p.out_base * cols[c].width;
+    else if (dev_out) dptr[c] = (char *)cols[c].host + origin * cols[c].width;
     else dptr[c] = stage + offs[c];
   }
   p.cls = (uint8_t *)dptr[0];
@@ -509,18 +523,25 @@ fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counte
   p.dz_out = (double2 *)dptr[6];
   p.dexp_out = (int64_t *)dptr[7];
   p.status = (uint8_t *)dptr[8];
+  p.out_pitch = dev_out ? j.nx : p.cols;
   if (j.mask) {
     p.mask = (const uint8_t *)(stage + offs[9]);
-    CK(cudaMemcpyAsync(stage + offs[9], j.mask + p.out_base, n_rows, cudaMemcpyHostToDevice, ctx->stream));
+    CK(window_copy(stage + offs[9], p.cols, j.mask + origin, j.nx, p.cols, cudaMemcpyHostToDevice));
   }
   if (j.offsets) {
     p.offsets = (const double2 *)(stage + offs[10]);
-    CK(cudaMemcpyAsync(stage + offs[10], j.offsets + 2 * p.out_base, n_rows * 16, cudaMemcpyHostToDevice,
-                       ctx->stream));
+    CK(window_copy(stage + offs[10], p.cols * 16ull, j.offsets + 2 * origin, j.nx * 16ull, p.cols * 16ull,
+                   cudaMemcpyHostToDevice));
   }
   // Samples that are never reached keep zeroed columns and status 0.
-  for (int c = 0; c < 9; ++c)
-    if (dptr[c]) CK(cudaMemsetAsync(dptr[c], 0, n_rows * cols[c].width, ctx->stream));
+  for (int c = 0; c < 9; ++c) {
+    if (!dptr[c]) continue;
+    const size_t w = cols[c].width;
+    if (!dev_out || full)
+      CK(cudaMemsetAsync(dptr[c], 0, n_rows * w, ctx->stream));
+    else
+      CK(cudaMemset2DAsync(dptr[c], j.nx * w, 0, p.cols * w, rows, ctx->stream));
+  }
   p.queue = &ctx->scratch->queue;
   p.counters = &ctx->scratch->counters;
   p.timed_out = &ctx->scratch->timed_out;
@@ -546,9 +567,11 @@ fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counte
   CK(cudaEventRecord(ctx->ev1, ctx->stream));
   if (!dev_out) {
     for (int c = 0; c < 9; ++c)
-      if (cols[c].host)
-        CK(cudaMemcpyAsync((char *)cols[c].host + p.out_base * cols[c].width, dptr[c], n_rows * cols[c].width,
-                           cudaMemcpyDeviceToHost, ctx->stream));
+      if (cols[c].host) {
+        const size_t w = cols[c].width;
+        CK(window_copy((char *)cols[c].host + origin * w, j.nx * w, dptr[c], p.cols * w, p.cols * w,
+                       cudaMemcpyDeviceToHost));
+      }
   }
   Scratch sc;
   CK(cudaMemcpyAsync(&sc, ctx->scratch, sizeof sc, cudaMemcpyDeviceToHost, ctx->stream));
@@ -610,7 +633,7 @@ fdc_status fdc_batch_create(fdc_ctx *ctx, const fdc_job *jobs, const fdc_out *ou
     }
     fdk::Params &p = params[k];
     const fdc_out &o = outs[k];
-    const uint64_t b0 = p.out_base;
+    const uint64_t b0 = (uint64_t)p.first_row * j.nx + p.first_col;  // the window's first sample
     p.cls = o.cls ? o.cls + b0 : nullptr;
     p.n_out = o.n ? o.n + b0 : nullptr;
     p.nu = o.nu ? o.nu + b0 : nullptr;

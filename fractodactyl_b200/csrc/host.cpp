@@ -218,28 +218,37 @@ inline bool sadd(bool an, const uint64_t *a, bool bn, const uint64_t *b, uint64_
 // o = floor(a^2 / 2^(64 (L-1))): column-wise (product-scanning) square with a 192-bit
 // column accumulator, doubling the off-diagonal terms as they are added.
 void square_trunc(const uint64_t *a, uint64_t *o, size_t L, uint64_t *prod) {
-  uint64_t c0 = 0, c1 = 0, c2 = 0;  // accumulator (c2:c1:c0)
+  // Column by column (Comba): per column k the products a_i a_j with i < j, i + j = k,
+  // summed once into (d2:d1:d0) and doubled, plus the square a_{k/2}^2 for even k, added
+  // to the carry (c1:c0) of the columns below. Exact: the full 2L-limb product.
+  uint64_t c0 = 0, c1 = 0;
   for (size_t k = 0; k < 2 * L - 1; ++k) {
-    size_t lo = k >= L ? k - L + 1 : 0;
-    size_t hi = k / 2;  // i <= j = k - i
-    for (size_t i = lo; i <= hi; ++i) {
-      size_t j = k - i;
-      if (j >= L) continue;
-      u128 p = (u128)a[i] * a[j];
-      uint64_t pl = (uint64_t)p, ph = (uint64_t)(p >> 64);
-      int times = i == j ? 1 : 2;
-      for (int t = 0; t < times; ++t) {
-        u128 s = (u128)c0 + pl;
-        c0 = (uint64_t)s;
-        s = (u128)c1 + ph + (uint64_t)(s >> 64);
-        c1 = (uint64_t)s;
-        c2 += (uint64_t)(s >> 64);
-      }
+    const size_t lo = k >= L ? k - L + 1 : 0;
+    uint64_t d0 = 0, d1 = 0, d2 = 0;
+    for (size_t i = lo; 2 * i < k; ++i) {
+      const u128 p = (u128)a[i] * a[k - i];
+      u128 t = (u128)d0 + (uint64_t)p;
+      d0 = (uint64_t)t;
+      t = (u128)d1 + (uint64_t)(p >> 64) + (uint64_t)(t >> 64);
+      d1 = (uint64_t)t;
+      d2 += (uint64_t)(t >> 64);
     }
-    prod[k] = c0;
-    c0 = c1;
-    c1 = c2;
-    c2 = 0;
+    d2 = (d2 << 1) | (d1 >> 63);
+    d1 = (d1 << 1) | (d0 >> 63);
+    d0 <<= 1;
+    if ((k & 1) == 0) {
+      const u128 p = (u128)a[k / 2] * a[k / 2];
+      u128 t = (u128)d0 + (uint64_t)p;
+      d0 = (uint64_t)t;
+      t = (u128)d1 + (uint64_t)(p >> 64) + (uint64_t)(t >> 64);
+      d1 = (uint64_t)t;
+      d2 += (uint64_t)(t >> 64);
+    }
+    u128 t = (u128)d0 + c0;
+    prod[k] = (uint64_t)t;
+    t = (u128)d1 + c1 + (uint64_t)(t >> 64);
+    c0 = (uint64_t)t;
+    c1 = d2 + (uint64_t)(t >> 64);
   }
   prod[2 * L - 1] = c0;
   std::memcpy(o, prod + (L - 1), L * sizeof(uint64_t));

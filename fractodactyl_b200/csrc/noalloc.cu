@@ -131,6 +131,9 @@ extern "C" fdc_status fdc_render_noalloc(int device, const double *orbit, uint64
     return fail(FDC_INVALID, "nucleus_period must be -1 or in [0, 2^31 - 1)", error, error_cap);
   uint32_t first = j.first_row, rows = j.rows ? j.rows : j.ny - j.first_row;
   if (first >= j.ny || rows > j.ny - first) return fail(FDC_INVALID, "row range outside the grid", error, error_cap);
+  const uint32_t cols = j.cols ? j.cols : j.nx - j.first_col;
+  if (j.first_col >= j.nx || cols > j.nx - j.first_col)
+    return fail(FDC_INVALID, "column range outside the grid", error, error_cap);
   if (HEADER_BYTES + 8ull * rows > SCRATCH_BYTES)
     return fail(FDC_INVALID, "job needs " + std::to_string(HEADER_BYTES + 8ull * rows) +
                                  " bytes of scratch; this entry point has " + std::to_string(SCRATCH_BYTES) +
@@ -162,8 +165,12 @@ extern "C" fdc_status fdc_render_noalloc(int device, const double *orbit, uint64
   p.ny = j.ny;
   p.first_row = first;
   p.rows = rows;
+  p.first_col = j.first_col;
+  p.cols = cols;
+  p.in_pitch = cols;
+  p.out_pitch = j.nx;
   p.tile_shift = 3;  // 8x4-sample tiles
-  p.tiles_x = (j.nx + 7) / 8;
+  p.tiles_x = (cols + 7) / 8;
   p.tier = j.tier;
   p.flags = deriv ? fdk::F_DERIV : 0;
   p.c_re = j.c_re;
@@ -180,16 +187,16 @@ extern "C" fdc_status fdc_render_noalloc(int device, const double *orbit, uint64
   p.nucleus = j.nucleus_period;
   p.px_m = j.h_m * (double)j.ss;
   p.px_e = j.h_e;
-  p.out_base = (uint64_t)first * j.nx;
-  p.cls = out->cls ? out->cls + p.out_base : nullptr;
-  p.n_out = out->n ? out->n + p.out_base : nullptr;
-  p.nu = out->nu ? out->nu + p.out_base : nullptr;
-  p.de = out->de ? out->de + p.out_base : nullptr;
-  p.normal = out->normal ? out->normal + p.out_base : nullptr;
-  p.z_out = out->z ? (double2 *)out->z + p.out_base : nullptr;
-  p.dz_out = out->dz ? (double2 *)out->dz + p.out_base : nullptr;
-  p.dexp_out = out->dexp ? out->dexp + p.out_base : nullptr;
-  p.status = out->status ? out->status + p.out_base : nullptr;
+  const uint64_t b0 = (uint64_t)first * j.nx + j.first_col;  // the window's first sample
+  p.cls = out->cls ? out->cls + b0 : nullptr;
+  p.n_out = out->n ? out->n + b0 : nullptr;
+  p.nu = out->nu ? out->nu + b0 : nullptr;
+  p.de = out->de ? out->de + b0 : nullptr;
+  p.normal = out->normal ? out->normal + b0 : nullptr;
+  p.z_out = out->z ? (double2 *)out->z + b0 : nullptr;
+  p.dz_out = out->dz ? (double2 *)out->dz + b0 : nullptr;
+  p.dexp_out = out->dexp ? out->dexp + b0 : nullptr;
+  p.status = out->status ? out->status + b0 : nullptr;
   p.total = (uint64_t)p.tiles_x * ((rows + 3) / 4) * 32;
   p.queue = (unsigned long long *)pd.scratch;
   p.counters = (fdk::Counters *)(pd.scratch + 8);

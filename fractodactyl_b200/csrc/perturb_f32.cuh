@@ -410,16 +410,17 @@ __device__ __forceinline__ int init_f32(const Params &p, uint64_t slot, StateF &
   uint64_t tile = slot >> 5;
   uint32_t w = (uint32_t)slot & 31u;
   uint32_t tx = (uint32_t)(tile % p.tiles_x), ty = (uint32_t)(tile / p.tiles_x);
-  uint32_t i = (tx << p.tile_shift) + (w & ((1u << p.tile_shift) - 1u));
+  uint32_t ii = (tx << p.tile_shift) + (w & ((1u << p.tile_shift) - 1u));
   uint32_t jj = ty * (32u >> p.tile_shift) + (w >> p.tile_shift);
-  if (i >= p.nx || jj >= p.rows) return 0;
-  uint32_t j = p.first_row + jj;
+  if (ii >= p.cols || jj >= p.rows) return 0;
+  uint32_t i = p.first_col + ii, j = p.first_row + jj;
   uint32_t idx = j * p.nx + i;
-  if (p.mask && !p.mask[idx - p.out_base]) return 0;
+  const uint64_t in = (uint64_t)jj * p.in_pitch + ii;
+  if (p.mask && !p.mask[in]) return 0;
   s.idx = idx;
   double ux, uy;
   if (p.offsets) {
-    double2 o = p.offsets[idx - p.out_base];
+    double2 o = p.offsets[in];
     ux = o.x;
     uy = o.y;
   } else {

@@ -51,6 +51,9 @@ struct Params {
   uint32_t bla_count[MAX_LEVELS];
   // frame
   uint32_t nx, ny, first_row, rows, tiles_x;
+  uint32_t first_col, cols;        // rendered window: columns [first_col, first_col + cols) of those rows
+  uint32_t in_pitch, out_pitch;    // row pitch (samples) of the mask/offsets inputs and of the outputs,
+                                   // whose pointers address the window's first sample
   uint32_t tile_shift;  // tiles are 2^tile_shift samples wide and 32 / 2^tile_shift rows high
   int32_t tier;
   uint32_t flags;
@@ -79,7 +82,6 @@ struct Params {
   uint64_t total;        // queue slots (tiles * 32)
   uint64_t deadline_ns;  // 0 = none
   uint32_t *timed_out;
-  uint64_t out_base;  // outputs hold the rendered rows only: index idx - out_base
   uint32_t defer;     // BLA lanes a warp gathers before it applies their blocks (warp_step)
 };
 
@@ -594,16 +596,17 @@ __device__ __forceinline__ int init(const Params &p, uint64_t slot, State<EXT> &
   uint64_t tile = slot >> 5;
   uint32_t w = (uint32_t)slot & 31u;
   uint32_t tx = (uint32_t)(tile % p.tiles_x), ty = (uint32_t)(tile / p.tiles_x);
-  uint32_t i = (tx << p.tile_shift) + (w & ((1u << p.tile_shift) - 1u));
+  uint32_t ii = (tx << p.tile_shift) + (w & ((1u << p.tile_shift) - 1u));
   uint32_t jj = ty * (32u >> p.tile_shift) + (w >> p.tile_shift);
-  if (i >= p.nx || jj >= p.rows) return 0;
-  uint32_t j = p.first_row + jj;
+  if (ii >= p.cols || jj >= p.rows) return 0;
+  uint32_t i = p.first_col + ii, j = p.first_row + jj;
   uint32_t idx = j * p.nx + i;
-  if (p.mask && !p.mask[idx - p.out_base]) return 0;  // inputs hold the rendered rows only
+  const uint64_t in = (uint64_t)jj * p.in_pitch + ii;  // inputs hold the window only
+  if (p.mask && !p.mask[in]) return 0;
   s.idx = idx;
   double ux, uy;
   if (p.offsets) {
-    double2 o = p.offsets[idx - p.out_base];
+    double2 o = p.offsets[in];
     ux = o.x;
     uy = o.y;
   } else {  // view.rs:118-122
@@ -668,7 +671,8 @@ __device__ __forceinline__ int init(const Params &p, uint64_t slot, State<EXT> &
 
 // Column encoder (store.rs:66-112, Bound absent) and raw state.
 __device__ __forceinline__ void put(const Params &p, uint32_t sample, const Result &r) {
-  const uint64_t idx = sample - p.out_base;
+  const uint32_t j = sample / p.nx, i = sample - j * p.nx;
+  const uint64_t idx = (uint64_t)(j - p.first_row) * p.out_pitch + (i - p.first_col);
   if (p.status) p.status[idx] = 1;
   if (p.n_out) p.n_out[idx] = (uint32_t)(r.kind == 2 ? p.max_iter : r.n);
   if (r.kind != 0) {

@@ -68,6 +68,8 @@ typedef struct {
   const double *offsets;  /* optional, 2*nx*ny host doubles: per-sample (ux, uy) instead of the grid */
   uint32_t first_row, rows; /* render rows [first_row, first_row + rows); rows 0 = all */
   double deadline_ms;     /* stop taking new samples after this long; 0 = none */
+  uint32_t first_col, cols; /* and of those rows columns [first_col, first_col + cols); cols 0 = all.
+                             * Outputs, mask and offsets still span whole rows of nx samples. */
 } fdc_job;
 
 /* Caller-owned outputs, nx*ny entries each (only rows rendered are written); any may be

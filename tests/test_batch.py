@@ -48,6 +48,10 @@ def _job(dev, frame):
 
 def test_batch_equals_single_renders(dev):
     handles, jobs = zip(*[_job(dev, f) for f in FRAMES])
+    # plus a window (rows 4..33, columns 16..95) of the second frame
+    hw, jw = _job(dev, FRAMES[1])
+    jw.first_row, jw.rows, jw.first_col, jw.cols = 4, 30, 16, 80
+    handles, jobs = handles + (hw,), jobs + (jw,)
     singles = [dev.render_job(j, raw=True, columns=("nu", "de", "normal")) for j in jobs]
     b = dev.batch(jobs, columns=("nu", "de", "normal"), raw=True)
     try:
@@ -56,11 +60,12 @@ def test_batch_equals_single_renders(dev):
             assert total.launches >= 2
             for k, (arrays, cnt, _) in enumerate(singles):
                 got = b.columns(k)
-                assert np.all(got["status"] == 1), (replay, k)
+                assert np.array_equal(got["status"], arrays["status"]), (replay, k)
+                assert got["status"].sum() == cnt.samples, (replay, k)
                 for name in ("cls", "n", "z", "dz", "dexp"):
                     assert np.array_equal(got[name], arrays[name]), (replay, k, name)
                 for name in ("nu", "de", "normal"):
-                    if FRAMES[k][6] and name in FRAMES[k][6]:
+                    if k < len(FRAMES) and name in FRAMES[k][6]:
                         assert np.array_equal(got[name], arrays[name]), (replay, k, name)
                 assert per[k].samples == cnt.samples and per[k].iterations == cnt.iterations, (replay, k)
                 assert per[k].blocks == cnt.blocks and per[k].skipped == cnt.skipped, (replay, k)

@@ -251,6 +251,65 @@ def test_mask_rows_and_status(dev):
     assert cnt.samples == sel.sum()
 
 
+def test_column_window_host_and_device_outputs(dev):
+    """A window of columns and rows (first_col/cols, first_row/rows) renders exactly the
+    samples of the full frame inside it, with host outputs (staged as the window, with a
+    mask and per-sample offsets) and with device outputs of whole rows; nothing outside it
+    is written."""
+    import torch
+    view = fd.View("-0.7453", "0.1127", "0.0065")
+    nx, ny = 72, 40
+    p = fd.Params(nx, ny, max_iter=3000)
+    r, bits = fd.reference(view, p)
+    plane = fd.Plane.new(view, nx, ny)
+    h = dev.upload(r)
+    win = np.zeros((ny, nx), bool)
+    win[7:30, 13:50] = True
+    win = win.ravel()
+    try:
+        job = lambda: fd.route.make_job(plane, plane.tier, p, h, r.nucleus_period(), _lib.DERIVATIVE)
+        full, _, _ = dev.render_job(job(), raw=True)
+        j = job()
+        j.first_row, j.rows, j.first_col, j.cols = 7, 23, 13, 37
+        a, cnt, _ = dev.render_job(j, raw=True)
+        assert cnt.samples == win.sum()
+        assert np.all(a["status"][win] == 1) and np.all(a["status"][~win] == 0)
+        for k in ("cls", "n", "nu", "de", "normal", "z", "dz", "dexp"):
+            assert np.array_equal(a[k][win], full[k][win]), k
+            assert not np.any(a[k][~win]), k
+        # mask and offsets inside a window: the offsets of the grid reproduce the grid
+        mask = (np.arange(nx * ny) % 4 != 1).astype(np.uint8)
+        ii, jj = np.meshgrid(np.arange(nx), np.arange(ny))
+        x, y = ii.ravel() + 0.5 - nx / 2.0, jj.ravel() + 0.5 - ny / 2.0
+        offs = np.ascontiguousarray(np.stack([plane.cos_rot * x + plane.sin_rot * y,
+                                              plane.sin_rot * x - plane.cos_rot * y], axis=1))
+        j = job()
+        j.first_row, j.rows, j.first_col, j.cols = 7, 23, 13, 37
+        j.mask, j.offsets = mask.ctypes.data, offs.ctypes.data
+        b, cnt, _ = dev.render_job(j, raw=True)
+        sel = win & (mask == 1)
+        assert cnt.samples == sel.sum() and np.all(b["status"][~sel] == 0)
+        for k in ("cls", "n", "z", "dz", "dexp"):
+            assert np.array_equal(b[k][sel], full[k][sel]), k
+        # device outputs of whole rows
+        bufs = {k: torch.zeros(nx * ny * (2 if k in ("z",) else 1), dtype=t, device="cuda:0")
+                for k, t in (("cls", torch.uint8), ("n", torch.int32), ("status", torch.uint8), ("z", torch.float64))}
+        j = job()
+        j.first_row, j.rows, j.first_col, j.cols = 7, 23, 13, 37
+        j.flags |= _lib.DEVICE_OUT
+        dev.render_job(j, device_out={k: v.data_ptr() for k, v in bufs.items()})
+        got = {k: v.cpu().numpy() for k, v in bufs.items()}
+        assert np.array_equal(got["status"].astype(bool), win)
+        assert np.array_equal(got["cls"][win], full["cls"][win])
+        assert np.array_equal(got["n"].view(np.uint32)[win], full["n"][win])
+        assert np.array_equal(got["z"].reshape(-1, 2)[win], full["z"][win])
+        j.first_col, j.cols = 60, 13  # past the last column
+        with pytest.raises(fd.route.RouteError, match="column range"):
+            dev.render_job(j, device_out={k: v.data_ptr() for k, v in bufs.items()})
+    finally:
+        dev.free(h)
+
+
 def test_invalid_inputs_are_refused_not_crashed(dev):
     L = _lib.lib()
     h = C.c_int32()
