@@ -16,6 +16,7 @@ time = max over ranks. --impl reference: the reference CPU kernel (this repo's C
 restatement of it, oracle/) on the host cores over a bounded sample of the frame's rows.
 """
 import argparse
+import ctypes as C
 import json
 import os
 import statistics
@@ -344,13 +345,175 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_set(args):
+    """Configs 3-5: the jittered 4-spp frame (one fdc_render per step, offsets staged), the
+    60-frame film and the 256 mixed-location tiles (one batch graph replay per step), in
+    both forms; value = effective pixel-iterations of a step / its device time."""
+    import dataclasses
+
+    import torch
+
+    import fractodactyl_b200 as fd
+    from fractodactyl_b200 import _lib, locations, workloads
+
+    rank, world, local = dist_init(args.gpus)
+    dev = fd.Device(local)
+    cfg = args.config
+    if cfg == 3:
+        fr = locations.config3()
+        if args.nx or args.ny:
+            fr.params.nx, fr.params.ny = args.nx or fr.params.nx, args.ny or fr.params.ny
+            fr.name += f"-grid{fr.params.nx}x{fr.params.ny}"
+        js = workloads.jittered(dev, fr)
+        name, frames = fr.name, [fr]
+    elif cfg == 4:
+        frames = locations.config4(frames=args.frames or 60)
+        js = workloads.film(dev, frames)
+        name = f"c4-film-{len(frames)}x{frames[0].params.nx}x{frames[0].params.ny}-1e-10..1e-500"
+    else:
+        frames = locations.config5()[:args.frames or None]
+        js = workloads.tiles(dev, frames, (256, 256))
+        name = f"c5-mixed-{len(js.jobs)}tiles-256x256-{len(frames)}loc"
+    cols = ["cls", "n", "status", "nu", "de", "normal"]
+    samples = sum(w[1] * w[3] for w in js.windows)
+
+    def with_flag(extra):
+        out = []
+        for j in js.jobs:
+            c = _lib.Job()
+            C.memmove(C.byref(c), C.byref(j), C.sizeof(_lib.Job))
+            c.flags = (j.flags & ~_lib.F32) | extra
+            out.append(c)
+        return out
+
+    clocks = Clocks(local)
+    clocks.start()
+    forms, e2e = {}, None
+    for form, extra in (("fp64_plain", 0), ("fp32_floatexp", _lib.F32)):
+        if args.form != "both" and form != {"fp64": "fp64_plain", "f32": "fp32_floatexp"}[args.form]:
+            continue
+        jobs = with_flag(extra)
+        tot = dict(it=0, blocks=0, skipped=0, ms=0.0, launches=0)
+        if cfg == 3:
+            j = jobs[0]
+            n = j.nx * j.ny
+            dt = {"cls": torch.uint8, "n": torch.int32, "status": torch.uint8, "nu": torch.float64,
+                  "de": torch.float32, "normal": torch.int16}
+            bufs = {c: torch.empty(n, dtype=dt[c], device=f"cuda:{local}") for c in cols}
+            j.flags |= _lib.DEVICE_OUT
+
+            def step():
+                _, cnt, _ = dev.render_job(j, device_out={c: bufs[c].data_ptr() for c in cols})
+                return cnt
+
+            snap = lambda: {c: bufs[c].cpu().numpy().copy() for c in ("cls", "n")}
+        else:
+            b = dev.batch(jobs, columns=("nu", "de", "normal"))
+
+            def step():
+                total, _ = b.run()
+                return total
+
+            snap = lambda: {c: np.concatenate([b.columns(k)[c] for k in range(len(jobs))]) for c in ("cls", "n")}
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        barrier(world)
+        for _ in range(args.steps):
+            cnt = step()
+            tot["it"] += cnt.iterations
+            tot["blocks"] += cnt.blocks
+            tot["skipped"] += cnt.skipped
+            tot["ms"] += cnt.kernel_ms
+            tot["launches"] += cnt.launches
+        barrier(world)
+        sn = snap()
+        if cfg != 3:
+            b.free()
+        else:
+            del bufs
+        ms = allmax(tot["ms"], world)
+        forms[form] = dict(tot=tot, snap=sn, ms=ms, value=(tot["it"] - tot["blocks"] + tot["skipped"]) * world /
+                           (ms * 1e-3))
+        torch.cuda.empty_cache()
+    clk = clocks.stop()
+    agree = None
+    if len(forms) == 2:
+        a, bb = forms["fp64_plain"]["snap"], forms["fp32_floatexp"]["snap"]
+        ea, eb = a["cls"] == 0, bb["cls"] == 0
+        dn = np.abs(a["n"].astype(np.int64) - bb["n"].astype(np.int64))
+        agree = {"count_match": float(((ea == eb) & (~ea | (dn == 0))).mean()),
+                 "within_one": float(((ea == eb) & (~ea | (dn <= 1))).mean())}
+    head = "fp32_floatexp" if ("fp32_floatexp" in forms and (agree is None or agree["count_match"] >= 0.999)) \
+        else "fp64_plain"
+    # e2e through the public API with host buffers, one step: uploads, render(s), columns to host
+    h2d = sum(16 * len(r) + (56 * len(bl.blocks) if bl is not None else 0) for r, bl in zip(js.refs, js.blas))
+    if cfg == 3:
+        h2d += 16 * samples
+    d2h = samples * sum(OUT_BYTES[c] for c in cols)
+    js.free(dev)
+    barrier(world)
+    t0 = time.perf_counter()
+    if cfg == 3:
+        h = dev.upload(js.refs[0], js.blas[0])
+        j = with_flag(_lib.F32 if head == "fp32_floatexp" else 0)[0]
+        j.orbit = h
+        _, cnt, _ = dev.render_job(j, columns=("nu", "de", "normal"))
+        dev.free(h)
+        eff = cnt.iterations - cnt.blocks + cnt.skipped
+    else:
+        hs = {}
+        jobs = with_flag(_lib.F32 if head == "fp32_floatexp" else 0)
+        for j, old in zip(jobs, js.handles):
+            if old not in hs:  # locations appear in order; a film has one
+                loc = 0 if len(js.refs) == 1 else len(hs)
+                hs[old] = dev.upload(js.refs[loc], js.blas[loc])
+            j.orbit = hs[old]
+        b = dev.batch(jobs, columns=("nu", "de", "normal"))
+        total, _ = b.run()
+        host = [b.columns(k) for k in range(len(jobs))]
+        b.free()
+        for h in hs.values():
+            dev.free(h)
+        eff = total.iterations - total.blocks + total.skipped
+    e2e_s = allmax(time.perf_counter() - t0, world)
+    e2e = {"value": eff * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+           "steps": 1}
+    if rank == 0:
+        rf = forms.get("fp64_plain", forms[head])
+        line = {"metric": METRIC, "value": forms[head]["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": forms[head]["ms"] / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded locations)",
+                "config": {"workload": name, "samples_per_step": samples, "jobs": len(js.jobs),
+                           "locations": len(js.refs), "reference_points": [len(r) for r in js.refs][:4],
+                           "bits": sorted({r.bits for r in js.refs})[-1], "form": head,
+                           "l2": "inputs larger than L2 per step" if samples * 20 > (126 << 20) else "not flushed",
+                           "parallelism": f"replicas x{world}"},
+                "forms": {k: {"value": v["value"], "ms_per_step": v["ms"] / args.steps,
+                              "iterations": v["tot"]["it"] // args.steps, "blocks": v["tot"]["blocks"] // args.steps,
+                              "skipped": v["tot"]["skipped"] // args.steps,
+                              "launches_per_step": v["tot"]["launches"] // args.steps} for k, v in forms.items()},
+                "fp32_vs_fp64": (forms["fp32_floatexp"]["value"] / forms["fp64_plain"]["value"]
+                                 if len(forms) == 2 else None),
+                "agreement_fp32_vs_fp64": agree,
+                "setup_seconds": {"orbit": js.orbit_seconds, "bla": js.bla_seconds},
+                "cpu_baseline": None, "clocks": clk,
+                "gpu_launches": sum(v["tot"]["launches"] for v in forms.values()), "e2e": e2e}
+        print(json.dumps(line), flush=True)
+    dev.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--config", type=int, choices=(1, 2), default=2)
+    ap.add_argument("--config", type=int, choices=(1, 2, 3, 4, 5), default=2)
+    ap.add_argument("--frames", type=int, default=0, help="configs 4/5: first N frames / locations only")
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -361,7 +524,13 @@ def main():
     ap.add_argument("--form", choices=("both", "fp64", "f32"), default="both")
     args = ap.parse_args()
     if args.impl == "reference":
+        if args.config > 2:
+            print(json.dumps({"impl": "reference", "unavailable": "configs 3-5 are measured on the GPU only; the "
+                              "reference CPU arm runs configs 1 and 2"}))
+            return
         run_reference(args)
+    elif args.config > 2:
+        run_set(args)
     else:
         run_ours(args)
 

@@ -23,6 +23,7 @@ struct BlaDev {
   double *r2 = nullptr;
   double2 *coef = nullptr;
   double2 *ab = nullptr;
+  uint64_t points = 0, blocks = 0;  // sizes of the buffers above: fused 32 B per point; 8, 32, 16 B per block
   uint32_t levels = 0;
   uint32_t off[fdk::MAX_LEVELS] = {};
   uint32_t count[fdk::MAX_LEVELS] = {};
@@ -46,7 +47,8 @@ struct Scratch {
   unsigned long long pad[3];
   fdk::Counters counters;
   uint32_t timed_out;
-  uint32_t pad2[7];
+  uint32_t bad;  // fdc_upload_bla's value checks
+  uint32_t pad2[6];
 };
 
 }  // namespace
@@ -70,6 +72,10 @@ struct fdc_ctx {
   int blocks_per_sm_batch[8] = {};
   int blocks_per_sm_batch_f32[4] = {};
   fdc_tuning tune{FDC_DEFAULT_DEFER, 0, 0};
+  // Device buffers of freed orbits and tables (and upload staging), kept by size for the
+  // next upload of the same size: a film or a service re-uploading per frame allocates
+  // once. Stream-ordered: every user runs on `stream`. Freed by fdc_close.
+  std::multimap<size_t, void *> pool;
 };
 
 // Persistent grid of a plain-form kernel: the occupancy limit, or fewer blocks per SM
@@ -120,13 +126,102 @@ fdc_status fail(fdc_ctx *c, fdc_status s, const std::string &msg) {
       return fail(ctx, FDC_DEVICE_ERROR, std::string(#call) + ": " + cudaGetErrorString(e_)); \
   } while (0)
 
-void free_bla(BlaDev &b) {
-  cudaFree(b.fused);
-  cudaFree(b.r2);
-  cudaFree(b.coef);
-  cudaFree(b.ab);
+void *pool_get(fdc_ctx *ctx, size_t bytes) {
+  if (bytes == 0) return nullptr;
+  auto it = ctx->pool.find(bytes);
+  if (it != ctx->pool.end()) {
+    void *p = it->second;
+    ctx->pool.erase(it);
+    return p;
+  }
+  void *p = nullptr;
+  return cudaMalloc(&p, bytes) == cudaSuccess ? p : nullptr;
+}
+
+void pool_put(fdc_ctx *ctx, void *p, size_t bytes) {
+  if (p && bytes) ctx->pool.emplace(bytes, p);
+}
+
+void free_bla(fdc_ctx *ctx, BlaDev &b) {
+  pool_put(ctx, b.fused, 32 * b.points);
+  pool_put(ctx, b.r2, 8 * b.blocks);
+  pool_put(ctx, b.coef, 32 * b.blocks);
+  pool_put(ctx, b.ab, 16 * b.blocks);
   b = BlaDev{};
 }
+
+void free_orbit_buffers(fdc_ctx *ctx, OrbitDev &o) {
+  pool_put(ctx, o.z, 16 * o.len);
+  pool_put(ctx, o.z32, 32 * o.len);
+  free_bla(ctx, o.bla);
+  o.z = nullptr;
+  o.z32 = nullptr;
+}
+
+// Orbit layouts built on the device from the caller's SoA (re[], im[]): interleaved
+// double2 points, and the precision form's 32-byte entries (zr, zi f64; zr, zi f32 in one
+// word, NaN where |Z| < 2^-60, whose steps take the exact path; r^2 of the 2-step block
+// at m, -1 until a table is uploaded).
+__global__ void pack_orbit(const double *__restrict__ re, const double *__restrict__ im, uint64_t len,
+                           double2 *__restrict__ z, double *__restrict__ z32) {
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < len; k += (uint64_t)gridDim.x * blockDim.x) {
+    const double x = re[k], y = im[k];
+    z[k] = make_double2(x, y);
+    float fr = __double2float_rn(x);
+    const float fi = __double2float_rn(y);
+    if (fmax(fabs(x), fabs(y)) < 0x1p-60) fr = __int_as_float(0x7fc00000);
+    double *e = z32 + 4 * k;
+    e[0] = x;
+    e[1] = y;
+    e[2] = __longlong_as_double((long long)(((unsigned long long)__float_as_uint(fi) << 32) | __float_as_uint(fr)));
+    e[3] = -1.0;
+  }
+}
+
+// Table of the export form ([f64; 7] per block: a.re, a.im, b.re, b.im, r, alpha, beta)
+// split into r^2, (a, b) and (alpha, beta); bad |= 1 for a non-finite value, 2 for a
+// negative radius (Bla::new's value checks, bla.rs:184-216).
+__global__ void pack_bla(const double *__restrict__ b7, uint64_t total, double *__restrict__ r2,
+                         double2 *__restrict__ coef, double2 *__restrict__ ab, unsigned *bad) {
+  for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < total;
+       k += (uint64_t)gridDim.x * blockDim.x) {
+    const double *v = b7 + 7 * k;
+    double w[7];
+    bool finite = true;
+    for (int f = 0; f < 7; ++f) {
+      w[f] = v[f];
+      finite = finite && isfinite(w[f]);
+    }
+    if (!finite) atomicOr(bad, 1u);
+    if (w[4] < 0.0) atomicOr(bad, 2u);
+    r2[k] = w[4] * w[4];
+    coef[2 * k] = make_double2(w[0], w[1]);
+    coef[2 * k + 1] = make_double2(w[2], w[3]);
+    ab[k] = make_double2(w[5], w[6]);
+  }
+}
+
+// The fused stream: point m with the squared radii of the level-0 and level-1 blocks
+// starting at Z_m (block t of level i starts at m = 1 + t 2^(i+1), bla.rs:131-135), -1
+// where none starts; the level-0 radius also goes into the precision-form entries.
+__global__ void fuse_bla(const double2 *__restrict__ z, uint64_t len, const double *__restrict__ r2, uint32_t levels,
+                         uint64_t off0, uint64_t cnt0, uint64_t off1, uint64_t cnt1, double *__restrict__ fused,
+                         double *__restrict__ z32) {
+  for (uint64_t m = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; m < len; m += (uint64_t)gridDim.x * blockDim.x) {
+    const double2 p = z[m];
+    double a = -1.0, b = -1.0;
+    if (m >= 1 && levels > 0 && ((m - 1) & 1) == 0 && ((m - 1) >> 1) < cnt0) a = r2[off0 + ((m - 1) >> 1)];
+    if (m >= 1 && levels > 1 && ((m - 1) & 3) == 0 && ((m - 1) >> 2) < cnt1) b = r2[off1 + ((m - 1) >> 2)];
+    double *f = fused + 4 * m;
+    f[0] = p.x;
+    f[1] = p.y;
+    f[2] = a;
+    f[3] = b;
+    z32[4 * m + 3] = a;
+  }
+}
+
+unsigned grid_for(uint64_t n) { return (unsigned)std::min<uint64_t>((n + 255) / 256, 148 * 16); }
 
 template <bool EXT, bool D, bool L>
 void *kernel_ptr() {
@@ -325,11 +420,9 @@ void fdc_close(fdc_ctx *ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-  for (auto &kv : ctx->orbits) {
-    cudaFree(kv.second.z);
-    cudaFree(kv.second.z32);
-    free_bla(kv.second.bla);
-  }
+  for (auto &kv : ctx->orbits) free_orbit_buffers(ctx, kv.second);
+  for (auto &kv : ctx->pool) cudaFree(kv.second);
+  ctx->pool.clear();
   cudaFree(ctx->scratch);
   cudaFree(ctx->stage);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -345,20 +438,32 @@ fdc_status fdc_upload_orbit(fdc_ctx *ctx, const double *re, const double *im, ui
   if (re[0] != 0.0 || im[0] != 0.0)
     return fail(ctx, FDC_INVALID, "supplied reference orbit must start at Z_0 = 0");
   CK(cudaSetDevice(ctx->device));
-  std::vector<double2> z(len);
-  for (uint64_t k = 0; k < len; ++k) z[k] = make_double2(re[k], im[k]);
   OrbitDev o;
   o.len = len;
   o.bits = bits;
   o.z0r = re[0];
   o.z0i = im[0];
-  CK(cudaMalloc(&o.z, len * sizeof(double2)));
-  CK(cudaMemcpyAsync(o.z, z.data(), len * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
-  std::vector<double> e32;
-  pack_entries32(z, {}, e32);
-  CK(cudaMalloc(&o.z32, e32.size() * sizeof(double)));
-  CK(cudaMemcpyAsync(o.z32, e32.data(), e32.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
+  o.z = (double2 *)pool_get(ctx, 16 * len);
+  o.z32 = (double *)pool_get(ctx, 32 * len);
+  double *raw = (double *)pool_get(ctx, 16 * len);  // re[], im[] as the caller holds them
+  if (!o.z || !o.z32 || !raw) {
+    pool_put(ctx, raw, 16 * len);
+    free_orbit_buffers(ctx, o);
+    return fail(ctx, FDC_DEVICE_ERROR, "device memory for the orbit");
+  }
+  cudaError_t e = cudaMemcpyAsync(raw, re, 8 * len, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(raw + len, im, 8 * len, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) {
+    pack_orbit<<<grid_for(len), 256, 0, ctx->stream>>>(raw, raw + len, len, o.z, o.z32);
+    e = cudaGetLastError();
+  }
+  pool_put(ctx, raw, 16 * len);  // stream-ordered: the next user of it runs after the pack
+  // the caller's arrays may be freed once this returns, pinned ones included
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) {
+    free_orbit_buffers(ctx, o);
+    return fail(ctx, FDC_DEVICE_ERROR, std::string("orbit upload: ") + cudaGetErrorString(e));
+  }
   int32_t id = ctx->next_orbit++;
   ctx->orbits[id] = o;
   *orbit = id;
@@ -369,11 +474,7 @@ fdc_status fdc_free_orbit(fdc_ctx *ctx, int32_t orbit) {
   if (!ctx) return FDC_INVALID;
   auto it = ctx->orbits.find(orbit);
   if (it == ctx->orbits.end()) return fail(ctx, FDC_INVALID, "unknown orbit handle");
-  CK(cudaSetDevice(ctx->device));
-  CK(cudaStreamSynchronize(ctx->stream));
-  cudaFree(it->second.z);
-  cudaFree(it->second.z32);
-  free_bla(it->second.bla);
+  free_orbit_buffers(ctx, it->second);  // to the pool: later uploads reuse them in stream order
   ctx->orbits.erase(it);
   return FDC_OK;
 }
@@ -396,63 +497,56 @@ fdc_status fdc_upload_bla(fdc_ctx *ctx, int32_t orbit, const double *blocks7, co
       return fail(ctx, FDC_INVALID, "BLA level offsets must be contiguous and level-major");
     total += steps >> (i + 1);
   }
-  std::vector<double> r2(total);
-  std::vector<double2> coef(2 * total), ab(total);
-  for (uint64_t b = 0; b < total; ++b) {
-    const double *v = blocks7 + 7 * b;
-    for (int f = 0; f < 7; ++f)
-      if (!std::isfinite(v[f])) return fail(ctx, FDC_INVALID, "BLA level holds a non-finite value");
-    if (v[4] < 0.0) return fail(ctx, FDC_INVALID, "BLA level holds a negative radius");
-    r2[b] = v[4] * v[4];
-    coef[2 * b] = make_double2(v[0], v[1]);
-    coef[2 * b + 1] = make_double2(v[2], v[3]);
-    ab[b] = make_double2(v[5], v[6]);
-  }
-  // Fused stream: orbit point m with the radii of the first two levels' blocks at m.
-  std::vector<double> fused(4 * o.len, -1.0);
-  {
-    std::vector<double2> z(o.len);
-    CK(cudaSetDevice(ctx->device));
-    CK(cudaMemcpy(z.data(), o.z, o.len * sizeof(double2), cudaMemcpyDeviceToHost));
-    for (uint64_t m = 0; m < o.len; ++m) {
-      fused[4 * m] = z[m].x;
-      fused[4 * m + 1] = z[m].y;
-    }
-    for (uint32_t i = 0; i < levels && i < 2; ++i) {
-      uint64_t cnt = steps >> (i + 1);
-      for (uint64_t t = 0; t < cnt; ++t) {
-        uint64_t m = 1 + (t << (i + 1));  // block t of level i starts at Z_m (bla.rs:131-135)
-        fused[4 * m + 2 + i] = r2[level_offsets[i] + t];
-      }
-    }
-    std::vector<double> r2a(o.len), e32;
-    for (uint64_t m = 0; m < o.len; ++m) r2a[m] = fused[4 * m + 2];
-    pack_entries32(z, r2a, e32);
-    CK(cudaMemcpy(o.z32, e32.data(), e32.size() * sizeof(double), cudaMemcpyHostToDevice));
-  }
-  CK(cudaStreamSynchronize(ctx->stream));
-  free_bla(o.bla);
-  o.has_bla = false;
-  BlaDev &d = o.bla;
+  CK(cudaSetDevice(ctx->device));
+  BlaDev d;
   d.levels = levels;
   d.eps = eps;
   d.dc_max = dc_max;
   d.dc_exp = dc_exp;
+  d.points = o.len;
+  d.blocks = total;
   for (uint32_t i = 0; i < levels; ++i) {
     d.off[i] = (uint32_t)level_offsets[i];
     d.count[i] = (uint32_t)(steps >> (i + 1));
   }
-  CK(cudaMalloc(&d.fused, 4 * o.len * sizeof(double)));
-  CK(cudaMemcpyAsync(d.fused, fused.data(), 4 * o.len * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-  if (total) {
-    CK(cudaMalloc(&d.r2, total * sizeof(double)));
-    CK(cudaMalloc(&d.coef, 2 * total * sizeof(double2)));
-    CK(cudaMalloc(&d.ab, total * sizeof(double2)));
-    CK(cudaMemcpyAsync(d.r2, r2.data(), total * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaMemcpyAsync(d.coef, coef.data(), 2 * total * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
-    CK(cudaMemcpyAsync(d.ab, ab.data(), total * sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
+  d.fused = (double *)pool_get(ctx, 32 * o.len);
+  d.r2 = (double *)pool_get(ctx, 8 * total);
+  d.coef = (double2 *)pool_get(ctx, 32 * total);
+  d.ab = (double2 *)pool_get(ctx, 16 * total);
+  double *raw = (double *)pool_get(ctx, 56 * total);  // the export form as the caller holds it
+  if (!d.fused || (total && (!d.r2 || !d.coef || !d.ab || !raw))) {
+    pool_put(ctx, raw, 56 * total);
+    free_bla(ctx, d);
+    return fail(ctx, FDC_DEVICE_ERROR, "device memory for the BLA table");
   }
-  CK(cudaStreamSynchronize(ctx->stream));
+  // split and check the table first; only a valid table touches the orbit's entries
+  unsigned *bad = &ctx->scratch->bad;
+  cudaError_t e = cudaMemsetAsync(bad, 0, sizeof(unsigned), ctx->stream);
+  if (e == cudaSuccess && total) e = cudaMemcpyAsync(raw, blocks7, 56 * total, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess && total) {
+    pack_bla<<<grid_for(total), 256, 0, ctx->stream>>>(raw, total, d.r2, d.coef, d.ab, bad);
+    e = cudaGetLastError();
+  }
+  pool_put(ctx, raw, 56 * total);
+  unsigned flags = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&flags, bad, sizeof flags, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess || flags) {
+    free_bla(ctx, d);
+    if (e != cudaSuccess) return fail(ctx, FDC_DEVICE_ERROR, std::string("BLA upload: ") + cudaGetErrorString(e));
+    return fail(ctx, FDC_INVALID, (flags & 1) ? "BLA level holds a non-finite value"
+                                              : "BLA level holds a negative radius");
+  }
+  fuse_bla<<<grid_for(o.len), 256, 0, ctx->stream>>>(o.z, o.len, d.r2, levels, levels > 0 ? d.off[0] : 0,
+                                                     levels > 0 ? d.count[0] : 0, levels > 1 ? d.off[1] : 0,
+                                                     levels > 1 ? d.count[1] : 0, d.fused, o.z32);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    free_bla(ctx, d);
+    return fail(ctx, FDC_DEVICE_ERROR, std::string("BLA upload: ") + cudaGetErrorString(e));
+  }
+  free_bla(ctx, o.bla);
+  o.bla = d;
   o.has_bla = true;
   return FDC_OK;
 }

@@ -50,3 +50,17 @@ def test_bands_cover_the_frame_within_bounds():
 def test_candidates_without_bla_have_no_deferral():
     assert all(s.defer == 0 for s in tune.candidates(bla=False))
     assert {s.defer for s in tune.candidates(bla=True)} == set(tune.DEFERS)
+
+
+def test_cached_centres_follow_their_recipe():
+    """The cached centres of configurations 3-5 carry the seeds, widths and precisions the
+    recipe specifies; the cheapest one (a 1e-21 location) is recomputed and equal."""
+    from fractodactyl_b200 import locations
+    spec = locations.specs()
+    for name, entries in spec.items():
+        got = locations.cached(name)
+        assert [(d["seed"], d["log10_width"], d["bits"]) for d in got] == \
+            [(d["seed"], d["log10_width"], d["bits"]) for d in entries]
+        assert all(d["period"] > 0 and -3.0 < d["log10_size_over_width"] < -0.5 for d in got)
+    d = min(locations.cached("c5"), key=lambda d: d["bits"])
+    assert locations._compute({k: d[k] for k in ("seed", "log10_width", "bits")}) == d
