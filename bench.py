@@ -359,6 +359,7 @@ def run_set(args):
     rank, world, local = dist_init(args.gpus)
     dev = fd.Device(local)
     cfg = args.config
+    t_start = time.perf_counter()
     if cfg == 3:
         fr = locations.config3()
         if args.nx or args.ny:
@@ -376,6 +377,8 @@ def run_set(args):
         name = f"c5-mixed-{len(js.jobs)}tiles-256x256-{len(frames)}loc"
     cols = ["cls", "n", "status", "nu", "de", "normal"]
     samples = sum(w[1] * w[3] for w in js.windows)
+    log(f"{name}: {len(js.jobs)} jobs, {samples} samples; orbits {js.orbit_seconds:.1f} s, tables "
+        f"{js.bla_seconds:.1f} s, set-up {time.perf_counter() - t_start:.1f} s")
 
     def with_flag(extra):
         out = []
@@ -416,11 +419,13 @@ def run_set(args):
 
             snap = lambda: {c: np.concatenate([b.columns(k)[c] for k in range(len(jobs))]) for c in ("cls", "n")}
         for _ in range(args.warmup):
-            step()
+            cnt = step()
+            log(f"{form} warm-up step: {cnt.kernel_ms:.1f} ms device")
         torch.cuda.synchronize()
         barrier(world)
         for _ in range(args.steps):
             cnt = step()
+            log(f"{form} step: {cnt.kernel_ms:.1f} ms device")
             tot["it"] += cnt.iterations
             tot["blocks"] += cnt.blocks
             tot["skipped"] += cnt.skipped
@@ -451,6 +456,7 @@ def run_set(args):
     if cfg == 3:
         h2d += 16 * samples
     d2h = samples * sum(OUT_BYTES[c] for c in cols)
+    old_handles = list(js.handles)
     js.free(dev)
     barrier(world)
     t0 = time.perf_counter()
@@ -464,7 +470,7 @@ def run_set(args):
     else:
         hs = {}
         jobs = with_flag(_lib.F32 if head == "fp32_floatexp" else 0)
-        for j, old in zip(jobs, js.handles):
+        for j, old in zip(jobs, old_handles):
             if old not in hs:  # locations appear in order; a film has one
                 loc = 0 if len(js.refs) == 1 else len(hs)
                 hs[old] = dev.upload(js.refs[loc], js.blas[loc])

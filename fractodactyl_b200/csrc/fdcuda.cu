@@ -242,24 +242,6 @@ void *pick_kernel(bool ext, bool d, bool l, int &variant) {
   }
 }
 
-// Precision-form entries: (zr, zi) f64, (zr, zi) f32 packed in one 8-byte word (NaN where
-// |Z| < 2^-60, whose steps take the exact path), and r^2 of the 2-step block at m (or -1).
-void pack_entries32(const std::vector<double2> &z, const std::vector<double> &r2a, std::vector<double> &out) {
-  out.assign(4 * z.size(), 0.0);
-  for (size_t m = 0; m < z.size(); ++m) {
-    out[4 * m] = z[m].x;
-    out[4 * m + 1] = z[m].y;
-    float fr = (float)z[m].x, fi = (float)z[m].y;
-    if (std::fmax(std::fabs(z[m].x), std::fabs(z[m].y)) < 0x1p-60) fr = std::nanf("");
-    uint32_t a, b;
-    std::memcpy(&a, &fr, 4);
-    std::memcpy(&b, &fi, 4);
-    uint64_t w = (uint64_t)a | ((uint64_t)b << 32);
-    std::memcpy(&out[4 * m + 2], &w, 8);
-    out[4 * m + 3] = r2a.empty() ? -1.0 : r2a[m];
-  }
-}
-
 void *pick_batch_kernel(bool ext, bool d, bool l, int &variant) {
   variant = (ext ? 4 : 0) | (d ? 2 : 0) | (l ? 1 : 0);
   switch (variant) {

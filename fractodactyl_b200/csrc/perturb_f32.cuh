@@ -215,15 +215,11 @@ __device__ __forceinline__ void plain_update_f32(StateF &s) {
     }
   }
   if (!isnan(s.zr32)) {
-    // FP32: w' = 2 Z w + 2^e w^2 + dc 2^-e, the complex products as packed pairs
-    // (sm_100's FFMA2/FMUL2 do the real and imaginary parts in one instruction)
+    // FP32: w' = 2 Z w + 2^e w^2 + dc 2^-e
     const float wr = s.wr, wi = s.wi;
-    const float2 w = make_float2(wr, wi), ws = make_float2(wi, wr);
-    const float2 zw = __ffma2_rn(make_float2(-s.zi32, s.zi32), ws, __fmul2_rn(make_float2(s.zr32, s.zr32), w));
-    const float2 w2 = __ffma2_rn(make_float2(-wi, wi), ws, __fmul2_rn(make_float2(wr, wr), w));
-    const float2 u = __ffma2_rn(make_float2(s.s32, s.s32), w2, make_float2(s.dcr, s.dci));
-    const float2 nw = __ffma2_rn(make_float2(2.0f, 2.0f), zw, u);
-    const float nwr = nw.x, nwi = nw.y;
+    const float zwr = s.zr32 * wr - s.zi32 * wi, zwi = s.zr32 * wi + s.zi32 * wr;
+    const float nwr = 2.0f * zwr + s.s32 * (wr * wr - wi * wi) + s.dcr;
+    const float nwi = 2.0f * zwi + s.s32 * (2.0f * wr * wi) + s.dci;
     s.wr = nwr;
     s.wi = nwi;
     const float mag = fmaxf(fabsf(nwr), fabsf(nwi));
@@ -262,29 +258,6 @@ __device__ __forceinline__ bool post_f32(const Params &p, const Entry32 *__restr
   const double pr = phys(s.wr, s.e, s.s64), pi = phys(s.wi, s.e, s.s64);
   const double fr = Z.x + pr, fi = Z.y + pi;
   const double f2 = fr * fr + fi * fi;
-  {
-    // Quiet iterations (no escape, nucleus gate, rebase or periodicity event) leave only
-    // z and |delta|^2 for the next one: one test of every event, the sequence below only
-    // when one of them may fire.
-    const double delta2 = pr * pr + pi * pi;
-    const bool quiet = !(f2 > p.r2) && !(f2 <= delta2) && s.m != p.last &&
-                       !(s.nucleus >= 0 && s.n == (uint32_t)s.nucleus + 1);
-    const bool judge = delta2 > RES2 * f2;
-    bool calm;
-    if (judge) {
-      const float gr = (float)fr, gi = (float)fi;
-      const float dist = fabsf(gr - s.sr) + fabsf(gi - s.si), size = fabsf(s.sr) + fabsf(s.si);
-      calm = !(dist < 1e-3f * size) && (s.hold > 0 ? s.n - s.sn < s.hold : !(s.pending || s.n >= s.chk));
-    } else {
-      calm = s.hold > 0 ? s.n - s.sn < s.hold : s.n < s.chk;
-    }
-    if (__builtin_expect(quiet && calm, 1)) {
-      s.d2 = delta2;
-      s.fr = fr;
-      s.fi = fi;
-      return false;
-    }
-  }
   if (f2 > p.r2) {
     res.kind = 0;
     res.n = s.n;
