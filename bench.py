@@ -282,6 +282,13 @@ def run_ours(args):
     plain_steps = rf["it"] - rf["blocks"]
     flops = FLOPS_PLAIN[(ext, deriv)] * plain_steps + FLOPS_BLOCK[deriv] * rf["blocks"]
     achieved = flops / (rf["ms"] * 1e-3) / 1e12
+    # DRAM bytes per launch of this workload's plain kernel from one ncu capture
+    # (dram__bytes_read.sum + dram__bytes_write.sum), kept in profiles/traffic.json
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tf):
+        with open(tf) as f:
+            traffic = json.load(f).get(f"{fr.name}/fp64_plain")
     f64, f32 = C.c_double(), C.c_double()
     lib = C.CDLL(_lib.LIB_PATH)
     lib.fdk_alu_peaks.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
@@ -333,7 +340,8 @@ def run_ours(args):
                 "counters": {"iterations": totals["it"] // args.steps, "blocks": totals["blocks"] // args.steps,
                              "skipped": totals["skipped"] // args.steps},
                 "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                             "frac": achieved / peak if peak > 0 else None, "traffic": None,
+                             "frac": achieved / peak if peak > 0 else None, "traffic": traffic,
+                             "traffic_unit": "bytes per launch (DRAM, ncu)",
                              "peak_source": "measured live: unfused DMUL+DADD chains on all SMs (fdk_alu_peaks)"},
                 "cpu_baseline": cpu, "clocks": clk, "gpu_launches": sum(v["tot"]["launches"] for v in forms.values()),
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

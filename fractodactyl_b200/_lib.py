@@ -75,7 +75,10 @@ class Plane(C.Structure):
 
 
 class Tuning(C.Structure):
-    _fields_ = [("defer", C.c_uint32), ("blocks_per_sm", C.c_uint32), ("tile_w", C.c_uint32)]
+    _fields_ = [("defer", C.c_uint32), ("blocks_per_sm", C.c_uint32), ("tile_w", C.c_uint32), ("order", C.c_uint32)]
+
+
+ORDER_ROWS, ORDER_CENTRE = 1, 2  # FDC_ORDER_*
 
 
 DEFAULT_DEFER = 0  # FDC_DEFAULT_DEFER: each kernel variant's measured default

@@ -8,6 +8,8 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <numeric>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -71,11 +73,13 @@ struct fdc_ctx {
   int blocks_per_sm_f32[4] = {};
   int blocks_per_sm_batch[8] = {};
   int blocks_per_sm_batch_f32[4] = {};
-  fdc_tuning tune{FDC_DEFAULT_DEFER, 0, 0};
+  fdc_tuning tune{FDC_DEFAULT_DEFER, 0, 0, 0};
   // Device buffers of freed orbits and tables (and upload staging), kept by size for the
   // next upload of the same size: a film or a service re-uploading per frame allocates
   // once. Stream-ordered: every user runs on `stream`. Freed by fdc_close.
   std::multimap<size_t, void *> pool;
+  // centre-first tile orders per window shape (tiles_x, tiles_y, tile_shift)
+  std::map<std::tuple<uint32_t, uint32_t, uint32_t>, uint32_t *> orders;
 };
 
 // Persistent grid of a plain-form kernel: the occupancy limit, or fewer blocks per SM
@@ -84,6 +88,35 @@ struct fdc_ctx {
 static uint32_t defer_for(const fdc_ctx *ctx, bool ext) {
   if (ctx->tune.defer > 0) return ctx->tune.defer;
   return ext ? 12u : 4u;
+}
+
+// The tiles of a window, nearest to its centre first (squared distance of the tile's
+// centre, ties in row-major order). Benchmark views and zoom films centre on a nucleus,
+// whose surroundings hold the longest samples: handing those out first leaves the cheap
+// border for the end of the launch, where warps run out of work.
+static const uint32_t *centre_first(fdc_ctx *ctx, uint32_t tiles_x, uint32_t tiles_y, uint32_t shift) {
+  auto key = std::make_tuple(tiles_x, tiles_y, shift);
+  auto it = ctx->orders.find(key);
+  if (it != ctx->orders.end()) return it->second;
+  const uint64_t n = (uint64_t)tiles_x * tiles_y;
+  const double tw = (double)(1u << shift), th = (double)(32u >> shift);
+  std::vector<double> d(n);
+  for (uint64_t t = 0; t < n; ++t) {
+    const double x = ((double)(t % tiles_x) + 0.5) * tw - 0.5 * tiles_x * tw;
+    const double y = ((double)(t / tiles_x) + 0.5) * th - 0.5 * tiles_y * th;
+    d[t] = x * x + y * y;
+  }
+  std::vector<uint32_t> order(n);
+  std::iota(order.begin(), order.end(), 0u);
+  std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return d[a] < d[b]; });
+  uint32_t *dev = nullptr;
+  if (cudaMalloc(&dev, n * sizeof(uint32_t)) != cudaSuccess) return nullptr;
+  if (cudaMemcpy(dev, order.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(dev);
+    return nullptr;
+  }
+  ctx->orders[key] = dev;
+  return dev;
 }
 
 static int grid_blocks(const fdc_ctx *ctx, int occupancy) {
@@ -363,7 +396,13 @@ fdc_status prepare(fdc_ctx *ctx, const OrbitDev &o, const fdc_job &j, fdk::Param
   p.px_m = j.h_m * (double)j.ss;
   p.px_e = j.h_e;
   const uint32_t tile_h = 32u >> p.tile_shift;
-  p.total = (uint64_t)p.tiles_x * ((rows + tile_h - 1) / tile_h) * 32;
+  const uint32_t tiles_y = (rows + tile_h - 1) / tile_h;
+  p.total = (uint64_t)p.tiles_x * tiles_y * 32;
+  p.tile_order = nullptr;
+  if (ctx->tune.order != FDC_ORDER_ROWS) {
+    p.tile_order = centre_first(ctx, p.tiles_x, tiles_y, p.tile_shift);
+    if (!p.tile_order) return fail(ctx, FDC_DEVICE_ERROR, "device memory for the tile order");
+  }
   p.deadline_ns = j.deadline_ms > 0 ? (uint64_t)(j.deadline_ms * 1e6) : 0;
   p.defer = defer_for(ctx, p.tier == FDC_TIER_SCALED);
 
@@ -405,6 +444,8 @@ void fdc_close(fdc_ctx *ctx) {
   for (auto &kv : ctx->orbits) free_orbit_buffers(ctx, kv.second);
   for (auto &kv : ctx->pool) cudaFree(kv.second);
   ctx->pool.clear();
+  for (auto &kv : ctx->orders) cudaFree(kv.second);
+  ctx->orders.clear();
   cudaFree(ctx->scratch);
   cudaFree(ctx->stage);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -677,6 +718,7 @@ fdc_status fdc_set_tuning(fdc_ctx *ctx, const fdc_tuning *t) {
   if (t->blocks_per_sm > 64) return fail(ctx, FDC_INVALID, "blocks_per_sm must be at most 64");
   if (t->tile_w > 32 || (t->tile_w & (t->tile_w - 1)))
     return fail(ctx, FDC_INVALID, "tile_w must be 0 or a power of two up to 32");
+  if (t->order > FDC_ORDER_CENTRE) return fail(ctx, FDC_INVALID, "unknown tile order");
   ctx->tune = *t;
   return FDC_OK;
 }

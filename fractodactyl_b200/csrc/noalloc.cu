@@ -169,7 +169,8 @@ extern "C" fdc_status fdc_render_noalloc(int device, const double *orbit, uint64
   p.cols = cols;
   p.in_pitch = cols;
   p.out_pitch = j.nx;
-  p.tile_shift = 3;  // 8x4-sample tiles
+  p.tile_shift = 3;  // 8x4-sample tiles in row-major order
+  p.tile_order = nullptr;
   p.tiles_x = (cols + 7) / 8;
   p.tier = j.tier;
   p.flags = deriv ? fdk::F_DERIV : 0;

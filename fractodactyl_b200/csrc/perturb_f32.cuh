@@ -54,6 +54,20 @@ struct MulF {
       exp += e;
     }
   }
+  // The same for an FP64 factor of any size (a BLA block's multiplier A can exceed f32's
+  // range): scaled by a power of two into [1, 2) before the f32 product, the power carried
+  // in the exponent, as Contraction::multiply scales its factors (sample.rs:672-681).
+  __device__ __forceinline__ void multiply_wide(double r, double i) {
+    const double a = fmax(fabs(r), fabs(i));
+    if (a == 0.0 || !isfinite(a)) {
+      multiply((float)r, (float)i);
+      return;
+    }
+    const int k = floor_log2(a);
+    const double h = exp2i(-(k / 2)), l = exp2i(-(k - k / 2));
+    multiply((float)(r * h * l), (float)(i * h * l));
+    exp += k;
+  }
   __device__ __forceinline__ bool below(float lim) const {  // |v|^2 < lim
     return isfinite(re) && isfinite(im) &&
            (exp < -64 || (exp <= 64 && ((double)re * re + (double)im * im) * exp2i(2 * exp) < lim));
@@ -102,8 +116,15 @@ __device__ __forceinline__ void set_delta(StateF &s, double re, double im, int64
   s.dci = (float)(s.ai * g);
 }
 
-// Sum of two wide-exponent complex terms (as sum2, sample.rs:1094-1114).
-__device__ __forceinline__ Cx3 add3(Cx3 a, Cx3 b) { return sum2(a, b, a.e); }
+// Sum of two wide-exponent complex terms (as sum2, sample.rs:1094-1114), with a zero
+// term passed over: sum2 scales every term by 2^(e - top), and a zero term whose
+// exponent lies more than 2046 above the other's (an orbit point that is 0 in f64 next
+// to a delta far below f64's range) would give 0 * inf.
+__device__ __forceinline__ Cx3 add3(Cx3 a, Cx3 b) {
+  if (a.re == 0.0 && a.im == 0.0) return b;
+  if (b.re == 0.0 && b.im == 0.0) return a;
+  return sum2(a, b, a.e);
+}
 
 // delta = w 2^e as f64 (the physical delta of the FP64 steps): the f32 bits moved into
 // an f64 with the exponent e added, exact; subnormal, zero and non-finite w, and results
@@ -120,8 +141,11 @@ __device__ __forceinline__ double phys(float w, int e, double s64) {
 }
 
 // Bla::find's iteration limit with n left out (relimit of the plain form).
+// On the scaled tier a pending save never lifts the budget (the extended tier's rule:
+// blocks stop at the next power-of-two save point, sample.rs:246-263).
 __device__ __forceinline__ void relimit_f32(const Params &p, StateF &s) {
-  uint64_t cap = s.hold > 0 ? (uint64_t)s.sn + s.hold : (s.pending ? ~0ull : (uint64_t)s.chk);
+  const bool open = s.pending && p.tier != 2;
+  uint64_t cap = s.hold > 0 ? (uint64_t)s.sn + s.hold : (open ? ~0ull : (uint64_t)s.chk);
   uint64_t b = p.max_iter < cap ? p.max_iter : cap;
   if (s.nucleus >= 0 && (uint64_t)s.nucleus + 1 < b) b = (uint64_t)s.nucleus + 1;
   s.lim = (uint32_t)b;
@@ -171,10 +195,10 @@ __device__ __forceinline__ void apply_block_f32(const Params &p, StateF &s, int 
   const double2 A = __ldg(p.bla_coef + 2 * b), B = __ldg(p.bla_coef + 2 * b + 1);
   const uint32_t len = 2u << lv;
   if (s.nucleus >= 0 && s.n >= 1) {
-    s.ct.multiply((float)A.x, (float)A.y);
+    s.ct.multiply_wide(A.x, A.y);
     s.ct_started = true;
   }
-  if (s.hold > 0) s.mu.multiply((float)A.x, (float)A.y);
+  if (s.hold > 0) s.mu.multiply_wide(A.x, A.y);
   if (D) {
     normalise(s.dr, s.di, s.dexp, INT64_MAX / 4);
     s.inverse = exp2i(-s.dexp);
@@ -279,7 +303,12 @@ __device__ __forceinline__ bool post_f32(const Params &p, const Entry32 *__restr
   }
   const double delta2 = pr * pr + pi * pi;
   if (f2 <= delta2 || s.m == p.last) {  // rebase onto Z_0 (extended-tier rule)
-    set_delta(s, fr, fi, 0);
+    if (f2 > SQUARE_OK) {
+      set_delta(s, fr, fi, 0);
+    } else {  // z below f64's reach: Z + delta with wide exponents (sample.rs:421-429)
+      const Cx3 t = add3(Cx3{Z.x, Z.y, 0}, Cx3{(double)s.wr, (double)s.wi, s.e});
+      set_delta(s, t.re, t.im, t.e);
+    }
     s.m = 0;
     s.Zr = p.z0r;
     s.Zi = p.z0i;
@@ -298,7 +327,20 @@ __device__ __forceinline__ bool post_f32(const Params &p, const Entry32 *__restr
   // periodicity in FP32 (ordinary-tier rule, sample.rs:473-574) on the rebased delta
   const bool judge = s.d2 > RES2 * f2;
   if (!judge) {
-    if (s.hold > 0) {
+    if (p.tier == 2) {
+      // Scaled tier: an unjudged save point advances as the extended tier's does
+      // (sample.rs:479-486). Below f64's range no iterate is ever judged; an unlimited
+      // budget would then let blocks run each sample to the orbit's last point, whose
+      // rebase onto z = Z_last (delta below f64) would put every sample on the
+      // reference orbit.
+      if (s.n >= s.chk) {
+        s.sr = (float)fr;
+        s.si = (float)fi;
+        s.sn = s.n;
+        s.chk = s.chk >= 0x80000000u ? 0xffffffffu : s.chk * 2;
+        relimit_f32(p, s);
+      }
+    } else if (s.hold > 0) {
       if (s.n >= s.sn + s.hold) {
         s.hold = 0;
         s.predicted = false;
@@ -408,6 +450,7 @@ __device__ __forceinline__ bool warp_step_f32(const Params &p, const Entry32 *__
 template <bool D, bool L>
 __device__ __forceinline__ int init_f32(const Params &p, uint64_t slot, StateF &s, Result &res) {
   uint64_t tile = slot >> 5;
+  if (p.tile_order) tile = __ldg(p.tile_order + tile);  // queue position -> row-major tile
   uint32_t w = (uint32_t)slot & 31u;
   uint32_t tx = (uint32_t)(tile % p.tiles_x), ty = (uint32_t)(tile / p.tiles_x);
   uint32_t ii = (tx << p.tile_shift) + (w & ((1u << p.tile_shift) - 1u));
@@ -429,20 +472,17 @@ __device__ __forceinline__ int init_f32(const Params &p, uint64_t slot, StateF &
     ux = p.cosr * x + p.sinr * y;
     uy = p.sinr * x - p.cosr * y;
   }
-  if (p.tier == 2) {
-    s.ar = ux * p.h_m;
-    s.ai = uy * p.h_m;
-    s.oe = (int)p.h_e;
-  } else {
-    s.ar = ux * p.h;
-    s.ai = uy * p.h;
-    s.oe = 0;
-    if (p.tier == 0 && in_main_components(p.c_re + s.ar, p.c_im + s.ai)) {
-      res.kind = 1;
-      res.n = 0;
-      return 2;
-    }
+  // dc = (ux, uy) h_m 2^h_e on every tier: the same value as the ordinary tiers' ux h
+  // (scaling by 2^h_e is exact), kept as mantissa and exponent so that dc 2^-e stays in
+  // f32's range however deep the view
+  if (p.tier == 0 && in_main_components(p.c_re + ux * p.h, p.c_im + uy * p.h)) {
+    res.kind = 1;
+    res.n = 0;
+    return 2;
   }
+  s.ar = ux * p.h_m;
+  s.ai = uy * p.h_m;
+  s.oe = (int)p.h_e;
   set_delta(s, 0.0, 0.0, s.oe);
   s.d2 = 0.0;
   s.Zr = p.z0r;

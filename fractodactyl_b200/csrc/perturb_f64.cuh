@@ -55,6 +55,7 @@ struct Params {
   uint32_t in_pitch, out_pitch;    // row pitch (samples) of the mask/offsets inputs and of the outputs,
                                    // whose pointers address the window's first sample
   uint32_t tile_shift;  // tiles are 2^tile_shift samples wide and 32 / 2^tile_shift rows high
+  const uint32_t *tile_order;  // order the queue hands tiles out in (row-major tile indices), or null
   int32_t tier;
   uint32_t flags;
   double c_re, c_im, h, h_m;
@@ -594,6 +595,7 @@ __device__ __forceinline__ bool warp_step(const Params &p, State<EXT> &s, Result
 template <bool EXT, bool D, bool L>
 __device__ __forceinline__ int init(const Params &p, uint64_t slot, State<EXT> &s, Result &res) {
   uint64_t tile = slot >> 5;
+  if (p.tile_order) tile = __ldg(p.tile_order + tile);  // queue position -> row-major tile
   uint32_t w = (uint32_t)slot & 31u;
   uint32_t tx = (uint32_t)(tile % p.tiles_x), ty = (uint32_t)(tile / p.tiles_x);
   uint32_t ii = (tx << p.tile_shift) + (w & ((1u << p.tile_shift) - 1u));

@@ -314,9 +314,12 @@ class Device:
         lib().fdc_get_tuning(self.h, C.byref(t))
         return t
 
-    def tune(self, defer: Optional[int] = None, blocks_per_sm: Optional[int] = None, tile_w: Optional[int] = None):
+    def tune(self, defer: Optional[int] = None, blocks_per_sm: Optional[int] = None, tile_w: Optional[int] = None,
+             order: Optional[int] = None):
         """fdc_set_tuning: change the given launch settings, keep the others."""
         t = self.tuning
+        if order is not None:
+            t.order = order
         if defer is not None:
             t.defer = defer
         if blocks_per_sm is not None:

@@ -129,14 +129,20 @@ fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counte
  * the floatexp tier and 4 elsewhere); results do not depend on it. blocks_per_sm:
  * resident 128-thread blocks per SM of the persistent launch, 0 for as many as fit.
  * tile_w: width of the warp-sized tiles of samples the work queue hands out (1, 2, 4, 8,
- * 16 or 32; the height is 32 / tile_w), 0 for 8. A context starts with all three 0;
+ * 16 or 32; the height is 32 / tile_w), 0 for 8. order: FDC_ORDER_CENTRE hands tiles out
+ * nearest to the window's centre first (a nucleus-centred view's longest samples start
+ * early instead of ending the launch), FDC_ORDER_ROWS in row-major order; 0 for
+ * centre-first. Neither changes any result. A context starts with all four 0;
  * settings apply to later fdc_render calls and to batches created after them.
  * fractodactyl_b200.tune measures and picks them. */
 #define FDC_DEFAULT_DEFER 0
+#define FDC_ORDER_ROWS 1
+#define FDC_ORDER_CENTRE 2
 typedef struct fdc_tuning {
   uint32_t defer;
   uint32_t blocks_per_sm;
   uint32_t tile_w;
+  uint32_t order;
 } fdc_tuning;
 fdc_status fdc_set_tuning(fdc_ctx *ctx, const fdc_tuning *tuning);
 fdc_status fdc_get_tuning(const fdc_ctx *ctx, fdc_tuning *tuning);

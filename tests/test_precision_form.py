@@ -137,3 +137,41 @@ def test_precision_form_against_direct_iteration(dev):
           f"precision nu error {worst:.3e}")
     assert miss_a <= 2, miss_a
     assert miss_b <= 0.25 * len(idx) and worst <= 1e-4, (miss_b, worst)
+
+
+def test_precision_form_on_a_deep_fixed_tier_view(dev):
+    """Ordinary-tier views far below f32's range (1e-200 wide): the precision form keeps
+    dc as mantissa and exponent on every tier, so its deltas grow from dc as the plain
+    form's do. A dc held as one f32-scaled value would vanish here and leave samples on
+    the reference orbit until max_iter."""
+    from fractodactyl_b200 import locations
+    c = locations.cached("c4")[0]
+    v = fd.View(c["re"], c["im"], "1e-200")
+    p = fd.Params(96, 54, max_iter=100_000, columns=("nu", "de"), tier="fixed")
+    plane, tier, a, b, cp, cq = both_forms(dev, v, p, 2.0 ** -50)
+    assert tier == 1
+    same, off1 = agreement(a, b)
+    escaping = float(((a["cls"] == 0) == (b["cls"] == 0)).mean())
+    print(f"deep fixed tier: counts equal {same:.4f}, escape agreement {escaping:.4f}, "
+          f"iterations {cp.iterations} vs {cq.iterations}")
+    assert escaping >= 0.99 and same >= 0.5
+    assert cq.iterations <= 2 * cp.iterations
+
+
+def test_precision_form_below_f64_range(dev):
+    """Scaled-tier views so deep that every delta stays below f64's range for thousands
+    of iterations (1e-999, the deepest seeded mixed location): the precision form
+    advances its save points as the extended tier does, its blocks stop there, and its
+    samples escape with the plain form's instead of being rebased onto the reference
+    orbit at its last point."""
+    from fractodactyl_b200 import locations
+    c = min(locations.cached("c5"), key=lambda d: d["log10_width"])
+    v = fd.View(c["re"], c["im"], "1.5e-999")
+    p = fd.Params(64, 32, max_iter=10_000_000, columns=("nu",), tier="scaled")
+    plane, tier, a, b, cp, cq = both_forms(dev, v, p, 2.0 ** -50)
+    escaping = float(((a["cls"] == 0) == (b["cls"] == 0)).mean())
+    same, _ = agreement(a, b)
+    print(f"1e-999: counts equal {same:.4f}, escape agreement {escaping:.4f}, "
+          f"iterations {cp.iterations} vs {cq.iterations}")
+    assert escaping >= 0.99
+    assert cq.iterations <= 2 * cp.iterations
