@@ -9,6 +9,7 @@
 #include <cstring>
 #include <map>
 #include <numeric>
+#include <thread>
 #include <tuple>
 #include <string>
 #include <vector>
@@ -78,6 +79,10 @@ struct fdc_ctx {
   // next upload of the same size: a film or a service re-uploading per frame allocates
   // once. Stream-ordered: every user runs on `stream`. Freed by fdc_close.
   std::multimap<size_t, void *> pool;
+  // pinned staging for large host<->device copies: two chunk slots, each with the event
+  // of the last transfer that used it
+  char *pinned = nullptr;
+  cudaEvent_t slot_ev[2] = {nullptr, nullptr};
   // centre-first tile orders per window shape (tiles_x, tiles_y, tile_shift)
   std::map<std::tuple<uint32_t, uint32_t, uint32_t>, uint32_t *> orders;
 };
@@ -308,7 +313,73 @@ fdc_status open_resources(fdc_ctx *ctx) {
   CK(cudaEventCreate(&ctx->ev0));
   CK(cudaEventCreate(&ctx->ev1));
   CK(cudaMalloc(&ctx->scratch, sizeof(Scratch)));
+  CK(cudaEventCreateWithFlags(&ctx->slot_ev[0], cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&ctx->slot_ev[1], cudaEventDisableTiming));
   return FDC_OK;
+}
+
+// Large copies between the caller's (pageable) host arrays and the device go through two
+// pinned chunks: the host side of chunk k is copied by several threads while the DMA of
+// chunk k - 1 runs, and the DMA itself runs at pinned speed. Small copies go direct.
+constexpr size_t CHUNK = 8u << 20;
+
+void parallel_copy(void *dst, const void *src, size_t bytes) {
+  const unsigned hw = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+  const unsigned t = bytes < (1u << 20) ? 1u : hw;
+  if (t == 1) {
+    std::memcpy(dst, src, bytes);
+    return;
+  }
+  std::vector<std::thread> pool;
+  const size_t part = (bytes + t - 1) / t;
+  for (unsigned k = 0; k < t; ++k) {
+    const size_t a = k * part, b = std::min(bytes, a + part);
+    if (a >= b) break;
+    pool.emplace_back([=] { std::memcpy((char *)dst + a, (const char *)src + a, b - a); });
+  }
+  for (auto &th : pool) th.join();
+}
+
+cudaError_t ensure_pinned(fdc_ctx *ctx) {
+  if (ctx->pinned) return cudaSuccess;
+  return cudaHostAlloc((void **)&ctx->pinned, 2 * CHUNK, cudaHostAllocDefault);
+}
+
+cudaError_t upload(fdc_ctx *ctx, void *dst, const void *src, size_t bytes) {
+  if (bytes < CHUNK) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream);
+  cudaError_t e = ensure_pinned(ctx);
+  int slot = 0;
+  for (size_t off = 0; e == cudaSuccess && off < bytes; off += CHUNK, slot ^= 1) {
+    const size_t n = std::min(CHUNK, bytes - off);
+    char *stage = ctx->pinned + slot * CHUNK;
+    e = cudaEventSynchronize(ctx->slot_ev[slot]);  // the DMA that last read this chunk is done
+    if (e != cudaSuccess) break;
+    parallel_copy(stage, (const char *)src + off, n);
+    e = cudaMemcpyAsync((char *)dst + off, stage, n, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->slot_ev[slot], ctx->stream);
+  }
+  return e;
+}
+
+cudaError_t download(fdc_ctx *ctx, void *dst, const void *src, size_t bytes) {
+  if (bytes < CHUNK) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+  cudaError_t e = ensure_pinned(ctx);
+  const size_t chunks = (bytes + CHUNK - 1) / CHUNK;
+  auto issue = [&](size_t k) {
+    const size_t off = k * CHUNK, n = std::min(CHUNK, bytes - off);
+    cudaError_t r = cudaMemcpyAsync(ctx->pinned + (k & 1) * CHUNK, (const char *)src + off, n,
+                                    cudaMemcpyDeviceToHost, ctx->stream);
+    return r == cudaSuccess ? cudaEventRecord(ctx->slot_ev[k & 1], ctx->stream) : r;
+  };
+  if (e == cudaSuccess) e = issue(0);
+  for (size_t k = 0; e == cudaSuccess && k < chunks; ++k) {
+    e = cudaEventSynchronize(ctx->slot_ev[k & 1]);  // chunk k has arrived
+    if (e == cudaSuccess && k + 1 < chunks) e = issue(k + 1);  // the other slot is free: its copy-out is done
+    if (e != cudaSuccess) break;
+    const size_t off = k * CHUNK;
+    parallel_copy((char *)dst + off, ctx->pinned + (k & 1) * CHUNK, std::min(CHUNK, bytes - off));
+  }
+  return e;
 }
 
 // Validate a job against its orbit (the refusals of render_bla, grid.rs:378-413) and fill
@@ -446,6 +517,9 @@ void fdc_close(fdc_ctx *ctx) {
   ctx->pool.clear();
   for (auto &kv : ctx->orders) cudaFree(kv.second);
   ctx->orders.clear();
+  if (ctx->pinned) cudaFreeHost(ctx->pinned);
+  for (auto &ev : ctx->slot_ev)
+    if (ev) cudaEventDestroy(ev);
   cudaFree(ctx->scratch);
   cudaFree(ctx->stage);
   if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -474,8 +548,8 @@ fdc_status fdc_upload_orbit(fdc_ctx *ctx, const double *re, const double *im, ui
     free_orbit_buffers(ctx, o);
     return fail(ctx, FDC_DEVICE_ERROR, "device memory for the orbit");
   }
-  cudaError_t e = cudaMemcpyAsync(raw, re, 8 * len, cudaMemcpyHostToDevice, ctx->stream);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(raw + len, im, 8 * len, cudaMemcpyHostToDevice, ctx->stream);
+  cudaError_t e = upload(ctx, raw, re, 8 * len);
+  if (e == cudaSuccess) e = upload(ctx, raw + len, im, 8 * len);
   if (e == cudaSuccess) {
     pack_orbit<<<grid_for(len), 256, 0, ctx->stream>>>(raw, raw + len, len, o.z, o.z32);
     e = cudaGetLastError();
@@ -545,7 +619,7 @@ fdc_status fdc_upload_bla(fdc_ctx *ctx, int32_t orbit, const double *blocks7, co
   // split and check the table first; only a valid table touches the orbit's entries
   unsigned *bad = &ctx->scratch->bad;
   cudaError_t e = cudaMemsetAsync(bad, 0, sizeof(unsigned), ctx->stream);
-  if (e == cudaSuccess && total) e = cudaMemcpyAsync(raw, blocks7, 56 * total, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess && total) e = upload(ctx, raw, blocks7, 56 * total);
   if (e == cudaSuccess && total) {
     pack_bla<<<grid_for(total), 256, 0, ctx->stream>>>(raw, total, d.r2, d.coef, d.ab, bad);
     e = cudaGetLastError();
@@ -596,7 +670,8 @@ fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counte
   const uint64_t origin = (uint64_t)first * j.nx + p.first_col;
   auto window_copy = [&](void *dst, size_t dpitch, const void *src, size_t spitch, size_t width,
                          cudaMemcpyKind kind) {
-    if (full) return cudaMemcpyAsync(dst, src, width * rows, kind, ctx->stream);
+    if (full)
+      return kind == cudaMemcpyHostToDevice ? upload(ctx, dst, src, width * rows) : download(ctx, dst, src, width * rows);
     return cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, rows, kind, ctx->stream);
   };
 
