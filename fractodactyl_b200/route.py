@@ -279,14 +279,20 @@ class Device:
     def free(self, orbit: int):
         lib().fdc_free_orbit(self.h, orbit)
 
-    def render_job(self, job: _lib.Job, raw=False, columns=COLUMNS, device_out=None):
-        """fdc_render into fresh host arrays (or caller device buffers)."""
+    def render_job(self, job: _lib.Job, raw=False, columns=COLUMNS, device_out=None, host_out=None):
+        """fdc_render into fresh host arrays, into the caller's host arrays (host_out: the
+        dict an earlier call returned, reused frame after frame) or into caller device
+        buffers (device_out)."""
         n = job.nx * job.ny
         out = _lib.Out()
         arrays = {}
         if device_out is not None:
             for k, v in device_out.items():
                 setattr(out, k, v)
+        elif host_out is not None:
+            arrays = host_out
+            for k, a in arrays.items():
+                setattr(out, k, a.ctypes.data)
         else:
             want = {"cls": np.uint8, "status": np.uint8, "n": np.uint32}
             if "nu" in columns:
