@@ -141,10 +141,14 @@ __device__ __forceinline__ double phys(float w, int e, double s64) {
 }
 
 // Bla::find's iteration limit with n left out (relimit of the plain form).
-// On the scaled tier a pending save never lifts the budget (the extended tier's rule:
-// blocks stop at the next power-of-two save point, sample.rs:246-263).
+// Views whose deltas can fall below f64's range (spacing under 2^-960): save points
+// advance as the extended tier's do and a pending save never lifts the budget (blocks
+// stop at the next power-of-two save point, sample.rs:246-263). Shallower views keep
+// the ordinary tier's rule, whose longer blocks are faster.
+__device__ __forceinline__ bool below_f64(const Params &p) { return p.h_e < -960; }
+
 __device__ __forceinline__ void relimit_f32(const Params &p, StateF &s) {
-  const bool open = s.pending && p.tier != 2;
+  const bool open = s.pending && !below_f64(p);
   uint64_t cap = s.hold > 0 ? (uint64_t)s.sn + s.hold : (open ? ~0ull : (uint64_t)s.chk);
   uint64_t b = p.max_iter < cap ? p.max_iter : cap;
   if (s.nucleus >= 0 && (uint64_t)s.nucleus + 1 < b) b = (uint64_t)s.nucleus + 1;
@@ -327,12 +331,11 @@ __device__ __forceinline__ bool post_f32(const Params &p, const Entry32 *__restr
   // periodicity in FP32 (ordinary-tier rule, sample.rs:473-574) on the rebased delta
   const bool judge = s.d2 > RES2 * f2;
   if (!judge) {
-    if (p.tier == 2) {
-      // Scaled tier: an unjudged save point advances as the extended tier's does
-      // (sample.rs:479-486). Below f64's range no iterate is ever judged; an unlimited
-      // budget would then let blocks run each sample to the orbit's last point, whose
-      // rebase onto z = Z_last (delta below f64) would put every sample on the
-      // reference orbit.
+    if (below_f64(p)) {
+      // An unjudged save point advances as the extended tier's does (sample.rs:479-486).
+      // Below f64's range no iterate is ever judged; an unlimited budget would then let
+      // blocks run each sample to the orbit's last point, whose rebase onto z = Z_last
+      // (delta below f64) would put every sample on the reference orbit.
       if (s.n >= s.chk) {
         s.sr = (float)fr;
         s.si = (float)fi;
