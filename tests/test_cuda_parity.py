@@ -347,3 +347,34 @@ def test_route_reproduces_reference_fds_hashes(dev, case):
     h, s, st, _ = fd.render_with(view, p, dev=dev, host_encode=True)
     h.kernel = h.kernel.replace(" gpu-perturb-cuda/1", "")
     assert fdref.fnv1a64(fds.encode(h, s, minor=0)) == int(case["fnv"], 16)
+
+
+@pytest.mark.parametrize("tile_w", [1, 8, 32])
+def test_ragged_windows_and_tile_shapes(dev, tile_w):
+    """Windows of odd sizes at the grid's edges (one column, one row, a single sample,
+    the last rows and columns) under narrow, default and wide tiles equal the full
+    frame's samples there, and nothing else is written."""
+    view = fd.View("-0.7453", "0.1127", "0.0065")
+    nx, ny = 37, 23
+    p = fd.Params(nx, ny, max_iter=2500)
+    r, bits = fd.reference(view, p)
+    plane = fd.Plane.new(view, nx, ny)
+    h = dev.upload(r)
+    try:
+        dev.tune(tile_w=tile_w)
+        job = lambda: fd.route.make_job(plane, plane.tier, p, h, r.nucleus_period(), _lib.DERIVATIVE)
+        full, _, _ = dev.render_job(job(), raw=True)
+        for (x0, cw, y0, rh) in ((nx - 1, 1, 0, ny), (0, nx, ny - 1, 1), (nx - 1, 1, ny - 1, 1), (5, 31, 3, 19),
+                                 (0, 1, 0, 1)):
+            j = job()
+            j.first_col, j.cols, j.first_row, j.rows = x0, cw, y0, rh
+            a, cnt, _ = dev.render_job(j, raw=True)
+            win = np.zeros((ny, nx), bool)
+            win[y0:y0 + rh, x0:x0 + cw] = True
+            win = win.ravel()
+            assert cnt.samples == win.sum() and np.all(a["status"][~win] == 0)
+            for k in ("cls", "n", "z", "dz", "dexp", "nu"):
+                assert np.array_equal(a[k][win], full[k][win]), (k, x0, cw, y0, rh)
+    finally:
+        dev.tune(tile_w=0)
+        dev.free(h)
