@@ -71,3 +71,44 @@ def test_masks_partition_the_frame():
     for world in (1, 2, 3, 8):
         m = sum(shard.mask_for(17, 37, r, world).astype(int) for r in range(world))
         assert np.all(m == 1)
+
+
+def _share_worker(rank, world, port, q):
+    import datetime
+
+    import torch.distributed as dist
+
+    import fractodactyl_b200 as fd
+    from fractodactyl_b200 import shard
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        r = bla = None
+        if rank == 0:
+            v = fd.View("-0.743643887037158704752191506114774", "0.131825904205311970493132056385139", "1e-28")
+            p = fd.Params(64, 36, max_iter=20_000, columns=("nu",))
+            r, bits = fd.reference(v, p)
+            r.bits = bits
+            dc, e = fd.bla_dc_bound(v, p)
+            bla = fd.Bla.build_scaled(r, 2.0 ** -50, dc, e)
+        r, bla = shard.share_reference(r, bla)
+        q.put((rank, r.re.tobytes(), r.im.tobytes(), r.bits, bla.blocks.tobytes(), bla.level_offsets.tolist(),
+               bla.eps, bla.dc_max, bla.dc_exp))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_rank_zero_shares_orbit_and_table():
+    """The serial host work runs once: rank 0's orbit and BLA table reach rank 1 bit for bit."""
+    world, port = 2, _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_share_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    got = dict((res[0], res[1:]) for res in (q.get(timeout=120) for _ in range(world)))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert got[0] == got[1]
+    assert len(got[0][3]) > 0 and got[0][2] > 100  # a BLA table and a fixed-point orbit
