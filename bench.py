@@ -37,6 +37,11 @@ UNIT = "pixel-iter/s"
 # the reference formulas (sample.rs:266-575, number.rs:92-124).
 FLOPS_PLAIN = {(False, True): 40, (False, False): 31, (True, True): 47, (True, False): 38}
 FLOPS_BLOCK = {True: 37, False: 27}
+# The precision form's step: the FP32 delta recurrence w' = 2 Z w + 2^e w^2 + dc 2^-e
+# (21 FP32 operations) and its FP64 steps (derivative 9 with D, z = Z + delta 2, |z|^2 3,
+# |delta|^2 3, the periodicity judge 2).
+F32_STEP_FP32 = 21
+F32_STEP_FP64 = {True: 19, False: 10}
 OUT_BYTES = {"cls": 1, "n": 4, "nu": 8, "de": 4, "normal": 2, "status": 1}
 
 
@@ -294,6 +299,15 @@ def run_ours(args):
     lib.fdk_alu_peaks.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     lib.fdk_alu_peaks(local, C.byref(f64), C.byref(f32))
     peak = f64.value / 1e12
+    precision_roofline = None
+    if "fp32_floatexp" in forms:
+        pf = forms["fp32_floatexp"]["tot"]
+        steps = pf["it"] - pf["blocks"]
+        sec = pf["ms"] * 1e-3
+        a32 = F32_STEP_FP32 * steps / sec / 1e12
+        a64 = (F32_STEP_FP64[deriv] * steps + FLOPS_BLOCK[deriv] * pf["blocks"]) / sec / 1e12
+        precision_roofline = {"fp32": {"achieved": a32, "peak": f32.value / 1e12, "frac": a32 / (f32.value / 1e12)},
+                              "fp64": {"achieved": a64, "peak": peak, "frac": a64 / peak}, "unit": "TFLOP/s"}
 
     # e2e through the public API with host buffers: uploads (H2D), render, host columns (D2H)
     h2d = 16 * len(r) + (56 * len(bla.blocks) if bla is not None else 0)
@@ -344,6 +358,7 @@ def run_ours(args):
                              "frac": achieved / peak if peak > 0 else None, "traffic": traffic,
                              "traffic_unit": "bytes per launch (DRAM, ncu)",
                              "peak_source": "measured live: unfused DMUL+DADD chains on all SMs (fdk_alu_peaks)"},
+                "roofline_precision_form": precision_roofline,
                 "cpu_baseline": cpu, "clocks": clk, "gpu_launches": sum(v["tot"]["launches"] for v in forms.values()),
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "steps": args.e2e_steps}}
