@@ -1,8 +1,9 @@
 // The plain (FP64) perturbation kernel: one lane per sample, persistent warps that
 // refill finished lanes from an atomic tile queue. The per-sample state machine is
 // iterate() of crates/fd-kernel/src/sample.rs:170-581 (Binary64 and Binary64Exponent,
-// number.rs:92-124), one loop iteration per call of step(), with the reference's
-// operation order. Compile with -fmad=false.
+// number.rs:92-124) with the reference's operation order: one loop iteration is
+// find_block, then apply_block or plain_update, then post; warp_step runs it for a
+// warp (with BLA deferral), step for one lane. Compile with -fmad=false.
 #pragma once
 #include <cstdint>
 
