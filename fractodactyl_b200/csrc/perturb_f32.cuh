@@ -157,9 +157,8 @@ __device__ __forceinline__ void relimit_f32(const Params &p, StateF &s) {
 
 // Bla::find on the FP64 |delta|^2 of the iteration's start (s.d2).
 __device__ __forceinline__ int find_block_f32(const Params &p, const StateF &s, uint32_t &at) {
-  if (!(s.nucleus < 0 || s.m != 0)) return -1;
   const uint32_t budget = s.lim > s.n ? s.lim - s.n : 0u;
-  if (budget < 2 || !(s.d2 < s.r2a)) return -1;
+  if (!((s.nucleus < 0 || s.m != 0) & (budget >= 2) & (s.d2 < s.r2a))) return -1;
   const double d2 = s.d2;
   const uint32_t k = s.m - 1u;
   at = k >> 1;

@@ -139,12 +139,12 @@ __device__ __forceinline__ void relimit(const Params &p, State<EXT> &s) {
 // next PRE levels are loaded together before the comparisons that would stop at them.
 template <bool EXT>
 __device__ __forceinline__ int find_block(const Params &p, const State<EXT> &s, uint32_t &at) {
-  if (!(s.nucleus < 0 || s.m != 0)) return -1;
   const uint32_t budget = s.lim > s.n ? s.lim - s.n : 0u;
-  // r2a is -1 unless a block starts at m (d2 < r2a is then false whatever d2 is)
-  if (budget < 2 || !(s.r2a >= 0.0)) return -1;
   const double d2 = EXT ? (s.xr * s.xr + s.xi * s.xi) * s.scale * s.scale : s.xr * s.xr + s.xi * s.xi;
-  if (!(d2 < s.r2a)) return -1;
+  // One test for the nucleus gate, the budget and the level-1 block (r2a is -1 unless a
+  // block starts at m): every operand is evaluated, which costs fewer branches than
+  // returning at the first that fails.
+  if (!((s.nucleus < 0 || s.m != 0) & (budget >= 2) & (d2 < s.r2a))) return -1;
   const uint32_t k = s.m - 1u;     // m = 0 wraps: odd, no block
   at = k >> 1;
   if (budget < 4 || !(d2 < s.r2b)) return 0;
