@@ -173,13 +173,15 @@ __device__ __forceinline__ int find_block_f32(const Params &p, const StateF &s, 
     ok[q] = i < top && (2u << i) <= budget && a < p.bla_count[i];
     r[q] = ok[q] ? __ldg(p.bla_r2 + p.bla_off[i] + a) : -1.0;
   }
-  int lv = 0;
+  // the prefetched levels that pass, as bits; the block is the last level of the passing
+  // run from level 1 up (the same level and index as testing them in order)
+  uint32_t pass = 0;
 #pragma unroll
-  for (uint32_t q = 0; q < PRE; ++q) {
-    if (!ok[q] || !(d2 < r[q])) return lv;
-    lv = (int)(1 + q);
-    at = k >> (2 + q);
-  }
+  for (uint32_t q = 0; q < PRE; ++q) pass |= (uint32_t)(ok[q] && d2 < r[q]) << q;
+  const uint32_t run = (uint32_t)__ffs((int)~pass) - 1u;  // bit PRE of ~pass is set: run <= PRE
+  if (run > 0) at = k >> (1 + run);
+  if (run < PRE) return (int)run;
+  int lv = (int)PRE;
   for (uint32_t i = 1 + PRE; i < top; ++i) {
     if ((2ull << i) > budget) break;
     const uint32_t a = k >> (i + 1);
