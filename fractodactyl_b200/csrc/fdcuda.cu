@@ -92,7 +92,7 @@ struct fdc_ctx {
 // Lanes a warp gathers before applying BLA blocks (fdc_tuning.defer; 0: per variant).
 static uint32_t defer_for(const fdc_ctx *ctx, bool ext) {
   if (ctx->tune.defer > 0) return ctx->tune.defer;
-  return ext ? 12u : 4u;
+  return ext ? 12u : 8u;
 }
 
 // The tiles of a window, nearest to its centre first (squared distance of the tile's

@@ -441,7 +441,12 @@ __device__ __forceinline__ bool warp_step_f32(const Params &p, const Entry32 *__
     const unsigned FULL = 0xffffffffu;
     const unsigned waiting = __ballot_sync(FULL, w.on);
     const unsigned stepping = __ballot_sync(FULL, upd);
-    if (waiting && ((uint32_t)__popc(waiting) >= defer || !stepping) && w.on) {
+    // the threshold is `defer` of 32 lanes, scaled to the lanes still busy (waiting or
+    // stepping): once the queue runs dry and lanes go idle, a fixed threshold would hold
+    // every waiting lane until the last plain-stepping lane finds a block
+    const uint32_t busy = (uint32_t)__popc(waiting | stepping);
+    const uint32_t thr = (busy * defer + 31u) >> 5;
+    if (waiting && ((uint32_t)__popc(waiting) >= thr || !stepping) && w.on) {
       apply_block_f32<D>(p, s, w.lv, w.at);
       w.on = false;
       upd = took = true;

@@ -546,8 +546,8 @@ struct Waiting {
 };
 
 // One iteration for the active lanes of a warp (every lane of the warp calls it). A lane
-// whose next operation is a BLA block waits until at least `defer` lanes of the warp wait
-// or no lane steps plainly; the waiting lanes then apply their blocks together. The warp
+// whose next operation is a BLA block waits until at least defer/32 of the warp's busy
+// lanes wait or no lane steps plainly; the waiting lanes then apply their blocks together. The warp
 // runs the block path for many lanes at a time instead of for one or two lanes on
 // nearly every iteration, and each lane's own sequence of operations is unchanged.
 template <bool EXT, bool D, bool L>
@@ -581,7 +581,12 @@ __device__ __forceinline__ bool warp_step(const Params &p, State<EXT> &s, Result
     const unsigned FULL = 0xffffffffu;
     const unsigned waiting = __ballot_sync(FULL, w.on);
     const unsigned stepping = __ballot_sync(FULL, upd);
-    if (waiting && ((uint32_t)__popc(waiting) >= defer || !stepping) && w.on) {
+    // the threshold is `defer` of 32 lanes, scaled to the lanes still busy (waiting or
+    // stepping): once the queue runs dry and lanes go idle, a fixed threshold would hold
+    // every waiting lane until the last plain-stepping lane finds a block
+    const uint32_t busy = (uint32_t)__popc(waiting | stepping);
+    const uint32_t thr = (busy * defer + 31u) >> 5;
+    if (waiting && ((uint32_t)__popc(waiting) >= thr || !stepping) && w.on) {
       apply_block<EXT, D>(p, s, w.lv, w.at);
       w.on = false;
       upd = took = true;

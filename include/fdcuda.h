@@ -124,9 +124,9 @@ fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counte
 
 /* Launch tuning (no counterpart in the reference; the reference's shader has fixed
  * workgroups). defer: lanes of a warp whose next operation is a BLA block wait until
- * this many lanes of the warp wait, or no lane steps plainly, and then apply their
+ * defer/32 of the warp's busy lanes wait, or no lane steps plainly, and then apply their
  * blocks together (1: at once; 0: the measured default of each kernel variant, 12 on
- * the floatexp tier and 4 elsewhere); results do not depend on it. blocks_per_sm:
+ * the floatexp tier and 8 elsewhere); results do not depend on it. blocks_per_sm:
  * resident 128-thread blocks per SM of the persistent launch, 0 for as many as fit.
  * tile_w: width of the warp-sized tiles of samples the work queue hands out (1, 2, 4, 8,
  * 16 or 32; the height is 32 / tile_w), 0 for 8. order: FDC_ORDER_CENTRE hands tiles out
