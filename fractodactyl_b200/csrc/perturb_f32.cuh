@@ -445,7 +445,7 @@ __device__ __forceinline__ bool warp_step_f32(const Params &p, const Entry32 *__
     // stepping): once the queue runs dry and lanes go idle, a fixed threshold would hold
     // every waiting lane until the last plain-stepping lane finds a block
     const uint32_t busy = (uint32_t)__popc(waiting | stepping);
-    const uint32_t thr = (busy * defer + 31u) >> 5;
+    const uint32_t thr = max(1u, (busy * defer) >> 5);
     if (waiting && ((uint32_t)__popc(waiting) >= thr || !stepping) && w.on) {
       apply_block_f32<D>(p, s, w.lv, w.at);
       w.on = false;
