@@ -7,7 +7,10 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <condition_variable>
 #include <map>
+#include <memory>
+#include <mutex>
 #include <numeric>
 #include <thread>
 #include <tuple>
@@ -54,6 +57,8 @@ struct Scratch {
   uint32_t pad2[6];
 };
 
+class CopyPool;  // host threads of the staging copies (below)
+
 }  // namespace
 
 struct fdc_batch;
@@ -83,6 +88,7 @@ struct fdc_ctx {
   // of the last transfer that used it
   char *pinned = nullptr;
   cudaEvent_t slot_ev[2] = {nullptr, nullptr};
+  std::unique_ptr<CopyPool> copier;  // host threads of the staging copies
   // centre-first tile orders per window shape (tiles_x, tiles_y, tile_shift)
   std::map<std::tuple<uint32_t, uint32_t, uint32_t>, uint32_t *> orders;
 };
@@ -319,42 +325,110 @@ fdc_status open_resources(fdc_ctx *ctx) {
 }
 
 // Large copies between the caller's (pageable) host arrays and the device go through two
-// pinned chunks: the host side of chunk k is copied by several threads while the DMA of
-// chunk k - 1 runs, and the DMA itself runs at pinned speed. Small copies go direct.
+// pinned chunk slots: the host side of chunk k is copied by several threads while the DMA
+// of chunk k - 1 runs, and the DMA itself runs at pinned speed. Copies below STAGE_MIN go
+// direct. A chunk is a quarter of the copy, between STAGE_MIN and CHUNK, so that even a
+// mid-size array overlaps its two sides.
 constexpr size_t CHUNK = 8u << 20;
+constexpr size_t STAGE_MIN = 1u << 20;
 
-void parallel_copy(void *dst, const void *src, size_t bytes) {
-  const unsigned hw = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
-  const unsigned t = bytes < (1u << 20) ? 1u : hw;
-  if (t == 1) {
-    std::memcpy(dst, src, bytes);
-    return;
-  }
-  std::vector<std::thread> pool;
-  const size_t part = (bytes + t - 1) / t;
-  for (unsigned k = 0; k < t; ++k) {
-    const size_t a = k * part, b = std::min(bytes, a + part);
-    if (a >= b) break;
-    pool.emplace_back([=] { std::memcpy((char *)dst + a, (const char *)src + a, b - a); });
-  }
-  for (auto &th : pool) th.join();
+size_t chunk_for(size_t bytes) {
+  const size_t quarter = ((bytes / 4) + 65535) & ~(size_t)65535;
+  return std::min(CHUNK, std::max(STAGE_MIN, quarter));
 }
 
+// Persistent host threads for the staging copies (created once per context instead of per
+// chunk): a copy is cut into equal parts; the calling thread copies the last, the workers
+// the others, and copy() returns when all are done.
+class CopyPool {
+ public:
+  explicit CopyPool(unsigned workers) {
+    try {
+      for (unsigned i = 0; i < workers; ++i) threads_.emplace_back([this, i] { run(i); });
+    } catch (...) {  // fewer threads than asked: the copies are cut into fewer parts
+    }
+  }
+  ~CopyPool() {
+    {
+      std::lock_guard<std::mutex> l(m_);
+      stop_ = true;
+    }
+    go_.notify_all();
+    for (auto &t : threads_) t.join();
+  }
+  void copy(void *dst, const void *src, size_t bytes) {
+    const size_t workers = threads_.size();
+    if (workers == 0 || bytes < (256u << 10)) {
+      std::memcpy(dst, src, bytes);
+      return;
+    }
+    {
+      std::lock_guard<std::mutex> l(m_);
+      dst_ = (char *)dst;
+      src_ = (const char *)src;
+      bytes_ = bytes;
+      part_ = ((bytes / (workers + 1)) + 63) & ~(size_t)63;
+      pending_ = workers;
+      ++gen_;
+    }
+    go_.notify_all();
+    piece(workers);
+    std::unique_lock<std::mutex> l(m_);
+    done_.wait(l, [&] { return pending_ == 0; });
+  }
+
+ private:
+  // part k of the current copy; its fields were set under the lock before the workers
+  // were woken and stay until every part is done
+  void piece(size_t k) {
+    const size_t a = std::min(bytes_, k * part_), b = std::min(bytes_, a + part_);
+    if (b > a) std::memcpy(dst_ + a, src_ + a, b - a);
+  }
+  void run(unsigned id) {
+    uint64_t seen = 0;
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> l(m_);
+        go_.wait(l, [&] { return stop_ || gen_ != seen; });
+        if (stop_) return;
+        seen = gen_;
+      }
+      piece(id);
+      std::lock_guard<std::mutex> l(m_);
+      if (--pending_ == 0) done_.notify_one();
+    }
+  }
+  std::vector<std::thread> threads_;
+  std::mutex m_;
+  std::condition_variable go_, done_;
+  uint64_t gen_ = 0;
+  size_t pending_ = 0;
+  bool stop_ = false;
+  char *dst_ = nullptr;
+  const char *src_ = nullptr;
+  size_t bytes_ = 0, part_ = 0;
+};
+
 cudaError_t ensure_pinned(fdc_ctx *ctx) {
+  if (!ctx->copier) {
+    const unsigned hw = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    ctx->copier = std::make_unique<CopyPool>(hw - 1);
+  }
   if (ctx->pinned) return cudaSuccess;
   return cudaHostAlloc((void **)&ctx->pinned, 2 * CHUNK, cudaHostAllocDefault);
 }
 
 cudaError_t upload(fdc_ctx *ctx, void *dst, const void *src, size_t bytes) {
-  if (bytes < CHUNK) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream);
+  if (bytes < STAGE_MIN) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream);
   cudaError_t e = ensure_pinned(ctx);
+  const size_t chunk = chunk_for(bytes);
   int slot = 0;
-  for (size_t off = 0; e == cudaSuccess && off < bytes; off += CHUNK, slot ^= 1) {
-    const size_t n = std::min(CHUNK, bytes - off);
+  for (size_t off = 0; e == cudaSuccess && off < bytes; off += chunk, slot ^= 1) {
+    const size_t n = std::min(chunk, bytes - off);
     char *stage = ctx->pinned + slot * CHUNK;
-    e = cudaEventSynchronize(ctx->slot_ev[slot]);  // the DMA that last read this chunk is done
+    e = cudaEventSynchronize(ctx->slot_ev[slot]);  // the DMA that last read this slot is done
     if (e != cudaSuccess) break;
-    parallel_copy(stage, (const char *)src + off, n);
+    ctx->copier->copy(stage, (const char *)src + off, n);
     e = cudaMemcpyAsync((char *)dst + off, stage, n, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) e = cudaEventRecord(ctx->slot_ev[slot], ctx->stream);
   }
@@ -362,11 +436,12 @@ cudaError_t upload(fdc_ctx *ctx, void *dst, const void *src, size_t bytes) {
 }
 
 cudaError_t download(fdc_ctx *ctx, void *dst, const void *src, size_t bytes) {
-  if (bytes < CHUNK) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream);
+  if (bytes < STAGE_MIN) return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream);
   cudaError_t e = ensure_pinned(ctx);
-  const size_t chunks = (bytes + CHUNK - 1) / CHUNK;
+  const size_t chunk = chunk_for(bytes);
+  const size_t chunks = (bytes + chunk - 1) / chunk;
   auto issue = [&](size_t k) {
-    const size_t off = k * CHUNK, n = std::min(CHUNK, bytes - off);
+    const size_t off = k * chunk, n = std::min(chunk, bytes - off);
     cudaError_t r = cudaMemcpyAsync(ctx->pinned + (k & 1) * CHUNK, (const char *)src + off, n,
                                     cudaMemcpyDeviceToHost, ctx->stream);
     return r == cudaSuccess ? cudaEventRecord(ctx->slot_ev[k & 1], ctx->stream) : r;
@@ -376,8 +451,8 @@ cudaError_t download(fdc_ctx *ctx, void *dst, const void *src, size_t bytes) {
     e = cudaEventSynchronize(ctx->slot_ev[k & 1]);  // chunk k has arrived
     if (e == cudaSuccess && k + 1 < chunks) e = issue(k + 1);  // the other slot is free: its copy-out is done
     if (e != cudaSuccess) break;
-    const size_t off = k * CHUNK;
-    parallel_copy((char *)dst + off, ctx->pinned + (k & 1) * CHUNK, std::min(CHUNK, bytes - off));
+    const size_t off = k * chunk;
+    ctx->copier->copy((char *)dst + off, ctx->pinned + (k & 1) * CHUNK, std::min(chunk, bytes - off));
   }
   return e;
 }
@@ -517,6 +592,7 @@ void fdc_close(fdc_ctx *ctx) {
   ctx->pool.clear();
   for (auto &kv : ctx->orders) cudaFree(kv.second);
   ctx->orders.clear();
+  ctx->copier.reset();
   if (ctx->pinned) cudaFreeHost(ctx->pinned);
   for (auto &ev : ctx->slot_ev)
     if (ev) cudaEventDestroy(ev);
