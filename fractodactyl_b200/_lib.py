@@ -87,8 +87,9 @@ DEFAULT_DEFER = 0  # FDC_DEFAULT_DEFER: each kernel variant's measured default
 FDC_SYMBOLS = ["fdc_abi_version", "fdc_open", "fdc_close", "fdc_last_error", "fdc_upload_orbit", "fdc_free_orbit",
                "fdc_upload_bla", "fdc_render", "fdc_batch_create", "fdc_batch_run", "fdc_batch_free",
                "fdc_render_noalloc", "fdc_set_tuning", "fdc_get_tuning"]
-FDH_SYMBOLS = ["fdh_last_error", "fdh_plane_new", "fdh_orbit_fixed", "fdh_orbit_f64", "fdh_nucleus_period",
-               "fdh_bla_build", "fdh_dc_bound", "fdh_encode", "fdh_location"]
+FDH_SYMBOLS = ["fdh_last_error", "fdh_plane_new", "fdh_orbit_fixed", "fdh_orbit_fixed_threads", "fdh_orbit_f64",
+               "fdh_nucleus_period",
+               "fdh_bla_build", "fdh_bla_build_into", "fdh_dc_bound", "fdh_encode", "fdh_location"]
 
 _lib = None
 
@@ -122,11 +123,15 @@ def lib():
     L.fdh_plane_new.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, D, U32, U32, C.POINTER(Plane)]
     L.fdh_orbit_fixed.restype = I64
     L.fdh_orbit_fixed.argtypes = [C.c_char_p, C.c_char_p, U64, U64, P, P, U64]
+    L.fdh_orbit_fixed_threads.restype = I64
+    L.fdh_orbit_fixed_threads.argtypes = [C.c_char_p, C.c_char_p, U64, U64, P, P, U64, C.c_int]
     L.fdh_orbit_f64.restype = I64
     L.fdh_orbit_f64.argtypes = [D, D, U64, D, P, P, U64]
     L.fdh_nucleus_period.restype = I64
     L.fdh_nucleus_period.argtypes = [P, P, U64]
     L.fdh_bla_build.argtypes = [P, P, U64, D, D, I64, C.c_int, P, P, C.POINTER(U32), C.POINTER(U64)]
+    L.fdh_bla_build_into.restype = C.c_int
+    L.fdh_bla_build_into.argtypes = [P, P, U64, D, D, I64, C.c_int, P, U64, P, U32, C.POINTER(U32), C.POINTER(U64)]
     L.fdh_encode.argtypes = [C.POINTER(Plane), U32, U64, P, P, P, P, P, P, P, P, C.c_int]
     L.fdh_dc_bound.argtypes = [C.POINTER(Plane), I32, U32, U32, C.POINTER(D), C.POINTER(I64)]
     L.fdh_location.argtypes = [C.c_char_p, C.c_char_p, D, D, U64, U64, C.c_char_p, C.c_char_p, C.c_size_t,

@@ -254,22 +254,109 @@ void square_trunc(const uint64_t *a, uint64_t *o, size_t L, uint64_t *prod) {
   std::memcpy(o, prod + (L - 1), L * sizeof(uint64_t));
 }
 
+// Spin on `ready` (a short pause per try), then yield: the thread being waited for is
+// always making progress, so the wait ends.
+template <class P>
+void spin_until(P ready) {
+  for (unsigned i = 0; !ready(); ++i) {
+    if (i < 4096) {
+#if defined(__x86_64__) || defined(__i386__)
+      __builtin_ia32_pause();
+#endif
+    } else {
+      std::this_thread::yield();
+    }
+  }
+}
+
+// Two helper threads for the squarings of a wide orbit step: the caller squares x while
+// one helper squares y and the other x + y. The caller publishes a step's inputs by
+// bumping `go`; each helper reports its square by storing that generation in its own
+// `done`. The arithmetic is that of the serial step, so every orbit point is the same.
+class SquareCrew {
+ public:
+  explicit SquareCrew(size_t L) : L_(L) {}
+  ~SquareCrew() { stop(); }
+  // Starts the helpers on (y -> y2) and (s -> s2); false (and no helper) if a thread
+  // cannot be created.
+  bool start(const uint64_t *y, uint64_t *y2, const uint64_t *s, uint64_t *s2) {
+    try {
+      threads_.emplace_back([this, y, y2] { run(0, y, y2); });
+      threads_.emplace_back([this, s, s2] { run(1, s, s2); });
+    } catch (...) {
+      stop();
+      return false;
+    }
+    return true;
+  }
+  void round() { go_.fetch_add(1, std::memory_order_release); }
+  void wait() {
+    const uint64_t g = go_.load(std::memory_order_relaxed);
+    for (auto &d : done_) spin_until([&] { return d.v.load(std::memory_order_acquire) == g; });
+  }
+  void stop() {
+    if (threads_.empty()) return;
+    stop_.store(true, std::memory_order_relaxed);
+    go_.fetch_add(1, std::memory_order_release);
+    for (auto &t : threads_) t.join();
+    threads_.clear();
+  }
+
+ private:
+  void run(int k, const uint64_t *in, uint64_t *out) {
+    std::vector<uint64_t> prod(2 * L_);
+    uint64_t seen = 0;
+    for (;;) {
+      uint64_t g = 0;
+      spin_until([&] { return (g = go_.load(std::memory_order_acquire)) != seen; });
+      if (stop_.load(std::memory_order_relaxed)) return;
+      seen = g;
+      square_trunc(in, out, L_, prod.data());
+      done_[k].v.store(g, std::memory_order_release);
+    }
+  }
+  struct alignas(64) Counter {
+    std::atomic<uint64_t> v{0};
+  };
+  size_t L_;
+  std::vector<std::thread> threads_;
+  alignas(64) std::atomic<uint64_t> go_{0};
+  Counter done_[2];
+  std::atomic<bool> stop_{false};
+};
+
+// Orbits of at least this many limbs (~1,450 bits) split each step's squarings over
+// three threads when asked to (threads >= 3); below it two barrier crossings per step
+// cost more than the squarings they share.
+constexpr size_t CREW_MIN_LIMBS = 24;
+
 // Z_{n+1} = Z_n^2 + C from Z_0 = 0 in L-limb fixed point with three squarings per step
 // (x' = x^2 - y^2 + cr, y' = (x + y)^2 - x^2 - y^2 + ci, crates/fd-fixed/src/orbit.rs:
 // 14-43), each point rounded to f64 by fix_to_f64; stops after `steps` points or at the
-// first point with |Z|^2 > escape2.
-uint64_t fixed_orbit(const Fix &cr, const Fix &ci, uint64_t steps, double escape2, double *re, double *im) {
+// first point with |Z|^2 > escape2. threads >= 3 runs the three squarings of a step in
+// parallel on wide orbits.
+uint64_t fixed_orbit(const Fix &cr, const Fix &ci, uint64_t steps, double escape2, double *re, double *im,
+                     int threads) {
   const size_t L = cr.mag.size();
   std::vector<uint64_t> buf(9 * L, 0);
   uint64_t *x = buf.data(), *y = x + L, *x2 = y + L, *y2 = x2 + L, *s = y2 + L, *s2 = s + L, *t = s2 + L;
   std::vector<uint64_t> prod(2 * L);
   bool xn = false, yn = false;
+  SquareCrew crew(L);
+  const bool par = threads >= 3 && L >= CREW_MIN_LIMBS && steps > 1 && crew.start(y, y2, s, s2);
   uint64_t n = 0;
   for (; n < steps;) {
-    square_trunc(x, x2, L, prod.data());
-    square_trunc(y, y2, L, prod.data());
-    sadd(xn, x, yn, y, s, L);
-    square_trunc(s, s2, L, prod.data());
+    if (par) {
+      sadd(xn, x, yn, y, s, L);
+      crew.round();
+      square_trunc(x, x2, L, prod.data());
+      crew.wait();
+    } else {
+      square_trunc(x, x2, L, prod.data());
+      square_trunc(y, y2, L, prod.data());
+      sadd(xn, x, yn, y, s, L);
+      square_trunc(s, s2, L, prod.data());
+    }
     bool tn = sadd(false, x2, true, y2, t, L);
     xn = sadd(tn, t, cr.neg, cr.mag.data(), x, L);
     mag_add(x2, y2, s, L);
@@ -337,6 +424,87 @@ void parallel_for(uint64_t n, int threads, F f) {
     pool.emplace_back([=] { f(a, b); });
   }
   for (auto &th : pool) th.join();
+}
+
+template <class F>
+bool parallel_any(uint64_t n, int threads, F f) {  // parallel_for whose parts return a flag: their OR
+  if (threads <= 1 || n < 4096) return f(0, n);
+  std::vector<std::thread> pool;
+  std::vector<char> hit(threads, 0);
+  uint64_t chunk = (n + threads - 1) / threads;
+  for (int t = 0; t < threads; ++t) {
+    uint64_t a = t * chunk, b = std::min<uint64_t>(n, a + chunk);
+    if (a >= b) break;
+    pool.emplace_back([=, &hit] { hit[t] = f(a, b); });
+  }
+  for (auto &th : pool) th.join();
+  return std::find(hit.begin(), hit.end(), 1) != hit.end();
+}
+
+inline void put_blk(double *dst, const Blk &b) { std::memcpy(dst, &b, sizeof(Blk)); }
+inline Blk get_blk(const double *src) {
+  Blk b;
+  std::memcpy(&b, src, sizeof(Blk));
+  return b;
+}
+
+// bla.rs:161-216: singles over Z_1..Z_steps, pairwise merges level by level, stopping
+// before the first level without a valid block. The levels are written level-major into
+// `out` ([f64; 7] blocks) as they are merged, each level from the one before it in place;
+// the level that stops the build is written after the kept ones, so `out` needs room for
+// steps - 1 blocks (the sum of steps >> i over i >= 1), steps = len - 2. False (with the
+// error set) on invalid eps / dc_max.
+bool bla_levels(const double *re, const double *im, uint64_t len, double eps, double dc_max, int64_t dc_exp,
+                       int threads, double *out, uint32_t &levels, uint64_t &total) {
+  if (!(eps > 0.0 && eps <= 1.0 / (double)(1u << 24) && dc_max > 0.0 && std::isfinite(dc_max))) {
+    g_err = "BLA needs 0 < eps <= 2^-24 and a finite dc_max > 0";
+    return false;
+  }
+  if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
+  const uint64_t steps = len >= 2 ? len - 2 : 0;
+  uint64_t n = steps / 2, off = 0;
+  // level 1 directly from pairs of singles
+  bool valid = parallel_any(n, threads, [&](uint64_t a, uint64_t b) {
+    bool any = false;
+    for (uint64_t t = a; t < b; ++t) {
+      const Blk z = blk_merge(blk_single(re[2 * t + 1], im[2 * t + 1], eps),
+                              blk_single(re[2 * t + 2], im[2 * t + 2], eps), dc_max, dc_exp);
+      put_blk(out + 7 * t, z);
+      any |= z.r > 0.0;
+    }
+    return any;
+  });
+  levels = 0;
+  total = 0;
+  while (valid) {  // keep this level; merge the next from it
+    levels += 1;
+    total += n;
+    const uint64_t m = n / 2, at = off + n;
+    valid = parallel_any(m, threads, [&](uint64_t a, uint64_t b) {
+      bool any = false;
+      for (uint64_t t = a; t < b; ++t) {
+        const Blk z = blk_merge(get_blk(out + 7 * (off + 2 * t)), get_blk(out + 7 * (off + 2 * t + 1)), dc_max, dc_exp);
+        put_blk(out + 7 * (at + t), z);
+        any |= z.r > 0.0;
+      }
+      return any;
+    });
+    off = at;
+    n = m;
+  }
+  return true;
+}
+
+// Level offsets of a table built by bla_levels: level i starts after levels 0..i-1, each
+// half the one before.
+void bla_offsets(uint64_t len, uint32_t levels, uint64_t *level_offsets) {
+  const uint64_t steps = len >= 2 ? len - 2 : 0;
+  uint64_t at = 0, n = steps / 2;
+  for (uint32_t i = 0; i < levels; ++i, n /= 2) {
+    level_offsets[i] = at;
+    at += n;
+  }
+  level_offsets[levels] = at;
 }
 
 // Fixed-point to decimal string with `digits` fraction digits (truncated).
@@ -440,6 +608,11 @@ int fdh_plane_new(const char *center_re, const char *center_im, const char *widt
 
 int64_t fdh_orbit_fixed(const char *center_re, const char *center_im, uint64_t bits, uint64_t max_iter, double *re,
                         double *im, uint64_t cap) {
+  return fdh_orbit_fixed_threads(center_re, center_im, bits, max_iter, re, im, cap, 1);
+}
+
+int64_t fdh_orbit_fixed_threads(const char *center_re, const char *center_im, uint64_t bits, uint64_t max_iter,
+                                double *re, double *im, uint64_t cap, int threads) {
   try {
     uint64_t steps = std::min<uint64_t>(max_iter, (1ull << 20) - 1);
     if (cap < steps + 1) throw std::runtime_error("orbit buffers too small");
@@ -447,7 +620,8 @@ int64_t fdh_orbit_fixed(const char *center_re, const char *center_im, uint64_t b
     Fix cr = to_fix(parse_decimal(center_re), L), ci = to_fix(parse_decimal(center_im), L);
     re[0] = 0.0;
     im[0] = 0.0;
-    return (int64_t)(1 + fixed_orbit(cr, ci, steps, 4294967296.0, re + 1, im + 1));
+    if (threads == 0) threads = std::thread::hardware_concurrency() >= 4 ? 3 : 1;
+    return (int64_t)(1 + fixed_orbit(cr, ci, steps, 4294967296.0, re + 1, im + 1, threads));
   } catch (std::exception &e) {
     g_err = e.what();
     return -1;
@@ -497,47 +671,40 @@ int64_t fdh_nucleus_period(const double *re, const double *im, uint64_t len) {
 
 int fdh_bla_build(const double *re, const double *im, uint64_t len, double eps, double dc_max, int64_t dc_exp,
                   int threads, double *blocks7, uint64_t *level_offsets, uint32_t *levels, uint64_t *blocks) {
-  // bla.rs:161-216: singles over Z_1..Z_steps, pairwise merges level by level, stopping
-  // before the first level without a valid block.
-  if (!(eps > 0.0 && eps <= 1.0 / (double)(1u << 24) && dc_max > 0.0 && std::isfinite(dc_max))) {
-    g_err = "BLA needs 0 < eps <= 2^-24 and a finite dc_max > 0";
+  const uint64_t steps = len >= 2 ? len - 2 : 0;
+  std::vector<double> buf(7 * std::max<uint64_t>(steps, 1));
+  if (!bla_levels(re, im, len, eps, dc_max, dc_exp, threads, buf.data(), *levels, *blocks)) return -1;
+  if (blocks7) {
+    std::memcpy(blocks7, buf.data(), *blocks * sizeof(Blk));
+    if (level_offsets) bla_offsets(len, *levels, level_offsets);
+  }
+  return 0;
+}
+
+int fdh_bla_build_into(const double *re, const double *im, uint64_t len, double eps, double dc_max, int64_t dc_exp,
+                       int threads, double *blocks7, uint64_t cap_blocks, uint64_t *level_offsets, uint32_t cap_levels,
+                       uint32_t *levels, uint64_t *blocks) {
+  const uint64_t steps = len >= 2 ? len - 2 : 0;
+  if (!level_offsets || (steps >= 2 && !blocks7)) {
+    g_err = "BLA table larger than the buffers given";
     return -1;
   }
-  if (threads <= 0) threads = (int)std::max(1u, std::thread::hardware_concurrency());
-  uint64_t steps = len >= 2 ? len - 2 : 0;
-  std::vector<Blk> cur(steps / 2), next;
-  // level 1 directly from pairs of singles
-  parallel_for(steps / 2, threads, [&](uint64_t a, uint64_t b) {
-    for (uint64_t t = a; t < b; ++t)
-      cur[t] = blk_merge(blk_single(re[2 * t + 1], im[2 * t + 1], eps), blk_single(re[2 * t + 2], im[2 * t + 2], eps),
-                         dc_max, dc_exp);
-  });
-  std::vector<std::vector<Blk>> lv;
-  auto any_valid = [](const std::vector<Blk> &l) {
-    for (auto &b : l)
-      if (b.r > 0.0) return true;
-    return false;
-  };
-  while (any_valid(cur)) {
-    next.assign(cur.size() / 2, Blk{});
-    parallel_for(next.size(), threads, [&](uint64_t a, uint64_t b) {
-      for (uint64_t t = a; t < b; ++t) next[t] = blk_merge(cur[2 * t], cur[2 * t + 1], dc_max, dc_exp);
-    });
-    lv.push_back(std::move(cur));
-    cur = std::move(next);
-  }
+  uint32_t lv = 0;
   uint64_t total = 0;
-  for (auto &l : lv) total += l.size();
-  *levels = (uint32_t)lv.size();
-  *blocks = total;
-  if (!blocks7) return 0;
-  uint64_t at = 0;
-  for (size_t i = 0; i < lv.size(); ++i) {
-    if (level_offsets) level_offsets[i] = at;
-    std::memcpy(blocks7 + 7 * at, lv[i].data(), lv[i].size() * sizeof(Blk));
-    at += lv[i].size();
+  if (cap_blocks >= steps) {  // room for every level the build writes: build in place
+    if (!bla_levels(re, im, len, eps, dc_max, dc_exp, threads, blocks7, lv, total)) return -1;
+  } else {
+    std::vector<double> buf(7 * std::max<uint64_t>(steps, 1));
+    if (!bla_levels(re, im, len, eps, dc_max, dc_exp, threads, buf.data(), lv, total)) return -1;
+    if (total <= cap_blocks && lv <= cap_levels) std::memcpy(blocks7, buf.data(), total * sizeof(Blk));
   }
-  if (level_offsets) level_offsets[lv.size()] = at;
+  *levels = lv;
+  *blocks = total;
+  if (total > cap_blocks || lv > cap_levels) {
+    g_err = "BLA table larger than the buffers given";
+    return -1;
+  }
+  bla_offsets(len, lv, level_offsets);
   return 0;
 }
 

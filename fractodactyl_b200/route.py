@@ -116,11 +116,14 @@ class Reference:
         return len(self.re)
 
     @classmethod
-    def from_fixed(cls, center_re: str, center_im: str, bits: int, max_iter: int) -> "Reference":
+    def from_fixed(cls, center_re: str, center_im: str, bits: int, max_iter: int, threads: int = 0) -> "Reference":
+        """threads: 3 shares each step's squarings among three threads on orbits of ~1,450
+        bits and more, 1 keeps the orbit on the calling thread, 0 picks 3 on hosts with 4
+        or more hardware threads. The orbit is the same bit for bit."""
         cap = min(max_iter, MAX_LEN - 1) + 1
         re, im = np.empty(cap), np.empty(cap)
-        n = lib().fdh_orbit_fixed(center_re.encode(), center_im.encode(), bits, max_iter, re.ctypes.data,
-                                  im.ctypes.data, cap)
+        n = lib().fdh_orbit_fixed_threads(center_re.encode(), center_im.encode(), bits, max_iter, re.ctypes.data,
+                                          im.ctypes.data, cap, threads)
         if n < 0:
             raise ValueError(_lib.host_error())
         return cls(re[:n].copy(), im[:n].copy(), bits)
@@ -158,15 +161,18 @@ class Bla:
     def build_scaled(cls, r: Reference, eps: float, dc_max: float, dc_exp: int = 0, threads: int = 0) -> "Bla":
         re, im = np.ascontiguousarray(r.re), np.ascontiguousarray(r.im)
         levels, blocks = C.c_uint32(), C.c_uint64()
-        L = lib()
-        if L.fdh_bla_build(re.ctypes.data, im.ctypes.data, len(re), eps, dc_max, dc_exp, threads, None, None,
-                           C.byref(levels), C.byref(blocks)) != 0:
+        # one pass into buffers of the largest possible size: at most len - 2 blocks (the
+        # levels halve from (len - 2) / 2) and 64 levels
+        cap = max(len(re) - 2, 1)
+        b = np.empty((cap, 7))
+        offs = np.empty(65, np.uint64)
+        if lib().fdh_bla_build_into(re.ctypes.data, im.ctypes.data, len(re), eps, dc_max, dc_exp, threads,
+                                    b.ctypes.data, cap, offs.ctypes.data, 64, C.byref(levels),
+                                    C.byref(blocks)) != 0:
             raise ValueError(_lib.host_error())
-        b = np.zeros((blocks.value, 7))
-        offs = np.zeros(levels.value + 1, np.uint64)
-        L.fdh_bla_build(re.ctypes.data, im.ctypes.data, len(re), eps, dc_max, dc_exp, threads, b.ctypes.data,
-                        offs.ctypes.data, C.byref(levels), C.byref(blocks))
-        return cls(b, offs, eps, dc_max, dc_exp, len(re))
+        n = blocks.value
+        b = b[:n] if 4 * n >= 3 * cap else b[:n].copy()  # a table well below the bound lets the rest go
+        return cls(b, offs[:levels.value + 1].copy(), eps, dc_max, dc_exp, len(re))
 
 
 @dataclasses.dataclass

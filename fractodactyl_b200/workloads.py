@@ -100,8 +100,9 @@ def film(dev, frames: List[Frame], extra_flags: int = 0, max_iter: Optional[int]
 
 def tiles(dev, frames: List[Frame], tile: Tuple[int, int], extra_flags: int = 0, max_iter: Optional[int] = None,
           locations_first: Optional[int] = None) -> JobSet:
-    """One job per tile-sized window of every frame (orbits computed in parallel threads:
-    the host orbit releases the interpreter while it runs)."""
+    """One job per tile-sized window of every frame (orbits computed in parallel threads,
+    one thread each: the host orbit releases the interpreter while it runs, and with many
+    orbits, parallelism across orbits beats sharing each orbit's squarings)."""
     frames = frames[:locations_first] if locations_first else frames
     setups = []
     for f in frames:
@@ -111,7 +112,7 @@ def tiles(dev, frames: List[Frame], tile: Tuple[int, int], extra_flags: int = 0,
 
     def orbit(s):
         f, p, plane, tier = s
-        r = Reference.from_fixed(f.view.center_re, f.view.center_im, max(plane.bits, 128), p.max_iter)
+        r = Reference.from_fixed(f.view.center_re, f.view.center_im, max(plane.bits, 128), p.max_iter, threads=1)
         r.bits = max(plane.bits, 128)
         return r
 

@@ -37,9 +37,16 @@ int fdh_plane_new(const char *center_re, const char *center_im, const char *widt
  * caller arrays of capacity cap (>= min(max_iter, 2^20 - 1) + 1); returns its length.
  *   fdh_orbit_fixed: Reference::from_fixed over fd_fixed::orbit (reference.rs:85-96,
  *                    crates/fd-fixed/src/orbit.rs:14-43) at the exact decimal centre.
+ *   fdh_orbit_fixed_threads: the same orbit, bit for bit; threads >= 3 splits each
+ *                    step's three squarings over three threads when the orbit has at
+ *                    least 24 limbs (~1,450 bits), 1 keeps it serial, 0 picks 3 when the
+ *                    host has 4 or more hardware threads (no counterpart: the
+ *                    reference's orbit is serial).
  *   fdh_orbit_f64:   Reference::new (reference.rs:21-48). */
 int64_t fdh_orbit_fixed(const char *center_re, const char *center_im, uint64_t bits, uint64_t max_iter, double *re,
                         double *im, uint64_t cap);
+int64_t fdh_orbit_fixed_threads(const char *center_re, const char *center_im, uint64_t bits, uint64_t max_iter,
+                                double *re, double *im, uint64_t cap, int threads);
 int64_t fdh_orbit_f64(double c_re, double c_im, uint64_t max_iter, double escape_radius, double *re, double *im,
                       uint64_t cap);
 
@@ -52,6 +59,15 @@ int64_t fdh_nucleus_period(const double *re, const double *im, uint64_t len);
  * threads <= 0: all cores. */
 int fdh_bla_build(const double *re, const double *im, uint64_t len, double eps, double dc_max, int64_t dc_exp,
                   int threads, double *blocks7, uint64_t *level_offsets, uint32_t *levels, uint64_t *blocks);
+
+/* The same table built once into caller buffers of cap_blocks blocks and cap_levels + 1
+ * offsets (len - 2 blocks and 64 levels always suffice); levels and blocks receive the
+ * sizes. With cap_blocks >= len - 2 the levels are merged in place in blocks7, whose
+ * entries past the table's are then scratch. Returns -1 if the table does not fit (the
+ * offsets untouched). */
+int fdh_bla_build_into(const double *re, const double *im, uint64_t len, double eps, double dc_max, int64_t dc_exp,
+                       int threads, double *blocks7, uint64_t cap_blocks, uint64_t *level_offsets, uint32_t cap_levels,
+                       uint32_t *levels, uint64_t *blocks);
 
 /* grid.rs:418-444: bound m 2^e on |dc| over a view's samples for a tier. */
 void fdh_dc_bound(const fdh_plane *plane, int32_t tier, uint32_t nx, uint32_t ny, double *dc, int64_t *e);

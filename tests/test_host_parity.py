@@ -87,6 +87,20 @@ def test_fixed_orbit_escaping_and_rung():
         assert a.nucleus_period() == b.nucleus_period()
 
 
+@pytest.mark.parametrize("threads", [1, 3])
+def test_fixed_orbit_shared_squarings_bit_exact(threads):
+    """A wide orbit (3,456 bits, 55 limbs) whose step squarings run on three threads equals
+    the serial one and the oracle's, bit for bit; so does one below the threshold."""
+    rung = KATS["rung_7676"]
+    for bits, n in ((3456, 4000), (1130, 3000)):
+        a = fdref.Ref.fixed(rung["re"], rung["im"], bits, n)
+        b = fd.Reference.from_fixed(rung["re"], rung["im"], bits, n, threads=threads)
+        ar, ai = a.arrays_()
+        assert len(b) == len(a) == n + 1
+        assert np.array_equal(ar.view(np.uint64), b.re.view(np.uint64))
+        assert np.array_equal(ai.view(np.uint64), b.im.view(np.uint64))
+
+
 def test_f64_orbit_and_nucleus_gate():
     for c in [(-0.7487, 0.0789), (0.2501, 0.0), (-1.7548776662466927, 0.0), (0.0, 1.0)]:
         a = fdref.Ref.f64(c[0], c[1], 100_000, 1e10)
@@ -106,6 +120,34 @@ def test_bla_table_bit_exact(eps, dc, e):
     ba, oa = ta.export()
     assert np.array_equal(oa, tb.level_offsets)
     assert np.array_equal(ba.view(np.uint64), tb.blocks.view(np.uint64))
+
+
+def test_bla_one_pass_build_equals_two_call_build():
+    """fdh_bla_build_into (one pass into bounded buffers, as Bla.build_scaled uses it)
+    gives the table of the two-call fdh_bla_build, and refuses buffers that are too small."""
+    import ctypes as C
+    from fractodactyl_b200._lib import lib
+    a = fdref.Ref.f64(-0.743643887037158, 0.131825904205312, 20_000, 1e10)
+    re_, im_ = a.arrays_()
+    re_, im_ = np.ascontiguousarray(re_), np.ascontiguousarray(im_)
+    tb = fd.Bla.build_scaled(fd.Reference(re_, im_, 53), 2.0 ** -50, 1e-25, 0)
+    L = lib()
+    lv, bl = C.c_uint32(), C.c_uint64()
+    args = (re_.ctypes.data, im_.ctypes.data, len(re_), 2.0 ** -50, 1e-25, 0, 2)
+    assert L.fdh_bla_build(*args, None, None, C.byref(lv), C.byref(bl)) == 0
+    b = np.zeros((bl.value, 7))
+    o = np.zeros(lv.value + 1, np.uint64)
+    assert L.fdh_bla_build(*args, b.ctypes.data, o.ctypes.data, C.byref(lv), C.byref(bl)) == 0
+    assert tb.levels == lv.value > 5 and len(tb.blocks) == bl.value
+    assert np.array_equal(b.view(np.uint64), tb.blocks.view(np.uint64))
+    assert np.array_equal(o, tb.level_offsets)
+    small = np.zeros((bl.value - 1, 7))
+    offs = np.zeros(65, np.uint64)
+    assert L.fdh_bla_build_into(*args, small.ctypes.data, bl.value - 1, offs.ctypes.data, 64, C.byref(lv),
+                                C.byref(bl)) == -1
+    assert not small.any() and not offs.any()
+    assert L.fdh_bla_build_into(*args, b.ctypes.data, len(b), offs.ctypes.data, tb.levels - 1, C.byref(lv),
+                                C.byref(bl)) == -1
 
 
 def test_bla_refuses_bad_eps():
