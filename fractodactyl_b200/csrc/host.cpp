@@ -215,43 +215,40 @@ inline bool sadd(bool an, const uint64_t *a, bool bn, const uint64_t *b, uint64_
   return an && nonzero(o, L);
 }
 
-// o = floor(a^2 / 2^(64 (L-1))): column-wise (product-scanning) square with a 192-bit
-// column accumulator, doubling the off-diagonal terms as they are added.
+// o = floor(a^2 / 2^(64 (L-1))), from the full 2L-limb square in prod. The products
+// a_i a_j with i < j are summed row by row (operand scanning: one 64-bit carry per row,
+// so the multiplies of a row do not wait on each other's additions), doubled by a one-bit
+// shift, and the squares a_i^2 added on the diagonal. Exact.
 void square_trunc(const uint64_t *a, uint64_t *o, size_t L, uint64_t *prod) {
-  // Column by column (Comba): per column k the products a_i a_j with i < j, i + j = k,
-  // summed once into (d2:d1:d0) and doubled, plus the square a_{k/2}^2 for even k, added
-  // to the carry (c1:c0) of the columns below. Exact: the full 2L-limb product.
-  uint64_t c0 = 0, c1 = 0;
-  for (size_t k = 0; k < 2 * L - 1; ++k) {
-    const size_t lo = k >= L ? k - L + 1 : 0;
-    uint64_t d0 = 0, d1 = 0, d2 = 0;
-    for (size_t i = lo; 2 * i < k; ++i) {
-      const u128 p = (u128)a[i] * a[k - i];
-      u128 t = (u128)d0 + (uint64_t)p;
-      d0 = (uint64_t)t;
-      t = (u128)d1 + (uint64_t)(p >> 64) + (uint64_t)(t >> 64);
-      d1 = (uint64_t)t;
-      d2 += (uint64_t)(t >> 64);
+  uint64_t *r = prod;
+  for (size_t k = 0; k < 2 * L; ++k) r[k] = 0;
+  for (size_t i = 0; i + 1 < L; ++i) {
+    const uint64_t ai = a[i];
+    uint64_t c = 0;
+    for (size_t j = i + 1; j < L; ++j) {
+      const u128 t = (u128)ai * a[j] + r[i + j] + c;  // < 2^128: (2^64-1)^2 + 2 (2^64-1)
+      r[i + j] = (uint64_t)t;
+      c = (uint64_t)(t >> 64);
     }
-    d2 = (d2 << 1) | (d1 >> 63);
-    d1 = (d1 << 1) | (d0 >> 63);
-    d0 <<= 1;
-    if ((k & 1) == 0) {
-      const u128 p = (u128)a[k / 2] * a[k / 2];
-      u128 t = (u128)d0 + (uint64_t)p;
-      d0 = (uint64_t)t;
-      t = (u128)d1 + (uint64_t)(p >> 64) + (uint64_t)(t >> 64);
-      d1 = (uint64_t)t;
-      d2 += (uint64_t)(t >> 64);
-    }
-    u128 t = (u128)d0 + c0;
-    prod[k] = (uint64_t)t;
-    t = (u128)d1 + c1 + (uint64_t)(t >> 64);
-    c0 = (uint64_t)t;
-    c1 = d2 + (uint64_t)(t >> 64);
+    r[i + L] = c;
   }
-  prod[2 * L - 1] = c0;
-  std::memcpy(o, prod + (L - 1), L * sizeof(uint64_t));
+  uint64_t top = 0;
+  for (size_t k = 0; k < 2 * L; ++k) {
+    const uint64_t v = r[k];
+    r[k] = (v << 1) | top;
+    top = v >> 63;
+  }
+  u128 c = 0;
+  for (size_t i = 0; i < L; ++i) {
+    const u128 p = (u128)a[i] * a[i];
+    c += (u128)r[2 * i] + (uint64_t)p;
+    r[2 * i] = (uint64_t)c;
+    c >>= 64;
+    c += (u128)r[2 * i + 1] + (uint64_t)(p >> 64);
+    r[2 * i + 1] = (uint64_t)c;
+    c >>= 64;
+  }
+  std::memcpy(o, r + (L - 1), L * sizeof(uint64_t));
 }
 
 // Spin on `ready` (a short pause per try), then yield: the thread being waited for is
@@ -325,10 +322,10 @@ class SquareCrew {
   std::atomic<bool> stop_{false};
 };
 
-// Orbits of at least this many limbs (~1,450 bits) split each step's squarings over
+// Orbits of at least this many limbs (~1,700 bits) split each step's squarings over
 // three threads when asked to (threads >= 3); below it two barrier crossings per step
 // cost more than the squarings they share.
-constexpr size_t CREW_MIN_LIMBS = 24;
+constexpr size_t CREW_MIN_LIMBS = 28;
 
 // Z_{n+1} = Z_n^2 + C from Z_0 = 0 in L-limb fixed point with three squarings per step
 // (x' = x^2 - y^2 + cr, y' = (x + y)^2 - x^2 - y^2 + ci, crates/fd-fixed/src/orbit.rs:
@@ -338,8 +335,11 @@ constexpr size_t CREW_MIN_LIMBS = 24;
 uint64_t fixed_orbit(const Fix &cr, const Fix &ci, uint64_t steps, double escape2, double *re, double *im,
                      int threads) {
   const size_t L = cr.mag.size();
-  std::vector<uint64_t> buf(9 * L, 0);
-  uint64_t *x = buf.data(), *y = x + L, *x2 = y + L, *y2 = x2 + L, *s = y2 + L, *s2 = s + L, *t = s2 + L;
+  // each array on cache lines of its own (the crew's threads write y2 and s2)
+  const size_t W = (L + 7) & ~(size_t)7;
+  std::vector<uint64_t> buf(7 * W + 8, 0);
+  uint64_t *x = buf.data() + ((8 - ((uintptr_t)buf.data() / 8) % 8) % 8);
+  uint64_t *y = x + W, *x2 = y + W, *y2 = x2 + W, *s = y2 + W, *s2 = s + W, *t = s2 + W;
   std::vector<uint64_t> prod(2 * L);
   bool xn = false, yn = false;
   SquareCrew crew(L);

@@ -117,7 +117,7 @@ class Reference:
 
     @classmethod
     def from_fixed(cls, center_re: str, center_im: str, bits: int, max_iter: int, threads: int = 0) -> "Reference":
-        """threads: 3 shares each step's squarings among three threads on orbits of ~1,450
+        """threads: 3 shares each step's squarings among three threads on orbits of ~1,700
         bits and more, 1 keeps the orbit on the calling thread, 0 picks 3 on hosts with 4
         or more hardware threads. The orbit is the same bit for bit."""
         cap = min(max_iter, MAX_LEN - 1) + 1

@@ -39,7 +39,7 @@ int fdh_plane_new(const char *center_re, const char *center_im, const char *widt
  *                    crates/fd-fixed/src/orbit.rs:14-43) at the exact decimal centre.
  *   fdh_orbit_fixed_threads: the same orbit, bit for bit; threads >= 3 splits each
  *                    step's three squarings over three threads when the orbit has at
- *                    least 24 limbs (~1,450 bits), 1 keeps it serial, 0 picks 3 when the
+ *                    least 28 limbs (~1,700 bits), 1 keeps it serial, 0 picks 3 when the
  *                    host has 4 or more hardware threads (no counterpart: the
  *                    reference's orbit is serial).
  *   fdh_orbit_f64:   Reference::new (reference.rs:21-48). */
