@@ -111,6 +111,38 @@ int fdref_render(const fdref_job *job, const fdref_ref *ref, const fdref_bla *bl
                  double *z_out, double *dz_out, int64_t *dexp_out, fdref_stats *stats,
                  char *kernel, size_t kernel_cap);
 
+/* sample::iterate from a supplied state (Start, sample.rs:69-80, 186-228): start_n
+ * iterates done, delta (start_xr, start_xi) and dz/dc (start_dr, start_di); start_n 0 is
+ * fdref_iterate. Refused on the extended tier and at or past the orbit's last point. */
+int fdref_iterate_from(const fdref_ref *r, const fdref_bla *bla, int extended, int derivative,
+                       int has_c, double cr, double ci, double ar, double ai, int64_t offset_exp,
+                       uint64_t max_iter, double r2, int64_t nucleus, uint64_t start_n,
+                       double start_xr, double start_xi, double start_dr, double start_di,
+                       fdref_outcome *out);
+/* Series (crates/fd-kernel/src/series.rs): Series::build with SeriesConfig::default()
+ * (series.rs:43-55) and build_stalled's bound (32 in Series::build; 0 = unbounded). */
+typedef struct fdref_series fdref_series;
+typedef struct {
+  uint64_t n, points, built_steps, coefficient_pairs, order, growth_count;
+  double rho, state_bound, derivative_bound, shift_px;
+  char stop[16];
+} fdref_series_info;
+fdref_series *fdref_series_build(const fdref_ref *r, double rho, double pixel, uint64_t max_iter,
+                                 uint64_t stalled_steps);
+/* info, and the coefficients b[1..order] as (re, im) pairs when coeffs != NULL */
+void fdref_series_get(const fdref_series *s, fdref_series_info *info, double *coeffs);
+/* a copy whose admitted prefix is n (n = 0: the plain kernel) */
+fdref_series *fdref_series_with_n(const fdref_series *s, uint64_t n);
+/* Series::eval (series.rs:247-271): out4 = delta re, im, dz/dc re, im (0 without derivative) */
+void fdref_series_eval(const fdref_series *s, int derivative, double ar, double ai, double *out4);
+void fdref_series_free(fdref_series *s);
+/* render_series / Series::render_masked (grid.rs:213-226, 341-373): fdref_render with every
+ * sample started from the series; mask (nx*ny bytes, NULL = all) renders only samples
+ * with mask != 0, leaving the others' outputs untouched. */
+int fdref_render_series(const fdref_job *job, const fdref_ref *ref, const fdref_bla *bla,
+                        const fdref_series *series, const uint8_t *mask, uint8_t *cls, double *nu,
+                        float *de, uint16_t *normal, uint64_t *n_out, double *z_out, double *dz_out,
+                        int64_t *dexp_out, fdref_stats *stats, char *kernel, size_t kernel_cap);
 /* Encode one escaped state's columns exactly as Store::put (store.rs:66-112). */
 void fdref_store_escaped(double h_m, int64_t h_e, uint32_t ss, double rotation, uint64_t n,
                          double zr, double zi, double dr, double di, int64_t dexp,

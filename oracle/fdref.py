@@ -62,6 +62,13 @@ class Stats(C.Structure):
     ]
 
 
+class SeriesInfo(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in ("n", "points", "built_steps", "coefficient_pairs", "order",
+                                          "growth_count")] + \
+               [(k, C.c_double) for k in ("rho", "state_bound", "derivative_bound", "shift_px")] + \
+               [("stop", C.c_char * 16)]
+
+
 def build():
     """Compile liboracle.so from the C++ restatement (make in oracle/)."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
@@ -117,6 +124,17 @@ def lib():
         L.fdref_direct.argtypes = [C.c_char_p, C.c_char_p, D, D, I64, U64, U64, D, C.POINTER(D), C.POINTER(D)]
         L.fdref_render_fds.restype = I64
         L.fdref_render_fds.argtypes = [C.POINTER(Job), P, P, P, U64]
+        L.fdref_iterate_from.argtypes = [P, P, C.c_int, C.c_int, C.c_int, D, D, D, D, I64, U64, D, I64,
+                                         U64, D, D, D, D, C.POINTER(Outcome)]
+        L.fdref_series_build.restype = P
+        L.fdref_series_build.argtypes = [P, D, D, U64, U64]
+        L.fdref_series_get.argtypes = [P, C.POINTER(SeriesInfo), P]
+        L.fdref_series_with_n.restype = P
+        L.fdref_series_with_n.argtypes = [P, U64]
+        L.fdref_series_eval.argtypes = [P, C.c_int, D, D, P]
+        L.fdref_series_free.argtypes = [P]
+        L.fdref_render_series.argtypes = [C.POINTER(Job), P, P, P, P, P, P, P, P, P, P, P, P, C.POINTER(Stats),
+                                          C.c_char_p, C.c_size_t]
         _lib = L
     return _lib
 
@@ -222,6 +240,75 @@ class Bla:
         return None if n == 0 else (int(lv.value), int(ix.value), int(n))
 
 
+class Series:
+    """A parameter-series start (crates/fd-kernel/src/series.rs:57-84) built by the oracle:
+    Series::build with SeriesConfig::default() over the oracle orbit `ref`."""
+
+    def __init__(self, ref, rho, pixel, max_iter, stalled_steps=32, _h=None):
+        self.ref = ref
+        self.h = _h if _h is not None else lib().fdref_series_build(ref.h, rho, pixel, max_iter, stalled_steps)
+        if not self.h:
+            raise ValueError(_err())
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.fdref_series_free(self.h)
+            self.h = None
+
+    def info(self):
+        i = SeriesInfo()
+        lib().fdref_series_get(self.h, C.byref(i), None)
+        d = {k: getattr(i, k) for k, _ in SeriesInfo._fields_}
+        d["stop"] = i.stop.decode()
+        return d
+
+    def coefficients(self):
+        """b[1..order] as an (order, 2) array of (re, im)."""
+        i = SeriesInfo()
+        lib().fdref_series_get(self.h, C.byref(i), None)
+        b = np.zeros((i.order, 2))
+        lib().fdref_series_get(self.h, C.byref(i), b.ctypes.data)
+        return b
+
+    def with_n(self, n):
+        return Series(self.ref, 0, 0, 0, _h=lib().fdref_series_with_n(self.h, n))
+
+    def eval(self, ar, ai, derivative=True):
+        out = np.zeros(4)
+        lib().fdref_series_eval(self.h, int(derivative), ar, ai, out.ctypes.data)
+        return tuple(out)
+
+
+def render_series(job, ref, series, bla=None, mask=None, raw=False):
+    """render_series / Series::render_masked: render() with every sample started from the
+    series; mask (nx*ny bytes) renders only the samples where it is nonzero."""
+    n = job.nx * job.ny
+    cls = np.zeros(n, np.uint8)
+    nu = np.zeros(n, np.float64)
+    de = np.zeros(n, np.float32)
+    normal = np.zeros(n, np.uint16)
+    it = np.zeros(n, np.uint64)
+    z = np.zeros(2 * n) if raw else None
+    dz = np.zeros(2 * n) if raw else None
+    dexp = np.zeros(n, np.int64) if raw else None
+    m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+    st = Stats()
+    kernel = C.create_string_buffer(256)
+    ptr = lambda a: a.ctypes.data if a is not None else None
+    rc = lib().fdref_render_series(C.byref(job), ref.h, bla.h if bla else None, series.h, ptr(m), ptr(cls), ptr(nu),
+                                   ptr(de), ptr(normal), ptr(it), ptr(z), ptr(dz), ptr(dexp), C.byref(st), kernel,
+                                   256)
+    if rc != 0:
+        raise ValueError(_err())
+    out = dict(cls=cls, nu=nu, de=de, normal=normal, n=it, kernel=kernel.value.decode(),
+               stats=dict(reference_len=st.reference_len, iterations=st.iterations, blocks=st.blocks,
+                          skipped=st.skipped, fallback_samples=st.fallback_samples,
+                          closed_form_samples=st.closed_form_samples, shift_px=st.shift_px))
+    if raw:
+        out.update(z=z.reshape(n, 2), dz=dz.reshape(n, 2), dexp=dexp)
+    return out
+
+
 def plane(job):
     hm, he, tier, bits, cr, ci = C.c_double(), C.c_int64(), C.c_int32(), C.c_uint64(), C.c_double(), C.c_double()
     if lib().fdref_plane(C.byref(job), C.byref(hm), C.byref(he), C.byref(tier), C.byref(bits), C.byref(cr),
@@ -238,12 +325,14 @@ def bla_dc_bound(job):
 
 
 def iterate(ref, bla=None, extended=False, derivative=True, c=None, ar=0.0, ai=0.0, offset_exp=0,
-            max_iter=1000, r2=1e20, nucleus=-2):
-    """One sample through sample.rs:170-581. nucleus -2: the orbit's own gate."""
+            max_iter=1000, r2=1e20, nucleus=-2, start=None):
+    """One sample through sample.rs:170-581. nucleus -2: the orbit's own gate. start:
+    (n, xr, xi, dr, di), a state after n iterates to continue from (sample.rs:69-80)."""
     o = Outcome()
-    rc = lib().fdref_iterate(ref.h, bla.h if bla else None, int(extended), int(derivative), c is not None,
-                             c[0] if c else 0.0, c[1] if c else 0.0, ar, ai, offset_exp, max_iter, r2,
-                             -1 if nucleus is None else nucleus, C.byref(o))
+    sn, sxr, sxi, sdr, sdi = start if start is not None else (0, 0.0, 0.0, 0.0, 0.0)
+    rc = lib().fdref_iterate_from(ref.h, bla.h if bla else None, int(extended), int(derivative), c is not None,
+                                  c[0] if c else 0.0, c[1] if c else 0.0, ar, ai, offset_exp, max_iter, r2,
+                                  -1 if nucleus is None else nucleus, sn, sxr, sxi, sdr, sdi, C.byref(o))
     if rc != 0:
         raise ValueError(_err())
     kind = {0: "escaped", 1: "interior", 2: "unresolved"}[o.kind]

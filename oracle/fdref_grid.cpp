@@ -117,9 +117,12 @@ static void bla_checks(const Plane &plane, Tier tier, const Params &p, const Ref
   if (std::isnan(dc) || over) throw std::runtime_error("view reaches |dc| beyond the BLA table's dc_max");
 }
 
-// grid.rs:446-535 + Job::one/one_from/fill (grid.rs:623-775), without series/mask/stripe.
+// grid.rs:446-535 + Job::one/one_from/fill (grid.rs:623-775), without stripe. series: a
+// start every sample takes (n > 0; Series::render_masked's refusals, grid.rs:341-373,
+// checked here); mask: render only samples with mask != 0 (the others keep their columns).
 static std::string run(const View &v, const Params &p, const Reference *supplied, const Bla *bla, Columns cols,
-                       Stats &st, Reference *computed_out = nullptr) {
+                       Stats &st, Reference *computed_out = nullptr, const Series *series = nullptr,
+                       const uint8_t *mask = nullptr) {
   auto [plane, tier] = setup(v, p);
   uint32_t need = precision(plane, tier);
   Reference computed;
@@ -137,7 +140,15 @@ static std::string run(const View &v, const Params &p, const Reference *supplied
     computed = compute(v, plane, tier, p);
     ref = &computed;
   }
+  const bool series_given = series != nullptr;
+  if (series) {  // grid.rs:350-366
+    if (tier == Tier::Scaled) throw std::runtime_error("a series start needs f64 deltas and no Bound column");
+    if (series->points != ref->len()) throw std::runtime_error("series built over another orbit");
+    const double dc = dc_bound(plane, tier, p).first;
+    if (std::isnan(dc) || dc > series->rho) throw std::runtime_error("view reaches |dc| beyond the series radius");
+  }
   if (bla) bla_checks(plane, tier, p, *ref, *bla);
+  if (series && series->n == 0) series = nullptr;  // grid.rs:491: no admitted prefix, the plain kernel
   const bool D = (p.columns & (FDREF_COL_DE | FDREF_COL_NORMAL)) != 0;
   const bool L = bla != nullptr;
   const double h = plane.h();
@@ -152,26 +163,38 @@ static std::string run(const View &v, const Params &p, const Reference *supplied
       if (jj >= p.ny) break;
       uint32_t j = (uint32_t)jj;
       for (uint32_t i = 0; i < p.nx; ++i) {
+        if (mask && !mask[(size_t)j * p.nx + i]) continue;
         double ux, uy;
         plane.unit_offset(i, j, ux, uy);
         Skip skip;
-        Outcome o;
-        switch (tier) {
-          case Tier::F64: {
-            double ar = ux * h, ai = uy * h;
-            o = iterate(false, D, L, *ref, bla, skip, std::make_pair(plane.c_re + ar, plane.c_im + ai), ar, ai, 0,
-                        p.max_iter, r2, nucleus);
-            break;
+        // Job::one_from (grid.rs:651-717): the series start on the f64 tiers
+        auto one_from = [&](bool use_series) {
+          auto start = [&](double ar, double ai) { return series && use_series ? series->eval(D, ar, ai) : Start{}; };
+          switch (tier) {
+            case Tier::F64: {
+              double ar = ux * h, ai = uy * h;
+              return iterate(false, D, L, *ref, bla, skip, std::make_pair(plane.c_re + ar, plane.c_im + ai), ar, ai,
+                             0, p.max_iter, r2, nucleus, start(ar, ai));
+            }
+            case Tier::Fixed:
+              return iterate(false, D, L, *ref, bla, skip, std::nullopt, ux * h, uy * h, 0, p.max_iter, r2, nucleus,
+                             start(ux * h, uy * h));
+            case Tier::Scaled:
+            default:
+              return iterate(true, D, L, *ref, bla, skip, std::nullopt, ux * plane.h_m, uy * plane.h_m, plane.h_e,
+                             p.max_iter, r2, nucleus);
           }
-          case Tier::Fixed:
-            o = iterate(false, D, L, *ref, bla, skip, std::nullopt, ux * h, uy * h, 0, p.max_iter, r2, nucleus);
-            break;
-          case Tier::Scaled:
-            o = iterate(true, D, L, *ref, bla, skip, std::nullopt, ux * plane.h_m, uy * plane.h_m, plane.h_e,
-                        p.max_iter, r2, nucleus);
-            break;
+        };
+        // Job::one (grid.rs:623-648): the prefix is not counted; an unresolved series start
+        // retries from zero (keeping the nucleus heuristic), counting both runs
+        const Outcome first = one_from(true);
+        const uint64_t prefix = series && !(first.kind == Kind::Interior && first.n == 0) ? series->n : 0;
+        uint64_t spent = first.iterations(p.max_iter) - prefix;
+        Outcome o = first;
+        if (prefix > 0 && first.kind == Kind::Unresolved) {
+          o = one_from(false);
+          spent += o.iterations(p.max_iter);
         }
-        uint64_t spent = o.iterations(p.max_iter);
         if (L) {
           spent = spent - skip.skipped + skip.blocks;
           local.blocks += skip.blocks;
@@ -204,6 +227,7 @@ static std::string run(const View &v, const Params &p, const Reference *supplied
   else st.shift = NAN;
   std::string kernel = plane.kernel(tier);
   if (bla) kernel += " bla/1";
+  if (series_given) kernel += " series/0";  // grid.rs:371
   if (computed_out && !supplied) *computed_out = std::move(computed);
   return kernel;
 }
@@ -272,6 +296,9 @@ struct fdref_ref {
 };
 struct fdref_bla {
   Bla t;
+};
+struct fdref_series {
+  Series s;
 };
 
 static thread_local std::string g_error;
@@ -418,6 +445,14 @@ int fdref_bla_dc_bound(const fdref_job *job, double *dc, int64_t *e) {
 int fdref_iterate(const fdref_ref *r, const fdref_bla *bla, int extended, int derivative, int has_c, double cr,
                   double ci, double ar, double ai, int64_t offset_exp, uint64_t max_iter, double r2,
                   int64_t nucleus, fdref_outcome *out) {
+  return fdref_iterate_from(r, bla, extended, derivative, has_c, cr, ci, ar, ai, offset_exp, max_iter, r2, nucleus, 0,
+                            0.0, 0.0, 0.0, 0.0, out);
+}
+
+int fdref_iterate_from(const fdref_ref *r, const fdref_bla *bla, int extended, int derivative, int has_c, double cr,
+                       double ci, double ar, double ai, int64_t offset_exp, uint64_t max_iter, double r2,
+                       int64_t nucleus, uint64_t start_n, double start_xr, double start_xi, double start_dr,
+                       double start_di, fdref_outcome *out) {
   FDREF_TRY({
     std::optional<size_t> nuc;
     if (nucleus == -2) nuc = r->r.nucleus_period();
@@ -425,8 +460,14 @@ int fdref_iterate(const fdref_ref *r, const fdref_bla *bla, int extended, int de
     std::optional<std::pair<double, double>> c;
     if (has_c) c = std::make_pair(cr, ci);
     Skip skip;
+    Start start;
+    start.n = start_n;
+    start.xr = start_xr;
+    start.xi = start_xi;
+    start.dr = start_dr;
+    start.di = start_di;
     Outcome o = iterate(extended != 0, derivative != 0, bla != nullptr, r->r, bla ? &bla->t : nullptr, skip, c, ar,
-                        ai, offset_exp, max_iter, r2, nuc);
+                        ai, offset_exp, max_iter, r2, nuc, start);
     out->kind = (int32_t)o.kind;
     out->n = o.n;
     out->zr = o.zr;
@@ -457,6 +498,87 @@ int fdref_render(const fdref_job *job, const fdref_ref *ref, const fdref_bla *bl
     c.dexp = dexp_out;
     Stats st;
     std::string k = run(to_view(job), to_params(job), ref ? &ref->r : nullptr, bla ? &bla->t : nullptr, c, st);
+    if (stats) {
+      stats->reference_len = st.reference_len;
+      stats->iterations = st.iterations;
+      stats->blocks = st.blocks;
+      stats->skipped = st.skipped;
+      stats->fallback_samples = st.fallback;
+      stats->closed_form_samples = st.closed;
+      stats->shift_px = st.shift;
+    }
+    if (kernel && kernel_cap) {
+      std::strncpy(kernel, k.c_str(), kernel_cap - 1);
+      kernel[kernel_cap - 1] = 0;
+    }
+    return 0;
+  })
+  return -1;
+}
+
+fdref_series *fdref_series_build(const fdref_ref *r, double rho, double pixel, uint64_t max_iter,
+                                 uint64_t stalled_steps) {
+  FDREF_TRY({ return new fdref_series{Series::build(r->r, rho, pixel, max_iter, SeriesConfig{}, stalled_steps)}; })
+  return nullptr;
+}
+
+void fdref_series_get(const fdref_series *s, fdref_series_info *info, double *coeffs) {
+  info->n = s->s.n;
+  info->points = s->s.points;
+  info->built_steps = s->s.built_steps;
+  info->coefficient_pairs = s->s.coefficient_pairs;
+  info->order = s->s.b.size();
+  info->growth_count = s->s.growth.size();
+  info->rho = s->s.rho;
+  info->state_bound = s->s.state_bound;
+  info->derivative_bound = s->s.derivative_bound;
+  info->shift_px = s->s.shift_px;
+  std::strncpy(info->stop, s->s.stop.c_str(), sizeof(info->stop) - 1);
+  info->stop[sizeof(info->stop) - 1] = 0;
+  if (coeffs)
+    for (size_t k = 0; k < s->s.b.size(); ++k) {
+      coeffs[2 * k] = s->s.b[k].first;
+      coeffs[2 * k + 1] = s->s.b[k].second;
+    }
+}
+
+fdref_series *fdref_series_with_n(const fdref_series *s, uint64_t n) {
+  FDREF_TRY({
+    fdref_series *c = new fdref_series{s->s};
+    c->s.n = n;
+    return c;
+  })
+  return nullptr;
+}
+
+void fdref_series_eval(const fdref_series *s, int derivative, double ar, double ai, double *out4) {
+  Start st = s->s.eval(derivative != 0, ar, ai);
+  out4[0] = st.xr;
+  out4[1] = st.xi;
+  out4[2] = st.dr;
+  out4[3] = st.di;
+}
+
+void fdref_series_free(fdref_series *s) { delete s; }
+
+int fdref_render_series(const fdref_job *job, const fdref_ref *ref, const fdref_bla *bla, const fdref_series *series,
+                        const uint8_t *mask, uint8_t *cls, double *nu, float *de, uint16_t *normal, uint64_t *n_out,
+                        double *z_out, double *dz_out, int64_t *dexp_out, fdref_stats *stats, char *kernel,
+                        size_t kernel_cap) {
+  FDREF_TRY({
+    if (!series) throw std::runtime_error("no series");
+    Columns c;
+    c.cls = cls;
+    c.nu = nu;
+    c.de = de;
+    c.normal = normal;
+    c.n = n_out;
+    c.z = z_out;
+    c.dz = dz_out;
+    c.dexp = dexp_out;
+    Stats st;
+    std::string k = run(to_view(job), to_params(job), ref ? &ref->r : nullptr, bla ? &bla->t : nullptr, c, st,
+                        nullptr, &series->s, mask);
     if (stats) {
       stats->reference_len = st.reference_len;
       stats->iterations = st.iterations;

@@ -106,9 +106,39 @@ struct Skip {
   double shift = 0.0;
 };
 
+// A sample's state after n iterates (sample.rs:69-80): delta (xr, xi) against Z_n and
+// dz/dc (dr, di); the default is the ordinary start at Z_0.
+struct Start {
+  uint64_t n = 0;
+  double xr = 0.0, xi = 0.0, dr = 0.0, di = 0.0;
+};
+
 Outcome iterate(bool extended, bool D, bool L, const Reference &r, const Bla *bla, Skip &skip,
                 std::optional<std::pair<double, double>> c, double ar, double ai, int64_t offset_exp,
-                uint64_t max_iter, double r2, std::optional<size_t> nucleus);
+                uint64_t max_iter, double r2, std::optional<size_t> nucleus, const Start &start = Start{});
+
+// series.rs:26-55
+struct SeriesConfig {
+  size_t start_order = 8, max_order = 64;
+  double grow_at = 1e-4, shift_px = 1e-8, derivative_rel = 1e-6;
+};
+
+// series.rs:57-84: an admitted prefix of n iterates for samples with |dc| <= rho.
+struct Series {
+  uint64_t n = 0;
+  double rho = 0.0;
+  uint64_t points = 0;
+  std::vector<std::pair<double, double>> b;  // b[1..], trimmed
+  double state_bound = 0.0, derivative_bound = 0.0, shift_px = 0.0;
+  uint64_t built_steps = 0;
+  std::string stop = "reference";
+  uint64_t coefficient_pairs = 0;
+  std::vector<uint64_t> growth;
+  static Series build(const Reference &r, double rho, double pixel, uint64_t max_iter, const SeriesConfig &cfg,
+                      uint64_t stalled_steps = 32);
+  // the state after n iterates for dc = (ar, ai): delta, and dz/dc when D
+  Start eval(bool D, double ar, double ai) const;
+};
 
 bool in_main_components(double cr, double ci);
 

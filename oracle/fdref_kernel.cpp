@@ -436,13 +436,13 @@ static inline uint64_t next_pow2(uint64_t x) {
 }
 
 // ---------------------------------------------------------------- sample.rs:170-581
-// The B (bounded), trace/stripe and series-start features are outside the hot path
-// (the GPU route declines Bound/Stripe frames, and starts every sample at n = 0).
+// The B (bounded) and trace/stripe features are outside the hot path (the GPU route
+// declines Bound/Stripe frames). A series start (Start, sample.rs:69-80) is supported.
 template <bool EXT, bool D, bool L>
 static Outcome iterate_t(const Reference &r, const Bla *bla, Skip &skip,
                          std::optional<std::pair<double, double>> c, double ar, double ai,
                          int64_t offset_exp, uint64_t max_iter, double r2,
-                         std::optional<size_t> nucleus) {
+                         std::optional<size_t> nucleus, const Start &start) {
   Outcome o;
   if (c && in_main_components(c->first, c->second)) {
     o.kind = Kind::Interior;
@@ -451,17 +451,25 @@ static Outcome iterate_t(const Reference &r, const Bla *bla, Skip &skip,
   }
   const double *zr = r.re.data(), *zi = r.im.data();
   size_t last = r.len() - 1;
-  double xr = 0.0, xi = 0.0;
+  // sample.rs:186: a supplied start is an ordinary-tier state below the last point
+  if (start.n > 0 && (EXT || start.n >= (uint64_t)last)) throw std::runtime_error("invalid start state");
+  double xr = start.xr, xi = start.xi;
   int64_t delta_exp = EXT ? offset_exp : 0;
   double scale = EXT ? exp2i(delta_exp) : 1.0;
   double dc_r = ar, dc_i = ai;
-  double dr = 0.0, di = 0.0;
+  double dr = start.dr, di = start.di;
   int64_t derivative_exp = 0;
   double inverse = 1.0;
-  size_t m = 0;
-  uint64_t n = 0;
+  size_t m = (size_t)start.n;
+  uint64_t n = start.n;
   double sr = 0.0, si = 0.0;
   uint64_t chk = 16, sn = EXT ? 0 : 8;
+  if (n > 0) {  // sample.rs:205-213: the supplied state is the first save
+    sr = zr[m] + xr;
+    si = zi[m] + xi;
+    sn = n;
+    chk = std::max<uint64_t>(next_pow2(n + 1), 16);
+  }
   int returns = 0;
   bool pending = false;
   Multiplier mu;
@@ -719,11 +727,18 @@ static Outcome iterate_t(const Reference &r, const Bla *bla, Skip &skip,
   return o;
 }
 
+// GCC flags the copy of a disengaged std::optional into iterate_t's parameter as a read
+// of its (unused) payload; the payload is only read when engaged.
+#pragma GCC diagnostic push
+#pragma GCC diagnostic ignored "-Wmaybe-uninitialized"
 Outcome iterate(bool extended, bool D, bool L, const Reference &r, const Bla *bla, Skip &skip,
                 std::optional<std::pair<double, double>> c, double ar, double ai, int64_t offset_exp,
-                uint64_t max_iter, double r2, std::optional<size_t> nucleus) {
+                uint64_t max_iter, double r2, std::optional<size_t> nucleus, const Start &start) {
+  // sample.rs:226-228: a supplied state skipped the contraction's products, so it
+  // declines the nucleus heuristic
+  if (start.n > 0) nucleus = std::nullopt;
 #define FDREF_IT(E, DD, LL) \
-  iterate_t<E, DD, LL>(r, bla, skip, c, ar, ai, offset_exp, max_iter, r2, nucleus)
+  iterate_t<E, DD, LL>(r, bla, skip, c, ar, ai, offset_exp, max_iter, r2, nucleus, start)
   if (extended) {
     if (D) return L ? FDREF_IT(true, true, true) : FDREF_IT(true, true, false);
     return L ? FDREF_IT(true, false, true) : FDREF_IT(true, false, false);
@@ -732,5 +747,6 @@ Outcome iterate(bool extended, bool D, bool L, const Reference &r, const Bla *bl
   return L ? FDREF_IT(false, false, true) : FDREF_IT(false, false, false);
 #undef FDREF_IT
 }
+#pragma GCC diagnostic pop
 
 }  // namespace fdref

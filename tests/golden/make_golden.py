@@ -6,7 +6,10 @@ under tests/golden/ are what the tests read. Sources, all from junovhs/fractodac
   truth_v1/*.tsv.gz, precision-edges.txt   bench/truth/v1 (frozen mpmath observations)
   kats.json                                constants of crates/fd-kernel/src/sample.rs tests
                                            (v0 centre :944-947, FNV cases :717-722) and the
-                                           k=7676 rung of tools/research/misiurewicz/ladder_rungs.txt
+                                           k=7676 rung of tools/research/misiurewicz/ladder_rungs.txt,
+                                           and the series frames (centre, width) of
+                                           docs/2026-10-20/series-frames/results/frames.txt, which
+                                           crates/fd-kernel/src/series.rs tests read
   kern05.json                              per-frame digests of crates/fd-kernel/fixtures/KERN-05.bundle
                                            (format: crates/fd-kernel/examples/kernel_contract.rs:82-96)
                                            plus the bench/locations.txt rows that produced them
@@ -55,7 +58,13 @@ def main(root):
         if line.startswith("7676 "):
             f = line.split()
             rung = {"k": 7676, "period": int(f[1]), "re": f[2], "im": f[3]}
-    kats = {"v0": {"re": v0[0], "im": v0[1]}, "fnv_views": fnv, "rung_7676": rung}
+    series_frames = []
+    for line in open(os.path.join(root, "docs/2026-10-20/series-frames/results/frames.txt")):
+        if line.startswith("#") or not line.strip():
+            continue
+        f = line.split()
+        series_frames.append({"re": f[0], "im": f[1], "width": f[2]})
+    kats = {"v0": {"re": v0[0], "im": v0[1]}, "fnv_views": fnv, "rung_7676": rung, "series_frames": series_frames}
     with open(os.path.join(HERE, "kats.json"), "w") as f:
         json.dump(kats, f, indent=1)
 
