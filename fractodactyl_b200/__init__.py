@@ -5,9 +5,10 @@ the kernels and the host set-up; this package is the Python mirror of the refere
 route interface over it (route.py) plus the .fds v1 writer (fds.py).
 """
 from .route import (EPS, EPS_MAX, FILM_EPS, Bla, BlaStats, Declined, Device, Header, Params, Plane, Reference,
-                    RouteError, RouteReport, Samples, Stats, View, bla_dc_bound, device, enabled, reference, render,
-                    render_bla, render_with)
+                    RouteError, RouteReport, Samples, Series, Stats, View, bla_dc_bound, device, enabled, reference,
+                    render, render_bla, render_with)
 
 __all__ = ["EPS", "EPS_MAX", "FILM_EPS", "Bla", "BlaStats", "Declined", "Device", "Header", "Params", "Plane",
-           "Reference", "RouteError", "RouteReport", "Samples", "Stats", "View", "bla_dc_bound", "device", "enabled",
+           "Reference", "RouteError", "RouteReport", "Samples", "Series", "Stats", "View", "bla_dc_bound", "device",
+           "enabled",
            "reference", "render", "render_bla", "render_with"]

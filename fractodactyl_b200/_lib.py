@@ -43,6 +43,22 @@ class Job(C.Structure):
     ]
 
 
+class SeriesInfo(C.Structure):  # fdh_series (include/fdhost.h)
+    _fields_ = [
+        ("n", C.c_uint64),
+        ("points", C.c_uint64),
+        ("built_steps", C.c_uint64),
+        ("coefficient_pairs", C.c_uint64),
+        ("order", C.c_uint32),
+        ("growth_count", C.c_uint32),
+        ("rho", C.c_double),
+        ("state_bound", C.c_double),
+        ("derivative_bound", C.c_double),
+        ("shift_px", C.c_double),
+        ("stop", C.c_char * 16),
+    ]
+
+
 class Out(C.Structure):
     _fields_ = [(name, C.c_void_p) for name in ("cls", "n", "nu", "de", "normal", "z", "dz", "dexp", "status")]
 
@@ -89,7 +105,7 @@ FDC_SYMBOLS = ["fdc_abi_version", "fdc_open", "fdc_close", "fdc_last_error", "fd
                "fdc_render_noalloc", "fdc_set_tuning", "fdc_get_tuning"]
 FDH_SYMBOLS = ["fdh_last_error", "fdh_plane_new", "fdh_orbit_fixed", "fdh_orbit_fixed_threads", "fdh_orbit_f64",
                "fdh_nucleus_period",
-               "fdh_bla_build", "fdh_bla_build_into", "fdh_dc_bound", "fdh_encode", "fdh_location"]
+               "fdh_bla_build", "fdh_bla_build_into", "fdh_series_build", "fdh_dc_bound", "fdh_encode", "fdh_location"]
 
 _lib = None
 
@@ -130,6 +146,8 @@ def lib():
     L.fdh_nucleus_period.restype = I64
     L.fdh_nucleus_period.argtypes = [P, P, U64]
     L.fdh_bla_build.argtypes = [P, P, U64, D, D, I64, C.c_int, P, P, C.POINTER(U32), C.POINTER(U64)]
+    L.fdh_series_build.restype = C.c_int
+    L.fdh_series_build.argtypes = [P, P, U64, D, D, U64, U64, C.POINTER(SeriesInfo), P, U32]
     L.fdh_bla_build_into.restype = C.c_int
     L.fdh_bla_build_into.argtypes = [P, P, U64, D, D, I64, C.c_int, P, U64, P, U32, C.POINTER(U32), C.POINTER(U64)]
     L.fdh_encode.argtypes = [C.POINTER(Plane), U32, U64, P, P, P, P, P, P, P, P, C.c_int]

@@ -708,6 +708,144 @@ int fdh_bla_build_into(const double *re, const double *im, uint64_t len, double 
   return 0;
 }
 
+// Series::build (crates/fd-kernel/src/series.rs:86-245) with SeriesConfig::default()
+// (series.rs:43-55): the coefficients b_k of delta_n(x) = sum b_k x^k, x = dc / rho, are
+// stepped with the orbit (b_1' = 2 Z b_1 + rho, b_k' = 2 Z b_k + sum_{i+j=k} b_i b_j) over
+// the first `active` orders, with majorants E (state) and F (its x-derivative) of what the
+// truncation omits; the last step whose error maps to at most shift_px output pixels is
+// admitted, then orders whose norms fit in half the remaining slack are trimmed. Every
+// expression is the reference's, in its order (the start decides each sample's outcome).
+int fdh_series_build(const double *re, const double *im, uint64_t len, double rho, double pixel, uint64_t max_iter,
+                     uint64_t stalled_steps, fdh_series *out, double *coeffs, uint32_t cap_order) {
+  const size_t start_order = 8, max_order = 64;
+  const double grow_at = 1e-4, shift_px = 1e-8, derivative_rel = 1e-6;
+  try {
+    std::memset(out, 0, sizeof(*out));
+    out->rho = rho;
+    out->points = len;
+    std::strncpy(out->stop, "reference", sizeof(out->stop) - 1);
+    const size_t k_max = max_order;
+    size_t active = start_order;
+    std::vector<double> br(k_max + 1, 0.0), bi(k_max + 1, 0.0), sq_r(2 * k_max + 1, 0.0), sq_i(2 * k_max + 1, 0.0);
+    std::vector<double> keep_r, keep_i;  // the admitted step's b_1..b_active
+    double e = 0.0, f = 0.0;
+    bool have = false;
+    uint64_t best_n = 0;
+    double best_e = 0, best_f = 0, best_budget_e = 0, best_budget_f = 0, best_dmin = 0;
+    const uint64_t limit = std::min(len >= 2 ? len - 2 : 0, max_iter >= 1 ? max_iter - 1 : 0);
+    auto set_stop = [&](const char *why) { std::strncpy(out->stop, why, sizeof(out->stop) - 1); };
+    if (!(rho > 0.0 && std::isfinite(rho) && pixel > 0.0)) {
+      set_stop("radius");
+      return 0;
+    }
+    const double cap_e = shift_px * pixel * 2.0 / rho, cap_f = derivative_rel * 2.0;
+    for (uint64_t n = 0; n < limit; ++n) {
+      const double zr = re[n], zi = im[n];
+      const double az = std::hypot(zr, zi);
+      std::fill(sq_r.begin(), sq_r.begin() + 2 * active + 1, 0.0);
+      std::fill(sq_i.begin(), sq_i.begin() + 2 * active + 1, 0.0);
+      for (size_t i = 1; i <= active; ++i) {  // the square of the active polynomial
+        const double ar = br[i], ai = bi[i];
+        if (ar == 0.0 && ai == 0.0) continue;
+        sq_r[2 * i] += ar * ar - ai * ai;
+        sq_i[2 * i] += 2.0 * ar * ai;
+        const double tr = 2.0 * ar, ti = 2.0 * ai;
+        for (size_t j = i + 1; j <= active; ++j) {
+          sq_r[i + j] += tr * br[j] - ti * bi[j];
+          sq_i[i + j] += tr * bi[j] + ti * br[j];
+        }
+      }
+      out->coefficient_pairs += (uint64_t)(active * (active + 1) / 2);
+      double mag = 0.0, dmag = 0.0, omit = 0.0, domit = 0.0;
+      for (size_t k = 1; k <= active; ++k) {
+        const double a = std::hypot(br[k], bi[k]);
+        mag += a;
+        dmag += (double)k * a;
+      }
+      for (size_t k = active + 1; k <= 2 * active; ++k) {  // the square's omitted orders
+        const double a = std::hypot(sq_r[k], sq_i[k]);
+        omit += a;
+        domit += (double)k * a;
+      }
+      const double e_next = 2.0 * (az + mag) * e + e * e + omit;
+      f = 2.0 * (az + mag + e) * f + 2.0 * e * dmag + domit;
+      e = e_next;
+      for (size_t k = 1; k <= active; ++k) {
+        const double xr = br[k], xi = bi[k];
+        br[k] = 2.0 * (zr * xr - zi * xi) + sq_r[k];
+        bi[k] = 2.0 * (zr * xi + zi * xr) + sq_i[k];
+      }
+      br[1] += rho;
+      const uint64_t step = n + 1;  // the state after step n + 1
+      out->built_steps = step;
+      double m1 = 0.0, tail_d = 0.0;
+      for (size_t k = 1; k <= active; ++k) {
+        const double a = std::hypot(br[k], bi[k]);
+        m1 += a;
+        if (k >= 2) tail_d += (double)k * a;
+      }
+      if (!(std::isfinite(e) && std::isfinite(f))) {
+        set_stop("non-finite");
+        break;
+      }
+      if (std::hypot(re[step], im[step]) + m1 + e >= 2.0) {
+        set_stop("escape");
+        break;
+      }
+      const double dmin = std::hypot(br[1], bi[1]) - tail_d - f;
+      const double budget = dmin > 0.0 ? shift_px * pixel * dmin / rho : 0.0;
+      if (dmin > 0.0 && e <= budget && f <= derivative_rel * dmin) {
+        have = true;
+        best_n = step;
+        keep_r.assign(br.begin() + 1, br.begin() + 1 + active);
+        keep_i.assign(bi.begin() + 1, bi.begin() + 1 + active);
+        best_e = e;
+        best_f = f;
+        best_budget_e = budget;
+        best_budget_f = derivative_rel * dmin;
+        best_dmin = dmin;
+      } else if (e > cap_e || f > cap_f) {
+        set_stop("budget");
+        break;
+      }
+      if (active < k_max && e > grow_at * budget) {
+        active = std::min(2 * active, k_max);
+        out->growth_count += 1;
+      }
+      if (stalled_steps > 0 && have && step - best_n >= stalled_steps) {
+        set_stop("stall");
+        break;
+      }
+    }
+    if (have) {
+      const double slack_e = best_budget_e - best_e, slack_f = best_budget_f - best_f;
+      double te = 0.0, tf = 0.0;
+      size_t order = keep_r.size();
+      while (order > 1) {
+        const double a = std::hypot(keep_r[order - 1], keep_i[order - 1]);
+        if (te + a > 0.5 * slack_e || tf + (double)order * a > 0.5 * slack_f) break;
+        te += a;
+        tf += (double)order * a;
+        order -= 1;
+      }
+      if (order > cap_order) throw std::runtime_error("series coefficients larger than the buffer given");
+      out->n = best_n;
+      out->order = (uint32_t)order;
+      out->state_bound = best_e + te;
+      out->derivative_bound = best_f + tf;
+      out->shift_px = out->state_bound * rho / (best_dmin * pixel);
+      for (size_t k = 0; k < order; ++k) {
+        coeffs[2 * k] = keep_r[k];
+        coeffs[2 * k + 1] = keep_i[k];
+      }
+    }
+    return 0;
+  } catch (std::exception &ex) {
+    g_err = ex.what();
+    return -1;
+  }
+}
+
 void fdh_encode(const fdh_plane *plane, uint32_t ss, uint64_t count, const uint8_t *cls, const uint32_t *n,
                 const double *z, const double *dz, const int64_t *dexp, double *nu, float *de, uint16_t *normal,
                 int threads) {

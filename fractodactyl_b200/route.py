@@ -176,6 +176,36 @@ class Bla:
 
 
 @dataclasses.dataclass
+class Series:
+    """A parameter-series start (crates/fd-kernel/src/series.rs:57-84): every sample with
+    |dc| <= rho may start at iterate n from delta = sum_k b_k (dc / rho)^k. n = 0: none
+    admitted (the plain kernel)."""
+    n: int
+    rho: float
+    points: int
+    b: np.ndarray  # (order, 2): b_1..b_order as (re, im)
+    state_bound: float
+    derivative_bound: float
+    shift_px: float
+    built_steps: int
+    coefficient_pairs: int
+    stop: str
+
+    @classmethod
+    def build(cls, r: Reference, rho: float, pixel: float, max_iter: int, stalled_steps: int = 32) -> "Series":
+        """Series::build with SeriesConfig::default() over orbit r, for |dc| <= rho and
+        output pixels of `pixel` in c."""
+        re, im = np.ascontiguousarray(r.re), np.ascontiguousarray(r.im)
+        info = _lib.SeriesInfo()
+        b = np.zeros((64, 2))
+        if lib().fdh_series_build(re.ctypes.data, im.ctypes.data, len(re), rho, pixel, max_iter, stalled_steps,
+                                  C.byref(info), b.ctypes.data, 64) != 0:
+            raise ValueError(_lib.host_error())
+        return cls(info.n, info.rho, info.points, b[:info.order].copy(), info.state_bound, info.derivative_bound,
+                   info.shift_px, info.built_steps, info.coefficient_pairs, info.stop.decode())
+
+
+@dataclasses.dataclass
 class Header:
     """crates/fd-samples/src/header.rs:29-45."""
     columns: tuple

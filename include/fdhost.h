@@ -69,6 +69,21 @@ int fdh_bla_build_into(const double *re, const double *im, uint64_t len, double 
                        int threads, double *blocks7, uint64_t cap_blocks, uint64_t *level_offsets, uint32_t cap_levels,
                        uint32_t *levels, uint64_t *blocks);
 
+/* Series::build (crates/fd-kernel/src/series.rs:86-245) with SeriesConfig::default()
+ * (series.rs:43-55) over an orbit, for samples with |dc| <= rho and output pixels of
+ * `pixel` in c: the parameter-series start every sample of a frame may take (n iterates
+ * skipped; n = 0: none admitted). stalled_steps bounds consecutive rejections (32 in
+ * Series::build, 0 unbounded). coeffs receives b_1..b_order as (re, im) pairs (room for
+ * cap_order pairs; 64 always suffice). */
+typedef struct fdh_series {
+  uint64_t n, points, built_steps, coefficient_pairs;
+  uint32_t order, growth_count;
+  double rho, state_bound, derivative_bound, shift_px;
+  char stop[16];
+} fdh_series;
+int fdh_series_build(const double *re, const double *im, uint64_t len, double rho, double pixel, uint64_t max_iter,
+                     uint64_t stalled_steps, fdh_series *out, double *coeffs, uint32_t cap_order);
+
 /* grid.rs:418-444: bound m 2^e on |dc| over a view's samples for a tier. */
 void fdh_dc_bound(const fdh_plane *plane, int32_t tier, uint32_t nx, uint32_t ny, double *dc, int64_t *e);
 

@@ -188,3 +188,35 @@ def test_fds_writer_and_host_encoder_bytes(case):
     fd.route.encode_host(plane, 1, s)
     h = fd.Header(("class", "nu", "de", "normal"), 8, 4, 1, 5000, 1e10, view, o["kernel"])
     assert fds.encode(h, s) == want
+
+
+@pytest.mark.parametrize("case", ["seahorse", "frame_first", "frame_last", "unbounded", "tight"])
+def test_series_build_bit_exact(case):
+    """fdh_series_build (Series::build, series.rs:86-245) equals the oracle's series bit for
+    bit: admitted prefix, coefficients, bounds and the work counters."""
+    frames = KATS["series_frames"]
+    stalled = 32
+    if case in ("seahorse", "unbounded", "tight"):
+        a = fdref.Ref.f64(-0.743643887037158, 0.131825904205312, 20_000, 1e10)
+        rho, pixel, max_iter = {"seahorse": (1e-11, 1e-13, 20_000), "unbounded": (1e-11, 1e-13, 20_000),
+                                "tight": (1e-6, 1e-9, 5_000)}[case]
+        stalled = 0 if case == "unbounded" else 32
+    else:
+        v = frames[0] if case == "frame_first" else frames[-1]
+        job = fdref.make_job(v["re"], v["im"], v["width"], 33, 19, 10_000)
+        a = fdref.Ref.for_job(job)
+        rho, _ = fdref.bla_dc_bound(job)
+        pixel, max_iter = float(v["width"]) / 33.0, 10_000
+    want = fdref.Series(a, rho, pixel, max_iter, stalled_steps=stalled)
+    re_, im_ = a.arrays_()
+    got = fd.Series.build(fd.Reference(np.ascontiguousarray(re_), np.ascontiguousarray(im_), a.bits), rho, pixel,
+                          max_iter, stalled_steps=stalled)
+    w = want.info()
+    assert (got.n, got.points, got.built_steps, got.coefficient_pairs, got.stop) == \
+        (w["n"], w["points"], w["built_steps"], w["coefficient_pairs"], w["stop"])
+    assert len(got.b) == w["order"]
+    assert np.array_equal(got.b.view(np.uint64), want.coefficients().view(np.uint64))
+    for k in ("rho", "state_bound", "derivative_bound", "shift_px"):
+        assert np.float64(getattr(got, k)).view(np.uint64) == np.float64(w[k]).view(np.uint64), k
+    if case != "tight":
+        assert got.n > 0
