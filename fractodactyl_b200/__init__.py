@@ -6,9 +6,9 @@ route interface over it (route.py) plus the .fds v1 writer (fds.py).
 """
 from .route import (EPS, EPS_MAX, FILM_EPS, Bla, BlaStats, Declined, Device, Header, Params, Plane, Reference,
                     RouteError, RouteReport, Samples, Series, Stats, View, bla_dc_bound, device, enabled, reference,
-                    render, render_bla, render_with)
+                    render, render_bla, render_series, render_with)
 
 __all__ = ["EPS", "EPS_MAX", "FILM_EPS", "Bla", "BlaStats", "Declined", "Device", "Header", "Params", "Plane",
            "Reference", "RouteError", "RouteReport", "Samples", "Series", "Stats", "View", "bla_dc_bound", "device",
            "enabled",
-           "reference", "render", "render_bla", "render_with"]
+           "reference", "render", "render_bla", "render_series", "render_with"]

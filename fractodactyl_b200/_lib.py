@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(HERE, "libfdcuda.so")
 OK, DECLINED, INVALID, DEVICE_ERROR, TIMEOUT, NO_DEVICE = range(6)
 STATUS_NAMES = {0: "OK", 1: "DECLINED", 2: "INVALID", 3: "DEVICE_ERROR", 4: "TIMEOUT", 5: "NO_DEVICE"}
 # fdc_job flags
-DERIVATIVE, BLA, SHIFT, F32, DEVICE_OUT = 1, 2, 4, 8, 16
+DERIVATIVE, BLA, SHIFT, F32, DEVICE_OUT, SERIES = 1, 2, 4, 8, 16, 32
 
 
 class Job(C.Structure):
@@ -101,7 +101,7 @@ DEFAULT_DEFER = 0  # FDC_DEFAULT_DEFER: each kernel variant's measured default
 
 # Every symbol the headers declare, for the export check.
 FDC_SYMBOLS = ["fdc_abi_version", "fdc_open", "fdc_close", "fdc_last_error", "fdc_upload_orbit", "fdc_free_orbit",
-               "fdc_upload_bla", "fdc_render", "fdc_batch_create", "fdc_batch_run", "fdc_batch_free",
+               "fdc_upload_bla", "fdc_upload_series", "fdc_render", "fdc_batch_create", "fdc_batch_run", "fdc_batch_free",
                "fdc_render_noalloc", "fdc_set_tuning", "fdc_get_tuning"]
 FDH_SYMBOLS = ["fdh_last_error", "fdh_plane_new", "fdh_orbit_fixed", "fdh_orbit_fixed_threads", "fdh_orbit_f64",
                "fdh_nucleus_period",
@@ -127,6 +127,7 @@ def lib():
     L.fdc_upload_orbit.argtypes = [P, P, P, U64, U32, C.POINTER(I32)]
     L.fdc_free_orbit.argtypes = [P, I32]
     L.fdc_upload_bla.argtypes = [P, I32, P, P, U32, D, D, I64]
+    L.fdc_upload_series.argtypes = [P, I32, U64, U64, D, P, U32]
     L.fdc_render.argtypes = [P, C.POINTER(Job), C.POINTER(Out), C.POINTER(Counters)]
     L.fdc_batch_create.argtypes = [P, P, P, U32, C.POINTER(P)]
     L.fdc_batch_run.argtypes = [P, P, C.POINTER(Counters), P]

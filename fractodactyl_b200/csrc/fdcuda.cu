@@ -45,7 +45,14 @@ struct OrbitDev {
   double z0r = 0, z0i = 0;
   bool has_bla = false;
   BlaDev bla;
+  // parameter-series start (fdc_upload_series): b_1..b_order in SERIES_SLOTS device entries
+  bool has_series = false;
+  uint32_t series_n = 0, series_order = 0;
+  double series_rho = 0.0, series_inv = 0.0;
+  double2 *series_b = nullptr;
 };
+
+constexpr uint32_t SERIES_SLOTS = 64;  // SeriesConfig::default().max_order (series.rs:45)
 
 // Device scratch of one context: work-queue head, counters, deadline flag.
 struct Scratch {
@@ -198,8 +205,11 @@ void free_orbit_buffers(fdc_ctx *ctx, OrbitDev &o) {
   pool_put(ctx, o.z, 16 * o.len);
   pool_put(ctx, o.z32, 32 * o.len);
   free_bla(ctx, o.bla);
+  pool_put(ctx, o.series_b, 16 * SERIES_SLOTS);
   o.z = nullptr;
   o.z32 = nullptr;
+  o.series_b = nullptr;
+  o.has_series = false;
 }
 
 // Orbit layouts built on the device from the caller's SoA (re[], im[]): interleaved
@@ -483,19 +493,31 @@ fdc_status prepare(fdc_ctx *ctx, const OrbitDev &o, const fdc_job &j, fdk::Param
   if (ext && o.len < 3) return fail(ctx, FDC_INVALID, "the scaled tier needs an orbit of at least 3 points");
   const bool bla = (j.flags & FDC_BLA) != 0;
   const bool deriv = (j.flags & FDC_DERIVATIVE) != 0;
+  const bool series = (j.flags & FDC_SERIES) != 0;
   double h = j.h_m * fdroute::exp2i(j.h_e);
-  if (bla) {
-    if (!o.has_bla) return fail(ctx, FDC_INVALID, "FDC_BLA without an uploaded BLA table");
-    // grid.rs:392-411
-    if (j.escape_radius < 4.0)
-      return fail(ctx, FDC_INVALID, "escape radius is below 4: BLA blocks may only skip iterates with |z| <= 2 (1 + 2 eps)");
-    // Largest unit offset: the grid's corner (grid.rs:428-444), or the supplied offsets'.
+  // Largest unit offset: the grid's corner (grid.rs:428-444), or the supplied offsets'.
+  auto largest_offset = [&]() {
     double half = std::hypot((double)j.nx / 2.0, (double)j.ny / 2.0);
     if (j.offsets) {
       half = 0.0;
       const uint64_t lo = 2ull * first * j.nx, hi = 2ull * (first + rows) * j.nx;
       for (uint64_t k = lo; k < hi; k += 2) half = std::max(half, std::hypot(j.offsets[k], j.offsets[k + 1]));
     }
+    return half;
+  };
+  if (series) {  // Series::render_masked's refusals (grid.rs:341-366)
+    if (!o.has_series) return fail(ctx, FDC_INVALID, "FDC_SERIES without an uploaded series");
+    if (ext) return fail(ctx, FDC_INVALID, "a series start needs f64 deltas: not on the scaled tier");
+    if (j.flags & FDC_F32) return fail(ctx, FDC_INVALID, "a series start runs on the plain form only");
+    const double dc = h * largest_offset();
+    if (std::isnan(dc) || dc > o.series_rho) return fail(ctx, FDC_INVALID, "view reaches |dc| beyond the series radius");
+  }
+  if (bla) {
+    if (!o.has_bla) return fail(ctx, FDC_INVALID, "FDC_BLA without an uploaded BLA table");
+    // grid.rs:392-411
+    if (j.escape_radius < 4.0)
+      return fail(ctx, FDC_INVALID, "escape radius is below 4: BLA blocks may only skip iterates with |z| <= 2 (1 + 2 eps)");
+    const double half = largest_offset();
     double dc = ext ? j.h_m * half : h * half;
     int64_t e = ext ? j.h_e : 0;
     bool over = e == o.bla.dc_exp ? dc > o.bla.dc_max
@@ -514,6 +536,12 @@ fdc_status prepare(fdc_ctx *ctx, const OrbitDev &o, const fdc_job &j, fdk::Param
     p.bla_levels = o.bla.levels;
     std::memcpy(p.bla_off, o.bla.off, sizeof p.bla_off);
     std::memcpy(p.bla_count, o.bla.count, sizeof p.bla_count);
+  }
+  if (series && o.series_n > 0) {  // n = 0: no admitted prefix, the plain kernel (grid.rs:491)
+    p.series_b = o.series_b;
+    p.series_order = o.series_order;
+    p.series_n = o.series_n;
+    p.series_inv = o.series_inv;
   }
   p.nx = j.nx;
   p.ny = j.ny;
@@ -724,6 +752,37 @@ fdc_status fdc_upload_bla(fdc_ctx *ctx, int32_t orbit, const double *blocks7, co
   return FDC_OK;
 }
 
+fdc_status fdc_upload_series(fdc_ctx *ctx, int32_t orbit, uint64_t points, uint64_t n, double rho,
+                             const double *coeffs, uint32_t order) {
+  if (!ctx) return FDC_INVALID;
+  auto it = ctx->orbits.find(orbit);
+  if (it == ctx->orbits.end()) return fail(ctx, FDC_INVALID, "unknown orbit handle");
+  OrbitDev &o = it->second;
+  if (points != o.len) return fail(ctx, FDC_INVALID, "series built over another orbit");  // grid.rs:353-355
+  if (order > SERIES_SLOTS) return fail(ctx, FDC_INVALID, "series order above 64");
+  if (n > 0) {
+    if (n + 1 >= o.len) return fail(ctx, FDC_INVALID, "series start at or past the orbit's last point");
+    if (order == 0 || !coeffs) return fail(ctx, FDC_INVALID, "series start without coefficients");
+    if (!(rho > 0.0 && std::isfinite(rho))) return fail(ctx, FDC_INVALID, "series radius must be positive and finite");
+  }
+  CK(cudaSetDevice(ctx->device));
+  if (!o.series_b) {
+    o.series_b = (double2 *)pool_get(ctx, 16 * SERIES_SLOTS);
+    if (!o.series_b) return fail(ctx, FDC_DEVICE_ERROR, "device memory for the series");
+  }
+  cudaError_t e = cudaSuccess;
+  if (n > 0) e = cudaMemcpyAsync(o.series_b, coeffs, 16ull * order, cudaMemcpyHostToDevice, ctx->stream);
+  // the caller's array may be freed once this returns
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return fail(ctx, FDC_DEVICE_ERROR, std::string("series upload: ") + cudaGetErrorString(e));
+  o.has_series = true;
+  o.series_n = (uint32_t)n;
+  o.series_order = n > 0 ? order : 0;
+  o.series_rho = rho;
+  o.series_inv = 1.0 / rho;  // series.rs:250
+  return FDC_OK;
+}
+
 fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counters *counters) {
   if (!ctx || !job || !out) return fail(ctx, FDC_INVALID, "null argument");
   auto it = ctx->orbits.find(job->orbit);
@@ -894,6 +953,7 @@ fdc_status fdc_batch_create(fdc_ctx *ctx, const fdc_job *jobs, const fdc_out *ou
     if (!(j.flags & FDC_DEVICE_OUT)) return fail(ctx, FDC_INVALID, "batch jobs write device outputs (FDC_DEVICE_OUT)");
     if (j.mask || j.offsets || j.deadline_ms > 0)
       return fail(ctx, FDC_INVALID, "batch jobs take no mask, offsets or deadline");
+    if (j.flags & FDC_SERIES) return fail(ctx, FDC_INVALID, "batch jobs start at Z_0 (no FDC_SERIES)");
     uint32_t first = 0, rows = 0;
     fdc_status st = prepare(ctx, it->second, j, params[k], first, rows);
     if (st != FDC_OK) {

@@ -113,8 +113,9 @@ extern "C" fdc_status fdc_render_noalloc(int device, const double *orbit, uint64
   if (!job || !out || !orbit) return fail(FDC_INVALID, "null argument", error, error_cap);
   if (device < 0 || device >= 64) return fail(FDC_INVALID, "device index out of range", error, error_cap);
   const fdc_job &j = *job;
-  if (j.flags & (FDC_BLA | FDC_F32 | FDC_SHIFT))
-    return fail(FDC_INVALID, "the allocation-free entry point renders the plain form without BLA only", error, error_cap);
+  if (j.flags & (FDC_BLA | FDC_F32 | FDC_SHIFT | FDC_SERIES))
+    return fail(FDC_INVALID, "the allocation-free entry point renders the plain form without BLA or series only", error,
+                error_cap);
   if (j.mask || j.offsets) return fail(FDC_INVALID, "the allocation-free entry point takes no mask or offsets", error, error_cap);
   if (len < 3 || len > (1ull << 20)) return fail(FDC_INVALID, "orbit length must be in [3, 2^20]", error, error_cap);
   if (j.nx == 0 || j.ny == 0 || j.ss == 0 || j.nx % j.ss || j.ny % j.ss)

@@ -85,6 +85,11 @@ struct Params {
   uint64_t deadline_ns;  // 0 = none
   uint32_t *timed_out;
   uint32_t defer;     // BLA lanes a warp gathers before it applies their blocks (warp_step)
+  // Parameter-series start (series.rs:57-84, ordinary tiers): every sample starts at
+  // iterate series_n from delta = sum_k b_k x^k, x = dc / rho; series_n = 0: none.
+  const double2 *__restrict__ series_b;  // b_1..b_order as (re, im)
+  uint32_t series_order, series_n;
+  double series_inv;  // 1 / rho
 };
 
 enum : uint32_t { F_DERIV = 1u, F_BLA = 2u, F_SHIFT = 4u };
@@ -596,10 +601,43 @@ __device__ __forceinline__ bool warp_step(const Params &p, State<EXT> &s, Result
   return done;
 }
 
+// Series::eval (series.rs:247-271): Horner on x = dc / rho for p = sum b_k x^(k-1) and
+// q = p'; delta = x p and, with D, dz/dc = (p + x q) / rho.
+template <bool D>
+__device__ __forceinline__ void series_start(const Params &p, double ar, double ai, double &xr, double &xi,
+                                             double &dr, double &di) {
+  const double sc = p.series_inv;
+  const double ur = ar * sc, ui = ai * sc;
+  double pr = 0.0, pi = 0.0, qr = 0.0, qi = 0.0;
+  for (int k = (int)p.series_order - 1; k >= 0; --k) {
+    const double2 c = __ldg(p.series_b + k);
+    if (D) {
+      const double nr = qr * ur - qi * ui + pr, ni = qr * ui + qi * ur + pi;
+      qr = nr;
+      qi = ni;
+    }
+    const double nr = pr * ur - pi * ui + c.x, ni = pr * ui + pi * ur + c.y;
+    pr = nr;
+    pi = ni;
+  }
+  xr = pr * ur - pi * ui;
+  xi = pr * ui + pi * ur;
+  if (D) {
+    dr = (pr + qr * ur - qi * ui) * sc;
+    di = (pi + qr * ui + qi * ur) * sc;
+  } else {
+    dr = 0.0;
+    di = 0.0;
+  }
+}
+
 // Start sample `slot` of the tile queue (one warp-sized tile per 32 slots, tiles in
 // row-major order; 8x4 samples unless tuned). Returns
 // false when the slot holds no sample to iterate (outside the grid, masked, or settled
 // by the closed-form main-component test, whose result is written here).
+template <bool EXT, bool D, bool L>
+__device__ __forceinline__ void start_sample(const Params &p, State<EXT> &s, bool use_series, bool keep_counts);
+
 template <bool EXT, bool D, bool L>
 __device__ __forceinline__ int init(const Params &p, uint64_t slot, State<EXT> &s, Result &res) {
   uint64_t tile = slot >> 5;
@@ -639,6 +677,16 @@ __device__ __forceinline__ int init(const Params &p, uint64_t slot, State<EXT> &
       return 2;
     }
   }
+  start_sample<EXT, D, L>(p, s, true, false);
+  return 1;
+}
+
+// The iteration state of a sample whose offset (ar, ai, offset_exp) and index are set:
+// the ordinary start at Z_0, or the series start when one is given and use_series.
+// keep_counts keeps the block counters (a retry from zero after a series start counts
+// both runs, grid.rs:623-648).
+template <bool EXT, bool D, bool L>
+__device__ __forceinline__ void start_sample(const Params &p, State<EXT> &s, bool use_series, bool keep_counts) {
   s.xr = 0.0;
   s.xi = 0.0;
   s.delta_exp = EXT ? s.offset_exp : 0;
@@ -672,11 +720,39 @@ __device__ __forceinline__ int init(const Params &p, uint64_t slot, State<EXT> &
   s.adc = L ? sqrt(s.ar * s.ar + s.ai * s.ai) : 0.0;
   s.nucleus = (int32_t)p.nucleus;
   s.ct.reset();
-  s.blocks = 0;
-  s.skipped = 0;
-  s.shift = 0.0;
+  if (!keep_counts) {
+    s.blocks = 0;
+    s.skipped = 0;
+    s.shift = 0.0;
+  }
+  if (!EXT && use_series && p.series_n > 0) {
+    // sample.rs:191-228 from the series' state: n = m = series_n, the state is the first
+    // Brent save (saves resume at the next power of two), no nucleus contraction
+    series_start<D>(p, s.ar, s.ai, s.xr, s.xi, s.dr, s.di);
+    const uint32_t m = p.series_n;
+    s.m = m;
+    s.n = m;
+    if (L) {
+      const double2 Z = __ldg(p.fused + 2 * m), R = __ldg(p.fused + 2 * m + 1);
+      s.Zr = Z.x;
+      s.Zi = Z.y;
+      s.r2a = R.x;
+      s.r2b = R.y;
+    } else {
+      const double2 Z = __ldg(p.orbit + m);
+      s.Zr = Z.x;
+      s.Zi = Z.y;
+    }
+    s.fr = s.Zr + s.xr;
+    s.fi = s.Zi + s.xi;
+    s.sr = s.Zr + s.xr;
+    s.si = s.Zi + s.xi;
+    s.sn = m;
+    const uint64_t np = next_pow2((uint64_t)m + 1);
+    s.chk = np > 16 ? (uint32_t)np : 16u;
+    s.nucleus = -1;
+  }
   relimit(p, s);
-  return 1;
 }
 
 // Column encoder (store.rs:66-112, Bound absent) and raw state.
@@ -723,9 +799,14 @@ __global__ void __launch_bounds__(128, Occupancy<EXT>::blocks) perturb_kernel(Pa
   uint64_t t0 = p.deadline_ns ? globaltimer() : 0;
   unsigned long long n_samples = 0, iters = 0, blocks = 0, skipped = 0, fallback = 0, closed = 0;
   double shift = 0.0;
+  // Series start (grid.rs:623-648): the iterations a sample's count leaves out. The prefix
+  // on a first run from the series (> 0); after an unresolved first run retried from zero,
+  // prefix - max_iter, so that the first run counts max_iter - prefix.
+  int64_t bias = 0;
   auto finish = [&](uint32_t idx, const Result &r, uint64_t nblocks, uint64_t nskipped, double sh) {
     put(p, idx, r);
-    uint64_t spent = r.kind == 2 ? p.max_iter : r.n;
+    uint64_t spent = (uint64_t)((int64_t)(r.kind == 2 ? p.max_iter : r.n) - bias);
+    bias = 0;
     if (L) {
       spent = spent - nskipped + nblocks;
       blocks += nblocks;
@@ -765,6 +846,7 @@ __global__ void __launch_bounds__(128, Occupancy<EXT>::blocks) perturb_kernel(Pa
           int got = init<EXT, D, L>(p, slot, s, res);
           if (got == 1) {
             active = true;
+            if (!EXT) bias = p.series_n;
           } else if (got == 2) {
             finish(s.idx, res, 0, 0, 0.0);
           }
@@ -774,8 +856,15 @@ __global__ void __launch_bounds__(128, Occupancy<EXT>::blocks) perturb_kernel(Pa
     }
     if (!__any_sync(FULL, active)) break;
     if (warp_step<EXT, D, L>(p, s, res, active, w, p.defer)) {
-      finish(s.idx, res, s.blocks, s.skipped, s.shift);
-      active = false;
+      if (!EXT && bias > 0 && res.kind == 2) {
+        // an unresolved series start retries from zero, keeping the nucleus heuristic
+        // (grid.rs:637-642); its count and blocks carry over
+        bias -= (int64_t)p.max_iter;
+        start_sample<EXT, D, L>(p, s, false, true);
+      } else {
+        finish(s.idx, res, s.blocks, s.skipped, s.shift);
+        active = false;
+      }
     }
   }
   // warp reduction of the counters, one atomic per warp

@@ -10,6 +10,7 @@ Frames the route declines raise Declined: the caller restarts them on the CPU fr
 (frame.rs:357-368), as the reference's route does.
 """
 import ctypes as C
+import math
 import dataclasses
 import os
 import sys
@@ -312,6 +313,12 @@ class Device:
                    "upload BLA")
         return h.value
 
+    def upload_series(self, orbit: int, series: "Series"):
+        """fdc_upload_series: the series start for jobs on `orbit` with the SERIES flag."""
+        b = np.ascontiguousarray(series.b, dtype=np.float64)
+        _check(lib().fdc_upload_series(self.h, orbit, series.points, series.n, series.rho,
+                                       b.ctypes.data if len(b) else None, len(b)), self, "upload series")
+
     def free(self, orbit: int):
         lib().fdc_free_orbit(self.h, orbit)
 
@@ -491,11 +498,13 @@ def encode_host(plane: Plane, ss: int, s: "Samples", columns=("nu", "de", "norma
 
 
 def render_with(view: View, p: Params, orbit=None, bla: Optional[Bla] = None, dev: Optional[Device] = None,
-                raw=False, shift=True, report: Optional[RouteReport] = None, quiet=True, host_encode=False):
-    """fd_kernel::render_with / render_bla (grid.rs:106-208) on the CUDA route.
+                raw=False, shift=True, report: Optional[RouteReport] = None, quiet=True, host_encode=False,
+                series: Optional["Series"] = None):
+    """fd_kernel::render_with / render_bla (grid.rs:106-208) on the CUDA route; with
+    `series`, every sample starts from it (Series::render_masked, grid.rs:341-373).
 
     Returns (Header, Samples, Stats, BlaStats or None). Refusals are the reference's
-    (grid.rs:378-413, :461-475); Bound/Stripe columns are declined (frame.rs:129-144).
+    (grid.rs:350-366, :378-413, :461-475); Bound/Stripe columns are declined (frame.rs:129-144).
     """
     started = time.perf_counter()
     if "bound" in p.columns or "stripe" in p.columns:
@@ -517,10 +526,21 @@ def render_with(view: View, p: Params, orbit=None, bla: Optional[Bla] = None, de
     reference_seconds = time.perf_counter() - t
     if bla is not None and bla.points != len(r):
         raise ValueError(f"BLA table covers a {bla.points}-point orbit, not this {len(r)}-point one")
+    if series is not None:
+        if tier == 2:
+            raise ValueError("a series start needs f64 deltas and no Bound column")
+        if series.points != len(r):
+            raise ValueError("series built over another orbit")
+        dc = plane.h() * math.hypot(p.nx / 2.0, p.ny / 2.0)
+        if math.isnan(dc) or dc > series.rho:
+            raise ValueError(f"view reaches |dc| = {dc:e}, beyond the series radius {series.rho:e}")
     dev = dev or device(0)
     h = dev.upload(r, bla)
     try:
         flags = (_lib.DERIVATIVE if p.needs_derivative() else 0) | (_lib.BLA if bla is not None else 0)
+        if series is not None:
+            dev.upload_series(h, series)
+            flags |= _lib.SERIES
         if bla is not None and shift and p.needs_derivative():
             flags |= _lib.SHIFT
         job = make_job(plane, tier, p, h, r.nucleus_period(), flags)
@@ -530,7 +550,8 @@ def render_with(view: View, p: Params, orbit=None, bla: Optional[Bla] = None, de
         gpu_seconds = time.perf_counter() - g
     finally:
         dev.free(h)
-    kernel = plane.kernel(tier) + (" bla/1" if bla is not None else "") + " gpu-perturb-cuda/1"
+    kernel = plane.kernel(tier) + (" bla/1" if bla is not None else "") + (" series/0" if series is not None else "") \
+        + " gpu-perturb-cuda/1"
     cols = ("class",) + tuple(c for c in ("nu", "de", "normal") if c in p.columns)
     header = Header(cols, p.nx, p.ny, p.ss, p.max_iter, p.escape_radius, view, kernel)
     s = Samples(cls=arrays["cls"], nu=arrays.get("nu"), de=arrays.get("de"), normal=arrays.get("normal"),
@@ -564,6 +585,13 @@ def render(view: View, p: Params, orbit=None, **kw):
     """perturb_gpu::render (frame.rs:70-76) on the CUDA route: plain perturbation."""
     h, s, st, _ = render_with(view, p, orbit, None, **kw)
     return h, s, st
+
+
+def render_series(view: View, p: Params, orbit, series: "Series", bla: Optional[Bla] = None, **kw):
+    """fd_kernel::render_series (grid.rs:213-226) on the CUDA route: every sample starts at
+    the series' admitted iterate, and a sample that ends unresolved from there retries from
+    zero. Returns (Header, Samples, Stats, BlaStats or None)."""
+    return render_with(view, p, orbit, bla, series=series, **kw)
 
 
 def render_bla(view: View, p: Params, orbit=None, eps: float = EPS, **kw):

@@ -44,7 +44,8 @@ enum {
   FDC_BLA = 1u << 1,        /* apply the uploaded BLA table (sample.rs "L") */
   FDC_SHIFT = 1u << 2,      /* accumulate the BLA first-order shift estimate (BlaStats.shift_px) */
   FDC_F32 = 1u << 3,        /* precision form: FP32-mantissa floatexp deltas (not bit-exact) */
-  FDC_DEVICE_OUT = 1u << 4  /* fdc_out pointers are device pointers (no host copies) */
+  FDC_DEVICE_OUT = 1u << 4, /* fdc_out pointers are device pointers (no host copies) */
+  FDC_SERIES = 1u << 5      /* start every sample from the orbit's uploaded series */
 };
 
 typedef struct fdc_ctx fdc_ctx;
@@ -117,6 +118,16 @@ fdc_status fdc_free_orbit(fdc_ctx *ctx, int32_t orbit);
 fdc_status fdc_upload_bla(fdc_ctx *ctx, int32_t orbit, const double *blocks7, const uint64_t *level_offsets,
                           uint32_t levels, double eps, double dc_max, int64_t dc_exp);
 
+/* Upload a parameter-series start built over that orbit (Series, series.rs:57-84, e.g. by
+ * fdh_series_build): jobs with FDC_SERIES start every sample at iterate n from delta =
+ * sum_k b_k (dc / rho)^k, coeffs = b_1..b_order as (re, im) pairs (order <= 64), on the
+ * F64 / Fixed tiers of the plain form, for views with |dc| <= rho; a sample whose series
+ * start ends unresolved retries from zero (grid.rs:623-648). n = 0: no admitted prefix,
+ * the plain kernel. Refused: points other than the orbit's length, n + 1 >= points.
+ * Replaces the series arm of grid::run (render_series, grid.rs:213-226). */
+fdc_status fdc_upload_series(fdc_ctx *ctx, int32_t orbit, uint64_t points, uint64_t n, double rho,
+                             const double *coeffs, uint32_t order);
+
 /* Render a job (replaces dispatch_batched, frame.rs:242-260, and the readback checks,
  * :271-286). Results are those of the CPU kernel (sample.rs:170-581) for the plain form:
  * class and n bit-exact, z and dz bit-exact, nu/de/normal within CUDA libm's ulps. */
@@ -151,7 +162,7 @@ fdc_status fdc_get_tuning(const fdc_ctx *ctx, fdc_tuning *tuning);
  * its own orbit handle, tier and device outputs) rendered by ONE persistent launch per
  * kernel variant from a single work queue over all jobs' tiles, deepest jobs first, the
  * whole run captured once in a CUDA graph and replayed by fdc_batch_run. Results equal
- * fdc_render's per job. Jobs need FDC_DEVICE_OUT, no mask/offsets/deadline; orbits and
+ * fdc_render's per job. Jobs need FDC_DEVICE_OUT, no mask/offsets/deadline/FDC_SERIES; orbits and
  * tables must stay uploaded while the batch exists. per_job (optional) has njobs
  * entries; counters->kernel_ms is the device time of the whole replay. */
 typedef struct fdc_batch fdc_batch;
@@ -164,7 +175,7 @@ void fdc_batch_free(fdc_ctx *ctx, fdc_batch *batch);
  * allocate device memory: a render service that owns all device memory through its own
  * pool or arena (other allocations would fragment it or break its memory budget) and
  * hands the library buffers carved from it. It renders the plain form (FP64,
- * no BLA, no mask or offsets) with no context, no cudaMalloc, no cudaFree and no
+ * no BLA, series, mask or offsets) with no context, no cudaMalloc, no cudaFree and no
  * allocating library call: the caller passes the orbit (2*len doubles, interleaved
  * re/im, Z_0 = 0) and every output column of `out` as DEVICE pointers, and the kernel's
  * scratch (work-queue head, counters, per-row iteration sums) lives in one fixed device
