@@ -82,7 +82,7 @@ struct fdc_ctx {
   // staging for host outputs / inputs, grown on demand
   void *stage = nullptr;
   size_t stage_bytes = 0;
-  int blocks_per_sm[8] = {};
+  int blocks_per_sm[12] = {};
   int blocks_per_sm_f32[4] = {};
   int blocks_per_sm_batch[8] = {};
   int blocks_per_sm_batch_f32[4] = {};
@@ -277,13 +277,23 @@ __global__ void fuse_bla(const double2 *__restrict__ z, uint64_t len, const doub
 
 unsigned grid_for(uint64_t n) { return (unsigned)std::min<uint64_t>((n + 255) / 256, 148 * 16); }
 
-template <bool EXT, bool D, bool L>
+template <bool EXT, bool D, bool L, bool S = false>
 void *kernel_ptr() {
-  return (void *)fdk::perturb_kernel<EXT, D, L>;
+  return (void *)fdk::perturb_kernel<EXT, D, L, S>;
 }
 
-void *pick_kernel(bool ext, bool d, bool l, int &variant) {
+// series: a job starting from an admitted series (ordinary tiers only): variants 8-11
+void *pick_kernel(bool ext, bool d, bool l, bool series, int &variant) {
   variant = (ext ? 4 : 0) | (d ? 2 : 0) | (l ? 1 : 0);
+  if (series && !ext) {
+    variant += 8;
+    switch (variant) {
+      case 8: return kernel_ptr<false, false, false, true>();
+      case 9: return kernel_ptr<false, false, true, true>();
+      case 10: return kernel_ptr<false, true, false, true>();
+      default: return kernel_ptr<false, true, true, true>();
+    }
+  }
   switch (variant) {
     case 0: return kernel_ptr<false, false, false>();
     case 1: return kernel_ptr<false, false, true>();
@@ -880,7 +890,7 @@ fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counte
                        ctx->blocks_per_sm_f32));
   } else {
     int variant = 0;
-    void *fn = pick_kernel(ext, deriv, bla, variant);
+    void *fn = pick_kernel(ext, deriv, bla, p.series_n > 0, variant);
     if (!ctx->blocks_per_sm[variant]) {
       int b = 0;
       CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, 128, 0));

@@ -638,7 +638,7 @@ __device__ __forceinline__ void series_start(const Params &p, double ar, double 
 template <bool EXT, bool D, bool L>
 __device__ __forceinline__ void start_sample(const Params &p, State<EXT> &s, bool use_series, bool keep_counts);
 
-template <bool EXT, bool D, bool L>
+template <bool EXT, bool D, bool L, bool S = false>
 __device__ __forceinline__ int init(const Params &p, uint64_t slot, State<EXT> &s, Result &res) {
   uint64_t tile = slot >> 5;
   if (p.tile_order) tile = __ldg(p.tile_order + tile);  // queue position -> row-major tile
@@ -677,7 +677,7 @@ __device__ __forceinline__ int init(const Params &p, uint64_t slot, State<EXT> &
       return 2;
     }
   }
-  start_sample<EXT, D, L>(p, s, true, false);
+  start_sample<EXT, D, L>(p, s, S, false);
   return 1;
 }
 
@@ -787,7 +787,9 @@ __device__ __forceinline__ void put(const Params &p, uint32_t sample, const Resu
   }
 }
 
-template <bool EXT, bool D, bool L>
+// S: the series-start variant (ordinary tiers, jobs with an admitted series); the others
+// compile without the series start and its retry.
+template <bool EXT, bool D, bool L, bool S = false>
 __global__ void __launch_bounds__(128, Occupancy<EXT>::blocks) perturb_kernel(Params p) {
   const unsigned FULL = 0xffffffffu;
   const unsigned lane = threadIdx.x & 31u;
@@ -843,10 +845,10 @@ __global__ void __launch_bounds__(128, Occupancy<EXT>::blocks) perturb_kernel(Pa
       if (!active) {
         uint64_t slot = base + __popc(need & lt);
         if (slot < p.total) {
-          int got = init<EXT, D, L>(p, slot, s, res);
+          int got = init<EXT, D, L, S>(p, slot, s, res);
           if (got == 1) {
             active = true;
-            if (!EXT) bias = p.series_n;
+            if (S) bias = p.series_n;
           } else if (got == 2) {
             finish(s.idx, res, 0, 0, 0.0);
           }
@@ -856,7 +858,7 @@ __global__ void __launch_bounds__(128, Occupancy<EXT>::blocks) perturb_kernel(Pa
     }
     if (!__any_sync(FULL, active)) break;
     if (warp_step<EXT, D, L>(p, s, res, active, w, p.defer)) {
-      if (!EXT && bias > 0 && res.kind == 2) {
+      if (S && bias > 0 && res.kind == 2) {
         // an unresolved series start retries from zero, keeping the nucleus heuristic
         // (grid.rs:637-642); its count and blocks carry over
         bias -= (int64_t)p.max_iter;
