@@ -686,7 +686,7 @@ int fdh_bla_build_into(const double *re, const double *im, uint64_t len, double 
                        uint32_t *levels, uint64_t *blocks) {
   const uint64_t steps = len >= 2 ? len - 2 : 0;
   if (!level_offsets || (steps >= 2 && !blocks7)) {
-    g_err = "BLA table larger than the buffers given";
+    g_err = "null BLA buffers";
     return -1;
   }
   uint32_t lv = 0;
@@ -828,7 +828,7 @@ int fdh_series_build(const double *re, const double *im, uint64_t len, double rh
         tf += (double)order * a;
         order -= 1;
       }
-      if (order > cap_order) throw std::runtime_error("series coefficients larger than the buffer given");
+      if (order > cap_order || !coeffs) throw std::runtime_error("series coefficients larger than the buffer given");
       out->n = best_n;
       out->order = (uint32_t)order;
       out->state_bound = best_e + te;
