@@ -26,7 +26,7 @@ extern "C" {
 #endif
 
 /* Column bits, as fd-samples Column (crates/fd-samples/src/column.rs:7-24). */
-enum { FDREF_COL_CLASS = 1, FDREF_COL_NU = 2, FDREF_COL_DE = 4, FDREF_COL_NORMAL = 8 };
+enum { FDREF_COL_CLASS = 1, FDREF_COL_NU = 2, FDREF_COL_DE = 4, FDREF_COL_NORMAL = 8, FDREF_COL_BOUND = 16 };
 
 /* Tier (crates/fd-kernel/src/view.rs:7-14); -1 = cheapest valid. */
 enum { FDREF_TIER_AUTO = -1, FDREF_TIER_F64 = 0, FDREF_TIER_FIXED = 1, FDREF_TIER_SCALED = 2 };
@@ -57,6 +57,7 @@ typedef struct {
   int64_t dexp;
   uint64_t blocks, skipped;
   double shift;
+  double ez, ed; /* error radii of an escaped bounded sample (infinite otherwise) */
 } fdref_outcome;
 
 /* Work counters: Stats (grid.rs:41-49) + BlaStats (grid.rs:53-70). */
@@ -143,6 +144,33 @@ int fdref_render_series(const fdref_job *job, const fdref_ref *ref, const fdref_
                         const fdref_series *series, const uint8_t *mask, uint8_t *cls, double *nu,
                         float *de, uint16_t *normal, uint64_t *n_out, double *z_out, double *dz_out,
                         int64_t *dexp_out, fdref_stats *stats, char *kernel, size_t kernel_cap);
+/* Reference::error_radius (reference.rs:122-148) into q (len entries): bits >= 0 for a
+ * fixed-point orbit of that many fraction bits, -1 for an f64 orbit from (c_re, c_im). */
+int fdref_error_radius(const fdref_ref *r, int64_t bits, double c_re, double c_im, double *q);
+/* sample::iterate's bounded variant (B, sample.rs:221-229, 338-350, 373-377, 419-421) on
+ * an ordinary tier: the orbit's error radii from (bits, c_re, c_im) as above; out->ez,
+ * out->ed receive the escaped sample's radii. */
+int fdref_iterate_bounded(const fdref_ref *r, int derivative, int has_c, double cr, double ci, double ar,
+                          double ai, uint64_t max_iter, double r2, int64_t bits, double c_re, double c_im,
+                          fdref_outcome *out);
+/* All outputs of a render, any NULL: the fdref_render columns plus the Bound column
+ * (FDREF_COL_BOUND: f32 nu error bound, store.rs:104-106) and the raw error radii of
+ * escaped samples. */
+typedef struct {
+  uint8_t *cls;
+  double *nu;
+  float *de;
+  uint16_t *normal;
+  float *bound;
+  uint64_t *n;
+  double *z, *dz;
+  int64_t *dexp;
+  double *ez, *ed;
+} fdref_columns;
+/* fdref_render / fdref_render_series with every output: series and mask may be NULL. */
+int fdref_render_columns(const fdref_job *job, const fdref_ref *ref, const fdref_bla *bla,
+                         const fdref_series *series, const uint8_t *mask, const fdref_columns *out,
+                         fdref_stats *stats, char *kernel, size_t kernel_cap);
 /* Encode one escaped state's columns exactly as Store::put (store.rs:66-112). */
 void fdref_store_escaped(double h_m, int64_t h_e, uint32_t ss, double rotation, uint64_t n,
                          double zr, double zi, double dr, double di, int64_t dexp,

@@ -12,7 +12,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 
-COL_CLASS, COL_NU, COL_DE, COL_NORMAL = 1, 2, 4, 8
+COL_CLASS, COL_NU, COL_DE, COL_NORMAL, COL_BOUND = 1, 2, 4, 8, 16
 TIER = {None: -1, "auto": -1, "f64": 0, "fx": 1, "fixed": 1, "scaled": 2}
 
 
@@ -47,6 +47,8 @@ class Outcome(C.Structure):
         ("blocks", C.c_uint64),
         ("skipped", C.c_uint64),
         ("shift", C.c_double),
+        ("ez", C.c_double),
+        ("ed", C.c_double),
     ]
 
 
@@ -60,6 +62,10 @@ class Stats(C.Structure):
         ("closed_form_samples", C.c_uint64),
         ("shift_px", C.c_double),
     ]
+
+
+class Columns(C.Structure):  # fdref_columns
+    _fields_ = [(k, C.c_void_p) for k in ("cls", "nu", "de", "normal", "bound", "n", "z", "dz", "dexp", "ez", "ed")]
 
 
 class SeriesInfo(C.Structure):
@@ -135,6 +141,10 @@ def lib():
         L.fdref_series_free.argtypes = [P]
         L.fdref_render_series.argtypes = [C.POINTER(Job), P, P, P, P, P, P, P, P, P, P, P, P, C.POINTER(Stats),
                                           C.c_char_p, C.c_size_t]
+        L.fdref_error_radius.argtypes = [P, I64, D, D, P]
+        L.fdref_iterate_bounded.argtypes = [P, C.c_int, C.c_int, D, D, D, D, U64, D, I64, D, D, C.POINTER(Outcome)]
+        L.fdref_render_columns.argtypes = [C.POINTER(Job), P, P, P, P, C.POINTER(Columns), C.POINTER(Stats),
+                                           C.c_char_p, C.c_size_t]
         _lib = L
     return _lib
 
@@ -306,6 +316,49 @@ def render_series(job, ref, series, bla=None, mask=None, raw=False):
                           closed_form_samples=st.closed_form_samples, shift_px=st.shift_px))
     if raw:
         out.update(z=z.reshape(n, 2), dz=dz.reshape(n, 2), dexp=dexp)
+    return out
+
+
+def error_radius(ref, bits, c_re, c_im):
+    """Reference::error_radius (reference.rs:122-148); bits None for an f64 orbit."""
+    q = np.zeros(len(ref))
+    if lib().fdref_error_radius(ref.h, -1 if bits is None else bits, c_re, c_im, q.ctypes.data) != 0:
+        raise ValueError(_err())
+    return q
+
+
+def iterate_bounded(ref, bits, c_re, c_im, c=None, ar=0.0, ai=0.0, max_iter=1000, r2=1e20, derivative=True):
+    """The bounded variant of sample.rs:170-581 (B) with the orbit's error radii from
+    (bits, c_re, c_im); the result carries the escaped sample's radii ez, ed."""
+    o = Outcome()
+    rc = lib().fdref_iterate_bounded(ref.h, int(derivative), c is not None, c[0] if c else 0.0, c[1] if c else 0.0,
+                                     ar, ai, max_iter, r2, -1 if bits is None else bits, c_re, c_im, C.byref(o))
+    if rc != 0:
+        raise ValueError(_err())
+    kind = {0: "escaped", 1: "interior", 2: "unresolved"}[o.kind]
+    return dict(kind=kind, n=o.n, zr=o.zr, zi=o.zi, dr=o.dr, di=o.di, dexp=o.dexp, ez=o.ez, ed=o.ed)
+
+
+def render_columns(job, ref=None, bla=None, series=None, mask=None):
+    """Every output of a render (fdref_render_columns): the columns, the Bound column
+    (with COL_BOUND) and the raw state with the error radii of escaped samples."""
+    n = job.nx * job.ny
+    out = dict(cls=np.zeros(n, np.uint8), nu=np.zeros(n), de=np.zeros(n, np.float32), normal=np.zeros(n, np.uint16),
+               bound=np.zeros(n, np.float32), n=np.zeros(n, np.uint64), z=np.zeros((n, 2)), dz=np.zeros((n, 2)),
+               dexp=np.zeros(n, np.int64), ez=np.zeros(n), ed=np.zeros(n))
+    cols = Columns(**{k: v.ctypes.data for k, v in out.items()})
+    m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
+    st = Stats()
+    kernel = C.create_string_buffer(256)
+    rc = lib().fdref_render_columns(C.byref(job), ref.h if ref else None, bla.h if bla else None,
+                                    series.h if series else None, m.ctypes.data if m is not None else None,
+                                    C.byref(cols), C.byref(st), kernel, 256)
+    if rc != 0:
+        raise ValueError(_err())
+    out["kernel"] = kernel.value.decode()
+    out["stats"] = dict(reference_len=st.reference_len, iterations=st.iterations, blocks=st.blocks,
+                        skipped=st.skipped, fallback_samples=st.fallback_samples,
+                        closed_form_samples=st.closed_form_samples, shift_px=st.shift_px)
     return out
 
 

@@ -15,6 +15,7 @@
 namespace fdref {
 
 static const double LN_2 = 0.693147180559945309417232121458176568;
+static const double U = 1.1102230246251565e-16;  // sample.rs:54 (EPSILON / 2)
 static const double TAU = 6.28318530717958647692528676655900577;
 
 // store.rs:145-150
@@ -37,12 +38,34 @@ struct Columns {
   double *nu = nullptr;
   float *de = nullptr;
   uint16_t *normal = nullptr;
+  float *bound = nullptr;
   uint64_t *n = nullptr;
   double *z = nullptr, *dz = nullptr;
   int64_t *dexp = nullptr;
+  double *ez = nullptr, *ed = nullptr;  // raw error radii of escaped samples (bounded renders)
 };
 
-// store.rs:66-112 with the Bound column absent (class evidence Heuristic).
+// store.rs:115-151: Bounded evidence for an escaped sample with |z| = az, |dz/dc| = ad
+// and error radii ez, ed: (de_lo, bound), or false unless the radii prove escape
+// (|z| - ez > 2) and ed < ad / 2.
+static bool bounds(uint64_t n, double az, double ez, double ad, double ed, double &de_lo_out, double &bound_out) {
+  const double lo = az - ez;
+  if (!(lo > 2.0 && ed < 0.5 * ad)) return false;
+  const double lnz = std::log(az), llo = std::log(lo), lhi = std::log(az + ez);
+  // nu = n + 1 - log2(ln|z| / ln 2): |z| within ez moves it by at most
+  // log2(ln|z| / ln(|z| - ez)); plus the rounding of nu itself
+  const double nu = std::log1p(-std::log1p(-ez / az) / llo) / LN_2 + 8.0 * U * ((double)n + 8.0);
+  // Koebe: distance >= e^-G de / 4 with G <= ln|z| 2^-n
+  const double g = lhi * std::exp2(-(double)n);
+  const double de_lo = (lo * llo) / (az * lnz) * ad / (ad + ed) * std::exp(-g) * (1.0 - 4.0 / (lo * lo)) * (1.0 - 1e-6);
+  const double de_hi = ((az + ez) * lhi) / (az * lnz) * ad / (ad - ed) * (1.0 + 1e-6);
+  de_lo_out = de_lo;
+  bound_out = nu * de_hi / de_lo * (1.0 + 1e-6);
+  return true;
+}
+
+// store.rs:66-112 (the class byte is kind | evidence << 2: Bounded when the error radii
+// prove it, sample.rs:22-26).
 static void put(const Plane &pl, uint32_t ss, uint32_t cols, const Outcome &o, size_t idx, Columns &c,
                 uint64_t max_iter = 0) {
   if (c.n) c.n[idx] = o.iterations(max_iter);  // Outcome::iterations (sample.rs:45-50)
@@ -61,10 +84,17 @@ static void put(const Plane &pl, uint32_t ss, uint32_t cols, const Outcome &o, s
   }
   double z2 = o.zr * o.zr + o.zi * o.zi;
   double log2z = 0.5 * std::log2(z2);
-  if (c.cls) c.cls[idx] = 0;
+  double de_lo = 0.0, bnd = 0.0;
+  const bool bounded = bounds(o.n, std::sqrt(z2), o.ez, std::hypot(o.dr, o.di), o.ed, de_lo, bnd);
+  if (c.cls) c.cls[idx] = bounded ? 4 : 0;
+  if (c.ez) c.ez[idx] = o.ez;
+  if (c.ed) c.ed[idx] = o.ed;
   if ((cols & FDREF_COL_NU) && c.nu) c.nu[idx] = (double)o.n + 1.0 - std::log2(log2z);
-  if ((cols & FDREF_COL_DE) && c.de)
-    c.de[idx] = de_px(std::sqrt(z2), log2z, o.dr, o.di, o.dexp, pl.h_m * (double)ss, pl.h_e);
+  if ((cols & FDREF_COL_DE) && c.de) {
+    const float d = de_px(std::sqrt(z2), log2z, o.dr, o.di, o.dexp, pl.h_m * (double)ss, pl.h_e);
+    c.de[idx] = bounded ? (float)((double)d * de_lo) : d;
+  }
+  if ((cols & FDREF_COL_BOUND) && c.bound) c.bound[idx] = bounded ? (float)bnd : 0.0f;
   if ((cols & FDREF_COL_NORMAL) && c.normal) {
     double x, y;
     pl.to_screen(o.zr * o.dr + o.zi * o.di, o.zi * o.dr - o.zr * o.di, x, y);
@@ -142,14 +172,23 @@ static std::string run(const View &v, const Params &p, const Reference *supplied
   }
   const bool series_given = series != nullptr;
   if (series) {  // grid.rs:350-366
-    if (tier == Tier::Scaled) throw std::runtime_error("a series start needs f64 deltas and no Bound column");
+    if (tier == Tier::Scaled || (p.columns & FDREF_COL_BOUND))
+      throw std::runtime_error("a series start needs f64 deltas and no Bound column");
     if (series->points != ref->len()) throw std::runtime_error("series built over another orbit");
     const double dc = dc_bound(plane, tier, p).first;
     if (std::isnan(dc) || dc > series->rho) throw std::runtime_error("view reaches |dc| beyond the series radius");
   }
+  if (bla && (p.columns & FDREF_COL_BOUND))  // grid.rs:379-384
+    throw std::runtime_error("--columns bound certifies every step; BLA remainders are not certified (ACC-02)");
   if (bla) bla_checks(plane, tier, p, *ref, *bla);
   if (series && series->n == 0) series = nullptr;  // grid.rs:491: no admitted prefix, the plain kernel
-  const bool D = (p.columns & (FDREF_COL_DE | FDREF_COL_NORMAL)) != 0;
+  // grid.rs:588-593: error radii for the Bound column on the ordinary tiers
+  std::vector<double> q;
+  if ((p.columns & FDREF_COL_BOUND) && tier != Tier::Scaled)
+    q = ref->error_radius(tier == Tier::F64 ? std::nullopt : std::optional<uint64_t>(plane.bits), plane.c_re,
+                          plane.c_im);
+  const double *qp = q.empty() ? nullptr : q.data();
+  const bool D = (p.columns & (FDREF_COL_DE | FDREF_COL_NORMAL)) != 0 || qp;
   const bool L = bla != nullptr;
   const double h = plane.h();
   const double r2 = p.escape_radius * p.escape_radius;
@@ -174,11 +213,11 @@ static std::string run(const View &v, const Params &p, const Reference *supplied
             case Tier::F64: {
               double ar = ux * h, ai = uy * h;
               return iterate(false, D, L, *ref, bla, skip, std::make_pair(plane.c_re + ar, plane.c_im + ai), ar, ai,
-                             0, p.max_iter, r2, nucleus, start(ar, ai));
+                             0, p.max_iter, r2, nucleus, start(ar, ai), qp);
             }
             case Tier::Fixed:
               return iterate(false, D, L, *ref, bla, skip, std::nullopt, ux * h, uy * h, 0, p.max_iter, r2, nucleus,
-                             start(ux * h, uy * h));
+                             start(ux * h, uy * h), qp);
             case Tier::Scaled:
             default:
               return iterate(true, D, L, *ref, bla, skip, std::nullopt, ux * plane.h_m, uy * plane.h_m, plane.h_e,
@@ -478,6 +517,81 @@ int fdref_iterate_from(const fdref_ref *r, const fdref_bla *bla, int extended, i
     out->blocks = skip.blocks;
     out->skipped = skip.skipped;
     out->shift = skip.shift;
+    out->ez = o.ez;
+    out->ed = o.ed;
+    return 0;
+  })
+  return -1;
+}
+
+int fdref_error_radius(const fdref_ref *r, int64_t bits, double c_re, double c_im, double *q) {
+  FDREF_TRY({
+    auto v = r->r.error_radius(bits >= 0 ? std::optional<uint64_t>((uint64_t)bits) : std::nullopt, c_re, c_im);
+    std::copy(v.begin(), v.end(), q);
+    return 0;
+  })
+  return -1;
+}
+
+int fdref_iterate_bounded(const fdref_ref *r, int derivative, int has_c, double cr, double ci, double ar,
+                          double ai, uint64_t max_iter, double r2, int64_t bits, double c_re, double c_im,
+                          fdref_outcome *out) {
+  FDREF_TRY({
+    auto q = r->r.error_radius(bits >= 0 ? std::optional<uint64_t>((uint64_t)bits) : std::nullopt, c_re, c_im);
+    std::optional<std::pair<double, double>> c;
+    if (has_c) c = std::make_pair(cr, ci);
+    Skip skip;
+    Outcome o = iterate(false, derivative != 0, false, r->r, nullptr, skip, c, ar, ai, 0, max_iter, r2, std::nullopt,
+                        Start{}, q.data());
+    out->kind = (int32_t)o.kind;
+    out->n = o.n;
+    out->zr = o.zr;
+    out->zi = o.zi;
+    out->dr = o.dr;
+    out->di = o.di;
+    out->dexp = o.dexp;
+    out->blocks = skip.blocks;
+    out->skipped = skip.skipped;
+    out->shift = skip.shift;
+    out->ez = o.ez;
+    out->ed = o.ed;
+    return 0;
+  })
+  return -1;
+}
+
+int fdref_render_columns(const fdref_job *job, const fdref_ref *ref, const fdref_bla *bla,
+                         const fdref_series *series, const uint8_t *mask, const fdref_columns *out,
+                         fdref_stats *stats, char *kernel, size_t kernel_cap) {
+  FDREF_TRY({
+    Columns c;
+    c.cls = out->cls;
+    c.nu = out->nu;
+    c.de = out->de;
+    c.normal = out->normal;
+    c.bound = out->bound;
+    c.n = out->n;
+    c.z = out->z;
+    c.dz = out->dz;
+    c.dexp = out->dexp;
+    c.ez = out->ez;
+    c.ed = out->ed;
+    Stats st;
+    std::string k = run(to_view(job), to_params(job), ref ? &ref->r : nullptr, bla ? &bla->t : nullptr, c, st,
+                        nullptr, series ? &series->s : nullptr, mask);
+    if (stats) {
+      stats->reference_len = st.reference_len;
+      stats->iterations = st.iterations;
+      stats->blocks = st.blocks;
+      stats->skipped = st.skipped;
+      stats->fallback_samples = st.fallback;
+      stats->closed_form_samples = st.closed;
+      stats->shift_px = st.shift;
+    }
+    if (kernel && kernel_cap) {
+      std::strncpy(kernel, k.c_str(), kernel_cap - 1);
+      kernel[kernel_cap - 1] = 0;
+    }
     return 0;
   })
   return -1;

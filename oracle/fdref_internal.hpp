@@ -72,6 +72,10 @@ struct Reference {
   static Reference make_f64(double c_re, double c_im, uint64_t max_iter, double escape_radius);
   static Reference from_fixed(const Fixed &cr, const Fixed &ci, uint64_t max_iter);
   std::optional<size_t> nucleus_period() const;
+  // reference.rs:122-148: bounds q[m] >= |A_m - Z_m| on each point's distance from the
+  // exact orbit of the exact centre; bits: the fixed-point orbit's fraction bits, or none
+  // for an f64 orbit from the correctly rounded centre (c_re, c_im)
+  std::vector<double> error_radius(std::optional<uint64_t> bits, double c_re, double c_im) const;
   size_t len() const { return re.size(); }
 };
 
@@ -98,6 +102,9 @@ struct Outcome {
   uint64_t n = 0;
   double zr = 0, zi = 0, dr = 0, di = 0;
   int64_t dexp = 0;
+  // error radii of an escaped sample on z and dz/dc (sample.rs:22-26; infinite unless
+  // tracked, B)
+  double ez = __builtin_inf(), ed = __builtin_inf();
   uint64_t iterations(uint64_t max_iter) const { return kind == Kind::Unresolved ? max_iter : n; }
 };
 
@@ -113,9 +120,12 @@ struct Start {
   double xr = 0.0, xi = 0.0, dr = 0.0, di = 0.0;
 };
 
+// q: the orbit's error radii (Reference::error_radius) to track the bounded variant
+// (B, ordinary tiers: no BLA, no nucleus gate, no series start); null otherwise.
 Outcome iterate(bool extended, bool D, bool L, const Reference &r, const Bla *bla, Skip &skip,
                 std::optional<std::pair<double, double>> c, double ar, double ai, int64_t offset_exp,
-                uint64_t max_iter, double r2, std::optional<size_t> nucleus, const Start &start = Start{});
+                uint64_t max_iter, double r2, std::optional<size_t> nucleus, const Start &start = Start{},
+                const double *q = nullptr);
 
 // series.rs:26-55
 struct SeriesConfig {

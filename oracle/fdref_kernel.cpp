@@ -19,6 +19,7 @@ static const double LO = 1.0 / HI;      // sample.rs:15
 static const double SQUARE_OK = 1e-290; // sample.rs:16
 static const double TINY = 1.0 / 1e270; // sample.rs:17
 static const double U = 1.1102230246251565e-16;  // sample.rs:54 (EPSILON / 2)
+static const double SAFE = 1.0 + 8.0 * U;         // sample.rs:56
 static const double RESOLVABLE = 1e-12;          // sample.rs:702
 static const double LN_2 = 0.693147180559945309417232121458176568;
 static const double TAU = 6.28318530717958647692528676655900577;
@@ -148,6 +149,33 @@ std::optional<size_t> Reference::nucleus_period() const {
     record = rmin(record, radius);
   }
   return std::nullopt;
+}
+
+// reference.rs:122-148
+std::vector<double> Reference::error_radius(std::optional<uint64_t> bits, double c_re, double c_im) const {
+  const double MIN_POSITIVE = 2.2250738585072014e-308;
+  const double c1 = std::fabs(c_re) + std::fabs(c_im);
+  // fixed point: three truncated squares per component plus the centre's own truncation,
+  // each under one unit of 2^-bits
+  const bool fixed = bits.has_value();
+  const double d = fixed ? rmax(exp2i(4 - (int64_t)*bits), MIN_POSITIVE) : 0.0;
+  std::vector<double> q;
+  q.reserve(len());
+  double a = 0.0;  // |A_m - F_m|, F the orbit as computed before rounding to f64
+  for (size_t m = 0; m < len(); ++m) {
+    const double s = std::sqrt(re[m] * re[m] + im[m] * im[m]) * (1.0 + 4.0 * U);
+    double round, defect;
+    if (fixed) {
+      round = 2.0 * U * s + MIN_POSITIVE;
+      defect = d;
+    } else {  // f64: rounding of x^2 - y^2 + c and 2xy + c, plus the centre's rounding
+      round = 0.0;
+      defect = 8.0 * U * (s * s + c1) + 2.0 * U * c1 + MIN_POSITIVE;
+    }
+    q.push_back(a + round);
+    a = (a * (2.0 * (s + round) + a) + defect) * (1.0 + 8.0 * U);
+  }
+  return q;
 }
 
 // ---------------------------------------------------------------- bla.rs
@@ -438,11 +466,11 @@ static inline uint64_t next_pow2(uint64_t x) {
 // ---------------------------------------------------------------- sample.rs:170-581
 // The B (bounded) and trace/stripe features are outside the hot path (the GPU route
 // declines Bound/Stripe frames). A series start (Start, sample.rs:69-80) is supported.
-template <bool EXT, bool D, bool L>
+template <bool EXT, bool D, bool L, bool B>
 static Outcome iterate_t(const Reference &r, const Bla *bla, Skip &skip,
                          std::optional<std::pair<double, double>> c, double ar, double ai,
                          int64_t offset_exp, uint64_t max_iter, double r2,
-                         std::optional<size_t> nucleus, const Start &start) {
+                         std::optional<size_t> nucleus, const Start &start, const double *q) {
   Outcome o;
   if (c && in_main_components(c->first, c->second)) {
     o.kind = Kind::Interior;
@@ -477,6 +505,10 @@ static Outcome iterate_t(const Reference &r, const Bla *bla, Skip &skip,
   bool predicted = false;
   double qr = 0.0, qi = 0.0, qstep = 0.0;
   double adc = L ? std::sqrt(ar * ar + ai * ai) : 0.0;
+  // sample.rs:221-225 (B): error radii e >= |z_exact - (A_m + delta)|, ed on dz/dc; rc:
+  // the f64 offset's distance from the exact sample position
+  double e = 0.0, ed = 0.0;
+  const double rc = 16.0 * U * (std::fabs(ar) + std::fabs(ai)) + 1e-300;
   Contraction contraction;
   uint64_t limit = max_iter;
   while (n < limit) {
@@ -533,6 +565,17 @@ static Outcome iterate_t(const Reference &r, const Bla *bla, Skip &skip,
       double fr = zr[m] + scale * xr, fi = zi[m] + scale * xi;
       if (nucleus && n >= 1) contraction.multiply(2.0 * fr, 2.0 * fi, 0);
       if (!EXT && hold > 0) mu.multiply(2.0 * fr, 2.0 * fi);
+      if (B) {  // sample.rs:338-350
+        const double af = std::sqrt(fr * fr + fi * fi) * (1.0 + 4.0 * U) + 1e-150;  // >= |f|
+        const double ef = e + q[m] + 2.0 * U * af;                                   // >= |z_exact - f|
+        const double ad = std::fabs(dr) + std::fabs(di);
+        ed = (2.0 * (af + ef) * ed + 2.0 * ef * ad + 8.0 * U * (2.0 * af * ad + 1.0)) * SAFE;
+        const double aw = std::fabs(zr[m]) + std::fabs(zi[m]), ax = std::fabs(xr) + std::fabs(xi);
+        // the delta step's defect against 2 A delta + delta^2 + dc_exact
+        const double rho = 8.0 * U * (2.0 * aw * ax + ax * ax + std::fabs(ar) + std::fabs(ai)) + 2.0 * q[m] * ax + rc;
+        const double w = af + q[m] + 2.0 * U * af;  // >= |A_m + delta|
+        e = (e * (2.0 * w + e) + rho) * SAFE;
+      }
       if (D) {
         double t = 2.0 * (fr * dr - fi * di) + inverse;
         di = 2.0 * (fr * di + fi * dr);
@@ -569,6 +612,10 @@ static Outcome iterate_t(const Reference &r, const Bla *bla, Skip &skip,
       o.dr = dr;
       o.di = di;
       o.dexp = derivative_exp;
+      if (B) {  // sample.rs:373-377
+        o.ez = e + q[m] + 4.0 * U * std::sqrt(f2);
+        o.ed = ed;
+      }
       return o;
     }
     if (nucleus && n == (uint64_t)*nucleus + 1) {
@@ -582,6 +629,7 @@ static Outcome iterate_t(const Reference &r, const Bla *bla, Skip &skip,
     double delta2 = physical_r * physical_r + physical_i * physical_i;
     bool rebase = EXT ? f2 <= delta2 : f2 < delta2;
     if (rebase || m == last) {
+      if (B) e += q[m] + 4.0 * U * std::sqrt(f2) + 1e-300;  // sample.rs:419-421: delta := f
       if (EXT) {
         if (f2 > SQUARE_OK) {
           xr = fr;
@@ -733,12 +781,18 @@ static Outcome iterate_t(const Reference &r, const Bla *bla, Skip &skip,
 #pragma GCC diagnostic ignored "-Wmaybe-uninitialized"
 Outcome iterate(bool extended, bool D, bool L, const Reference &r, const Bla *bla, Skip &skip,
                 std::optional<std::pair<double, double>> c, double ar, double ai, int64_t offset_exp,
-                uint64_t max_iter, double r2, std::optional<size_t> nucleus, const Start &start) {
-  // sample.rs:226-228: a supplied state skipped the contraction's products, so it
-  // declines the nucleus heuristic
-  if (start.n > 0) nucleus = std::nullopt;
+                uint64_t max_iter, double r2, std::optional<size_t> nucleus, const Start &start,
+                const double *q) {
+  // sample.rs:226-229: a supplied state skipped the contraction's products, and a
+  // bounded render has no proof for the heuristic, so both decline it
+  if (start.n > 0 || q) nucleus = std::nullopt;
+  if (q) {  // sample.rs:185-186, 246: the bounded variant is ordinary-tier, unblocked, from Z_0
+    if (extended || start.n > 0) throw std::runtime_error("bounded iteration needs an ordinary tier and no series start");
+    return D ? iterate_t<false, true, false, true>(r, nullptr, skip, c, ar, ai, 0, max_iter, r2, nucleus, start, q)
+             : iterate_t<false, false, false, true>(r, nullptr, skip, c, ar, ai, 0, max_iter, r2, nucleus, start, q);
+  }
 #define FDREF_IT(E, DD, LL) \
-  iterate_t<E, DD, LL>(r, bla, skip, c, ar, ai, offset_exp, max_iter, r2, nucleus, start)
+  iterate_t<E, DD, LL, false>(r, bla, skip, c, ar, ai, offset_exp, max_iter, r2, nucleus, start, nullptr)
   if (extended) {
     if (D) return L ? FDREF_IT(true, true, true) : FDREF_IT(true, true, false);
     return L ? FDREF_IT(true, false, true) : FDREF_IT(true, false, false);
