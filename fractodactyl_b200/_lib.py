@@ -105,7 +105,7 @@ FDC_SYMBOLS = ["fdc_abi_version", "fdc_open", "fdc_close", "fdc_last_error", "fd
                "fdc_render_noalloc", "fdc_set_tuning", "fdc_get_tuning"]
 FDH_SYMBOLS = ["fdh_last_error", "fdh_plane_new", "fdh_orbit_fixed", "fdh_orbit_fixed_threads", "fdh_orbit_f64",
                "fdh_nucleus_period",
-               "fdh_bla_build", "fdh_bla_build_into", "fdh_series_build", "fdh_dc_bound", "fdh_encode", "fdh_location"]
+               "fdh_bla_build", "fdh_bla_build_into", "fdh_series_build", "fdh_error_radius", "fdh_dc_bound", "fdh_encode", "fdh_location"]
 
 _lib = None
 
@@ -147,6 +147,8 @@ def lib():
     L.fdh_nucleus_period.restype = I64
     L.fdh_nucleus_period.argtypes = [P, P, U64]
     L.fdh_bla_build.argtypes = [P, P, U64, D, D, I64, C.c_int, P, P, C.POINTER(U32), C.POINTER(U64)]
+    L.fdh_error_radius.restype = C.c_int
+    L.fdh_error_radius.argtypes = [P, P, U64, I64, D, D, P]
     L.fdh_series_build.restype = C.c_int
     L.fdh_series_build.argtypes = [P, P, U64, D, D, U64, U64, C.POINTER(SeriesInfo), P, U32]
     L.fdh_bla_build_into.restype = C.c_int

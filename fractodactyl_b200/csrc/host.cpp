@@ -708,6 +708,34 @@ int fdh_bla_build_into(const double *re, const double *im, uint64_t len, double 
   return 0;
 }
 
+// Reference::error_radius (crates/fd-kernel/src/reference.rs:122-148): bounds
+// q[m] >= |A_m - Z_m| on each stored point's distance from the exact orbit A of the exact
+// centre. A fixed-point orbit (bits >= 0) carries its three truncated squares and the
+// centre's truncation, each under 2^-bits, plus the rounding to f64; an f64 orbit
+// (bits < 0) from the correctly rounded centre (c_re, c_im) carries the roundings of
+// x^2 - y^2 + c and 2xy + c and of the centre.
+int fdh_error_radius(const double *re, const double *im, uint64_t len, int64_t bits, double c_re, double c_im,
+                     double *q) {
+  const double U = 1.1102230246251565e-16, MIN_POSITIVE = 2.2250738585072014e-308;
+  if (len && (!re || !im || !q)) {
+    g_err = "null orbit or output";
+    return -1;
+  }
+  const double c1 = std::fabs(c_re) + std::fabs(c_im);
+  const bool fixed = bits >= 0;
+  double unit = fixed ? exp2i(4 - bits) : 0.0;
+  if (fixed && !(unit > MIN_POSITIVE)) unit = MIN_POSITIVE;
+  double a = 0.0;  // |A_m - F_m|, F the orbit as computed before its rounding to f64
+  for (uint64_t m = 0; m < len; ++m) {
+    const double s = std::sqrt(re[m] * re[m] + im[m] * im[m]) * (1.0 + 4.0 * U);
+    const double round = fixed ? 2.0 * U * s + MIN_POSITIVE : 0.0;
+    const double defect = fixed ? unit : 8.0 * U * (s * s + c1) + 2.0 * U * c1 + MIN_POSITIVE;
+    q[m] = a + round;
+    a = (a * (2.0 * (s + round) + a) + defect) * (1.0 + 8.0 * U);
+  }
+  return 0;
+}
+
 // Series::build (crates/fd-kernel/src/series.rs:86-245) with SeriesConfig::default()
 // (series.rs:43-55): the coefficients b_k of delta_n(x) = sum b_k x^k, x = dc / rho, are
 // stepped with the orbit (b_1' = 2 Z b_1 + rho, b_k' = 2 Z b_k + sum_{i+j=k} b_i b_j) over

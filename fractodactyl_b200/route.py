@@ -129,6 +129,16 @@ class Reference:
             raise ValueError(_lib.host_error())
         return cls(re[:n].copy(), im[:n].copy(), bits)
 
+    def error_radius(self, bits: Optional[int], c_re: float, c_im: float) -> np.ndarray:
+        """Reference::error_radius (reference.rs:122-148): q[m] >= |A_m - Z_m| for each
+        point; bits None for an f64 orbit from the correctly rounded centre (c_re, c_im)."""
+        re, im = np.ascontiguousarray(self.re), np.ascontiguousarray(self.im)
+        q = np.empty(len(re))
+        if lib().fdh_error_radius(re.ctypes.data, im.ctypes.data, len(re), -1 if bits is None else bits, c_re, c_im,
+                                  q.ctypes.data) != 0:
+            raise ValueError(_lib.host_error())
+        return q
+
     @classmethod
     def new(cls, c_re: float, c_im: float, max_iter: int, escape_radius: float) -> "Reference":
         cap = min(max_iter, MAX_LEN - 1) + 1

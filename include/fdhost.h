@@ -69,6 +69,13 @@ int fdh_bla_build_into(const double *re, const double *im, uint64_t len, double 
                        int threads, double *blocks7, uint64_t cap_blocks, uint64_t *level_offsets, uint32_t cap_levels,
                        uint32_t *levels, uint64_t *blocks);
 
+/* Reference::error_radius (crates/fd-kernel/src/reference.rs:122-148) into q (len
+ * entries): bounds on each orbit point's distance from the exact orbit of the exact centre,
+ * for the Bound column (fdc_upload_error_radius). bits >= 0: a fixed-point orbit of that
+ * many fraction bits; bits < 0: an f64 orbit from the correctly rounded centre (c_re, c_im). */
+int fdh_error_radius(const double *re, const double *im, uint64_t len, int64_t bits, double c_re, double c_im,
+                     double *q);
+
 /* Series::build (crates/fd-kernel/src/series.rs:86-245) with SeriesConfig::default()
  * (series.rs:43-55) over an orbit, for samples with |dc| <= rho and output pixels of
  * `pixel` in c: the parameter-series start every sample of a frame may take (n iterates

@@ -220,3 +220,23 @@ def test_series_build_bit_exact(case):
         assert np.float64(getattr(got, k)).view(np.uint64) == np.float64(w[k]).view(np.uint64), k
     if case != "tight":
         assert got.n > 0
+
+
+@pytest.mark.parametrize("case", ["f64", "fixed", "deep"])
+def test_error_radius_bit_exact(case):
+    """fdh_error_radius (Reference::error_radius, reference.rs:122-148) equals the
+    oracle's bit for bit, for f64 and fixed-point orbits (bits beyond the subnormal range
+    clamp the unit to the smallest normal)."""
+    if case == "f64":
+        a = fdref.Ref.f64(-0.7453, 0.1127, 5_000, 1e10)
+        bits, c = None, (-0.7453, 0.1127)
+    else:
+        rung = KATS["rung_7676"]
+        bits = 256 if case == "fixed" else 3456
+        a = fdref.Ref.fixed(rung["re"], rung["im"], bits, 4_000)
+        c = (float(rung["re"]), float(rung["im"]))
+    re_, im_ = a.arrays_()
+    want = fdref.error_radius(a, bits, *c)
+    got = fd.Reference(np.ascontiguousarray(re_), np.ascontiguousarray(im_), a.bits).error_radius(bits, *c)
+    assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
+    assert np.all(got >= 0)
