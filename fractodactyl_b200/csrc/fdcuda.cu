@@ -50,6 +50,7 @@ struct OrbitDev {
   uint32_t series_n = 0, series_order = 0;
   double series_rho = 0.0, series_inv = 0.0;
   double2 *series_b = nullptr;
+  double *q = nullptr;  // error radii of the orbit's points (fdc_upload_error_radius), len entries
 };
 
 constexpr uint32_t SERIES_SLOTS = 64;  // SeriesConfig::default().max_order (series.rs:45)
@@ -82,7 +83,7 @@ struct fdc_ctx {
   // staging for host outputs / inputs, grown on demand
   void *stage = nullptr;
   size_t stage_bytes = 0;
-  int blocks_per_sm[12] = {};
+  int blocks_per_sm[13] = {};
   int blocks_per_sm_f32[4] = {};
   int blocks_per_sm_batch[8] = {};
   int blocks_per_sm_batch_f32[4] = {};
@@ -206,10 +207,12 @@ void free_orbit_buffers(fdc_ctx *ctx, OrbitDev &o) {
   pool_put(ctx, o.z32, 32 * o.len);
   free_bla(ctx, o.bla);
   pool_put(ctx, o.series_b, 16 * SERIES_SLOTS);
+  pool_put(ctx, o.q, 8 * o.len);
   o.z = nullptr;
   o.z32 = nullptr;
   o.series_b = nullptr;
   o.has_series = false;
+  o.q = nullptr;
 }
 
 // Orbit layouts built on the device from the caller's SoA (re[], im[]): interleaved
@@ -277,13 +280,18 @@ __global__ void fuse_bla(const double2 *__restrict__ z, uint64_t len, const doub
 
 unsigned grid_for(uint64_t n) { return (unsigned)std::min<uint64_t>((n + 255) / 256, 148 * 16); }
 
-template <bool EXT, bool D, bool L, bool S = false>
+template <bool EXT, bool D, bool L, bool S = false, bool B = false>
 void *kernel_ptr() {
-  return (void *)fdk::perturb_kernel<EXT, D, L, S>;
+  return (void *)fdk::perturb_kernel<EXT, D, L, S, B>;
 }
 
-// series: a job starting from an admitted series (ordinary tiers only): variants 8-11
-void *pick_kernel(bool ext, bool d, bool l, bool series, int &variant) {
+// series: a job starting from an admitted series (ordinary tiers only): variants 8-11;
+// bounded: the bounded variant (ordinary tiers, derivative, no BLA or series): 12
+void *pick_kernel(bool ext, bool d, bool l, bool series, bool bounded, int &variant) {
+  if (bounded) {
+    variant = 12;
+    return kernel_ptr<false, true, false, false, true>();
+  }
   variant = (ext ? 4 : 0) | (d ? 2 : 0) | (l ? 1 : 0);
   if (series && !ext) {
     variant += 8;
@@ -793,7 +801,14 @@ fdc_status fdc_upload_series(fdc_ctx *ctx, int32_t orbit, uint64_t points, uint6
   return FDC_OK;
 }
 
-fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counters *counters) {
+}  // extern "C"
+
+namespace {
+
+// fdc_render and fdc_render_bounded: bout (the Bound column and raw radii) is null for the
+// former; with it, ordinary-tier jobs run the bounded variant (derivative on).
+fdc_status render_impl(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, const fdc_bound_out *bout,
+                       fdc_counters *counters) {
   if (!ctx || !job || !out) return fail(ctx, FDC_INVALID, "null argument");
   auto it = ctx->orbits.find(job->orbit);
   if (it == ctx->orbits.end()) return fail(ctx, FDC_INVALID, "unknown orbit handle");
@@ -805,7 +820,20 @@ fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counte
   if (ps != FDC_OK) return ps;
   const bool ext = j.tier == FDC_TIER_SCALED;
   const bool bla = (j.flags & FDC_BLA) != 0;
-  const bool deriv = (j.flags & FDC_DERIVATIVE) != 0;
+  // Bounded renders (grid.rs:379-384, 588-593): every step certified, so no BLA blocks, no
+  // series start and the plain form; the scaled tier has no radii and renders as usual
+  // (Bound column 0, heuristic evidence).
+  const bool bounded = bout != nullptr && !ext;
+  if (bout) {
+    if (bla) return fail(ctx, FDC_INVALID, "--columns bound certifies every step; BLA remainders are not certified (ACC-02)");
+    if (j.flags & (FDC_SERIES | FDC_F32)) return fail(ctx, FDC_INVALID, "a bounded render runs the plain form from Z_0");
+    if (bounded && !o.q) return fail(ctx, FDC_INVALID, "bounded render without uploaded error radii");
+  }
+  if (bounded) {
+    p.q = o.q;
+    p.flags |= fdk::F_DERIV;
+  }
+  const bool deriv = (j.flags & FDC_DERIVATIVE) != 0 || bounded;
   CK(cudaSetDevice(ctx->device));
   // the window: rows x cols samples; outputs and inputs of full frame rows (pitch nx),
   // staged as the window (pitch cols)
@@ -821,20 +849,22 @@ fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counte
   };
 
   // Device buffers: caller's (FDC_DEVICE_OUT) or staging for the rendered rows.
+  constexpr int NCOL = 12;
   struct Col {
     void *host;
     size_t width;
-  } cols[9] = {{out->cls, 1}, {out->n, 4}, {out->nu, 8}, {out->de, 4}, {out->normal, 2},
-               {out->z, 16}, {out->dz, 16}, {out->dexp, 8}, {out->status, 1}};
+  } cols[NCOL] = {{out->cls, 1}, {out->n, 4}, {out->nu, 8}, {out->de, 4}, {out->normal, 2},
+                  {out->z, 16}, {out->dz, 16}, {out->dexp, 8}, {out->status, 1},
+                  {bout ? bout->bound : nullptr, 4}, {bout ? bout->ez : nullptr, 8}, {bout ? bout->ed : nullptr, 8}};
   size_t need = 0;
-  size_t offs[11];
-  for (int c = 0; c < 9; ++c) {
+  size_t offs[NCOL + 2];
+  for (int c = 0; c < NCOL; ++c) {
     offs[c] = need;
     if (cols[c].host && !dev_out) need += (n_rows * cols[c].width + 255) & ~(size_t)255;
   }
-  offs[9] = need;  // mask
+  offs[NCOL] = need;  // mask
   if (j.mask) need += (n_rows + 255) & ~(size_t)255;
-  offs[10] = need;  // offsets
+  offs[NCOL + 1] = need;  // offsets
   if (j.offsets) need += (n_rows * 16 + 255) & ~(size_t)255;
   if (need > ctx->stage_bytes) {
     CK(cudaStreamSynchronize(ctx->stream));
@@ -845,8 +875,8 @@ fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counte
     ctx->stage_bytes = need;
   }
   char *stage = (char *)ctx->stage;
-  void *dptr[9];
-  for (int c = 0; c < 9; ++c) {
+  void *dptr[NCOL];
+  for (int c = 0; c < NCOL; ++c) {
     if (!cols[c].host) dptr[c] = nullptr;
     else if (dev_out) dptr[c] = (char *)cols[c].host + origin * cols[c].width;
     else dptr[c] = stage + offs[c];
@@ -860,18 +890,21 @@ fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counte
   p.dz_out = (double2 *)dptr[6];
   p.dexp_out = (int64_t *)dptr[7];
   p.status = (uint8_t *)dptr[8];
+  p.bound_out = (float *)dptr[9];
+  p.ez_out = (double *)dptr[10];
+  p.ed_out = (double *)dptr[11];
   p.out_pitch = dev_out ? j.nx : p.cols;
   if (j.mask) {
-    p.mask = (const uint8_t *)(stage + offs[9]);
-    CK(window_copy(stage + offs[9], p.cols, j.mask + origin, j.nx, p.cols, cudaMemcpyHostToDevice));
+    p.mask = (const uint8_t *)(stage + offs[NCOL]);
+    CK(window_copy(stage + offs[NCOL], p.cols, j.mask + origin, j.nx, p.cols, cudaMemcpyHostToDevice));
   }
   if (j.offsets) {
-    p.offsets = (const double2 *)(stage + offs[10]);
-    CK(window_copy(stage + offs[10], p.cols * 16ull, j.offsets + 2 * origin, j.nx * 16ull, p.cols * 16ull,
+    p.offsets = (const double2 *)(stage + offs[NCOL + 1]);
+    CK(window_copy(stage + offs[NCOL + 1], p.cols * 16ull, j.offsets + 2 * origin, j.nx * 16ull, p.cols * 16ull,
                    cudaMemcpyHostToDevice));
   }
   // Samples that are never reached keep zeroed columns and status 0.
-  for (int c = 0; c < 9; ++c) {
+  for (int c = 0; c < NCOL; ++c) {
     if (!dptr[c]) continue;
     const size_t w = cols[c].width;
     if (!dev_out || full)
@@ -890,7 +923,7 @@ fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counte
                        ctx->blocks_per_sm_f32));
   } else {
     int variant = 0;
-    void *fn = pick_kernel(ext, deriv, bla, p.series_n > 0, variant);
+    void *fn = pick_kernel(ext, deriv, bla, p.series_n > 0, bounded, variant);
     if (!ctx->blocks_per_sm[variant]) {
       int b = 0;
       CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, 128, 0));
@@ -903,7 +936,7 @@ fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counte
   }
   CK(cudaEventRecord(ctx->ev1, ctx->stream));
   if (!dev_out) {
-    for (int c = 0; c < 9; ++c)
+    for (int c = 0; c < NCOL; ++c)
       if (cols[c].host) {
         const size_t w = cols[c].width;
         CK(window_copy((char *)cols[c].host + origin * w, j.nx * w, dptr[c], p.cols * w, p.cols * w,
@@ -929,6 +962,39 @@ fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counte
     counters->launches = 1;
   }
   if (sc.timed_out) return fail(ctx, FDC_TIMEOUT, "deadline passed; unfinished samples have status 0");
+  return FDC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counters *counters) {
+  return render_impl(ctx, job, out, nullptr, counters);
+}
+
+fdc_status fdc_render_bounded(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, const fdc_bound_out *bound,
+                              fdc_counters *counters) {
+  if (!bound) return fail(ctx, FDC_INVALID, "null argument");
+  return render_impl(ctx, job, out, bound, counters);
+}
+
+fdc_status fdc_upload_error_radius(fdc_ctx *ctx, int32_t orbit, const double *q, uint64_t len) {
+  if (!ctx) return FDC_INVALID;
+  auto it = ctx->orbits.find(orbit);
+  if (it == ctx->orbits.end()) return fail(ctx, FDC_INVALID, "unknown orbit handle");
+  OrbitDev &o = it->second;
+  if (len != o.len || !q) return fail(ctx, FDC_INVALID, "error radii must cover the orbit's points");
+  for (uint64_t m = 0; m < len; ++m)
+    if (!(q[m] >= 0.0)) return fail(ctx, FDC_INVALID, "error radii must be non-negative");
+  CK(cudaSetDevice(ctx->device));
+  if (!o.q) {
+    o.q = (double *)pool_get(ctx, 8 * o.len);
+    if (!o.q) return fail(ctx, FDC_DEVICE_ERROR, "device memory for the error radii");
+  }
+  cudaError_t e = upload(ctx, o.q, q, 8 * len);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);  // the caller's array may go after return
+  if (e != cudaSuccess) return fail(ctx, FDC_DEVICE_ERROR, std::string("error radii upload: ") + cudaGetErrorString(e));
   return FDC_OK;
 }
 

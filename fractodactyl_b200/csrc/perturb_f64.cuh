@@ -90,7 +90,14 @@ struct Params {
   const double2 *__restrict__ series_b;  // b_1..b_order as (re, im)
   uint32_t series_order, series_n;
   double series_inv;  // 1 / rho
+  // Bounded variant (B, ordinary tiers): the orbit's error radii q[m] >= |A_m - Z_m|
+  // (reference.rs:122-148) and the outputs it adds: the Bound column and the raw radii
+  const double *__restrict__ q;
+  float *bound_out;
+  double *ez_out, *ed_out;
 };
+
+constexpr double SAFE = 1.0 + 8.0 * U;  // sample.rs:56
 
 enum : uint32_t { F_DERIV = 1u, F_BLA = 2u, F_SHIFT = 4u };
 
@@ -107,6 +114,7 @@ struct State {
   Multiplier mu;
   Contraction ct;
   double adc, shift;
+  double e, ed, rc;  // B: error radii on z and dz/dc, the offset's own error (sample.rs:221-225)
   int32_t offset_exp, delta_exp;  // |h_e| <= 2^30 (checked by the route): deltas stay within 32 bits
   int64_t derivative_exp;
   int32_t nucleus;               // < 2^31 - 1 (checked by the route)
@@ -123,6 +131,7 @@ struct Result {
   uint64_t n;
   double zr, zi, dr, di;
   int64_t dexp;
+  double ez, ed;  // B: error radii of an escaped sample (sample.rs:373-377)
 };
 
 // The iteration limit behind Bla::find's budget (sample.rs:246-263) with n left out:
@@ -235,11 +244,23 @@ __device__ __forceinline__ void apply_block(const Params &p, State<EXT> &s, int 
 
 // One ordinary step (sample.rs:331-380; number.rs:92-124): z = Z[m] + delta is carried
 // from the end of the previous iteration in (fr, fi).
-template <bool EXT, bool D>
-__device__ __forceinline__ void plain_update(State<EXT> &s) {
+template <bool EXT, bool D, bool B = false>
+__device__ __forceinline__ void plain_update(State<EXT> &s, const double *__restrict__ q = nullptr) {
   const double fr = s.fr, fi = s.fi;
   if (s.nucleus >= 0 && s.n >= 1) s.ct.multiply(2.0 * fr, 2.0 * fi);
   if (!EXT && s.hold > 0) s.mu.multiply(2.0 * fr, 2.0 * fi);
+  if (B) {  // sample.rs:338-350: the radii through this step, from the state before it
+    const double qm = __ldg(q + s.m);
+    const double af = sqrt(fr * fr + fi * fi) * (1.0 + 4.0 * U) + 1e-150;  // >= |f|
+    const double ef = s.e + qm + 2.0 * U * af;                              // >= |z_exact - f|
+    const double ad = fabs(s.dr) + fabs(s.di);
+    s.ed = (2.0 * (af + ef) * s.ed + 2.0 * ef * ad + 8.0 * U * (2.0 * af * ad + 1.0)) * SAFE;
+    const double aw = fabs(s.Zr) + fabs(s.Zi), ax = fabs(s.xr) + fabs(s.xi);
+    // the delta step's defect against 2 A delta + delta^2 + dc_exact
+    const double rho = 8.0 * U * (2.0 * aw * ax + ax * ax + fabs(s.ar) + fabs(s.ai)) + 2.0 * qm * ax + s.rc;
+    const double w = af + qm + 2.0 * U * af;  // >= |A_m + delta|
+    s.e = (s.e * (2.0 * w + s.e) + rho) * SAFE;
+  }
   if (D) {
     double t = 2.0 * (fr * s.dr - fi * s.di) + s.inverse;
     s.di = 2.0 * (fr * s.di + fi * s.dr);
@@ -267,7 +288,7 @@ __device__ __forceinline__ void plain_update(State<EXT> &s) {
 // bailout, nucleus gate, rebase, rescaling and periodicity. Zn/Rn hold the prefetched
 // entry m + 1 of the iteration's start, right after a plain step; after a block (took)
 // the entry at the new m is loaded here. Returns true when the sample has an outcome.
-template <bool EXT, bool D, bool L>
+template <bool EXT, bool D, bool L, bool B = false>
 __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res, bool took, double2 Zn,
                                      double2 Rn) {
   double2 Z = Zn;
@@ -322,6 +343,10 @@ __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res
     res.dr = s.dr;
     res.di = s.di;
     res.dexp = s.derivative_exp;
+    if (B) {  // sample.rs:373-377
+      res.ez = s.e + __ldg(p.q + s.m) + 4.0 * U * sqrt(f2);
+      res.ed = s.ed;
+    }
     return true;
   }
   if (__builtin_expect(s.nucleus >= 0, 0) && s.n == (uint32_t)s.nucleus + 1u) {
@@ -340,6 +365,7 @@ __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res
   bool moved = false;
   if (__builtin_expect(rebase || s.m == p.last, 0)) {
     moved = true;
+    if (B) s.e += __ldg(p.q + s.m) + 4.0 * U * sqrt(f2) + 1e-300;  // sample.rs:419-421: delta := f
     if (EXT) {
       if (f2 > SQUARE_OK) {
         s.xr = fr;
@@ -555,7 +581,7 @@ struct Waiting {
 // lanes wait or no lane steps plainly; the waiting lanes then apply their blocks together. The warp
 // runs the block path for many lanes at a time instead of for one or two lanes on
 // nearly every iteration, and each lane's own sequence of operations is unchanged.
-template <bool EXT, bool D, bool L>
+template <bool EXT, bool D, bool L, bool B = false>
 __device__ __forceinline__ bool warp_step(const Params &p, State<EXT> &s, Result &res, bool active, Waiting &w,
                                           uint32_t defer) {
   bool upd = false, took = false, done = false;
@@ -577,7 +603,7 @@ __device__ __forceinline__ bool warp_step(const Params &p, State<EXT> &s, Result
         w.on = true;
         w.lv = lv;
       } else {
-        plain_update<EXT, D>(s);
+        plain_update<EXT, D, B>(s, p.q);
         upd = true;
       }
     }
@@ -597,7 +623,7 @@ __device__ __forceinline__ bool warp_step(const Params &p, State<EXT> &s, Result
       upd = took = true;
     }
   }
-  if (upd) done = post<EXT, D, L>(p, s, res, took, Zn, Rn);
+  if (upd) done = post<EXT, D, L, B>(p, s, res, took, Zn, Rn);
   return done;
 }
 
@@ -635,10 +661,10 @@ __device__ __forceinline__ void series_start(const Params &p, double ar, double 
 // row-major order; 8x4 samples unless tuned). Returns
 // false when the slot holds no sample to iterate (outside the grid, masked, or settled
 // by the closed-form main-component test, whose result is written here).
-template <bool EXT, bool D, bool L>
+template <bool EXT, bool D, bool L, bool B = false>
 __device__ __forceinline__ void start_sample(const Params &p, State<EXT> &s, bool use_series, bool keep_counts);
 
-template <bool EXT, bool D, bool L, bool S = false>
+template <bool EXT, bool D, bool L, bool S = false, bool B = false>
 __device__ __forceinline__ int init(const Params &p, uint64_t slot, State<EXT> &s, Result &res) {
   uint64_t tile = slot >> 5;
   if (p.tile_order) tile = __ldg(p.tile_order + tile);  // queue position -> row-major tile
@@ -677,7 +703,7 @@ __device__ __forceinline__ int init(const Params &p, uint64_t slot, State<EXT> &
       return 2;
     }
   }
-  start_sample<EXT, D, L>(p, s, S, false);
+  start_sample<EXT, D, L, B>(p, s, S, false);
   return 1;
 }
 
@@ -685,7 +711,7 @@ __device__ __forceinline__ int init(const Params &p, uint64_t slot, State<EXT> &
 // the ordinary start at Z_0, or the series start when one is given and use_series.
 // keep_counts keeps the block counters (a retry from zero after a series start counts
 // both runs, grid.rs:623-648).
-template <bool EXT, bool D, bool L>
+template <bool EXT, bool D, bool L, bool B>
 __device__ __forceinline__ void start_sample(const Params &p, State<EXT> &s, bool use_series, bool keep_counts) {
   s.xr = 0.0;
   s.xi = 0.0;
@@ -752,10 +778,34 @@ __device__ __forceinline__ void start_sample(const Params &p, State<EXT> &s, boo
     s.chk = np > 16 ? (uint32_t)np : 16u;
     s.nucleus = -1;
   }
+  if (B) {  // sample.rs:221-229: radii from zero; a bounded render has no nucleus heuristic
+    s.e = 0.0;
+    s.ed = 0.0;
+    s.rc = 16.0 * U * (fabs(s.ar) + fabs(s.ai)) + 1e-300;
+    s.nucleus = -1;
+  }
   relimit(p, s);
 }
 
 // Column encoder (store.rs:66-112, Bound absent) and raw state.
+// store.rs:115-151 (B): Bounded evidence for an escaped sample with |z| = az, |dz/dc| = ad
+// and radii ez, ed: the lower DE factor and the nu bound, or false unless the radii prove
+// escape (|z| - ez > 2) and ed < ad / 2. CUDA's log / log1p / exp / exp2 (the columns
+// within their ulps of the host's; byte-exact columns come from the raw radii).
+__device__ __forceinline__ bool bounds(uint64_t n, double az, double ez, double ad, double ed, double &de_lo,
+                                       double &bound) {
+  const double lo = az - ez;
+  if (!(lo > 2.0 && ed < 0.5 * ad)) return false;
+  const double lnz = log(az), llo = log(lo), lhi = log(az + ez);
+  const double nu = log1p(-log1p(-ez / az) / llo) / LN_2 + 8.0 * U * ((double)n + 8.0);
+  const double g = lhi * exp2(-(double)n);
+  de_lo = (lo * llo) / (az * lnz) * ad / (ad + ed) * exp(-g) * (1.0 - 4.0 / (lo * lo)) * (1.0 - 1e-6);
+  const double de_hi = ((az + ez) * lhi) / (az * lnz) * ad / (ad - ed) * (1.0 + 1e-6);
+  bound = nu * de_hi / de_lo * (1.0 + 1e-6);
+  return true;
+}
+
+template <bool B = false>
 __device__ __forceinline__ void put(const Params &p, uint32_t sample, const Result &r) {
   const uint32_t j = sample / p.nx, i = sample - j * p.nx;
   const uint64_t idx = (uint64_t)(j - p.first_row) * p.out_pitch + (i - p.first_col);
@@ -765,19 +815,28 @@ __device__ __forceinline__ void put(const Params &p, uint32_t sample, const Resu
     if (p.cls) p.cls[idx] = (uint8_t)(r.kind == 2 ? 2 : 1);
     return;
   }
-  if (p.cls) p.cls[idx] = 0;
   if (p.z_out) p.z_out[idx] = make_double2(r.zr, r.zi);
   if (p.dz_out) p.dz_out[idx] = make_double2(r.dr, r.di);
   if (p.dexp_out) p.dexp_out[idx] = r.dexp;
   double z2 = r.zr * r.zr + r.zi * r.zi;
   double log2z = 0.5 * log2(z2);
+  double de_lo = 0.0, bnd = 0.0;
+  bool bounded = false;
+  if (B) {  // store.rs:88-106
+    bounded = bounds(r.n, sqrt(z2), r.ez, hypot(r.dr, r.di), r.ed, de_lo, bnd);
+    if (p.bound_out) p.bound_out[idx] = bounded ? (float)bnd : 0.0f;
+    if (p.ez_out) p.ez_out[idx] = r.ez;
+    if (p.ed_out) p.ed_out[idx] = r.ed;
+  }
+  if (p.cls) p.cls[idx] = bounded ? 4 : 0;  // Escaped | Bounded << 2
   if (p.nu) p.nu[idx] = (double)r.n + 1.0 - log2(log2z);
   if (p.de) {  // store.rs:145-150
     double lnz = log2z * LN_2;
     double base = 2.0 * sqrt(z2) * lnz / (hypot(r.dr, r.di) * p.px_m);
     int64_t k = -(r.dexp + p.px_e);
     k = k < -4000 ? -4000 : (k > 4000 ? 4000 : k);
-    p.de[idx] = (float)(base * exp2i(k / 2) * exp2i(k - k / 2));
+    const float d = (float)(base * exp2i(k / 2) * exp2i(k - k / 2));
+    p.de[idx] = bounded ? (float)((double)d * de_lo) : d;
   }
   if (p.normal) {  // samples.rs:45-48 through view.rs:132-134
     double re = r.zr * r.dr + r.zi * r.di, im = r.zi * r.dr - r.zr * r.di;
@@ -789,7 +848,9 @@ __device__ __forceinline__ void put(const Params &p, uint32_t sample, const Resu
 
 // S: the series-start variant (ordinary tiers, jobs with an admitted series); the others
 // compile without the series start and its retry.
-template <bool EXT, bool D, bool L, bool S = false>
+// B: the bounded variant (ordinary tiers, derivative on, no BLA or series): error radii,
+// Bounded evidence and the Bound column.
+template <bool EXT, bool D, bool L, bool S = false, bool B = false>
 __global__ void __launch_bounds__(128, Occupancy<EXT>::blocks) perturb_kernel(Params p) {
   const unsigned FULL = 0xffffffffu;
   const unsigned lane = threadIdx.x & 31u;
@@ -806,7 +867,7 @@ __global__ void __launch_bounds__(128, Occupancy<EXT>::blocks) perturb_kernel(Pa
   // prefix - max_iter, so that the first run counts max_iter - prefix.
   int64_t bias = 0;
   auto finish = [&](uint32_t idx, const Result &r, uint64_t nblocks, uint64_t nskipped, double sh) {
-    put(p, idx, r);
+    put<B>(p, idx, r);
     uint64_t spent = (uint64_t)((int64_t)(r.kind == 2 ? p.max_iter : r.n) - bias);
     bias = 0;
     if (L) {
@@ -845,7 +906,7 @@ __global__ void __launch_bounds__(128, Occupancy<EXT>::blocks) perturb_kernel(Pa
       if (!active) {
         uint64_t slot = base + __popc(need & lt);
         if (slot < p.total) {
-          int got = init<EXT, D, L, S>(p, slot, s, res);
+          int got = init<EXT, D, L, S, B>(p, slot, s, res);
           if (got == 1) {
             active = true;
             if (S) bias = p.series_n;
@@ -857,12 +918,12 @@ __global__ void __launch_bounds__(128, Occupancy<EXT>::blocks) perturb_kernel(Pa
       need = __ballot_sync(FULL, !active);
     }
     if (!__any_sync(FULL, active)) break;
-    if (warp_step<EXT, D, L>(p, s, res, active, w, p.defer)) {
+    if (warp_step<EXT, D, L, B>(p, s, res, active, w, p.defer)) {
       if (S && bias > 0 && res.kind == 2) {
         // an unresolved series start retries from zero, keeping the nucleus heuristic
         // (grid.rs:637-642); its count and blocks carry over
         bias -= (int64_t)p.max_iter;
-        start_sample<EXT, D, L>(p, s, false, true);
+        start_sample<EXT, D, L, B>(p, s, false, true);
       } else {
         finish(s.idx, res, s.blocks, s.skipped, s.shift);
         active = false;

@@ -241,6 +241,9 @@ class Samples:
     dz: Optional[np.ndarray] = None
     dexp: Optional[np.ndarray] = None
     status: Optional[np.ndarray] = None
+    bound: Optional[np.ndarray] = None  # Bound column (f32 nu error bound; bounded renders)
+    ez: Optional[np.ndarray] = None     # raw error radii of escaped samples (bounded renders)
+    ed: Optional[np.ndarray] = None
 
 
 @dataclasses.dataclass
@@ -332,10 +335,16 @@ class Device:
     def free(self, orbit: int):
         lib().fdc_free_orbit(self.h, orbit)
 
-    def render_job(self, job: _lib.Job, raw=False, columns=COLUMNS, device_out=None, host_out=None):
+    def upload_error_radius(self, orbit: int, q: np.ndarray):
+        """fdc_upload_error_radius: the orbit's error radii for bounded renders."""
+        q = np.ascontiguousarray(q, dtype=np.float64)
+        _check(lib().fdc_upload_error_radius(self.h, orbit, q.ctypes.data, len(q)), self, "upload error radii")
+
+    def render_job(self, job: _lib.Job, raw=False, columns=COLUMNS, device_out=None, host_out=None, bounded=False):
         """fdc_render into fresh host arrays, into the caller's host arrays (host_out: the
         dict an earlier call returned, reused frame after frame) or into caller device
-        buffers (device_out)."""
+        buffers (device_out). bounded: fdc_render_bounded, adding the host arrays
+        "bound", "ez" and "ed"."""
         n = job.nx * job.ny
         out = _lib.Out()
         arrays = {}
@@ -363,7 +372,14 @@ class Device:
             for k, a in arrays.items():
                 setattr(out, k, a.ctypes.data)
         cnt = _lib.Counters()
-        st = lib().fdc_render(self.h, C.byref(job), C.byref(out), C.byref(cnt))
+        if bounded:
+            for k, dt in (("bound", np.float32), ("ez", np.float64), ("ed", np.float64)):
+                if k not in arrays:
+                    arrays[k] = np.zeros(n, dt)
+            bout = _lib.BoundOut(arrays["bound"].ctypes.data, arrays["ez"].ctypes.data, arrays["ed"].ctypes.data)
+            st = lib().fdc_render_bounded(self.h, C.byref(job), C.byref(out), C.byref(bout), C.byref(cnt))
+        else:
+            st = lib().fdc_render(self.h, C.byref(job), C.byref(out), C.byref(cnt))
         _check(st, self, "render")
         return arrays, cnt, st
 
@@ -517,8 +533,15 @@ def render_with(view: View, p: Params, orbit=None, bla: Optional[Bla] = None, de
     (grid.rs:350-366, :378-413, :461-475); Bound/Stripe columns are declined (frame.rs:129-144).
     """
     started = time.perf_counter()
-    if "bound" in p.columns or "stripe" in p.columns:
-        raise Declined("frame declined (bound/stripe); CPU restart from zero")
+    if "stripe" in p.columns:
+        raise Declined("frame declined (stripe); CPU restart from zero")
+    bound = "bound" in p.columns
+    if bound and bla is not None:  # grid.rs:379-384
+        raise ValueError("--columns bound certifies every step; BLA remainders are not certified (ACC-02)")
+    if bound and series is not None:  # grid.rs:354
+        raise ValueError("a series start needs f64 deltas and no Bound column")
+    if bound and host_encode:
+        raise ValueError("the host encoder writes heuristic columns only: render the Bound column on the device")
     plane, tier = _setup(view, p)
     need = 53 if tier == 0 else plane.bits
     t = time.perf_counter()
@@ -547,26 +570,30 @@ def render_with(view: View, p: Params, orbit=None, bla: Optional[Bla] = None, de
     dev = dev or device(0)
     h = dev.upload(r, bla)
     try:
-        flags = (_lib.DERIVATIVE if p.needs_derivative() else 0) | (_lib.BLA if bla is not None else 0)
+        flags = (_lib.DERIVATIVE if p.needs_derivative() or (bound and tier != 2) else 0) | \
+            (_lib.BLA if bla is not None else 0)
         if series is not None:
             dev.upload_series(h, series)
             flags |= _lib.SERIES
+        if bound and tier != 2:  # grid.rs:588-593: the ordinary tiers' error radii
+            dev.upload_error_radius(h, r.error_radius(None if tier == 0 else bits, plane.c_re, plane.c_im))
         if bla is not None and shift and p.needs_derivative():
             flags |= _lib.SHIFT
         job = make_job(plane, tier, p, h, r.nucleus_period(), flags)
         g = time.perf_counter()
         arrays, cnt, status = dev.render_job(job, raw=raw or host_encode,
-                                             columns=() if host_encode else p.columns)
+                                             columns=() if host_encode else p.columns, bounded=bound)
         gpu_seconds = time.perf_counter() - g
     finally:
         dev.free(h)
     kernel = plane.kernel(tier) + (" bla/1" if bla is not None else "") + (" series/0" if series is not None else "") \
         + " gpu-perturb-cuda/1"
-    cols = ("class",) + tuple(c for c in ("nu", "de", "normal") if c in p.columns)
+    cols = ("class",) + tuple(c for c in ("nu", "de", "normal") if c in p.columns) + \
+        (("bound",) if bound else ())
     header = Header(cols, p.nx, p.ny, p.ss, p.max_iter, p.escape_radius, view, kernel)
     s = Samples(cls=arrays["cls"], nu=arrays.get("nu"), de=arrays.get("de"), normal=arrays.get("normal"),
                 n=arrays.get("n"), z=arrays.get("z"), dz=arrays.get("dz"), dexp=arrays.get("dexp"),
-                status=arrays.get("status"))
+                status=arrays.get("status"), bound=arrays.get("bound"), ez=arrays.get("ez"), ed=arrays.get("ed"))
     if host_encode:
         encode_host(plane, p.ss, s, p.columns, p.threads)
     stats = Stats(len(r), reference_seconds, int(cnt.iterations))

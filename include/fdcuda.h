@@ -133,6 +133,26 @@ fdc_status fdc_upload_series(fdc_ctx *ctx, int32_t orbit, uint64_t points, uint6
  * class and n bit-exact, z and dz bit-exact, nu/de/normal within CUDA libm's ulps. */
 fdc_status fdc_render(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, fdc_counters *counters);
 
+/* Bounded renders (the Bound column; sample.rs's B variant, store.rs:88-106, grid.rs:
+ * 379-384, 588-593). fdc_upload_error_radius attaches the orbit's error radii
+ * q[m] >= |A_m - Z_m| (Reference::error_radius, reference.rs:122-148, e.g. from
+ * fdh_error_radius; len = the orbit's points). fdc_render_bounded renders like fdc_render
+ * and, on the F64 / Fixed tiers, tracks error radii on z and dz/dc every step (derivative
+ * on): escaped samples whose radii prove escape get Bounded evidence (class byte
+ * Escaped | 1 << 2), de scaled by the certified lower factor, and bound[] the nu error
+ * bound (0 elsewhere); ez[] / ed[] receive each escaped sample's raw radii (the host
+ * encoder's inputs). The scaled tier has no radii and renders as fdc_render (bound 0).
+ * Refused: FDC_BLA (remainders are not certified), FDC_SERIES, FDC_F32. Any pointer of
+ * fdc_bound_out may be NULL; they follow fdc_out's layout (FDC_DEVICE_OUT included). */
+typedef struct {
+  float *bound;   /* nu error bound of Bounded samples (store.rs:104-106) */
+  double *ez;     /* error radius on z at escape */
+  double *ed;     /* error radius on the dz/dc mantissa at escape */
+} fdc_bound_out;
+fdc_status fdc_upload_error_radius(fdc_ctx *ctx, int32_t orbit, const double *q, uint64_t len);
+fdc_status fdc_render_bounded(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, const fdc_bound_out *bound,
+                              fdc_counters *counters);
+
 /* Launch tuning (no counterpart in the reference; the reference's shader has fixed
  * workgroups). defer: lanes of a warp whose next operation is a BLA block wait until
  * defer/32 of the warp's busy lanes wait, or no lane steps plainly, and then apply their

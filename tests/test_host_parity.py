@@ -168,8 +168,13 @@ def test_route_flag_and_declines():
     assert fd.enabled(None) is False and fd.enabled("cuda") and fd.enabled("cuda-bla") and fd.enabled("bla")
     with pytest.raises(ValueError):
         fd.enabled("fast")
-    with pytest.raises(fd.Declined):
-        fd.render(fd.View("0", "1", "1e-3"), fd.Params(8, 8, columns=("nu", "bound")))
+    with pytest.raises(fd.Declined):  # the Stripe column stays on the CPU
+        fd.render(fd.View("0", "1", "1e-3"), fd.Params(8, 8, columns=("nu", "stripe")))
+    # the Bound column certifies every step: no BLA (grid.rs:379-384), no series start
+    r = fd.Reference.new(-0.7453, 0.1127, 2_000, 1e10)
+    table = fd.Bla.build_scaled(r, 2.0 ** -50, 1e-5)
+    with pytest.raises(ValueError, match="not certified"):
+        fd.render_with(fd.View("-0.7453", "0.1127", "1e-3"), fd.Params(8, 8, columns=("nu", "bound")), None, table)
     with pytest.raises(ValueError):
         fd.route._setup(fd.View("0", "1", "1e-300"), fd.Params(8, 8, tier="f64"))
 
