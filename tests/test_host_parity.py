@@ -8,6 +8,7 @@ import ctypes as C
 import json
 import os
 import re
+import struct
 import subprocess
 
 import numpy as np
@@ -245,3 +246,25 @@ def test_error_radius_bit_exact(case):
     got = fd.Reference(np.ascontiguousarray(re_), np.ascontiguousarray(im_), a.bits).error_radius(bits, *c)
     assert np.array_equal(got.view(np.uint64), want.view(np.uint64))
     assert np.all(got >= 0)
+
+
+def test_fds_writer_bound_column():
+    """A Bound column (column bit 16, f32, crates/fd-samples/src/column.rs:18-19, 42) is
+    written last of the route's columns, in bit order after normal, padded to 8 bytes,
+    from the oracle's bounded render; the columns before it are the heuristic writer's."""
+    from fractodactyl_b200 import fds
+    view3 = ("-0.7453", "0.1127", "0.0065")
+    job = fdref.make_job(*view3, 7, 3, 4000, columns=fdref.COL_NU | fdref.COL_BOUND, threads=1)
+    o = fdref.render_columns(job, fdref.Ref.for_job(job))
+    view = fd.View(*view3)
+    s = fd.Samples(cls=o["cls"], nu=o["nu"], bound=o["bound"])
+    h = fd.Header(("class", "nu", "bound"), 7, 3, 1, 4000, 1e10, view, o["kernel"])
+    b = fds.encode(h, s)
+    assert struct.unpack_from("<I", b, 12)[0] == 1 | 2 | 16
+    assert (o["cls"] == 4).any() and (o["bound"] > 0).any()
+    tail = o["bound"].astype("<f4").tobytes()
+    assert b.endswith(tail + b"\0" * (-len(tail) % 8))
+    # the same file without the column: only the column bits differ, then the Bound bytes
+    plain = fds.encode(fd.Header(("class", "nu"), 7, 3, 1, 4000, 1e10, view, o["kernel"]), s)
+    assert b[:12] == plain[:12] and b[16:len(plain)] == plain[16:]
+    assert b[len(plain):] == tail + b"\0" * (-len(tail) % 8)
