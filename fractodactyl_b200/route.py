@@ -403,10 +403,10 @@ class Device:
             t.tile_w = tile_w
         _check(lib().fdc_set_tuning(self.h, C.byref(t)), self, "tuning")
 
-    def batch(self, jobs, columns=COLUMNS, raw=False) -> "Batch":
+    def batch(self, jobs, columns=COLUMNS, raw=False, groups=None) -> "Batch":
         """fdc_batch_create over `jobs` (uploaded orbits; FDC_DEVICE_OUT is set here) with
-        fresh device columns per job (torch tensors on this GPU)."""
-        return Batch(self, jobs, columns, raw)
+        fresh device columns per frame (torch tensors on this GPU; see Batch for groups)."""
+        return Batch(self, jobs, columns, raw, groups)
 
 
 _BATCH_DTYPES = {"cls": "uint8", "status": "uint8", "n": "int32", "nu": "float64", "de": "float32",
@@ -417,26 +417,42 @@ _HOST_DTYPES = {"cls": np.uint8, "status": np.uint8, "n": np.uint32, "nu": np.fl
 
 class Batch:
     """Many jobs rendered by one graph replay (fdc_batch_run): one persistent launch per
-    kernel variant over all jobs' tiles. Outputs stay on the device between runs;
-    `columns(k)` copies job k's back."""
+    kernel variant over all jobs' tiles. Outputs stay on the device between runs, one
+    tensor per column holding every frame's samples; `columns(k)` copies job k's frame
+    back, `all_columns` every frame's with one copy per column. groups (optional, one
+    key per job): jobs with the same key are windows of one frame (same view, grid and
+    orbit) and write into one frame buffer; by default every job has a frame of its own."""
 
-    def __init__(self, dev: Device, jobs, columns=COLUMNS, raw=False):
+    def __init__(self, dev: Device, jobs, columns=COLUMNS, raw=False, groups=None):
         import torch
         self.dev, self.jobs, self.h = dev, list(jobs), C.c_void_p()
-        names = ["cls", "status", "n"] + [c for c in ("nu", "de", "normal") if c in columns]
+        self.names = ["cls", "status", "n"] + [c for c in ("nu", "de", "normal") if c in columns]
         if raw:
-            names += ["z", "dz", "dexp"]
-        self.bufs = []
+            self.names += ["z", "dz", "dexp"]
+        keys = list(range(len(self.jobs))) if groups is None else list(groups)
+        if len(keys) != len(self.jobs):
+            raise ValueError("one group key per job")
+        frame_of, sizes = {}, []
+        self.frame = []  # frame index per job
+        for j, key in zip(self.jobs, keys):
+            if key not in frame_of:
+                frame_of[key] = len(sizes)
+                sizes.append(j.nx * j.ny)
+            elif sizes[frame_of[key]] != j.nx * j.ny:
+                raise ValueError("jobs of one group must share their grid")
+            self.frame.append(frame_of[key])
+        self.starts = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+        total = int(self.starts[-1])
+        self.cols = {}
+        for name in self.names:
+            shape = (total, 2) if name in ("z", "dz") else (total,)
+            self.cols[name] = torch.zeros(shape, dtype=getattr(torch, _BATCH_DTYPES[name]), device=f"cuda:{dev.index}")
         outs = (_lib.Out * len(self.jobs))()
         cjobs = (_lib.Job * len(self.jobs))()
         for k, j in enumerate(self.jobs):
-            n = j.nx * j.ny
-            b = {}
-            for name in names:
-                shape = (n, 2) if name in ("z", "dz") else (n,)
-                b[name] = torch.zeros(shape, dtype=getattr(torch, _BATCH_DTYPES[name]), device=f"cuda:{dev.index}")
-                setattr(outs[k], name, b[name].data_ptr())
-            self.bufs.append(b)
+            a = int(self.starts[self.frame[k]])
+            for name, t in self.cols.items():
+                setattr(outs[k], name, t[a:].data_ptr())  # job k's frame starts here
             C.memmove(C.byref(cjobs[k]), C.byref(j), C.sizeof(_lib.Job))
             cjobs[k].flags |= _lib.DEVICE_OUT
         _check(lib().fdc_batch_create(dev.h, cjobs, outs, len(self.jobs), C.byref(self.h)), dev, "batch create")
@@ -449,7 +465,25 @@ class Batch:
         return total, list(per)
 
     def columns(self, k: int):
-        return {name: t.cpu().numpy().view(_HOST_DTYPES[name]) for name, t in self.bufs[k].items()}
+        f = self.frame[k]
+        a, b = int(self.starts[f]), int(self.starts[f + 1])
+        return {name: t[a:b].cpu().numpy().view(_HOST_DTYPES[name]) for name, t in self.cols.items()}
+
+    def host_arrays(self):
+        """Host arrays for all_columns, allocated once by the caller and reused."""
+        return {name: np.empty(tuple(t.shape), _HOST_DTYPES[name]) for name, t in self.cols.items()}
+
+    def all_columns(self, host_out=None):
+        """Every job's columns with one device-to-host copy per column: a list of per-job
+        dicts of views into one host array per column, host_out's when given (a dict an
+        earlier call returned as its second value, reused frame after frame)."""
+        import torch
+        host = host_out if host_out is not None else self.host_arrays()
+        for name, t in self.cols.items():
+            torch.from_numpy(host[name].view(_BATCH_DTYPES[name])).copy_(t)
+        per = [{name: a[int(self.starts[f]):int(self.starts[f + 1])] for name, a in host.items()}
+               for f in self.frame]
+        return per, host
 
     def free(self):
         if self.h:

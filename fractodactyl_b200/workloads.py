@@ -35,6 +35,9 @@ class JobSet:
     orbit_seconds: float
     bla_seconds: float
     keep: list = dataclasses.field(default_factory=list)  # host arrays jobs point to
+    # per job, the frame it is a window of (jobs of one frame may share output buffers:
+    # Batch groups); None: every job its own frame
+    groups: Optional[List[int]] = None
 
     def free(self, dev):
         for h in set(self.handles):
@@ -133,7 +136,8 @@ def tiles(dev, frames: List[Frame], tile: Tuple[int, int], extra_flags: int = 0,
     bla_s = time.perf_counter() - t
     jobs, handles, planes, tiers, windows = [], [], [], [], []
     tw, th = tile
-    for (f, p, plane, tier), r, b in zip(setups, refs, blas):
+    groups = []
+    for loc, ((f, p, plane, tier), r, b) in enumerate(zip(setups, refs, blas)):
         h = dev.upload(r, b)
         nuc = r.nucleus_period()
         tier = max(tier, TIERS["fixed"])
@@ -147,7 +151,8 @@ def tiles(dev, frames: List[Frame], tile: Tuple[int, int], extra_flags: int = 0,
                 planes.append(plane)
                 tiers.append(tier)
                 windows.append((x0, j.cols, y0, j.rows))
-    return JobSet(jobs, handles, refs, blas, planes, tiers, windows, orbit_s, bla_s)
+                groups.append(loc)
+    return JobSet(jobs, handles, refs, blas, planes, tiers, windows, orbit_s, bla_s, groups=groups)
 
 
 def jittered(dev, frame: Frame, seed: int = 3, extra_flags: int = 0, max_iter: Optional[int] = None) -> JobSet:

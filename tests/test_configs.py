@@ -113,8 +113,23 @@ def test_mixed_location_tiles(dev):
             got = [b.columns(k) for k in range(len(js.jobs))]
         finally:
             b.free()
+        # the tiles of a location sharing its frame (groups): each frame once, every
+        # tile's window filled, the same samples and counters
+        g = dev.batch(js.jobs, columns=("nu",), raw=True, groups=js.groups)
+        try:
+            total_g, per_g = g.run()
+            shared, host = g.all_columns()
+        finally:
+            g.free()
     finally:
         js.free(dev)
+    assert len(host["cls"]) == len(frames) * 64 * 32
+    assert host["status"].all()
+    assert total_g.iterations == total.iterations and [c.samples for c in per_g] == [c.samples for c in per]
+    for k in range(len(js.jobs)):
+        on = got[k]["status"].astype(bool)
+        for name in ("cls", "n", "z", "dz", "dexp", "nu"):
+            assert np.array_equal(shared[k][name][on], got[k][name][on]), (k, name)
     for loc, f in enumerate(frames):
         r, bla, tier = js.refs[loc], js.blas[loc], js.tiers[2 * loc]
         ref, t = oracle_tables(r, bla, f.bla_eps)
