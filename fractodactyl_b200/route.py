@@ -564,7 +564,8 @@ def render_with(view: View, p: Params, orbit=None, bla: Optional[Bla] = None, de
     `series`, every sample starts from it (Series::render_masked, grid.rs:341-373).
 
     Returns (Header, Samples, Stats, BlaStats or None). Refusals are the reference's
-    (grid.rs:350-366, :378-413, :461-475); Bound/Stripe columns are declined (frame.rs:129-144).
+    (grid.rs:350-366, :378-413, :461-475); the Stripe column is declined (frame.rs:129-144);
+    the Bound column renders through fdc_render_bounded on the F64 / Fixed tiers.
     """
     started = time.perf_counter()
     if "stripe" in p.columns:
