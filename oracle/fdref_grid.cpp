@@ -290,7 +290,8 @@ struct Out {
 // header.rs:62-81 + write.rs:8-53 (MAGIC/MAJOR/MINOR lib.rs:21-27).
 static std::vector<uint8_t> fds(const View &v, const Params &p, uint32_t colset, const std::string &kernel,
                                 const std::vector<uint8_t> &cls, const std::vector<double> &nu,
-                                const std::vector<float> &de, const std::vector<uint16_t> &normal) {
+                                const std::vector<float> &de, const std::vector<uint16_t> &normal,
+                                const std::vector<float> &bound) {
   Out o;
   o.bytes("FDSAMPLE", 8);
   o.u16(1);
@@ -320,6 +321,10 @@ static std::vector<uint8_t> fds(const View &v, const Params &p, uint32_t colset,
   }
   if (colset & FDREF_COL_NORMAL) {
     o.bytes(normal.data(), normal.size() * 2);
+    o.pad8();
+  }
+  if (colset & FDREF_COL_BOUND) {  // column.rs:18-19, 42: f32, after normal in bit order
+    o.bytes(bound.data(), bound.size() * 4);
     o.pad8();
   }
   return o.b;
@@ -745,14 +750,16 @@ int64_t fdref_render_fds(const fdref_job *job, const fdref_ref *ref, const fdref
     std::vector<double> nu((p.columns & FDREF_COL_NU) ? n : 0, 0.0);
     std::vector<float> de((p.columns & FDREF_COL_DE) ? n : 0, 0.0f);
     std::vector<uint16_t> normal((p.columns & FDREF_COL_NORMAL) ? n : 0, 0);
+    std::vector<float> bound((p.columns & FDREF_COL_BOUND) ? n : 0, 0.0f);
     Columns c;
     c.cls = cls.data();
     c.nu = nu.empty() ? nullptr : nu.data();
     c.de = de.empty() ? nullptr : de.data();
     c.normal = normal.empty() ? nullptr : normal.data();
+    c.bound = bound.empty() ? nullptr : bound.data();
     Stats st;
     std::string k = run(v, p, ref ? &ref->r : nullptr, bla ? &bla->t : nullptr, c, st);
-    std::vector<uint8_t> bytes = fds(v, p, p.columns, k, cls, nu, de, normal);
+    std::vector<uint8_t> bytes = fds(v, p, p.columns, k, cls, nu, de, normal, bound);
     if (buf && cap) std::memcpy(buf, bytes.data(), std::min<uint64_t>(cap, bytes.size()));
     return (int64_t)bytes.size();
   })

@@ -249,22 +249,21 @@ def test_error_radius_bit_exact(case):
 
 
 def test_fds_writer_bound_column():
-    """A Bound column (column bit 16, f32, crates/fd-samples/src/column.rs:18-19, 42) is
-    written last of the route's columns, in bit order after normal, padded to 8 bytes,
-    from the oracle's bounded render; the columns before it are the heuristic writer's."""
+    """A bounded render's .fds file (the Bound column, bit 16, f32, after normal:
+    crates/fd-samples/src/column.rs:18-19, 42) written by fds.encode from the oracle's
+    bounded columns equals the oracle's own .fds bytes, on the F64 and Fixed tiers."""
     from fractodactyl_b200 import fds
-    view3 = ("-0.7453", "0.1127", "0.0065")
-    job = fdref.make_job(*view3, 7, 3, 4000, columns=fdref.COL_NU | fdref.COL_BOUND, threads=1)
-    o = fdref.render_columns(job, fdref.Ref.for_job(job))
-    view = fd.View(*view3)
-    s = fd.Samples(cls=o["cls"], nu=o["nu"], bound=o["bound"])
-    h = fd.Header(("class", "nu", "bound"), 7, 3, 1, 4000, 1e10, view, o["kernel"])
-    b = fds.encode(h, s)
-    assert struct.unpack_from("<I", b, 12)[0] == 1 | 2 | 16
-    assert (o["cls"] == 4).any() and (o["bound"] > 0).any()
-    tail = o["bound"].astype("<f4").tobytes()
-    assert b.endswith(tail + b"\0" * (-len(tail) % 8))
-    # the same file without the column: only the column bits differ, then the Bound bytes
-    plain = fds.encode(fd.Header(("class", "nu"), 7, 3, 1, 4000, 1e10, view, o["kernel"]), s)
-    assert b[:12] == plain[:12] and b[16:len(plain)] == plain[16:]
-    assert b[len(plain):] == tail + b"\0" * (-len(tail) % 8)
+    for view3, max_iter in ((("-0.7453", "0.1127", "0.0065"), 4000),
+                            (("-0.743643887037158", "0.131825904205312", "1e-14"), 20000)):
+        cols = fdref.COL_NU | fdref.COL_DE | fdref.COL_NORMAL | fdref.COL_BOUND
+        job = fdref.make_job(*view3, 9, 5, max_iter, rotation=0.2, columns=cols, threads=1)
+        ref = fdref.Ref.for_job(job)
+        want = fdref.render_fds(job, ref)
+        o = fdref.render_columns(job, ref)
+        assert (o["cls"] == 4).any() and (o["bound"] > 0).any()
+        view = fd.View(*view3, 0.2)
+        s = fd.Samples(cls=o["cls"], nu=o["nu"], de=o["de"], normal=o["normal"], bound=o["bound"])
+        h = fd.Header(("class", "nu", "de", "normal", "bound"), 9, 5, 1, max_iter, 1e10, view, o["kernel"])
+        b = fds.encode(h, s)
+        assert struct.unpack_from("<I", b, 12)[0] == 1 | 2 | 4 | 8 | 16
+        assert b == want
