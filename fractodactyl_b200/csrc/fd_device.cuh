@@ -243,9 +243,13 @@ static __device__ __noinline__ bool contracting(const double2 *__restrict__ orbi
 __device__ __forceinline__ uint64_t next_pow2(uint64_t x) { return x <= 1 ? 1 : 1ull << (64 - __clzll(x - 1)); }
 
 __device__ __forceinline__ uint64_t globaltimer() {
+#if defined(__CUDA_ARCH__)
   uint64_t t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
+#else
+  return 0;  // host builds of this header (no device timer; deadlines are device-only)
+#endif
 }
 
 }  // namespace fdk

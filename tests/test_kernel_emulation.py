@@ -1,0 +1,183 @@
+"""The plain-form CUDA kernel's own source (fractodactyl_b200/csrc/perturb_f64.cuh) built
+for the host (tests/emu: builtins shimmed, the persistent kernel run as a single-lane
+warp) against the oracle, on the CPU: class, escape count, z, dz/dc and the work
+counters bit for bit on the F64, Fixed and Scaled tiers with and without BLA and the
+derivative, from a parameter-series start (with its retries from zero) and in the
+bounded variant (error radii, Bounded evidence, Bound column). Host libm stands in for
+CUDA's, so nu, de and the Bound column also equal the oracle's here. This checks the
+kernel's state machine without a GPU; its arithmetic on the device is checked by the
+GPU suite."""
+import ctypes as C
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import fdref
+import fractodactyl_b200 as fd
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+KATS = json.load(open(os.path.join(HERE, "golden", "kats.json")))
+LIB = os.path.join(HERE, "emu", "libemu.so")
+SEAHORSE = ("-0.743643887037158", "0.131825904205312")
+
+
+@pytest.fixture(scope="module")
+def emu():
+    src = [os.path.join(HERE, "emu", "emu.cpp"), os.path.join(HERE, "emu", "cuda_host_shim.hpp"),
+           os.path.join(ROOT, "fractodactyl_b200", "csrc", "perturb_f64.cuh"),
+           os.path.join(ROOT, "fractodactyl_b200", "csrc", "fd_device.cuh")]
+    if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(s) for s in src):
+        subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-Wno-unknown-pragmas",
+                        "-I", os.path.join(HERE, "emu"), "-I", os.path.join(ROOT, "fractodactyl_b200", "csrc"),
+                        src[0], "-o", LIB], check=True)
+    L = C.CDLL(LIB)
+    P, D, U32, U64, I32, I64 = C.c_void_p, C.c_double, C.c_uint32, C.c_uint64, C.c_int32, C.c_int64
+    L.emu_render.restype = C.c_int
+    L.emu_render.argtypes = [P, P, U64, P, P, U32, P, U32, U32, D, P, I32, U32, U32, U32, U32, D, D, D, I64, D, D,
+                             U32, D, I64] + [P] * 12 + [P]
+    return L
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+def emulate(emu, r, plane, tier, p, flags, bla=None, series=None, q=None, nucleus=None):
+    n = p.nx * p.ny
+    out = dict(cls=np.zeros(n, np.uint8), n=np.zeros(n, np.uint32), nu=np.zeros(n), de=np.zeros(n, np.float32),
+               normal=np.zeros(n, np.uint16), z=np.zeros((n, 2)), dz=np.zeros((n, 2)), dexp=np.zeros(n, np.int64),
+               status=np.zeros(n, np.uint8), bound=np.zeros(n, np.float32), ez=np.zeros(n), ed=np.zeros(n))
+    cnt = np.zeros(6, np.uint64)
+    re_, im_ = np.ascontiguousarray(r.re), np.ascontiguousarray(r.im)
+    blocks = offs = sb = None
+    if bla is not None:
+        blocks = np.ascontiguousarray(bla.blocks)
+        offs = np.ascontiguousarray(bla.level_offsets, dtype=np.uint64)
+    if series is not None:
+        sb = np.ascontiguousarray(series.b, dtype=np.float64)
+    nuc = r.nucleus_period() if nucleus is None else nucleus
+    rc = emu.emu_render(_ptr(re_), _ptr(im_), len(re_), _ptr(blocks), _ptr(offs), bla.levels if bla else 0, _ptr(sb),
+                        len(sb) if sb is not None else 0, series.n if series else 0, series.rho if series else 0.0,
+                        _ptr(q), tier, flags, p.nx, p.ny, p.ss, plane.c_re, plane.c_im, plane.h_m, plane.h_e,
+                        plane.cos_rot, plane.sin_rot, p.max_iter, p.escape_radius, -1 if nuc is None else nuc,
+                        *[_ptr(out[k]) for k in ("cls", "n", "nu", "de", "normal", "z", "dz", "dexp", "status", "bound",
+                                                 "ez", "ed")], _ptr(cnt))
+    assert rc == 0
+    out["counters"] = dict(zip(("samples", "iterations", "blocks", "skipped", "fallback_samples",
+                                "closed_form_samples"), (int(c) for c in cnt)))
+    return out
+
+
+def _setup(view3, nx, ny, max_iter, tier=None, columns=("nu", "de", "normal")):
+    v = fd.View(*view3)
+    p = fd.Params(nx, ny, max_iter=max_iter, columns=columns, tier=tier)
+    plane, t = fd.route._setup(v, p)
+    r, bits = fd.reference(v, p)
+    r.bits = bits
+    plane.bits = bits
+    return v, p, plane, t, r
+
+
+def _oracle_job(view3, p, tier, columns):
+    return fdref.make_job(*view3, p.nx, p.ny, p.max_iter, escape_radius=p.escape_radius, columns=columns, tier=tier,
+                          threads=2)
+
+
+def _check(got, want, counters=True, escaped=True):
+    assert np.array_equal(got["cls"], want["cls"])
+    assert np.array_equal(got["n"], want["n"].astype(np.uint32))
+    esc = (want["cls"] & 3) == 0
+    assert esc.any() or not escaped
+    for k in ("z", "dz", "dexp"):
+        if k in want:
+            assert np.array_equal(got[k][esc], want[k][esc]), k
+    assert np.array_equal(got["nu"][esc], want["nu"][esc])
+    assert np.array_equal(got["de"][esc], want["de"][esc])
+    assert np.all(np.abs(got["normal"][esc].astype(np.int64) - want["normal"][esc]) <= 1)
+    assert got["status"].all()
+    if counters:
+        st = want["stats"]
+        for k in ("iterations", "blocks", "skipped", "fallback_samples", "closed_form_samples"):
+            assert got["counters"][k] == st[k], k
+
+
+@pytest.mark.parametrize("case", ["f64", "f64-bla", "fixed-bla", "scaled-bla", "scaled-nod"])
+def test_kernel_equals_oracle(emu, case):
+    eps = fd.route.EPS
+    if case == "f64":
+        view3, nx, ny, it, tier = ("-0.7453", "0.1127", "0.0065"), 40, 24, 4_000, None
+    elif case == "f64-bla":  # F64-tier depths admit no block at eps 2^-50: a looser table
+        view3, nx, ny, it, tier, eps = (*SEAHORSE, "1e-10"), 40, 24, 20_000, None, 2.0 ** -30
+    elif case == "fixed-bla":  # a series frame deep enough for eps 2^-50 blocks
+        f = KATS["series_frames"][18]
+        view3, nx, ny, it, tier = (f["re"], f["im"], f["width"]), 33, 19, 10_000, None
+    else:
+        view3, nx, ny, it, tier = ("0", "1", "1e-300"), 32, 16, 5_000, None
+    bla = "bla" in case
+    cols = ("nu",) if case == "scaled-nod" else ("nu", "de", "normal")
+    v, p, plane, t, r = _setup(view3, nx, ny, it, tier, cols)
+    table = None
+    if bla:
+        dc, e = fd.bla_dc_bound(v, p)
+        table = fd.Bla.build_scaled(r, eps, dc, e)
+        assert table.levels > 0
+    flags = (1 if p.needs_derivative() else 0) | (2 if bla else 0)
+    got = emulate(emu, r, plane, t, p, flags, bla=table)
+    ref = fdref.Ref.arrays(r.re, r.im, r.bits)
+    ob = fdref.Bla(ref, eps, table.dc_max, table.dc_exp) if bla else None
+    ocols = fdref.COL_NU | (fdref.COL_DE | fdref.COL_NORMAL if p.needs_derivative() else 0)
+    want = fdref.render(_oracle_job(view3, p, t, ocols), ref, ob, raw=True)
+    if not p.needs_derivative():  # the oracle's dz without the derivative is not a column
+        want.pop("dz")
+        want.pop("dexp")
+        got["de"][:] = want["de"]
+        got["normal"][:] = want["normal"]
+    _check(got, want)
+    if bla:
+        assert got["counters"]["blocks"] > 0
+
+
+@pytest.mark.parametrize("frame", [18, -1])
+def test_kernel_series_start_equals_oracle(emu, frame):
+    """Frame 18 (BLA blocks, a few unresolved starts) and the nucleus frame, whose series
+    admits 9,999 of 10,000 iterations so nearly every sample retries from zero."""
+    f = KATS["series_frames"][frame]
+    view3 = (f["re"], f["im"], f["width"])
+    v, p, plane, t, r = _setup(view3, 33, 19, 10_000)
+    rho, e = fd.bla_dc_bound(v, p)
+    series = fd.Series.build(r, rho, float(f["width"]) / 33, p.max_iter)
+    assert series.n > 0
+    ref = fdref.Ref.arrays(r.re, r.im, r.bits)
+    o_series = fdref.Series(ref, rho, float(f["width"]) / 33, p.max_iter)
+    table = ob = None
+    if frame == 18:
+        table = fd.Bla.build_scaled(r, fd.route.EPS, rho, 0)
+        ob = fdref.Bla(ref, fd.route.EPS, rho, 0)
+    got = emulate(emu, r, plane, t, p, 1 | (2 if table else 0) | 4, bla=table, series=series)
+    want = fdref.render_series(_oracle_job(view3, p, t, fdref.COL_NU | fdref.COL_DE | fdref.COL_NORMAL), ref,
+                               o_series, bla=ob, raw=True)
+    _check(got, want, escaped=frame == 18)  # the nucleus frame has no escaping sample
+    if frame == -1:
+        assert (got["cls"] & 3 == 1).any()  # its interior survives the retries (series.rs:644-693)
+
+
+@pytest.mark.parametrize("view3,max_iter", [(("-0.7453", "0.1127", "0.0065"), 4_000),
+                                           ((*SEAHORSE, "1e-14"), 20_000)])
+def test_kernel_bounded_equals_oracle(emu, view3, max_iter):
+    v, p, plane, t, r = _setup(view3, 40, 24, max_iter, columns=("nu", "de", "bound"))
+    q = r.error_radius(None if t == 0 else r.bits, plane.c_re, plane.c_im)
+    got = emulate(emu, r, plane, t, p, 1 | 8, q=q)
+    ref = fdref.Ref.arrays(r.re, r.im, r.bits)
+    want = fdref.render_columns(_oracle_job(view3, p, t, fdref.COL_NU | fdref.COL_DE | fdref.COL_BOUND), ref)
+    esc = (want["cls"] & 3) == 0
+    assert (want["cls"] == 4).sum() > 0.5 * esc.sum()
+    for k in ("cls", "bound"):
+        assert np.array_equal(got[k], want[k]), k
+    assert np.array_equal(got["n"], want["n"].astype(np.uint32))
+    for k in ("z", "ez", "ed", "nu", "de"):
+        assert np.array_equal(got[k][esc], want[k][esc]), k
+    assert got["counters"]["iterations"] == want["stats"]["iterations"]
