@@ -181,3 +181,49 @@ def test_kernel_bounded_equals_oracle(emu, view3, max_iter):
     for k in ("z", "ez", "ed", "nu", "de"):
         assert np.array_equal(got[k][esc], want[k][esc]), k
     assert got["counters"]["iterations"] == want["stats"]["iterations"]
+
+
+def test_kernel_fuzz_equals_oracle(emu):
+    """Seeded random frames on structure at every depth (the seeded nucleus locations of
+    1e-20 .. 1e-1000 and the reference's series frames, each at a random multiple of its
+    width, plus classic shallow views; every tier, derivative and BLA on or off): the
+    emulated kernel equals the oracle on each."""
+    from fractodactyl_b200 import locations
+    rng = np.random.default_rng(20261203)
+    views = [(d["re"], d["im"], float(d["log10_width"])) for d in locations.cached("c5")]
+    views += [(f["re"], f["im"], float(np.log10(float(f["width"])))) for f in KATS["series_frames"]]
+    views += [("-0.7453", "0.1127", np.log10(0.0065)), (*SEAHORSE, -10.0), ("-0.1011", "0.9563", -3.0)]
+    kinds, tiers, blocks = set(), set(), 0
+    for case in range(36):
+        re_, im_, lw = views[int(rng.integers(0, len(views)))]
+        width = f"{10 ** (lw % 1) * rng.uniform(0.5, 4):.4f}e{int(np.floor(lw))}"
+        max_iter = int(rng.integers(2_000, 20_000))
+        deriv, bla = bool(rng.integers(0, 2)), bool(rng.integers(0, 2))
+        cols = ("nu", "de", "normal") if deriv else ("nu",)
+        view3 = (re_, im_, width)
+        v, p, plane, t, r = _setup(view3, 12, 8, max_iter, None, cols)
+        table = ob = None
+        if bla:
+            dc, e = fd.bla_dc_bound(v, p)
+            table = fd.Bla.build_scaled(r, fd.route.EPS if t else 2.0 ** -30, dc, e)
+            if table.levels == 0:
+                table = None
+        got = emulate(emu, r, plane, t, p, (1 if deriv else 0) | (2 if table else 0), bla=table)
+        ref = fdref.Ref.arrays(r.re, r.im, r.bits)
+        if table is not None:
+            ob = fdref.Bla(ref, table.eps, table.dc_max, table.dc_exp)
+        ocols = fdref.COL_NU | (fdref.COL_DE | fdref.COL_NORMAL if deriv else 0)
+        want = fdref.render(_oracle_job(view3, p, t, ocols), ref, ob, raw=True)
+        assert np.array_equal(got["cls"], want["cls"]), (case, view3, max_iter, deriv, bla)
+        assert np.array_equal(got["n"], want["n"].astype(np.uint32)), (case, view3)
+        esc = (want["cls"] & 3) == 0
+        assert np.array_equal(got["z"][esc], want["z"][esc]), (case, view3)
+        if deriv:
+            assert np.array_equal(got["dz"][esc], want["dz"][esc]) and np.array_equal(got["dexp"][esc],
+                                                                                     want["dexp"][esc]), (case, view3)
+        for k in ("iterations", "blocks", "skipped"):
+            assert got["counters"][k] == want["stats"][k], (case, view3, k)
+        kinds |= set(np.unique(want["cls"] & 3).tolist())
+        tiers.add(t)
+        blocks += want["stats"]["blocks"]
+    assert kinds == {0, 1, 2} and tiers == {0, 1, 2} and blocks > 0  # the draw covers every path
