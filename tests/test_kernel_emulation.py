@@ -227,3 +227,55 @@ def test_kernel_fuzz_equals_oracle(emu):
         tiers.add(t)
         blocks += want["stats"]["blocks"]
     assert kinds == {0, 1, 2} and tiers == {0, 1, 2} and blocks > 0  # the draw covers every path
+
+
+def test_kernel_fuzz_series_and_bounded_equal_oracle(emu):
+    """Seeded random ordinary-tier frames on the same locations, started from their
+    parameter series (BLA on or off) or rendered bounded: the emulated kernel equals the
+    oracle's render_series / bounded render on each."""
+    from fractodactyl_b200 import locations
+    rng = np.random.default_rng(20261204)
+    views = [(d["re"], d["im"], float(d["log10_width"])) for d in locations.cached("c5")
+             if float(d["log10_width"]) > -260]
+    views += [(f["re"], f["im"], float(np.log10(float(f["width"])))) for f in KATS["series_frames"]]
+    views += [(*SEAHORSE, -10.0), (*SEAHORSE, -14.0)]
+    started, bounded_samples = 0, 0
+    for case in range(24):
+        re_, im_, lw = views[int(rng.integers(0, len(views)))]
+        width = f"{10 ** (lw % 1) * rng.uniform(0.5, 4):.4f}e{int(np.floor(lw))}"
+        max_iter = int(rng.integers(2_000, 20_000))
+        view3 = (re_, im_, width)
+        if case % 2 == 0:  # series start
+            v, p, plane, t, r = _setup(view3, 11, 7, max_iter)
+            if t == 2:
+                continue
+            rho, _ = fd.bla_dc_bound(v, p)
+            pixel = float(width) / 11
+            series = fd.Series.build(r, rho, pixel, max_iter)
+            if series.n == 0:
+                continue
+            ref = fdref.Ref.arrays(r.re, r.im, r.bits)
+            table = fd.Bla.build_scaled(r, fd.route.EPS, rho, 0) if rng.integers(0, 2) else None
+            table = table if table is not None and table.levels else None
+            ob = fdref.Bla(ref, fd.route.EPS, rho, 0) if table is not None else None
+            got = emulate(emu, r, plane, t, p, 1 | (2 if table else 0) | 4, bla=table, series=series)
+            want = fdref.render_series(_oracle_job(view3, p, t, fdref.COL_NU | fdref.COL_DE | fdref.COL_NORMAL),
+                                       ref, fdref.Series(ref, rho, pixel, max_iter), bla=ob, raw=True)
+            _check(got, want, escaped=False)
+            started += 1
+        else:  # bounded
+            v, p, plane, t, r = _setup(view3, 11, 7, max_iter, columns=("nu", "de", "bound"))
+            if t == 2:
+                continue
+            q = r.error_radius(None if t == 0 else r.bits, plane.c_re, plane.c_im)
+            got = emulate(emu, r, plane, t, p, 1 | 8, q=q)
+            want = fdref.render_columns(_oracle_job(view3, p, t, fdref.COL_NU | fdref.COL_DE | fdref.COL_BOUND),
+                                        fdref.Ref.arrays(r.re, r.im, r.bits))
+            for k in ("cls", "bound"):
+                assert np.array_equal(got[k], want[k]), (case, view3, k)
+            assert np.array_equal(got["n"], want["n"].astype(np.uint32)), (case, view3)
+            esc = (want["cls"] & 3) == 0
+            for k in ("z", "ez", "ed", "de"):
+                assert np.array_equal(got[k][esc], want[k][esc]), (case, view3, k)
+            bounded_samples += int((want["cls"] == 4).sum())
+    assert started >= 4 and bounded_samples > 0
