@@ -39,14 +39,24 @@ def emu():
     L.emu_render.restype = C.c_int
     L.emu_render.argtypes = [P, P, U64, P, P, U32, P, U32, U32, D, P, I32, U32, U32, U32, U32, D, D, D, I64, D, D,
                              U32, D, I64] + [P] * 12 + [P]
+    L.emu_render_window.restype = C.c_int
+    L.emu_render_window.argtypes = L.emu_render.argtypes + [C.POINTER(Window)]
     return L
+
+
+class Window(C.Structure):
+    """emu.cpp's EmuWindow: fdc_job's window, mask and offsets (whole-frame arrays), the
+    tile width 2^tile_shift and the tile order (0 row-major, 1 reversed)."""
+    _fields_ = [("first_row", C.c_uint32), ("rows", C.c_uint32), ("first_col", C.c_uint32), ("cols", C.c_uint32),
+                ("tile_shift", C.c_uint32), ("tile_order", C.c_uint32), ("mask", C.c_void_p),
+                ("offsets", C.c_void_p)]
 
 
 def _ptr(a):
     return None if a is None else a.ctypes.data
 
 
-def emulate(emu, r, plane, tier, p, flags, bla=None, series=None, q=None, nucleus=None):
+def emulate(emu, r, plane, tier, p, flags, bla=None, series=None, q=None, nucleus=None, win=None):
     n = p.nx * p.ny
     out = dict(cls=np.zeros(n, np.uint8), n=np.zeros(n, np.uint32), nu=np.zeros(n), de=np.zeros(n, np.float32),
                normal=np.zeros(n, np.uint16), z=np.zeros((n, 2)), dz=np.zeros((n, 2)), dexp=np.zeros(n, np.int64),
@@ -60,12 +70,13 @@ def emulate(emu, r, plane, tier, p, flags, bla=None, series=None, q=None, nucleu
     if series is not None:
         sb = np.ascontiguousarray(series.b, dtype=np.float64)
     nuc = r.nucleus_period() if nucleus is None else nucleus
-    rc = emu.emu_render(_ptr(re_), _ptr(im_), len(re_), _ptr(blocks), _ptr(offs), bla.levels if bla else 0, _ptr(sb),
-                        len(sb) if sb is not None else 0, series.n if series else 0, series.rho if series else 0.0,
-                        _ptr(q), tier, flags, p.nx, p.ny, p.ss, plane.c_re, plane.c_im, plane.h_m, plane.h_e,
-                        plane.cos_rot, plane.sin_rot, p.max_iter, p.escape_radius, -1 if nuc is None else nuc,
-                        *[_ptr(out[k]) for k in ("cls", "n", "nu", "de", "normal", "z", "dz", "dexp", "status", "bound",
-                                                 "ez", "ed")], _ptr(cnt))
+    args = (_ptr(re_), _ptr(im_), len(re_), _ptr(blocks), _ptr(offs), bla.levels if bla else 0, _ptr(sb),
+            len(sb) if sb is not None else 0, series.n if series else 0, series.rho if series else 0.0,
+            _ptr(q), tier, flags, p.nx, p.ny, p.ss, plane.c_re, plane.c_im, plane.h_m, plane.h_e,
+            plane.cos_rot, plane.sin_rot, p.max_iter, p.escape_radius, -1 if nuc is None else nuc,
+            *[_ptr(out[k]) for k in ("cls", "n", "nu", "de", "normal", "z", "dz", "dexp", "status", "bound",
+                                     "ez", "ed")], _ptr(cnt))
+    rc = emu.emu_render(*args) if win is None else emu.emu_render_window(*args, C.byref(win))
     assert rc == 0
     out["counters"] = dict(zip(("samples", "iterations", "blocks", "skipped", "fallback_samples",
                                 "closed_form_samples"), (int(c) for c in cnt)))
@@ -279,3 +290,90 @@ def test_kernel_fuzz_series_and_bounded_equal_oracle(emu):
                 assert np.array_equal(got[k][esc], want[k][esc]), (case, view3, k)
             bounded_samples += int((want["cls"] == 4).sum())
     assert started >= 4 and bounded_samples > 0
+
+
+def _grid_offsets(plane, nx, ny):
+    """Every sample's unit offset from the centre, as the kernel derives it from the grid
+    (view.rs:118-122), frame-major (nx*ny, 2)."""
+    j, i = np.meshgrid(np.arange(ny, dtype=np.float64), np.arange(nx, dtype=np.float64), indexing="ij")
+    x = i + 0.5 - nx / 2.0
+    y = j + 0.5 - ny / 2.0
+    ux = plane.cos_rot * x + plane.sin_rot * y
+    uy = plane.sin_rot * x - plane.cos_rot * y
+    return np.ascontiguousarray(np.stack([ux.ravel(), uy.ravel()], axis=1))
+
+
+@pytest.mark.parametrize("case", ["f64-bla", "fixed-bla", "scaled"])
+def test_kernel_window_mask_offsets_equal_oracle(emu, case):
+    """The job inputs the other emulation tests leave at their defaults: a window of rows and
+    columns, a mask, 4x8 tiles handed out in reverse order, and per-sample offsets. The
+    windowed, masked render writes exactly the selected samples, each equal to the oracle's
+    masked render (columns and work counters), and nothing else; offsets equal to the grid's
+    own positions reproduce the grid render bit for bit; jittered offsets equal the oracle's
+    iteration of each sample at its own offset."""
+    rng = np.random.default_rng(20261205)
+    eps = fd.route.EPS
+    if case == "f64-bla":
+        view3, nx, ny, it, eps = (*SEAHORSE, "1e-10"), 40, 24, 20_000, 2.0 ** -30
+    elif case == "fixed-bla":
+        f = KATS["series_frames"][18]
+        view3, nx, ny, it = (f["re"], f["im"], f["width"]), 33, 19, 10_000
+    else:
+        view3, nx, ny, it = ("0", "1", "1e-300"), 32, 16, 5_000
+    v, p, plane, t, r = _setup(view3, nx, ny, it)
+    table = ob = None
+    ref = fdref.Ref.arrays(r.re, r.im, r.bits)
+    if "bla" in case:
+        dc, e = fd.bla_dc_bound(v, p)
+        table = fd.Bla.build_scaled(r, eps, dc, e)
+        assert table.levels > 0
+        ob = fdref.Bla(ref, eps, table.dc_max, table.dc_exp)
+    flags = 1 | (2 if table else 0)
+    full = emulate(emu, r, plane, t, p, flags, bla=table)
+    r0, rows, c0, cols = 3, ny - 8, 5, nx - 11
+    inwin = np.zeros((ny, nx), bool)
+    inwin[r0:r0 + rows, c0:c0 + cols] = True
+    inwin = inwin.ravel()
+    mask = (rng.random(nx * ny) < 0.6).astype(np.uint8)
+    sel = inwin & (mask != 0)
+    win = Window(r0, rows, c0, cols, 2, 1, mask.ctypes.data, None)
+    got = emulate(emu, r, plane, t, p, flags, bla=table, win=win)
+    want = fdref.render_columns(_oracle_job(view3, p, t, fdref.COL_NU | fdref.COL_DE | fdref.COL_NORMAL), ref, ob,
+                                mask=sel.astype(np.uint8))
+    assert sel.sum() > 0.3 * inwin.sum()
+    assert np.array_equal(got["status"] != 0, sel)
+    assert not got["cls"][~sel].any() and not got["n"][~sel].any() and not got["z"][~sel].any()
+    assert np.array_equal(got["cls"][sel], want["cls"][sel])
+    assert np.array_equal(got["n"][sel], want["n"][sel].astype(np.uint32))
+    esc = sel & ((want["cls"] & 3) == 0)
+    assert esc.any()
+    for k in ("z", "dz", "dexp", "nu", "de"):
+        assert np.array_equal(got[k][esc], want[k][esc]), k
+        assert np.array_equal(got[k][sel], full[k][sel]), k
+    for k in ("iterations", "blocks", "skipped", "fallback_samples", "closed_form_samples"):
+        assert got["counters"][k] == want["stats"][k], k
+    # offsets at the grid's own positions: the grid render, over the window
+    grid = _grid_offsets(plane, nx, ny)
+    got = emulate(emu, r, plane, t, p, flags, bla=table, win=Window(r0, rows, c0, cols, 3, 0, None, grid.ctypes.data))
+    for k in ("cls", "n", "z", "dz", "dexp", "nu", "de", "normal"):
+        assert np.array_equal(got[k][inwin], full[k][inwin]), k
+    assert np.array_equal(got["status"] != 0, inwin)
+    # jittered offsets: each sample is the oracle's iteration at its own offset
+    jit = np.ascontiguousarray(grid + rng.uniform(-0.5, 0.5, grid.shape))
+    got = emulate(emu, r, plane, t, p, flags, bla=table, win=Window(r0, rows, c0, cols, 5, 1, None, jit.ctypes.data))
+    h = np.ldexp(plane.h_m, plane.h_e)
+    kinds = {"escaped": 0, "interior": 1, "unresolved": 2}
+    for k in np.flatnonzero(inwin):
+        ux, uy = jit[k]
+        if t == 2:
+            o = fdref.iterate(ref, ob, extended=True, ar=ux * plane.h_m, ai=uy * plane.h_m, offset_exp=plane.h_e,
+                              max_iter=it, r2=p.escape_radius ** 2)
+        else:
+            ar, ai = ux * h, uy * h
+            o = fdref.iterate(ref, ob, c=(plane.c_re + ar, plane.c_im + ai) if t == 0 else None, ar=ar, ai=ai,
+                              max_iter=it, r2=p.escape_radius ** 2)
+        assert got["cls"][k] & 3 == kinds[o["kind"]], k
+        assert got["n"][k] == (it if o["kind"] == "unresolved" else o["n"]), k
+        if o["kind"] == "escaped":
+            assert tuple(got["z"][k]) == (o["zr"], o["zi"]) and tuple(got["dz"][k]) == (o["dr"], o["di"]), k
+            assert got["dexp"][k] == o["dexp"], k
