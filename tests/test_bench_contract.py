@@ -1,0 +1,62 @@
+"""bench.py's output contract on the CPU: the reference arm (the CPU kernel timed on a
+bounded sample of the workload's rows) prints one JSON line with every key the bench
+line carries, its cpu_baseline and e2e describing that same run; under a multi-rank
+launch only rank 0 prints; and the CUDA arm, given no device, fails with a non-zero exit
+and no bench line instead of falling back to the CPU."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+BENCH = os.path.join(ROOT, "bench.py")
+
+
+def _run(args, env=None, timeout=300):
+    e = dict(os.environ)
+    e.update(env or {})
+    return subprocess.run([sys.executable, BENCH, *args], cwd=ROOT, env=e, capture_output=True, text=True,
+                          timeout=timeout)
+
+
+def test_reference_arm_line():
+    r = _run(["--impl", "reference", "--config", "1", "--steps", "2", "--warmup", "3", "--cpu-seconds", "0.5"])
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    line = json.loads(lines[0])
+    sys.path.insert(0, ROOT)
+    import bench
+    assert line["metric"] == bench.METRIC and line["unit"] == bench.UNIT
+    assert line["impl"] == "reference"
+    assert line["value"] > 0 and line["ms_per_step"] > 0
+    assert (line["n_gpus"], line["steps"], line["warmup"]) == (1, 2, 3)
+    assert line["higher_is_better"] is True and line["scaling"] == "weak" and line["vs_baseline"] is None
+    assert line["dtype"] == "f64" and line["data"].startswith("synthetic")
+    cfg = line["config"]
+    assert cfg["workload"].startswith("c1-") and (cfg["nx"], cfg["ny"], cfg["max_iter"]) == (480, 270, 20_000)
+    assert 0 < cfg["sample_rows"] <= cfg["ny"]
+    cb = line["cpu_baseline"]
+    assert cb["value"] == line["value"] and cb["unit"] == line["unit"] and cb["kind"] in ("port", "reference")
+    assert cb["cores"] >= 1 and cb["sample"]
+    assert line["e2e"] == {"value": line["value"], "unit": line["unit"], "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
+
+
+def test_reference_arm_other_ranks_silent():
+    r = _run(["--impl", "reference", "--config", "1", "--steps", "1", "--warmup", "3"],
+             env={"RANK": "1", "LOCAL_RANK": "1", "WORLD_SIZE": "2"})
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.strip() == ""
+
+
+def test_cuda_arm_fails_without_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    r = _run(["--config", "1", "--steps", "1", "--warmup", "3", "--no-cpu"])
+    assert r.returncode != 0
+    assert not [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
+    assert "NO_DEVICE" in r.stderr or "CUDA" in r.stderr
