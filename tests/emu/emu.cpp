@@ -1,32 +1,20 @@
-// The plain-form persistent kernel (fractodactyl_b200/csrc/perturb_f64.cuh) compiled for
-// the host through cuda_host_shim.hpp and run on one thread as a single-lane warp over
-// every sample of a frame, with its inputs packed as the route packs them on the device
-// (pack_orbit / pack_bla / fuse_bla in fdcuda.cu). The kernel-emulation tests compare its
-// outputs with the oracle's on the CPU.
+// The plain-form persistent kernels (fractodactyl_b200/csrc/perturb_f64.cuh: the frame
+// kernel and the batch kernel) compiled for the host through cuda_host_shim.hpp and run on
+// one thread as a single-lane warp over every sample, with their inputs packed as the
+// route packs them on the device (pack_orbit / pack_bla / fuse_bla, prepare and
+// fdc_batch_create in fdcuda.cu). The kernel-emulation tests compare their outputs with
+// the oracle's on the CPU.
 // TEST INFRASTRUCTURE ONLY.
-#include "cuda_host_shim.hpp"
-
+// the standard headers first: the shim defines __noinline__, which libstdc++ uses
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <map>
+#include <memory>
 #include <vector>
 
+#include "cuda_host_shim.hpp"
 #include "perturb_f64.cuh"
-
-namespace {
-
-struct Inputs {
-  std::vector<double2> z, fused, coef, ab;
-  std::vector<double> r2;
-};
-
-template <bool EXT, bool D, bool L, bool S, bool B>
-void launch(fdk::Params &p) {
-  threadIdx.x = 0;
-  blockIdx.x = 0;
-  fdk::perturb_kernel<EXT, D, L, S, B>(p);
-}
-
-}  // namespace
 
 extern "C" {
 
@@ -40,89 +28,120 @@ struct EmuWindow {
   const double *offsets;
 };
 
-// One frame: tier 0 / 1 / 2, flags bit 0 derivative, bit 1 BLA, bit 2 series start, bit 3
-// bounded. blocks7 / level_offsets / levels: the BLA table in its export layout (or null);
-// series_b (b_1..b_order as re, im), series_n, series_rho; q: error radii (bounded).
-// Outputs (any null): class, n, nu, de, normal, z, dz, dexp, status, bound, ez, ed;
-// counters[6] = samples, iterations, blocks, skipped, fallback, closed-form.
-int emu_render_window(const double *re, const double *im, uint64_t len, const double *blocks7,
-                      const uint64_t *level_offsets, uint32_t levels, const double *series_b, uint32_t series_order,
-                      uint32_t series_n, double series_rho, const double *q, int32_t tier, uint32_t flags, uint32_t nx,
-                      uint32_t ny, uint32_t ss, double c_re, double c_im, double h_m, int64_t h_e, double cos_rot,
-                      double sin_rot, uint32_t max_iter, double escape_radius, int64_t nucleus, uint8_t *cls,
-                      uint32_t *n_out, double *nu, float *de, uint16_t *normal, double *z_out, double *dz_out,
-                      int64_t *dexp_out, uint8_t *status, float *bound, double *ez, double *ed, uint64_t *counters,
-                      const EmuWindow *win);
+// One job of a batch (fdc_job plus its orbit, BLA table and fdc_out): the orbit as re / im
+// arrays, the BLA table in its export layout (or null), the frame, the row and column
+// window (0 rows / cols: to the edge), whole-frame outputs (any null) and, returned, the
+// job's counters (samples, iterations, blocks, skipped, fallback, closed-form).
+struct EmuJob {
+  const double *re, *im;
+  uint64_t len;
+  const double *blocks7;
+  const uint64_t *level_offsets;
+  uint32_t levels;
+  int32_t tier;
+  uint32_t flags;  // bit 0 derivative, bit 1 BLA
+  uint32_t nx, ny, ss, max_iter;
+  double c_re, c_im, h_m;
+  int64_t h_e;
+  double cos_rot, sin_rot, escape_radius;
+  int64_t nucleus;
+  uint32_t first_row, rows, first_col, cols;
+  uint8_t *cls;
+  uint32_t *n;
+  double *nu;
+  float *de;
+  uint16_t *normal;
+  double *z, *dz;
+  int64_t *dexp;
+  uint8_t *status;
+  uint64_t counters[6];
+};
 
-int emu_render(const double *re, const double *im, uint64_t len, const double *blocks7, const uint64_t *level_offsets,
-               uint32_t levels, const double *series_b, uint32_t series_order, uint32_t series_n, double series_rho,
-               const double *q, int32_t tier, uint32_t flags, uint32_t nx, uint32_t ny, uint32_t ss, double c_re,
-               double c_im, double h_m, int64_t h_e, double cos_rot, double sin_rot, uint32_t max_iter,
-               double escape_radius, int64_t nucleus, uint8_t *cls, uint32_t *n_out, double *nu, float *de,
-               uint16_t *normal, double *z_out, double *dz_out, int64_t *dexp_out, uint8_t *status, float *bound,
-               double *ez, double *ed, uint64_t *counters) {
-  return emu_render_window(re, im, len, blocks7, level_offsets, levels, series_b, series_order, series_n, series_rho, q,
-                           tier, flags, nx, ny, ss, c_re, c_im, h_m, h_e, cos_rot, sin_rot, max_iter, escape_radius,
-                           nucleus, cls, n_out, nu, de, normal, z_out, dz_out, dexp_out, status, bound, ez, ed, counters,
-                           nullptr);
+}  // extern "C"
+
+namespace {
+
+// A job's Params and the staged arrays they point into.
+struct Setup {
+  std::vector<double2> z, fused, coef, ab, offs;
+  std::vector<double> r2;
+  std::vector<uint8_t> mask;
+  std::vector<uint32_t> order;
+  fdk::Params p{};
+  bool ext = false, deriv = false, bla = false;
+};
+
+template <bool EXT, bool D, bool L, bool S, bool B>
+void launch(fdk::Params &p) {
+  threadIdx.x = 0;
+  blockIdx.x = 0;
+  fdk::perturb_kernel<EXT, D, L, S, B>(p);
 }
 
-int emu_render_window(const double *re, const double *im, uint64_t len, const double *blocks7,
-                      const uint64_t *level_offsets, uint32_t levels, const double *series_b, uint32_t series_order,
-                      uint32_t series_n, double series_rho, const double *q, int32_t tier, uint32_t flags, uint32_t nx,
-                      uint32_t ny, uint32_t ss, double c_re, double c_im, double h_m, int64_t h_e, double cos_rot,
-                      double sin_rot, uint32_t max_iter, double escape_radius, int64_t nucleus, uint8_t *cls,
-                      uint32_t *n_out, double *nu, float *de, uint16_t *normal, double *z_out, double *dz_out,
-                      int64_t *dexp_out, uint8_t *status, float *bound, double *ez, double *ed, uint64_t *counters,
-                      const EmuWindow *win) {
-  const bool ext = tier == 2, deriv = flags & 1, bla = (flags & 2) && levels > 0, series = (flags & 4) && series_n > 0,
-             bounded = (flags & 8) && !ext;
-  if (len < 3 || (bla && bounded) || (series && (ext || bounded))) return -1;  // the route's refusals
-  Inputs in;
-  in.z.resize(len);
-  for (uint64_t m = 0; m < len; ++m) in.z[m] = make_double2(re[m], im[m]);
-  fdk::Params p{};
-  p.orbit = in.z.data();
+template <bool EXT, bool D, bool L>
+void launch_batch(const std::vector<fdk::Params> &jobs, const std::vector<unsigned long long> &starts,
+                  fdk::Counters *per_job, uint32_t defer) {
+  threadIdx.x = 0;
+  blockIdx.x = 0;
+  unsigned long long queue = 0;
+  fdk::perturb_batch_kernel<EXT, D, L>(jobs.data(), starts.data(), (uint32_t)jobs.size(), starts.back(), &queue,
+                                       per_job, defer);
+}
+
+// The orbit (pack_orbit) and BLA table (pack_bla, fuse_bla) of a job.
+void stage_orbit(Setup &s, const double *re, const double *im, uint64_t len, const double *blocks7,
+                 const uint64_t *level_offsets, uint32_t levels) {
+  fdk::Params &p = s.p;
+  s.z.resize(len);
+  for (uint64_t m = 0; m < len; ++m) s.z[m] = make_double2(re[m], im[m]);
+  p.orbit = s.z.data();
   p.last = (uint32_t)(len - 1);
   p.z0r = re[0];
   p.z0i = im[0];
-  if (bla) {  // pack_bla and fuse_bla
-    const uint64_t steps = len - 2, total = level_offsets[levels];
-    in.r2.resize(total);
-    in.coef.resize(2 * total);
-    in.ab.resize(total);
-    for (uint64_t k = 0; k < total; ++k) {
-      const double *w = blocks7 + 7 * k;
-      in.r2[k] = w[4] * w[4];
-      in.coef[2 * k] = make_double2(w[0], w[1]);
-      in.coef[2 * k + 1] = make_double2(w[2], w[3]);
-      in.ab[k] = make_double2(w[5], w[6]);
-    }
-    p.bla_levels = levels;
-    for (uint32_t i = 0; i < levels; ++i) {
-      p.bla_off[i] = (uint32_t)level_offsets[i];
-      p.bla_count[i] = (uint32_t)(steps >> (i + 1));
-    }
-    in.fused.resize(2 * len);
-    for (uint64_t m = 0; m < len; ++m) {
-      double a = -1.0, b = -1.0;
-      if (m >= 1 && levels > 0 && ((m - 1) & 1) == 0 && ((m - 1) >> 1) < p.bla_count[0])
-        a = in.r2[p.bla_off[0] + ((m - 1) >> 1)];
-      if (m >= 1 && levels > 1 && ((m - 1) & 3) == 0 && ((m - 1) >> 2) < p.bla_count[1])
-        b = in.r2[p.bla_off[1] + ((m - 1) >> 2)];
-      in.fused[2 * m] = in.z[m];
-      in.fused[2 * m + 1] = make_double2(a, b);
-    }
-    p.fused = in.fused.data();
-    p.bla_r2 = in.r2.data();
-    p.bla_coef = in.coef.data();
-    p.bla_ab = in.ab.data();
+  if (!s.bla) return;
+  const uint64_t steps = len - 2, total = level_offsets[levels];
+  s.r2.resize(total);
+  s.coef.resize(2 * total);
+  s.ab.resize(total);
+  for (uint64_t k = 0; k < total; ++k) {
+    const double *w = blocks7 + 7 * k;
+    s.r2[k] = w[4] * w[4];
+    s.coef[2 * k] = make_double2(w[0], w[1]);
+    s.coef[2 * k + 1] = make_double2(w[2], w[3]);
+    s.ab[k] = make_double2(w[5], w[6]);
   }
-  // the frame and window (prepare in fdcuda.cu); tiles of 2^shift x 32/2^shift samples
-  const uint32_t r0 = win ? win->first_row : 0, rows = win && win->rows ? win->rows : ny - r0;
-  const uint32_t c0 = win ? win->first_col : 0, cols = win && win->cols ? win->cols : nx - c0;
-  const uint32_t shift = win ? win->tile_shift : 3;
-  if (r0 >= ny || rows > ny - r0 || c0 >= nx || cols > nx - c0 || shift > 5) return -1;
+  p.bla_levels = levels;
+  for (uint32_t i = 0; i < levels; ++i) {
+    p.bla_off[i] = (uint32_t)level_offsets[i];
+    p.bla_count[i] = (uint32_t)(steps >> (i + 1));
+  }
+  s.fused.resize(2 * len);
+  for (uint64_t m = 0; m < len; ++m) {
+    double a = -1.0, b = -1.0;
+    if (m >= 1 && levels > 0 && ((m - 1) & 1) == 0 && ((m - 1) >> 1) < p.bla_count[0])
+      a = s.r2[p.bla_off[0] + ((m - 1) >> 1)];
+    if (m >= 1 && levels > 1 && ((m - 1) & 3) == 0 && ((m - 1) >> 2) < p.bla_count[1])
+      b = s.r2[p.bla_off[1] + ((m - 1) >> 2)];
+    s.fused[2 * m] = s.z[m];
+    s.fused[2 * m + 1] = make_double2(a, b);
+  }
+  p.fused = s.fused.data();
+  p.bla_r2 = s.r2.data();
+  p.bla_coef = s.coef.data();
+  p.bla_ab = s.ab.data();
+}
+
+// The frame, window, mask, offsets and tile order (prepare in fdcuda.cu); tiles of
+// 2^shift x 32/2^shift samples. False when the window leaves the grid.
+bool stage_frame(Setup &s, int32_t tier, uint32_t nx, uint32_t ny, uint32_t ss, double c_re, double c_im, double h_m,
+                 int64_t h_e, double cos_rot, double sin_rot, uint32_t max_iter, double escape_radius, int64_t nucleus,
+                 uint32_t first_row, uint32_t rows_in, uint32_t first_col, uint32_t cols_in, uint32_t shift,
+                 const uint8_t *mask, const double *offsets, bool reversed) {
+  fdk::Params &p = s.p;
+  const uint32_t r0 = first_row, c0 = first_col;
+  if (r0 >= ny || c0 >= nx || shift > 5) return false;
+  const uint32_t rows = rows_in ? rows_in : ny - r0, cols = cols_in ? cols_in : nx - c0;
+  if (rows > ny - r0 || cols > nx - c0) return false;
   p.nx = nx;
   p.ny = ny;
   p.first_row = r0;
@@ -134,25 +153,23 @@ int emu_render_window(const double *re, const double *im, uint64_t len, const do
   p.out_pitch = nx;
   p.tiles_x = (cols + (1u << shift) - 1) >> shift;
   const uint64_t origin = (uint64_t)r0 * nx + c0;
-  std::vector<uint8_t> mask;
-  std::vector<double2> offs;
-  if (win && win->mask) {
-    mask.resize((uint64_t)rows * cols);
+  if (mask) {
+    s.mask.resize((uint64_t)rows * cols);
     for (uint32_t j = 0; j < rows; ++j)
-      for (uint32_t i = 0; i < cols; ++i) mask[(uint64_t)j * cols + i] = win->mask[origin + (uint64_t)j * nx + i];
-    p.mask = mask.data();
+      for (uint32_t i = 0; i < cols; ++i) s.mask[(uint64_t)j * cols + i] = mask[origin + (uint64_t)j * nx + i];
+    p.mask = s.mask.data();
   }
-  if (win && win->offsets) {
-    offs.resize((uint64_t)rows * cols);
+  if (offsets) {
+    s.offs.resize((uint64_t)rows * cols);
     for (uint32_t j = 0; j < rows; ++j)
       for (uint32_t i = 0; i < cols; ++i) {
-        const double *o = win->offsets + 2 * (origin + (uint64_t)j * nx + i);
-        offs[(uint64_t)j * cols + i] = make_double2(o[0], o[1]);
+        const double *o = offsets + 2 * (origin + (uint64_t)j * nx + i);
+        s.offs[(uint64_t)j * cols + i] = make_double2(o[0], o[1]);
       }
-    p.offsets = offs.data();
+    p.offsets = s.offs.data();
   }
   p.tier = tier;
-  p.flags = (deriv || bounded ? fdk::F_DERIV : 0) | (bla ? fdk::F_BLA : 0);
+  p.flags = (s.deriv ? fdk::F_DERIV : 0) | (s.bla ? fdk::F_BLA : 0);
   p.c_re = c_re;
   p.c_im = c_im;
   p.h = h_m * fdk::exp2i(h_e);
@@ -167,7 +184,24 @@ int emu_render_window(const double *re, const double *im, uint64_t len, const do
   p.nucleus = nucleus;
   p.px_m = h_m * (double)ss;
   p.px_e = h_e;
-  // outputs address the window's first sample, rows nx apart
+  const uint32_t tile_h = 32u >> shift, tiles_y = (rows + tile_h - 1) / tile_h;
+  const uint64_t ntiles = (uint64_t)p.tiles_x * tiles_y;
+  p.total = ntiles * 32;
+  p.tile_order = nullptr;
+  if (reversed) {
+    s.order.resize(ntiles);
+    for (uint64_t t = 0; t < ntiles; ++t) s.order[t] = (uint32_t)(ntiles - 1 - t);
+    p.tile_order = s.order.data();
+  }
+  p.deadline_ns = 0;
+  p.defer = s.ext ? 12u : 8u;
+  return true;
+}
+
+// Outputs address the window's first sample, rows nx apart.
+void stage_outputs(fdk::Params &p, uint8_t *cls, uint32_t *n_out, double *nu, float *de, uint16_t *normal,
+                   double *z_out, double *dz_out, int64_t *dexp_out, uint8_t *status) {
+  const uint64_t origin = (uint64_t)p.first_row * p.nx + p.first_col;
   p.cls = cls ? cls + origin : nullptr;
   p.n_out = n_out ? n_out + origin : nullptr;
   p.nu = nu ? nu + origin : nullptr;
@@ -177,24 +211,56 @@ int emu_render_window(const double *re, const double *im, uint64_t len, const do
   p.dz_out = dz_out ? (double2 *)dz_out + origin : nullptr;
   p.dexp_out = dexp_out ? dexp_out + origin : nullptr;
   p.status = status ? status + origin : nullptr;
+}
+
+void copy_counters(const fdk::Counters &c, uint64_t *out) {
+  out[0] = c.samples;
+  out[1] = c.iterations;
+  out[2] = c.blocks;
+  out[3] = c.skipped;
+  out[4] = c.fallback;
+  out[5] = c.closed;
+}
+
+}  // namespace
+
+extern "C" {
+
+// One frame: tier 0 / 1 / 2, flags bit 0 derivative, bit 1 BLA, bit 2 series start, bit 3
+// bounded. blocks7 / level_offsets / levels: the BLA table in its export layout (or null);
+// series_b (b_1..b_order as re, im), series_n, series_rho; q: error radii (bounded).
+// Outputs (any null): class, n, nu, de, normal, z, dz, dexp, status, bound, ez, ed;
+// counters[6] = samples, iterations, blocks, skipped, fallback, closed-form. win: the job's
+// window and inputs, or null for the whole frame in row-major 8x4 tiles.
+int emu_render_window(const double *re, const double *im, uint64_t len, const double *blocks7,
+                      const uint64_t *level_offsets, uint32_t levels, const double *series_b, uint32_t series_order,
+                      uint32_t series_n, double series_rho, const double *q, int32_t tier, uint32_t flags, uint32_t nx,
+                      uint32_t ny, uint32_t ss, double c_re, double c_im, double h_m, int64_t h_e, double cos_rot,
+                      double sin_rot, uint32_t max_iter, double escape_radius, int64_t nucleus, uint8_t *cls,
+                      uint32_t *n_out, double *nu, float *de, uint16_t *normal, double *z_out, double *dz_out,
+                      int64_t *dexp_out, uint8_t *status, float *bound, double *ez, double *ed, uint64_t *counters,
+                      const EmuWindow *win) {
+  const bool ext = tier == 2, deriv = flags & 1, bla = (flags & 2) && levels > 0, series = (flags & 4) && series_n > 0,
+             bounded = (flags & 8) && !ext;
+  if (len < 3 || (bla && bounded) || (series && (ext || bounded))) return -1;  // the route's refusals
+  Setup s;
+  s.ext = ext;
+  s.deriv = deriv || bounded;
+  s.bla = bla;
+  stage_orbit(s, re, im, len, blocks7, level_offsets, levels);
+  if (!stage_frame(s, tier, nx, ny, ss, c_re, c_im, h_m, h_e, cos_rot, sin_rot, max_iter, escape_radius, nucleus,
+                   win ? win->first_row : 0, win ? win->rows : 0, win ? win->first_col : 0, win ? win->cols : 0,
+                   win ? win->tile_shift : 3, win ? win->mask : nullptr, win ? win->offsets : nullptr,
+                   win && win->tile_order))
+    return -1;
+  fdk::Params &p = s.p;
+  stage_outputs(p, cls, n_out, nu, de, normal, z_out, dz_out, dexp_out, status);
   unsigned long long queue = 0;
   fdk::Counters cnt{};
   uint32_t timed_out = 0;
   p.queue = &queue;
   p.counters = &cnt;
-  const uint32_t tile_h = 32u >> shift, tiles_y = (rows + tile_h - 1) / tile_h;
-  const uint64_t ntiles = (uint64_t)p.tiles_x * tiles_y;
-  p.total = ntiles * 32;
-  std::vector<uint32_t> order;
-  p.tile_order = nullptr;
-  if (win && win->tile_order) {
-    order.resize(ntiles);
-    for (uint64_t t = 0; t < ntiles; ++t) order[t] = (uint32_t)(ntiles - 1 - t);
-    p.tile_order = order.data();
-  }
-  p.deadline_ns = 0;
   p.timed_out = &timed_out;
-  p.defer = ext ? 12u : 8u;
   if (series) {
     p.series_b = (const double2 *)series_b;
     p.series_order = series_order;
@@ -202,12 +268,13 @@ int emu_render_window(const double *re, const double *im, uint64_t len, const do
     p.series_inv = 1.0 / series_rho;
   }
   if (bounded) {
+    const uint64_t origin = (uint64_t)p.first_row * nx + p.first_col;
     p.q = q;
     p.bound_out = bound ? bound + origin : nullptr;
     p.ez_out = ez ? ez + origin : nullptr;
     p.ed_out = ed ? ed + origin : nullptr;
   }
-  const bool d = deriv || bounded;
+  const bool d = s.deriv;
   if (bounded) launch<false, true, false, false, true>(p);
   else if (series) {
     if (d) bla ? launch<false, true, true, true, false>(p) : launch<false, true, false, true, false>(p);
@@ -219,12 +286,74 @@ int emu_render_window(const double *re, const double *im, uint64_t len, const do
     if (d) bla ? launch<false, true, true, false, false>(p) : launch<false, true, false, false, false>(p);
     else bla ? launch<false, false, true, false, false>(p) : launch<false, false, false, false, false>(p);
   }
-  counters[0] = cnt.samples;
-  counters[1] = cnt.iterations;
-  counters[2] = cnt.blocks;
-  counters[3] = cnt.skipped;
-  counters[4] = cnt.fallback;
-  counters[5] = cnt.closed;
+  copy_counters(cnt, counters);
+  return 0;
+}
+
+int emu_render(const double *re, const double *im, uint64_t len, const double *blocks7, const uint64_t *level_offsets,
+               uint32_t levels, const double *series_b, uint32_t series_order, uint32_t series_n, double series_rho,
+               const double *q, int32_t tier, uint32_t flags, uint32_t nx, uint32_t ny, uint32_t ss, double c_re,
+               double c_im, double h_m, int64_t h_e, double cos_rot, double sin_rot, uint32_t max_iter,
+               double escape_radius, int64_t nucleus, uint8_t *cls, uint32_t *n_out, double *nu, float *de,
+               uint16_t *normal, double *z_out, double *dz_out, int64_t *dexp_out, uint8_t *status, float *bound,
+               double *ez, double *ed, uint64_t *counters) {
+  return emu_render_window(re, im, len, blocks7, level_offsets, levels, series_b, series_order, series_n, series_rho, q,
+                           tier, flags, nx, ny, ss, c_re, c_im, h_m, h_e, cos_rot, sin_rot, max_iter, escape_radius,
+                           nucleus, cls, n_out, nu, de, normal, z_out, dz_out, dexp_out, status, bound, ez, ed, counters,
+                           nullptr);
+}
+
+// A batch as fdc_batch_create builds it and one replay of it: the jobs grouped by kernel
+// variant (Scaled tier, derivative, BLA), each group's jobs deepest first (stable by h_e),
+// their sample ranges laid end to end (starts), one batch-kernel run per group with a
+// queue of its own and per-job counters returned in each job's own slot.
+int emu_render_batch(EmuJob *jobs, uint32_t njobs) {
+  std::vector<std::unique_ptr<Setup>> setups(njobs);
+  std::map<int, std::vector<uint32_t>> by;
+  for (uint32_t k = 0; k < njobs; ++k) {
+    const EmuJob &j = jobs[k];
+    if (j.len < 3 || j.tier < 0 || j.tier > 2) return -1;
+    auto s = std::make_unique<Setup>();
+    s->ext = j.tier == 2;
+    s->deriv = j.flags & 1;
+    s->bla = (j.flags & 2) && j.levels > 0;
+    stage_orbit(*s, j.re, j.im, j.len, j.blocks7, j.level_offsets, j.levels);
+    if (!stage_frame(*s, j.tier, j.nx, j.ny, j.ss, j.c_re, j.c_im, j.h_m, j.h_e, j.cos_rot, j.sin_rot, j.max_iter,
+                     j.escape_radius, j.nucleus, j.first_row, j.rows, j.first_col, j.cols, 3, nullptr, nullptr,
+                     false))
+      return -1;
+    stage_outputs(s->p, j.cls, j.n, j.nu, j.de, j.normal, j.z, j.dz, j.dexp, j.status);
+    by[(s->ext ? 4 : 0) | (s->deriv ? 2 : 0) | (s->bla ? 1 : 0)].push_back(k);
+    setups[k] = std::move(s);
+  }
+  for (auto &kv : by) {
+    std::vector<uint32_t> order = kv.second;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t c) { return jobs[a].h_e < jobs[c].h_e; });
+    std::vector<fdk::Params> gp;
+    std::vector<unsigned long long> starts;
+    unsigned long long total = 0;
+    for (uint32_t k : order) {
+      starts.push_back(total);
+      gp.push_back(setups[k]->p);
+      total += setups[k]->p.total;
+    }
+    starts.push_back(total);
+    std::vector<fdk::Counters> cnt(order.size());
+    const bool ext = kv.first & 4, d = kv.first & 2, l = kv.first & 1;
+    const uint32_t defer = ext ? 12u : 8u;
+    if (ext) {
+      if (d) l ? launch_batch<true, true, true>(gp, starts, cnt.data(), defer)
+             : launch_batch<true, true, false>(gp, starts, cnt.data(), defer);
+      else l ? launch_batch<true, false, true>(gp, starts, cnt.data(), defer)
+             : launch_batch<true, false, false>(gp, starts, cnt.data(), defer);
+    } else {
+      if (d) l ? launch_batch<false, true, true>(gp, starts, cnt.data(), defer)
+             : launch_batch<false, true, false>(gp, starts, cnt.data(), defer);
+      else l ? launch_batch<false, false, true>(gp, starts, cnt.data(), defer)
+             : launch_batch<false, false, false>(gp, starts, cnt.data(), defer);
+    }
+    for (size_t i = 0; i < order.size(); ++i) copy_counters(cnt[i], jobs[order[i]].counters);
+  }
   return 0;
 }
 

@@ -41,6 +41,8 @@ def emu():
                              U32, D, I64] + [P] * 12 + [P]
     L.emu_render_window.restype = C.c_int
     L.emu_render_window.argtypes = L.emu_render.argtypes + [C.POINTER(Window)]
+    L.emu_render_batch.restype = C.c_int
+    L.emu_render_batch.argtypes = [C.POINTER(Job), U32]
     return L
 
 
@@ -50,6 +52,19 @@ class Window(C.Structure):
     _fields_ = [("first_row", C.c_uint32), ("rows", C.c_uint32), ("first_col", C.c_uint32), ("cols", C.c_uint32),
                 ("tile_shift", C.c_uint32), ("tile_order", C.c_uint32), ("mask", C.c_void_p),
                 ("offsets", C.c_void_p)]
+
+
+class Job(C.Structure):
+    """emu.cpp's EmuJob: one batch job (orbit, BLA table, frame, window, outputs) and its
+    returned counters."""
+    _fields_ = [("re", C.c_void_p), ("im", C.c_void_p), ("len", C.c_uint64), ("blocks7", C.c_void_p),
+                ("level_offsets", C.c_void_p), ("levels", C.c_uint32), ("tier", C.c_int32), ("flags", C.c_uint32),
+                ("nx", C.c_uint32), ("ny", C.c_uint32), ("ss", C.c_uint32), ("max_iter", C.c_uint32),
+                ("c_re", C.c_double), ("c_im", C.c_double), ("h_m", C.c_double), ("h_e", C.c_int64),
+                ("cos_rot", C.c_double), ("sin_rot", C.c_double), ("escape_radius", C.c_double),
+                ("nucleus", C.c_int64), ("first_row", C.c_uint32), ("rows", C.c_uint32), ("first_col", C.c_uint32),
+                ("cols", C.c_uint32)] + [(k, C.c_void_p) for k in ("cls", "n", "nu", "de", "normal", "z", "dz", "dexp",
+                                                                    "status")] + [("counters", C.c_uint64 * 6)]
 
 
 def _ptr(a):
@@ -377,3 +392,82 @@ def test_kernel_window_mask_offsets_equal_oracle(emu, case):
         if o["kind"] == "escaped":
             assert tuple(got["z"][k]) == (o["zr"], o["zi"]) and tuple(got["dz"][k]) == (o["dr"], o["di"]), k
             assert got["dexp"][k] == o["dexp"], k
+
+
+def _outputs(n):
+    return dict(cls=np.zeros(n, np.uint8), n=np.zeros(n, np.uint32), nu=np.zeros(n), de=np.zeros(n, np.float32),
+                normal=np.zeros(n, np.uint16), z=np.zeros((n, 2)), dz=np.zeros((n, 2)), dexp=np.zeros(n, np.int64),
+                status=np.zeros(n, np.uint8))
+
+
+def test_batch_kernel_equals_oracle(emu):
+    """The batch kernel as fdc_batch_create groups a mixed batch (jobs of every tier, with and
+    without BLA and the derivative, so several variant groups whose jobs are reordered deepest
+    first; one frame split into three row tiles that write one shared output): every job's
+    samples equal the oracle's frame, and every job's counters equal the oracle's render of
+    just that job's samples (its window as a mask)."""
+    frame18 = KATS["series_frames"][18]
+    specs = [  # view, nx, ny, max_iter, BLA eps (None: no table), derivative, row tiles
+        ((*SEAHORSE, "1e-10"), 24, 16, 20_000, 2.0 ** -30, True, 1),
+        ((frame18["re"], frame18["im"], frame18["width"]), 33, 19, 10_000, fd.route.EPS, True, 3),
+        (("0", "1", "1e-300"), 32, 16, 5_000, fd.route.EPS, False, 1),
+        (("-0.7453", "0.1127", "0.0065"), 20, 12, 4_000, None, True, 1),
+        ((frame18["re"], frame18["im"], frame18["width"]), 16, 8, 10_000, None, False, 1),
+    ]
+    keep, jobs, frames = [], [], []
+    for view3, nx, ny, it, eps, deriv, tiles in specs:
+        cols = ("nu", "de", "normal") if deriv else ("nu",)
+        v, p, plane, t, r = _setup(view3, nx, ny, it, None, cols)
+        table = ob = None
+        ref = fdref.Ref.arrays(r.re, r.im, r.bits)
+        if eps is not None:
+            dc, e = fd.bla_dc_bound(v, p)
+            table = fd.Bla.build_scaled(r, eps, dc, e)
+            assert table.levels > 0
+            ob = fdref.Bla(ref, eps, table.dc_max, table.dc_exp)
+        out = _outputs(nx * ny)
+        re_, im_ = np.ascontiguousarray(r.re), np.ascontiguousarray(r.im)
+        blocks = offs = None
+        if table is not None:
+            blocks = np.ascontiguousarray(table.blocks)
+            offs = np.ascontiguousarray(table.level_offsets, dtype=np.uint64)
+        keep += [re_, im_, blocks, offs]
+        nuc = r.nucleus_period()
+        edges = np.linspace(0, ny, tiles + 1).astype(int)
+        windows = []
+        for a, b in zip(edges[:-1], edges[1:]):
+            j = Job(re=re_.ctypes.data, im=im_.ctypes.data, len=len(re_), blocks7=_ptr(blocks),
+                    level_offsets=_ptr(offs), levels=table.levels if table else 0, tier=t,
+                    flags=(1 if deriv else 0) | (2 if table else 0), nx=nx, ny=ny, ss=p.ss, max_iter=it,
+                    c_re=plane.c_re, c_im=plane.c_im, h_m=plane.h_m, h_e=plane.h_e, cos_rot=plane.cos_rot,
+                    sin_rot=plane.sin_rot, escape_radius=p.escape_radius, nucleus=-1 if nuc is None else nuc,
+                    first_row=int(a), rows=int(b - a) if tiles > 1 else 0, first_col=0, cols=0,
+                    **{k: out[k].ctypes.data for k in out})
+            windows.append((len(jobs), int(a), int(b)))
+            jobs.append(j)
+        ocols = fdref.COL_NU | (fdref.COL_DE | fdref.COL_NORMAL if deriv else 0)
+        frames.append((view3, p, t, ref, ob, ocols, deriv, out, windows))
+    arr = (Job * len(jobs))(*jobs)
+    assert emu.emu_render_batch(arr, len(jobs)) == 0
+    tiers = set()
+    for view3, p, t, ref, ob, ocols, deriv, out, windows in frames:
+        want = fdref.render(_oracle_job(view3, p, t, ocols), ref, ob, raw=True)
+        tiers.add(t)
+        assert out["status"].all()
+        assert np.array_equal(out["cls"], want["cls"]), view3
+        assert np.array_equal(out["n"], want["n"].astype(np.uint32)), view3
+        esc = (want["cls"] & 3) == 0
+        assert np.array_equal(out["z"][esc], want["z"][esc]) and np.array_equal(out["nu"][esc], want["nu"][esc])
+        if deriv:
+            for k in ("dz", "dexp", "de"):
+                assert np.array_equal(out[k][esc], want[k][esc]), (view3, k)
+        for k, a, b in windows:
+            m = np.zeros((p.ny, p.nx), np.uint8)
+            m[a:b] = 1
+            st = fdref.render_columns(_oracle_job(view3, p, t, ocols), ref, ob, mask=m.ravel())["stats"]
+            got = dict(zip(("samples", "iterations", "blocks", "skipped", "fallback_samples", "closed_form_samples"),
+                           (int(c) for c in arr[k].counters)))
+            assert got["samples"] == (b - a) * p.nx, (view3, a, b)
+            for key in ("iterations", "blocks", "skipped", "fallback_samples", "closed_form_samples"):
+                assert got[key] == st[key], (view3, a, b, key)
+    assert tiers == {0, 1, 2}
