@@ -16,6 +16,7 @@
 #define __forceinline__ inline
 #define __noinline__ __attribute__((noinline))
 #define __launch_bounds__(...)
+#define __align__(n) alignas(n)
 
 using std::isfinite;
 using std::isnan;
@@ -47,6 +48,16 @@ inline long long __double_as_longlong(double d) {
 }
 inline double __hiloint2double(int hi, int lo) {
   return __longlong_as_double((long long)(((unsigned long long)(unsigned)hi << 32) | (unsigned)lo));
+}
+inline float __int_as_float(int v) {
+  float f;
+  std::memcpy(&f, &v, 4);
+  return f;
+}
+inline unsigned __float_as_uint(float f) {
+  unsigned v;
+  std::memcpy(&v, &f, 4);
+  return v;
 }
 inline int __double2hiint(double d) { return (int)((unsigned long long)__double_as_longlong(d) >> 32); }
 inline int __double2loint(double d) { return (int)(unsigned)(unsigned long long)__double_as_longlong(d); }

@@ -14,7 +14,7 @@
 #include <vector>
 
 #include "cuda_host_shim.hpp"
-#include "perturb_f64.cuh"
+#include "perturb_f32.cuh"
 
 extern "C" {
 
@@ -39,7 +39,7 @@ struct EmuJob {
   const uint64_t *level_offsets;
   uint32_t levels;
   int32_t tier;
-  uint32_t flags;  // bit 0 derivative, bit 1 BLA
+  uint32_t flags;  // bit 0 derivative, bit 1 BLA, bit 2 the precision form
   uint32_t nx, ny, ss, max_iter;
   double c_re, c_im, h_m;
   int64_t h_e;
@@ -63,6 +63,7 @@ namespace {
 
 // A job's Params and the staged arrays they point into.
 struct Setup {
+  std::vector<fdk::Entry32> z32;
   std::vector<double2> z, fused, coef, ab, offs;
   std::vector<double> r2;
   std::vector<uint8_t> mask;
@@ -78,6 +79,13 @@ void launch(fdk::Params &p) {
   fdk::perturb_kernel<EXT, D, L, S, B>(p);
 }
 
+template <bool D, bool L>
+void launch_f32(fdk::Params &p, const fdk::Entry32 *orbit) {
+  threadIdx.x = 0;
+  blockIdx.x = 0;
+  fdk::perturb_f32_kernel<D, L>(p, orbit);
+}
+
 template <bool EXT, bool D, bool L>
 void launch_batch(const std::vector<fdk::Params> &jobs, const std::vector<unsigned long long> &starts,
                   fdk::Counters *per_job, uint32_t defer) {
@@ -88,6 +96,16 @@ void launch_batch(const std::vector<fdk::Params> &jobs, const std::vector<unsign
                                        per_job, defer);
 }
 
+template <bool D, bool L>
+void launch_f32_batch(const std::vector<fdk::Params> &jobs, const std::vector<unsigned long long> &starts,
+                      fdk::Counters *per_job, uint32_t defer) {
+  threadIdx.x = 0;
+  blockIdx.x = 0;
+  unsigned long long queue = 0;
+  fdk::perturb_f32_batch_kernel<D, L>(jobs.data(), starts.data(), (uint32_t)jobs.size(), starts.back(), &queue,
+                                      per_job, defer);
+}
+
 // The orbit (pack_orbit) and BLA table (pack_bla, fuse_bla) of a job.
 void stage_orbit(Setup &s, const double *re, const double *im, uint64_t len, const double *blocks7,
                  const uint64_t *level_offsets, uint32_t levels) {
@@ -95,6 +113,17 @@ void stage_orbit(Setup &s, const double *re, const double *im, uint64_t len, con
   s.z.resize(len);
   for (uint64_t m = 0; m < len; ++m) s.z[m] = make_double2(re[m], im[m]);
   p.orbit = s.z.data();
+  // the precision form's entries (pack_orbit): f32 copies, NaN where |Z| < 2^-60
+  s.z32.resize(len);
+  for (uint64_t m = 0; m < len; ++m) {
+    fdk::Entry32 &e = s.z32[m];
+    e.zr = re[m];
+    e.zi = im[m];
+    e.zr32 = std::fmax(std::fabs(re[m]), std::fabs(im[m])) < 0x1p-60 ? __int_as_float(0x7fc00000) : (float)re[m];
+    e.zi32 = (float)im[m];
+    e.r2a = -1.0;
+  }
+  p.orbit32 = s.z32.data();
   p.last = (uint32_t)(len - 1);
   p.z0r = re[0];
   p.z0i = im[0];
@@ -125,6 +154,7 @@ void stage_orbit(Setup &s, const double *re, const double *im, uint64_t len, con
     s.fused[2 * m] = s.z[m];
     s.fused[2 * m + 1] = make_double2(a, b);
   }
+  for (uint64_t m = 0; m < len; ++m) s.z32[m].r2a = s.fused[2 * m + 1].x;
   p.fused = s.fused.data();
   p.bla_r2 = s.r2.data();
   p.bla_coef = s.coef.data();
@@ -227,7 +257,7 @@ void copy_counters(const fdk::Counters &c, uint64_t *out) {
 extern "C" {
 
 // One frame: tier 0 / 1 / 2, flags bit 0 derivative, bit 1 BLA, bit 2 series start, bit 3
-// bounded. blocks7 / level_offsets / levels: the BLA table in its export layout (or null);
+// bounded, bit 4 the precision form (perturb_f32_kernel). blocks7 / level_offsets / levels: the BLA table in its export layout (or null);
 // series_b (b_1..b_order as re, im), series_n, series_rho; q: error radii (bounded).
 // Outputs (any null): class, n, nu, de, normal, z, dz, dexp, status, bound, ez, ed;
 // counters[6] = samples, iterations, blocks, skipped, fallback, closed-form. win: the job's
@@ -241,8 +271,9 @@ int emu_render_window(const double *re, const double *im, uint64_t len, const do
                       int64_t *dexp_out, uint8_t *status, float *bound, double *ez, double *ed, uint64_t *counters,
                       const EmuWindow *win) {
   const bool ext = tier == 2, deriv = flags & 1, bla = (flags & 2) && levels > 0, series = (flags & 4) && series_n > 0,
-             bounded = (flags & 8) && !ext;
-  if (len < 3 || (bla && bounded) || (series && (ext || bounded))) return -1;  // the route's refusals
+             bounded = (flags & 8) && !ext, f32 = flags & 16;
+  if (len < 3 || (bla && bounded) || (series && (ext || bounded)) || (f32 && (series || bounded)))
+    return -1;  // the route's refusals
   Setup s;
   s.ext = ext;
   s.deriv = deriv || bounded;
@@ -275,7 +306,11 @@ int emu_render_window(const double *re, const double *im, uint64_t len, const do
     p.ed_out = ed ? ed + origin : nullptr;
   }
   const bool d = s.deriv;
-  if (bounded) launch<false, true, false, false, true>(p);
+  if (f32) {
+    const fdk::Entry32 *o = s.z32.data();
+    if (d) bla ? launch_f32<true, true>(p, o) : launch_f32<true, false>(p, o);
+    else bla ? launch_f32<false, true>(p, o) : launch_f32<false, false>(p, o);
+  } else if (bounded) launch<false, true, false, false, true>(p);
   else if (series) {
     if (d) bla ? launch<false, true, true, true, false>(p) : launch<false, true, false, true, false>(p);
     else bla ? launch<false, false, true, true, false>(p) : launch<false, false, false, true, false>(p);
@@ -304,7 +339,7 @@ int emu_render(const double *re, const double *im, uint64_t len, const double *b
 }
 
 // A batch as fdc_batch_create builds it and one replay of it: the jobs grouped by kernel
-// variant (Scaled tier, derivative, BLA), each group's jobs deepest first (stable by h_e),
+// variant (precision form, Scaled tier, derivative, BLA), each group's jobs deepest first (stable by h_e),
 // their sample ranges laid end to end (starts), one batch-kernel run per group with a
 // queue of its own and per-job counters returned in each job's own slot.
 int emu_render_batch(EmuJob *jobs, uint32_t njobs) {
@@ -323,7 +358,7 @@ int emu_render_batch(EmuJob *jobs, uint32_t njobs) {
                      false))
       return -1;
     stage_outputs(s->p, j.cls, j.n, j.nu, j.de, j.normal, j.z, j.dz, j.dexp, j.status);
-    by[(s->ext ? 4 : 0) | (s->deriv ? 2 : 0) | (s->bla ? 1 : 0)].push_back(k);
+    by[((j.flags & 4) ? 8 : 0) | (s->ext ? 4 : 0) | (s->deriv ? 2 : 0) | (s->bla ? 1 : 0)].push_back(k);
     setups[k] = std::move(s);
   }
   for (auto &kv : by) {
@@ -339,9 +374,14 @@ int emu_render_batch(EmuJob *jobs, uint32_t njobs) {
     }
     starts.push_back(total);
     std::vector<fdk::Counters> cnt(order.size());
-    const bool ext = kv.first & 4, d = kv.first & 2, l = kv.first & 1;
+    const bool f32 = kv.first & 8, ext = kv.first & 4, d = kv.first & 2, l = kv.first & 1;
     const uint32_t defer = ext ? 12u : 8u;
-    if (ext) {
+    if (f32) {
+      if (d) l ? launch_f32_batch<true, true>(gp, starts, cnt.data(), defer)
+             : launch_f32_batch<true, false>(gp, starts, cnt.data(), defer);
+      else l ? launch_f32_batch<false, true>(gp, starts, cnt.data(), defer)
+             : launch_f32_batch<false, false>(gp, starts, cnt.data(), defer);
+    } else if (ext) {
       if (d) l ? launch_batch<true, true, true>(gp, starts, cnt.data(), defer)
              : launch_batch<true, true, false>(gp, starts, cnt.data(), defer);
       else l ? launch_batch<true, false, true>(gp, starts, cnt.data(), defer)

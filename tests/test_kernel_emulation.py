@@ -3,10 +3,12 @@ for the host (tests/emu: builtins shimmed, the persistent kernel run as a single
 warp) against the oracle, on the CPU: class, escape count, z, dz/dc and the work
 counters bit for bit on the F64, Fixed and Scaled tiers with and without BLA and the
 derivative, from a parameter-series start (with its retries from zero) and in the
-bounded variant (error radii, Bounded evidence, Bound column). Host libm stands in for
+bounded variant (error radii, Bounded evidence, Bound column), in windows with masks,
+offsets and tile orders, and as batches. Host libm stands in for
 CUDA's, so nu, de and the Bound column also equal the oracle's here. This checks the
 kernel's state machine without a GPU; its arithmetic on the device is checked by the
-GPU suite."""
+GPU suite. The precision form (perturb_f32.cuh) runs here too, without the device's fused
+multiply-adds, so it is held to its own agreement bars rather than to bit equality."""
 import ctypes as C
 import json
 import os
@@ -29,6 +31,7 @@ SEAHORSE = ("-0.743643887037158", "0.131825904205312")
 def emu():
     src = [os.path.join(HERE, "emu", "emu.cpp"), os.path.join(HERE, "emu", "cuda_host_shim.hpp"),
            os.path.join(ROOT, "fractodactyl_b200", "csrc", "perturb_f64.cuh"),
+           os.path.join(ROOT, "fractodactyl_b200", "csrc", "perturb_f32.cuh"),
            os.path.join(ROOT, "fractodactyl_b200", "csrc", "fd_device.cuh")]
     if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(s) for s in src):
         subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-Wno-unknown-pragmas",
@@ -471,3 +474,99 @@ def test_batch_kernel_equals_oracle(emu):
             for key in ("iterations", "blocks", "skipped", "fallback_samples", "closed_form_samples"):
                 assert got[key] == st[key], (view3, a, b, key)
     assert tiers == {0, 1, 2}
+
+
+PRECISION_VIEWS = [  # view, nx, ny, max_iter, chaotic (the precision form's GPU bars per view)
+    (("-0.7453", "0.1127", "0.0065"), 64, 36, 20_000, True),
+    (("-0.743643887037158704752191506114774", "0.131825904205311970493132056385139", "1e-28"), 64, 36, 50_000, True),
+    (("0", "1", "1e-300"), 64, 36, 20_000, False),
+    (("-0.7436438870371587", "0.1318259042053120", "1e-12"), 60, 34, 20_000, True),
+]
+
+
+@pytest.mark.parametrize("view,bla", [(v, False) for v in PRECISION_VIEWS] +
+                         [(v, True) for v in PRECISION_VIEWS[1:3]],  # F64-tier views admit no block at 2^-50
+                         ids=lambda x: x[0][2] if isinstance(x, tuple) else ("bla" if x else "plain"))
+def test_precision_form_kernel_meets_its_bars(emu, view, bla):
+    """The precision-form kernel (perturb_f32.cuh, host float arithmetic without fused
+    multiply-adds, so not the device's roundings) against the oracle's FP64 render, held to
+    the bars its GPU tests set: escape agreement >= 99% and equal counts >= 75% on chaotic
+    views, equal counts >= 99.9% and none more than one apart on the non-chaotic view; smooth
+    iteration within 1e-5 relative (median) or 1e-6 (p99) where the counts agree."""
+    view3, nx, ny, it, chaotic = view
+    v, p, plane, t, r = _setup(view3, nx, ny, it)
+    table = ob = None
+    ref = fdref.Ref.arrays(r.re, r.im, r.bits)
+    if bla:
+        dc, e = fd.bla_dc_bound(v, p)
+        table = fd.Bla.build_scaled(r, fd.route.EPS, dc, e)
+        assert table.levels > 0
+        ob = fdref.Bla(ref, fd.route.EPS, table.dc_max, table.dc_exp)
+    got = emulate(emu, r, plane, t, p, 1 | (2 if table else 0) | 16, bla=table)
+    want = fdref.render(_oracle_job(view3, p, t, fdref.COL_NU | fdref.COL_DE | fdref.COL_NORMAL), ref, ob, raw=True)
+    assert got["status"].all()
+    ea, eb = (want["cls"] & 3) == 0, (got["cls"] & 3) == 0
+    dn = np.abs(want["n"].astype(np.int64) - got["n"].astype(np.int64))
+    same = ((ea == eb) & (~ea | (dn == 0))).mean()
+    off1 = ((ea == eb) & (~ea | (dn <= 1))).mean()
+    escaping = (ea == eb).mean()
+    agree = ea & eb & (dn == 0)
+    rel = np.abs(want["nu"][agree] - got["nu"][agree]) / np.abs(want["nu"][agree])
+    assert agree.any()
+    if chaotic:
+        assert escaping >= 0.99 and same >= 0.75, (same, escaping)
+        assert np.median(rel) <= 1e-5
+    else:
+        assert same >= 0.999 and off1 == 1.0, (same, off1)
+        assert np.quantile(rel, 0.99) <= 1e-6 and rel.max() <= 1e-3
+    if table is not None:
+        assert got["counters"]["blocks"] > 0
+
+
+def test_precision_form_batch_equals_single_frames(emu):
+    """The precision form's batch kernel over a mixed batch (three tiers, BLA on and off, one
+    frame in three row tiles) writes exactly what the precision form's frame kernel writes
+    for each frame, with equal per-job counters."""
+    specs = [(("-0.7453", "0.1127", "0.0065"), 24, 16, 4_000, False, 1),
+             (("-0.743643887037158704752191506114774", "0.131825904205311970493132056385139", "1e-28"), 33, 19,
+              50_000, True, 3),
+             (("0", "1", "1e-300"), 32, 16, 5_000, True, 1)]
+    keep, jobs, frames = [], [], []
+    for view3, nx, ny, it, bla, tiles in specs:
+        v, p, plane, t, r = _setup(view3, nx, ny, it)
+        table = None
+        if bla:
+            dc, e = fd.bla_dc_bound(v, p)
+            table = fd.Bla.build_scaled(r, fd.route.EPS, dc, e)
+            assert table.levels > 0
+        single = emulate(emu, r, plane, t, p, 1 | (2 if table else 0) | 16, bla=table)
+        out = _outputs(nx * ny)
+        re_, im_ = np.ascontiguousarray(r.re), np.ascontiguousarray(r.im)
+        blocks = offs = None
+        if table is not None:
+            blocks = np.ascontiguousarray(table.blocks)
+            offs = np.ascontiguousarray(table.level_offsets, dtype=np.uint64)
+        keep += [re_, im_, blocks, offs]
+        nuc = r.nucleus_period()
+        edges = np.linspace(0, ny, tiles + 1).astype(int)
+        ids = []
+        for a, b in zip(edges[:-1], edges[1:]):
+            ids.append(len(jobs))
+            jobs.append(Job(re=re_.ctypes.data, im=im_.ctypes.data, len=len(re_), blocks7=_ptr(blocks),
+                            level_offsets=_ptr(offs), levels=table.levels if table else 0, tier=t,
+                            flags=1 | (2 if table else 0) | 4, nx=nx, ny=ny, ss=p.ss, max_iter=it, c_re=plane.c_re,
+                            c_im=plane.c_im, h_m=plane.h_m, h_e=plane.h_e, cos_rot=plane.cos_rot,
+                            sin_rot=plane.sin_rot, escape_radius=p.escape_radius,
+                            nucleus=-1 if nuc is None else nuc, first_row=int(a),
+                            rows=int(b - a) if tiles > 1 else 0, first_col=0, cols=0,
+                            **{k: out[k].ctypes.data for k in out}))
+        frames.append((single, out, ids, t))
+    arr = (Job * len(jobs))(*jobs)
+    assert emu.emu_render_batch(arr, len(jobs)) == 0
+    assert {f[3] for f in frames} == {0, 1, 2}
+    for single, out, ids, _ in frames:
+        for k in ("cls", "n", "nu", "de", "normal", "z", "dz", "dexp", "status"):
+            assert np.array_equal(out[k], single[k]), k
+        total = np.sum([np.array(arr[i].counters, dtype=np.uint64) for i in ids], axis=0)
+        assert [int(c) for c in total] == [single["counters"][k] for k in (
+            "samples", "iterations", "blocks", "skipped", "fallback_samples", "closed_form_samples")]
