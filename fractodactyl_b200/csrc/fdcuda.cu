@@ -51,6 +51,7 @@ struct OrbitDev {
   double series_rho = 0.0, series_inv = 0.0;
   double2 *series_b = nullptr;
   double *q = nullptr;  // error radii of the orbit's points (fdc_upload_error_radius), len entries
+  uint32_t batch_refs = 0;  // live batches whose jobs read this orbit and its table
 };
 
 constexpr uint32_t SERIES_SLOTS = 64;  // SeriesConfig::default().max_order (series.rs:45)
@@ -157,6 +158,7 @@ struct fdc_batch {
     uint32_t counter_base = 0;
   };
   std::vector<Group> groups;
+  std::vector<int32_t> orbits;  // distinct orbit handles of the jobs, each holding a reference
   uint32_t njobs = 0;
   fdk::Counters *counters = nullptr;   // njobs, in group order
   unsigned long long *queues = nullptr;  // one per group
@@ -693,6 +695,8 @@ fdc_status fdc_free_orbit(fdc_ctx *ctx, int32_t orbit) {
   if (!ctx) return FDC_INVALID;
   auto it = ctx->orbits.find(orbit);
   if (it == ctx->orbits.end()) return fail(ctx, FDC_INVALID, "unknown orbit handle");
+  if (it->second.batch_refs)
+    return fail(ctx, FDC_INVALID, "orbit is read by a live batch: free the batch first");
   free_orbit_buffers(ctx, it->second);  // to the pool: later uploads reuse them in stream order
   ctx->orbits.erase(it);
   return FDC_OK;
@@ -704,6 +708,7 @@ fdc_status fdc_upload_bla(fdc_ctx *ctx, int32_t orbit, const double *blocks7, co
   auto it = ctx->orbits.find(orbit);
   if (it == ctx->orbits.end()) return fail(ctx, FDC_INVALID, "unknown orbit handle");
   OrbitDev &o = it->second;
+  if (o.batch_refs) return fail(ctx, FDC_INVALID, "orbit is read by a live batch: free the batch first");
   // bla.rs:26-33 and Bla::new's shape/value checks (bla.rs:184-216)
   if (!(eps > 0.0 && eps <= 1.0 / (double)(1u << 24) && dc_max > 0.0 && std::isfinite(dc_max)))
     return fail(ctx, FDC_INVALID, "BLA needs 0 < eps <= 2^-24 and a finite dc_max > 0");
@@ -1135,6 +1140,11 @@ fdc_status fdc_batch_create(fdc_ctx *ctx, const fdc_job *jobs, const fdc_out *ou
   if (e == cudaSuccess) e = e2;
   if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, b->graph, 0);
   if (e != cudaSuccess) return bail(fail(ctx, FDC_DEVICE_ERROR, std::string("batch graph: ") + cudaGetErrorString(e)));
+  // the jobs' orbits and tables stay put while the batch exists
+  for (uint32_t k = 0; k < njobs; ++k) b->orbits.push_back(jobs[k].orbit);
+  std::sort(b->orbits.begin(), b->orbits.end());
+  b->orbits.erase(std::unique(b->orbits.begin(), b->orbits.end()), b->orbits.end());
+  for (int32_t h : b->orbits) ++ctx->orbits.find(h)->second.batch_refs;  // each checked above
   *out = b;
   return FDC_OK;
 }
@@ -1179,6 +1189,11 @@ void fdc_batch_free(fdc_ctx *ctx, fdc_batch *b) {
   if (ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    if (b)
+      for (int32_t h : b->orbits) {
+        auto it = ctx->orbits.find(h);
+        if (it != ctx->orbits.end() && it->second.batch_refs) --it->second.batch_refs;
+      }
   }
   free_batch(b);
 }

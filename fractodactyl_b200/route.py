@@ -333,7 +333,8 @@ class Device:
                                        b.ctypes.data if len(b) else None, len(b)), self, "upload series")
 
     def free(self, orbit: int):
-        lib().fdc_free_orbit(self.h, orbit)
+        """fdc_free_orbit; refused (RouteError) while a live batch reads the orbit."""
+        _check(lib().fdc_free_orbit(self.h, orbit), self, "free orbit")
 
     def upload_error_radius(self, orbit: int, q: np.ndarray):
         """fdc_upload_error_radius: the orbit's error radii for bounded renders."""

@@ -183,7 +183,9 @@ fdc_status fdc_get_tuning(const fdc_ctx *ctx, fdc_tuning *tuning);
  * kernel variant from a single work queue over all jobs' tiles, deepest jobs first, the
  * whole run captured once in a CUDA graph and replayed by fdc_batch_run. Results equal
  * fdc_render's per job. Jobs need FDC_DEVICE_OUT, no mask/offsets/deadline/FDC_SERIES; orbits and
- * tables must stay uploaded while the batch exists. per_job (optional) has njobs
+ * tables must stay uploaded while the batch exists: fdc_free_orbit and fdc_upload_bla refuse
+ * (FDC_INVALID) an orbit that a live batch reads, until fdc_batch_free. Free batches before
+ * fdc_close. per_job (optional) has njobs
  * entries; counters->kernel_ms is the device time of the whole replay. */
 typedef struct fdc_batch fdc_batch;
 fdc_status fdc_batch_create(fdc_ctx *ctx, const fdc_job *jobs, const fdc_out *outs, uint32_t njobs,

@@ -84,3 +84,20 @@ def test_batch_refuses_host_only_jobs(dev):
             dev.batch([j])
     finally:
         dev.free(h)
+
+
+def test_orbit_held_while_a_batch_reads_it(dev):
+    """A live batch holds its jobs' orbits: freeing one is refused (the batch would read
+    recycled device memory) until the batch is freed."""
+    h, j = _job(dev, FRAMES[1])
+    b = dev.batch([j], columns=("nu",))
+    try:
+        with pytest.raises(fd.route.RouteError, match="live batch"):
+            dev.free(h)
+        total, _ = b.run()
+        assert total.samples == j.nx * j.ny
+    finally:
+        b.free()
+    dev.free(h)
+    with pytest.raises(fd.route.RouteError, match="unknown orbit"):
+        dev.free(h)
