@@ -1,6 +1,7 @@
-"""Frame sharding over two ranks (gloo, CPU): each rank renders its interleaved stripes
-with the oracle standing in for the per-GPU renderer, the reduction rebuilds the frame
-exactly as one render of the whole frame."""
+"""Frame sharding over two and three ranks (gloo, CPU): each rank renders only its
+interleaved stripes (the oracle's masked render standing in for the per-GPU renderer),
+and the reduction rebuilds the frame and its counters exactly as one render of the whole
+frame, including a ragged last stripe and stripes that do not divide evenly."""
 import os
 import socket
 
@@ -29,14 +30,15 @@ def _worker(rank, world, port, q):
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
         re_, im_, w, nx, ny, it = VIEW
-        job = fdref.make_job(re_, im_, w, nx, ny, it, threads=1)
+        job = fdref.make_job(re_, im_, w, nx, ny, it, columns=fdref.COL_NU | fdref.COL_DE | fdref.COL_NORMAL,
+                             threads=1)
 
         def render_masked(mask):
-            o = fdref.render(job, raw=True)  # the oracle renders everything; keep this rank's rows
-            keep = mask.astype(bool)
-            cols = {k: np.where(keep, o[k], 0) for k in ("cls", "nu", "de", "normal")}
-            cols["n"] = np.where(keep, o["n"], 0)
-            return cols, {"samples": int(keep.sum()), "iterations": int(o["n"][keep].sum())}
+            o = fdref.render_columns(job, mask=mask)  # this rank's samples only, zeros elsewhere
+            cols = {k: o[k] for k in ("cls", "n", "nu", "de", "normal")}
+            st = o["stats"]
+            return cols, {"samples": int(mask.sum()), "iterations": st["iterations"],
+                          "closed_form_samples": st["closed_form_samples"]}
 
         frame, counters = shard.render_frame(nx, ny, render_masked)
         q.put((rank, {k: v.tolist() for k, v in frame.items()}, counters))
@@ -44,8 +46,9 @@ def _worker(rank, world, port, q):
         dist.destroy_process_group()
 
 
-def test_two_rank_frame_equals_single_render():
-    world, port = 2, _free_port()
+@pytest.mark.parametrize("world", [2, 3])
+def test_sharded_frame_equals_single_render(world):
+    port = _free_port()
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     procs = [ctx.Process(target=_worker, args=(r, world, port, q)) for r in range(world)]
@@ -57,13 +60,15 @@ def test_two_rank_frame_equals_single_render():
         assert p.exitcode == 0
     re_, im_, w, nx, ny, it = VIEW
     o = fdref.render(fdref.make_job(re_, im_, w, nx, ny, it, threads=1), raw=True)
+    assert ny % (4 * world) != 0  # stripes that do not divide evenly over the ranks
     for rank, frame, counters in results:
         assert np.array_equal(np.array(frame["cls"], np.uint8), o["cls"])
         assert np.array_equal(np.array(frame["n"], np.uint64), o["n"])
         assert np.array_equal(np.array(frame["nu"]), o["nu"])
         assert np.array_equal(np.array(frame["de"], np.float32), o["de"])
         assert np.array_equal(np.array(frame["normal"], np.uint16), o["normal"])
-        assert counters["samples"] == nx * ny and counters["iterations"] == int(o["n"].sum())
+        assert counters["samples"] == nx * ny and counters["iterations"] == o["stats"]["iterations"]
+        assert counters["closed_form_samples"] == o["stats"]["closed_form_samples"]
 
 
 def test_masks_partition_the_frame():
