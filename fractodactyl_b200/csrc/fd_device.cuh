@@ -247,6 +247,8 @@ __device__ __forceinline__ uint64_t globaltimer() {
   uint64_t t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
+#elif defined(FDK_HOST_TIMER)
+  return FDK_HOST_TIMER();  // a host build that supplies its own clock (nanoseconds)
 #else
   return 0;  // host builds of this header (no device timer; deadlines are device-only)
 #endif

@@ -14,6 +14,15 @@
 #include <vector>
 
 #include "cuda_host_shim.hpp"
+
+// The kernels' deadline clock (globaltimer): 1 us per read, from 0 at each launch, so a
+// deadline of d ns lets a warp take about d / 1000 - 1 pickups.
+namespace emu_clock {
+inline uint64_t ticks = 0;
+inline uint64_t now() { return ticks += 1000; }
+}  // namespace emu_clock
+#define FDK_HOST_TIMER() emu_clock::now()
+
 #include "perturb_f32.cuh"
 
 extern "C" {
@@ -22,10 +31,12 @@ extern "C" {
 // mask and offsets over the whole frame, the tile width 2^tile_shift and the tile order)
 // as fdc_render stages them: outputs keep their frame pitch, mask and offsets are copied
 // to window pitch. tile_order: 0 row-major, 1 reversed (any permutation is legal).
+// deadline_ns: fdc_job's deadline (0 none) on the emulated clock.
 struct EmuWindow {
   uint32_t first_row, rows, first_col, cols, tile_shift, tile_order;
   const uint8_t *mask;
   const double *offsets;
+  uint64_t deadline_ns;
 };
 
 // One job of a batch (fdc_job plus its orbit, BLA table and fdc_out): the orbit as re / im
@@ -261,7 +272,8 @@ extern "C" {
 // series_b (b_1..b_order as re, im), series_n, series_rho; q: error radii (bounded).
 // Outputs (any null): class, n, nu, de, normal, z, dz, dexp, status, bound, ez, ed;
 // counters[6] = samples, iterations, blocks, skipped, fallback, closed-form. win: the job's
-// window and inputs, or null for the whole frame in row-major 8x4 tiles.
+// window and inputs, or null for the whole frame in row-major 8x4 tiles. Returns 0, 1 when
+// the deadline passed (the kernel's timed_out flag), -1 for a refused job.
 int emu_render_window(const double *re, const double *im, uint64_t len, const double *blocks7,
                       const uint64_t *level_offsets, uint32_t levels, const double *series_b, uint32_t series_order,
                       uint32_t series_n, double series_rho, const double *q, int32_t tier, uint32_t flags, uint32_t nx,
@@ -292,6 +304,8 @@ int emu_render_window(const double *re, const double *im, uint64_t len, const do
   p.queue = &queue;
   p.counters = &cnt;
   p.timed_out = &timed_out;
+  p.deadline_ns = win ? win->deadline_ns : 0;
+  emu_clock::ticks = 0;
   if (series) {
     p.series_b = (const double2 *)series_b;
     p.series_order = series_order;
@@ -322,7 +336,7 @@ int emu_render_window(const double *re, const double *im, uint64_t len, const do
     else bla ? launch<false, false, true, false, false>(p) : launch<false, false, false, false, false>(p);
   }
   copy_counters(cnt, counters);
-  return 0;
+  return timed_out ? 1 : 0;
 }
 
 int emu_render(const double *re, const double *im, uint64_t len, const double *blocks7, const uint64_t *level_offsets,

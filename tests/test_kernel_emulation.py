@@ -51,10 +51,11 @@ def emu():
 
 class Window(C.Structure):
     """emu.cpp's EmuWindow: fdc_job's window, mask and offsets (whole-frame arrays), the
-    tile width 2^tile_shift and the tile order (0 row-major, 1 reversed)."""
+    tile width 2^tile_shift, the tile order (0 row-major, 1 reversed) and the deadline in
+    ns of the emulated clock (1 us per read)."""
     _fields_ = [("first_row", C.c_uint32), ("rows", C.c_uint32), ("first_col", C.c_uint32), ("cols", C.c_uint32),
                 ("tile_shift", C.c_uint32), ("tile_order", C.c_uint32), ("mask", C.c_void_p),
-                ("offsets", C.c_void_p)]
+                ("offsets", C.c_void_p), ("deadline_ns", C.c_uint64)]
 
 
 class Job(C.Structure):
@@ -74,7 +75,7 @@ def _ptr(a):
     return None if a is None else a.ctypes.data
 
 
-def emulate(emu, r, plane, tier, p, flags, bla=None, series=None, q=None, nucleus=None, win=None):
+def emulate(emu, r, plane, tier, p, flags, bla=None, series=None, q=None, nucleus=None, win=None, timed_out=False):
     n = p.nx * p.ny
     out = dict(cls=np.zeros(n, np.uint8), n=np.zeros(n, np.uint32), nu=np.zeros(n), de=np.zeros(n, np.float32),
                normal=np.zeros(n, np.uint16), z=np.zeros((n, 2)), dz=np.zeros((n, 2)), dexp=np.zeros(n, np.int64),
@@ -95,7 +96,7 @@ def emulate(emu, r, plane, tier, p, flags, bla=None, series=None, q=None, nucleu
             *[_ptr(out[k]) for k in ("cls", "n", "nu", "de", "normal", "z", "dz", "dexp", "status", "bound",
                                      "ez", "ed")], _ptr(cnt))
     rc = emu.emu_render(*args) if win is None else emu.emu_render_window(*args, C.byref(win))
-    assert rc == 0
+    assert rc == (1 if timed_out else 0)
     out["counters"] = dict(zip(("samples", "iterations", "blocks", "skipped", "fallback_samples",
                                 "closed_form_samples"), (int(c) for c in cnt)))
     return out
@@ -570,3 +571,43 @@ def test_precision_form_batch_equals_single_frames(emu):
         total = np.sum([np.array(arr[i].counters, dtype=np.uint64) for i in ids], axis=0)
         assert [int(c) for c in total] == [single["counters"][k] for k in (
             "samples", "iterations", "blocks", "skipped", "fallback_samples", "closed_form_samples")]
+
+
+@pytest.mark.parametrize("case", ["f64", "scaled-bla", "precision"])
+def test_deadline_stops_taking_samples(emu, case):
+    """A job's deadline (fdc_job.deadline_ms; here on the emulated clock, 1 us per read):
+    once it has passed, warps take no new samples, finish the ones they hold and raise the
+    timed-out flag (FDC_TIMEOUT). Exactly the samples taken are written (status 1, equal
+    to the unlimited render's), the rest keep zeroed columns and status 0, and the counters
+    cover the finished samples only."""
+    if case == "f64":
+        view3, nx, ny, it, flags = ("-0.7453", "0.1127", "0.0065"), 40, 24, 4_000, 1
+    else:
+        view3, nx, ny, it, flags = ("0", "1", "1e-300"), 32, 16, 5_000, 3 | (16 if case == "precision" else 0)
+    v, p, plane, t, r = _setup(view3, nx, ny, it)
+    table = None
+    if flags & 2:
+        dc, e = fd.bla_dc_bound(v, p)
+        table = fd.Bla.build_scaled(r, fd.route.EPS, dc, e)
+    full = emulate(emu, r, plane, t, p, flags, bla=table)
+    took = 150  # the clock's first read is the kernel's start: a deadline of 1000 k ns admits k pickups
+    got = emulate(emu, r, plane, t, p, flags, bla=table, win=Window(0, 0, 0, 0, 3, 0, None, None, 1000 * took),
+                  timed_out=True)
+    done = got["status"] != 0
+    assert done.sum() == took == got["counters"]["samples"]
+    # one lane takes queue slots in order: slot s is lane s % 32 of row-major 8x4 tile s // 32
+    slots = np.arange(took)
+    tile, lane = slots // 32, slots % 32
+    tiles_x = (nx + 7) // 8
+    i, j = (tile % tiles_x) * 8 + lane % 8, (tile // tiles_x) * 4 + lane // 8
+    assert np.array_equal(np.flatnonzero(done), np.sort(j * nx + i))
+    for k in ("cls", "n", "nu", "de", "normal", "z", "dz", "dexp"):
+        assert np.array_equal(got[k][done], full[k][done]), k
+        assert not got[k][~done].any(), k
+    c = got["counters"]
+    assert c["iterations"] == int(got["n"][done].astype(np.int64).sum()) - c["skipped"] + c["blocks"]
+    # a deadline the frame does not reach changes nothing
+    late = emulate(emu, r, plane, t, p, flags, bla=table, win=Window(0, 0, 0, 0, 3, 0, None, None, 1 << 40))
+    for k in ("cls", "n", "nu", "z", "status"):
+        assert np.array_equal(late[k], full[k]), k
+    assert late["counters"] == full["counters"]
