@@ -9,7 +9,9 @@ under tests/golden/ are what the tests read. Sources, all from junovhs/fractodac
                                            k=7676 rung of tools/research/misiurewicz/ladder_rungs.txt,
                                            and the series frames (centre, width) of
                                            docs/2026-10-20/series-frames/results/frames.txt, which
-                                           crates/fd-kernel/src/series.rs tests read
+                                           crates/fd-kernel/src/series.rs tests read, and the
+                                           mpmath orbit point of crates/fd-fixed/tests/fixtures/v0_orbit.txt
+                                           (c, period, z_period and z/dz at 400 digits)
   kern05.json                              per-frame digests of crates/fd-kernel/fixtures/KERN-05.bundle
                                            (format: crates/fd-kernel/examples/kernel_contract.rs:82-96)
                                            plus the bench/locations.txt rows that produced them
@@ -64,7 +66,14 @@ def main(root):
             continue
         f = line.split()
         series_frames.append({"re": f[0], "im": f[1], "width": f[2]})
-    kats = {"v0": {"re": v0[0], "im": v0[1]}, "fnv_views": fnv, "rung_7676": rung, "series_frames": series_frames}
+    v0_orbit = {}
+    for line in open(os.path.join(root, "crates/fd-fixed/tests/fixtures/v0_orbit.txt")):
+        if line.startswith("#") or not line.strip():
+            continue
+        f = line.split()
+        v0_orbit[f[0]] = f[1:] if len(f) > 2 else f[1]
+    kats = {"v0": {"re": v0[0], "im": v0[1]}, "fnv_views": fnv, "rung_7676": rung, "series_frames": series_frames,
+            "v0_orbit": v0_orbit}
     with open(os.path.join(HERE, "kats.json"), "w") as f:
         json.dump(kats, f, indent=1)
 

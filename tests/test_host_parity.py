@@ -89,6 +89,24 @@ def test_fixed_orbit_escaping_and_rung():
 
 
 @pytest.mark.parametrize("threads", [1, 3])
+def test_fixed_orbit_reaches_the_mpmath_nucleus_return(threads):
+    """The period-764 nucleus orbit of crates/fd-fixed/tests/fixtures/v0_orbit.txt at
+    1,400 bits: the host orbit equals the oracle's bit for bit, lands within one ulp of
+    mpmath's 400-digit z_764 (~6e-54) and the nucleus gate finds the period."""
+    f = KATS["v0_orbit"]
+    period = int(f["period"])
+    a = fdref.Ref.fixed(f["c"][0], f["c"][1], 1400, 2 * period + 10)
+    b = fd.Reference.from_fixed(f["c"][0], f["c"][1], 1400, 2 * period + 10, threads=threads)
+    ar, ai = a.arrays_()
+    assert np.array_equal(ar.view(np.uint64), b.re.view(np.uint64))
+    assert np.array_equal(ai.view(np.uint64), b.im.view(np.uint64))
+    want = np.array([float(f["z"][0]), float(f["z"][1])])
+    got = np.array([b.re[period], b.im[period]])
+    assert np.all(np.abs(got - want) <= np.spacing(np.abs(want)))
+    assert b.nucleus_period() == a.nucleus_period() == period
+
+
+@pytest.mark.parametrize("threads", [1, 3])
 def test_fixed_orbit_shared_squarings_bit_exact(threads):
     """A wide orbit (3,456 bits, 55 limbs) whose step squarings run on three threads equals
     the serial one and the oracle's, bit for bit; so does one below the threshold."""

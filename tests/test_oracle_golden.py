@@ -233,3 +233,20 @@ def test_kern05_bundle_frames():
         assert counts[0] == fr["classes"][0]
         assert abs(counts[1] - fr["classes"][1]) <= 2 and counts[1] + counts[2] == sum(fr["classes"][1:])
     assert exact >= 7
+
+
+def test_fixed_orbit_reaches_the_mpmath_nucleus_return():
+    """crates/fd-fixed/tests/fixtures/v0_orbit.txt (mpmath at 400 digits): from c given to
+    78 digits, z_764 of the period-764 nucleus orbit. The fixed-point orbit at 1,400 bits
+    (orbit.rs:14-43, the f64 rounding of lib.rs:75-83) lands within one ulp of it on both
+    parts, although |z_764| ~ 6e-54 (a relative error of the fixed point's 2^-1400 grown
+    by |dz/dc| ~ 2^83 leaves ~1,000 bits to spare), and the nucleus gate finds the period."""
+    f = KATS["v0_orbit"]
+    period = int(f["period"])
+    r = fdref.Ref.fixed(f["c"][0], f["c"][1], 1400, 2 * period + 10)  # the gate reads z_2p (reference.rs:102-120)
+    re_, im_ = r.arrays_()
+    want = np.array([float(f["z"][0]), float(f["z"][1])])
+    got = np.array([re_[period], im_[period]])
+    assert np.all(np.abs(got - want) <= np.spacing(np.abs(want))), (got, want)
+    assert abs(want[0]) < 1e-53 and abs(want[1]) < 1e-53
+    assert r.nucleus_period() == period
