@@ -349,6 +349,26 @@ def test_route_reproduces_reference_fds_hashes(dev, case):
     assert fdref.fnv1a64(fds.encode(h, s, minor=0)) == int(case["fnv"], 16)
 
 
+MPMATH = json.load(open(os.path.join(ROOT, "tests", "golden", "mpmath_checks.json")))
+
+
+@pytest.mark.parametrize("rec", MPMATH, ids=lambda r: r["name"])
+def test_route_writes_the_renders_mpmath_passed(dev, rec):
+    """The route end to end (host orbit, host BLA builder, CUDA kernel, host encoder, .fds
+    writer) writes, once its kernel-id suffix is taken off, the very bytes the reference's
+    independent mpmath checker (tools/oracle.py) passed (tests/golden/mpmath_checks.json)."""
+    from fractodactyl_b200 import fds
+    view = fd.View(rec["re"], rec["im"], rec["width"], rec["rotation"])
+    p = fd.Params(rec["nx"], rec["ny"], max_iter=rec["max_iter"], columns=("nu", "de", "normal"))
+    if rec["bla_eps"] is None:
+        h, s, _, _ = fd.render_with(view, p, dev=dev, host_encode=True)
+    else:
+        h, s, _, bs = fd.render_bla(view, p, eps=rec["bla_eps"], dev=dev, host_encode=True)
+        assert bs is not None and bs.blocks > 0
+    h.kernel = h.kernel.replace(" gpu-perturb-cuda/1", "")
+    assert "0x%016x" % fdref.fnv1a64(fds.encode(h, s)) == rec["fnv"]
+
+
 @pytest.mark.parametrize("tile_w", [1, 8, 32])
 def test_ragged_windows_and_tile_shapes(dev, tile_w):
     """Windows of odd sizes at the grid's edges (one column, one row, a single sample,

@@ -250,3 +250,32 @@ def test_fixed_orbit_reaches_the_mpmath_nucleus_return():
     assert np.all(np.abs(got - want) <= np.spacing(np.abs(want))), (got, want)
     assert abs(want[0]) < 1e-53 and abs(want[1]) < 1e-53
     assert r.nucleus_period() == period
+
+
+MPMATH = json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "mpmath_checks.json")))
+
+
+@pytest.mark.parametrize("rec", MPMATH, ids=lambda r: r["name"])
+def test_renders_the_mpmath_checker_passed(rec):
+    """tests/golden/make_mpmath_checks.py ran the reference's independent mpmath checker
+    (tools/oracle.py: direct iteration at depth + 128 bits; class exact, nu / de / normal
+    within 1e-3 output pixels) on the oracle's .fds renders of these views (three tiers, BLA
+    on and off, rotation, interior samples in and outside the main components); it passed
+    every sampled point. The oracle still writes those exact bytes."""
+    assert rec["exit"] == 0 and rec["checker"]["ok"] and rec["checker"]["class_mismatch"] == 0
+    job = fdref.make_job(rec["re"], rec["im"], rec["width"], rec["nx"], rec["ny"], rec["max_iter"],
+                         rotation=rec["rotation"], columns=fdref.COL_NU | fdref.COL_DE | fdref.COL_NORMAL, threads=2)
+    ref = bla = None
+    if rec["bla_eps"] is not None:
+        ref = fdref.Ref.for_job(job)
+        dc, e = fdref.bla_dc_bound(job)
+        bla = fdref.Bla(ref, rec["bla_eps"], dc, e)
+    data = fdref.render_fds(job, ref, bla)
+    assert "0x%016x" % fdref.fnv1a64(data) == rec["fnv"]
+
+
+def test_mpmath_checks_cover_every_class_and_tier():
+    kernels = {r["checker"]["kernel"].split()[0] for r in MPMATH}
+    assert kernels == {"pert-f64/1", "pert-fx/1", "pert-fx-scaled/1"}
+    assert any("bla/1" in r["checker"]["kernel"] for r in MPMATH)
+    assert sum(r["checker"]["samples"] - r["checker"]["escaped"] for r in MPMATH) > 30  # bounded samples
