@@ -595,6 +595,18 @@ def render_with(view: View, p: Params, orbit=None, bla: Optional[Bla] = None, de
     reference_seconds = time.perf_counter() - t
     if bla is not None and bla.points != len(r):
         raise ValueError(f"BLA table covers a {bla.points}-point orbit, not this {len(r)}-point one")
+    # A table without levels skips nothing: its samples are the plain kernel's, so it is not
+    # uploaded; the header and BlaStats stay render_bla's (grid.rs:526-529), and its
+    # refusals (grid.rs:392-411), which the device checks for uploaded tables, are checked here.
+    table = bla if bla is not None and bla.levels > 0 else None
+    if bla is not None and table is None:
+        if p.escape_radius < 4.0:
+            raise ValueError("escape radius is below 4: BLA blocks may only skip iterates with |z| <= 2 (1 + 2 eps)")
+        dc, e = bla_dc_bound(view, p)
+        over = dc > bla.dc_max if e == bla.dc_exp else \
+            math.log2(dc) + e > math.log2(bla.dc_max) + bla.dc_exp
+        if math.isnan(dc) or over:
+            raise ValueError("view reaches |dc| beyond the BLA table's dc_max")
     if series is not None:
         if tier == 2:
             raise ValueError("a series start needs f64 deltas and no Bound column")
@@ -604,16 +616,16 @@ def render_with(view: View, p: Params, orbit=None, bla: Optional[Bla] = None, de
         if math.isnan(dc) or dc > series.rho:
             raise ValueError(f"view reaches |dc| = {dc:e}, beyond the series radius {series.rho:e}")
     dev = dev or device(0)
-    h = dev.upload(r, bla)
+    h = dev.upload(r, table)
     try:
         flags = (_lib.DERIVATIVE if p.needs_derivative() or (bound and tier != 2) else 0) | \
-            (_lib.BLA if bla is not None else 0)
+            (_lib.BLA if table is not None else 0)
         if series is not None:
             dev.upload_series(h, series)
             flags |= _lib.SERIES
         if bound and tier != 2:  # grid.rs:588-593: the ordinary tiers' error radii
             dev.upload_error_radius(h, r.error_radius(None if tier == 0 else bits, plane.c_re, plane.c_im))
-        if bla is not None and shift and p.needs_derivative():
+        if table is not None and shift and p.needs_derivative():
             flags |= _lib.SHIFT
         job = make_job(plane, tier, p, h, r.nucleus_period(), flags)
         g = time.perf_counter()
@@ -634,10 +646,14 @@ def render_with(view: View, p: Params, orbit=None, bla: Optional[Bla] = None, de
         encode_host(plane, p.ss, s, p.columns, p.threads)
     stats = Stats(len(r), reference_seconds, int(cnt.iterations))
     bstats = None
-    if bla is not None:
+    if table is not None:
         bstats = BlaStats(int(cnt.blocks), int(cnt.skipped), int(cnt.fallback_samples),
                           int(cnt.closed_form_samples),
                           cnt.shift / (plane.h() * p.ss) if (flags & _lib.SHIFT) else None)
+    elif bla is not None:  # no block anywhere: closed-form interiors, every other sample a fallback
+        closed = int((((arrays["cls"] & 3) == 1) & (arrays["n"] == 0) & (arrays["status"] != 0)).sum())
+        bstats = BlaStats(0, 0, int(cnt.samples) - closed, closed,
+                          0.0 if (shift and p.needs_derivative()) else None)
     rep = report if report is not None else RouteReport()
     rep.device = f"cuda:{dev.index}"
     rep.accepted = int(cnt.samples)
@@ -680,7 +696,4 @@ def render_bla(view: View, p: Params, orbit=None, eps: float = EPS, **kw):
     table = Bla.build_scaled(orbit[0], eps, dc, e, p.threads)
     report = kw.pop("report", None) or RouteReport()
     report.table_seconds = time.perf_counter() - t
-    if table.levels == 0:
-        h, s, st, _ = render_with(view, p, orbit, None, report=report, **kw)
-        return h, s, st, None
     return render_with(view, p, orbit, table, report=report, **kw)

@@ -356,7 +356,9 @@ MPMATH = json.load(open(os.path.join(ROOT, "tests", "golden", "mpmath_checks.jso
 def test_route_writes_the_renders_mpmath_passed(dev, rec):
     """The route end to end (host orbit, host BLA builder, CUDA kernel, host encoder, .fds
     writer) writes, once its kernel-id suffix is taken off, the very bytes the reference's
-    independent mpmath checker (tools/oracle.py) passed (tests/golden/mpmath_checks.json)."""
+    independent mpmath checker (tools/oracle.py) passed (tests/golden/mpmath_checks.json),
+    and render_bla's BlaStats equal the oracle's, also for the seahorse table that admits
+    no level at eps 2^-50 (grid.rs:526-529: the header still says bla/1)."""
     from fractodactyl_b200 import fds
     view = fd.View(rec["re"], rec["im"], rec["width"], rec["rotation"])
     p = fd.Params(rec["nx"], rec["ny"], max_iter=rec["max_iter"], columns=("nu", "de", "normal"))
@@ -364,7 +366,15 @@ def test_route_writes_the_renders_mpmath_passed(dev, rec):
         h, s, _, _ = fd.render_with(view, p, dev=dev, host_encode=True)
     else:
         h, s, _, bs = fd.render_bla(view, p, eps=rec["bla_eps"], dev=dev, host_encode=True)
-        assert bs is not None and bs.blocks > 0
+        job = fdref.make_job(rec["re"], rec["im"], rec["width"], rec["nx"], rec["ny"], rec["max_iter"],
+                             rotation=rec["rotation"], columns=fdref.COL_NU | fdref.COL_DE | fdref.COL_NORMAL,
+                             threads=2)
+        ref = fdref.Ref.for_job(job)
+        dc, e = fdref.bla_dc_bound(job)
+        want = fdref.render(job, ref, fdref.Bla(ref, rec["bla_eps"], dc, e))["stats"]
+        assert (bs.blocks, bs.skipped, bs.fallback_samples, bs.closed_form_samples) == (
+            want["blocks"], want["skipped"], want["fallback_samples"], want["closed_form_samples"])
+        assert h.kernel.endswith(" bla/1 gpu-perturb-cuda/1")
     h.kernel = h.kernel.replace(" gpu-perturb-cuda/1", "")
     assert "0x%016x" % fdref.fnv1a64(fds.encode(h, s)) == rec["fnv"]
 
