@@ -282,7 +282,7 @@ int emu_render_window(const double *re, const double *im, uint64_t len, const do
                       uint32_t *n_out, double *nu, float *de, uint16_t *normal, double *z_out, double *dz_out,
                       int64_t *dexp_out, uint8_t *status, float *bound, double *ez, double *ed, uint64_t *counters,
                       const EmuWindow *win) {
-  const bool ext = tier == 2, deriv = flags & 1, bla = (flags & 2) && levels > 0, series = (flags & 4) && series_n > 0,
+  const bool ext = tier == 2, deriv = flags & 1, bla = (flags & 2) != 0, series = (flags & 4) && series_n > 0,
              bounded = (flags & 8) && !ext, f32 = flags & 16;
   if (len < 3 || (bla && bounded) || (series && (ext || bounded)) || (f32 && (series || bounded)))
     return -1;  // the route's refusals
@@ -365,7 +365,7 @@ int emu_render_batch(EmuJob *jobs, uint32_t njobs) {
     auto s = std::make_unique<Setup>();
     s->ext = j.tier == 2;
     s->deriv = j.flags & 1;
-    s->bla = (j.flags & 2) && j.levels > 0;
+    s->bla = (j.flags & 2) != 0;
     stage_orbit(*s, j.re, j.im, j.len, j.blocks7, j.level_offsets, j.levels);
     if (!stage_frame(*s, j.tier, j.nx, j.ny, j.ss, j.c_re, j.c_im, j.h_m, j.h_e, j.cos_rot, j.sin_rot, j.max_iter,
                      j.escape_radius, j.nucleus, j.first_row, j.rows, j.first_col, j.cols, 3, nullptr, nullptr,

@@ -611,3 +611,25 @@ def test_deadline_stops_taking_samples(emu, case):
     for k in ("cls", "n", "nu", "z", "status"):
         assert np.array_equal(late[k], full[k]), k
     assert late["counters"] == full["counters"]
+
+
+@pytest.mark.parametrize("view3,it", [(("-0.7436438870371587", "0.1318259042053120", "1e-12"), 20_000),
+                                      (("-0.75", "0.1", "0.4"), 2_000)])
+def test_bla_kernel_with_a_table_without_levels(emu, view3, it):
+    """A table that admits no level (eps 2^-50 at these depths) uploaded as it is, as a
+    caller of fdc_upload_bla may: the BLA kernel skips nothing, so every sample equals the
+    plain kernel's, and its counters are the reference's for such a table (no block,
+    closed-form interiors, every other sample a fallback: grid.rs:767-768)."""
+    v, p, plane, t, r = _setup(view3, 48, 32, it)
+    dc, e = fd.bla_dc_bound(v, p)
+    table = fd.Bla.build_scaled(r, fd.route.EPS, dc, e)
+    assert table.levels == 0
+    plain = emulate(emu, r, plane, t, p, 1)
+    got = emulate(emu, r, plane, t, p, 1 | 2, bla=table)
+    for k in ("cls", "n", "z", "dz", "dexp", "nu", "de", "normal", "status"):
+        assert np.array_equal(got[k], plain[k]), k
+    ref = fdref.Ref.arrays(r.re, r.im, r.bits)
+    want = fdref.render(_oracle_job(view3, p, t, fdref.COL_NU | fdref.COL_DE | fdref.COL_NORMAL), ref,
+                        fdref.Bla(ref, fd.route.EPS, table.dc_max, table.dc_exp))["stats"]
+    for k in ("iterations", "blocks", "skipped", "fallback_samples", "closed_form_samples"):
+        assert got["counters"][k] == want[k], k
