@@ -49,6 +49,40 @@ def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
+EPS = 2.0 ** -50  # exact-mode BLA tolerance (crates/fd-cli/src/orbit.rs:16)
+LOCATIONS = os.path.join(ROOT, "fractodactyl_b200", "locations.json")
+
+
+def workload(args):
+    """The frame of configuration 1 or 2 as plain values for the reference arm, read with
+    json from fractodactyl_b200/locations.json: the CPU arm imports and loads nothing of
+    the CUDA route (fractodactyl_b200.locations.config1/config2 give the same frame)."""
+    from types import SimpleNamespace as NS
+    if args.config == 1:
+        fr = NS(name="c1-480x270-1e-12", view=NS(center_re="-0.7436438870371587", center_im="0.1318259042053120",
+                                                    width="1e-12", rotation=0.0),
+                params=NS(nx=480, ny=270, max_iter=20_000, escape_radius=256.0, columns=("nu",), tier=None),
+                bla_eps=None, period=None)
+    else:
+        with open(LOCATIONS) as f:
+            hit = [d for d in json.load(f)["c2"] if d["seed"] == args.seed]
+        if not hit:
+            raise SystemExit(f"configuration 2 with seed {args.seed} is not in {LOCATIONS}")
+        d = hit[0]
+        fr = NS(name=f"c2-1920x1080-1e-100-seed{args.seed}", view=NS(center_re=d["re"], center_im=d["im"],
+                                                                       width="1e-100", rotation=0.0),
+                params=NS(nx=1920, ny=1080, max_iter=1_000_000, escape_radius=1e10,
+                          columns=("nu", "de", "normal"), tier="scaled"),
+                bla_eps=EPS, period=d["period"])
+    if args.nx or args.ny:
+        fr.params.nx, fr.params.ny = args.nx or fr.params.nx, args.ny or fr.params.ny
+        fr.name += f"-grid{fr.params.nx}x{fr.params.ny}"
+    if args.tier:
+        fr.params.tier = args.tier
+        fr.name += f"-{args.tier}"
+    return fr
+
+
 def frame_for(args):
     from fractodactyl_b200 import locations
     fr = locations.config1() if args.config == 1 else locations.config2(seed=args.seed)
@@ -171,7 +205,7 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    fr = frame_for(args)
+    fr = workload(args)
     fdref, job, ref, bla, sample, step, setup, cores = reference_arm(args, fr)
     for _ in range(args.warmup):
         pass  # the CPU kernel has no warm state worth priming; warm-up steps are not repeated work

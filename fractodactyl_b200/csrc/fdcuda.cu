@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <condition_variable>
 #include <map>
@@ -171,6 +172,19 @@ namespace {
 fdc_status fail(fdc_ctx *c, fdc_status s, const std::string &msg) {
   if (c) c->err = msg;
   return s;
+}
+
+// An f64 as Rust's Display prints the values a refusal message names: the shortest
+// decimal that reads back to the same double, without a trailing ".0", NaN as "NaN".
+std::string rust_f64(double x) {
+  if (std::isnan(x)) return "NaN";
+  if (std::isinf(x)) return x > 0 ? "inf" : "-inf";
+  char buf[64];
+  for (int digits = 1; digits <= 17; ++digits) {
+    std::snprintf(buf, sizeof buf, "%.*g", digits, x);
+    if (std::strtod(buf, nullptr) == x) break;
+  }
+  return buf;
 }
 
 #define CK(call)                                                                                  \
@@ -535,8 +549,11 @@ fdc_status prepare(fdc_ctx *ctx, const OrbitDev &o, const fdc_job &j, fdk::Param
   if (bla) {
     if (!o.has_bla) return fail(ctx, FDC_INVALID, "FDC_BLA without an uploaded BLA table");
     // grid.rs:392-411
-    if (j.escape_radius < 4.0)
-      return fail(ctx, FDC_INVALID, "escape radius is below 4: BLA blocks may only skip iterates with |z| <= 2 (1 + 2 eps)");
+    if (std::isnan(j.escape_radius) || j.escape_radius < 4.0)
+      return fail(ctx, FDC_INVALID,
+                  "escape radius " + rust_f64(j.escape_radius) +
+                      " is below 4: BLA blocks may only skip iterates with |z| <= 2 (1 + 2 eps), which needs escape "
+                      "radius >= 4");
     const double half = largest_offset();
     double dc = ext ? j.h_m * half : h * half;
     int64_t e = ext ? j.h_e : 0;

@@ -8,7 +8,9 @@
 // Built with -fmad=false, like the other plain-form kernels: results are the same bits.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstring>
+#include <mutex>
 #include <string>
 
 #include "../../include/fdcuda.h"
@@ -23,13 +25,29 @@ constexpr unsigned long long HEADER_BYTES = 256;  // queue head, counters, deadl
 // Layout: [0] queue head, [8..71] Counters, [72] timed-out flag, [256..] row sums (u64).
 static __device__ __align__(256) unsigned char noalloc_scratch[SCRATCH_BYTES];
 
+// Set-up per device: the array's device address, the SM count and the resident blocks
+// per kernel variant. `ready` is published after the fields under g_setup, so concurrent
+// first calls on one device do the set-up once and every caller sees it complete.
 struct PerDevice {
-  bool ready = false;
+  std::atomic<bool> ready{false};
   unsigned char *scratch = nullptr;
   int sm_count = 0;
-  int blocks_per_sm[8] = {};
+  std::atomic<int> blocks_per_sm[4] = {};
 };
 PerDevice g_devices[64];
+std::mutex g_setup;
+
+// Puts the calling thread's current device back on every return.
+struct CurrentDevice {
+  int prev = -1;
+  ~CurrentDevice() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+// The checks fdc_open makes (a present sm_100 device), then the scratch array's device
+// address with `device` current. Called under g_setup.
+fdc_status setup_device(int device, PerDevice &pd, char *error, size_t cap);
 // Copies a message into the caller's error buffer (if any) and returns the status.
 fdc_status fail(fdc_status s, const std::string &m, char *error, size_t cap) {
   if (error && cap) {
@@ -105,6 +123,37 @@ void *noalloc_kernel(bool ext, bool d, int &variant) {
   }
 }
 
+fdc_status setup_device(int device, PerDevice &pd, char *error, size_t cap) {
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess)
+    return fail(FDC_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e), error, cap);
+  if (device >= count)
+    return fail(FDC_NO_DEVICE, "no CUDA device " + std::to_string(device) + " (" + std::to_string(count) + " present)",
+                error, cap);
+  cudaDeviceProp prop;
+  e = cudaGetDeviceProperties(&prop, device);
+  if (e != cudaSuccess)
+    return fail(FDC_NO_DEVICE, std::string("device properties: ") + cudaGetErrorString(e), error, cap);
+  if (prop.major != 10)
+    return fail(FDC_NO_DEVICE, "device " + std::to_string(device) + " is sm_" + std::to_string(prop.major) +
+                                   std::to_string(prop.minor) + ", not sm_100",
+                error, cap);
+  e = cudaSetDevice(device);
+  if (e != cudaSuccess) return fail(FDC_DEVICE_ERROR, std::string("cudaSetDevice: ") + cudaGetErrorString(e), error, cap);
+  void *ptr = nullptr;
+  e = cudaGetSymbolAddress(&ptr, noalloc_scratch);
+  if (e != cudaSuccess)
+    return fail(FDC_DEVICE_ERROR, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e), error, cap);
+  pd.scratch = (unsigned char *)ptr;
+  pd.sm_count = prop.multiProcessorCount;
+  pd.ready.store(true, std::memory_order_release);
+  return FDC_OK;
+}
+
+// A device pointer the kernel reads or writes as `align`-byte words must be aligned to it.
+bool misaligned(const void *ptr, uintptr_t align) { return ptr && ((uintptr_t)ptr & (align - 1)) != 0; }
+
 }  // namespace
 
 extern "C" fdc_status fdc_render_noalloc(int device, const double *orbit, uint64_t len, const fdc_job *job,
@@ -141,20 +190,32 @@ extern "C" fdc_status fdc_render_noalloc(int device, const double *orbit, uint64
                                  " (at most " + std::to_string((SCRATCH_BYTES - HEADER_BYTES) / 8) +
                                  " rows per call)",
                 error, error_cap);
+  // The kernel loads the orbit and stores z and dz as 16-byte words, the other columns
+  // as words of their own size: a pointer off that boundary would fault on the GPU.
+  if (misaligned(orbit, 16)) return fail(FDC_INVALID, "orbit must be 16-byte aligned", error, error_cap);
+  const struct {
+    const void *ptr;
+    uintptr_t align;
+    const char *name;
+  } columns[] = {{out->z, 16, "z"},  {out->dz, 16, "dz"}, {out->nu, 8, "nu"},        {out->dexp, 8, "dexp"},
+                 {out->n, 4, "n"},   {out->de, 4, "de"},  {out->normal, 2, "normal"}};
+  for (const auto &c : columns)
+    if (misaligned(c.ptr, c.align))
+      return fail(FDC_INVALID, std::string("output column ") + c.name + " must be " + std::to_string(c.align) +
+                                   "-byte aligned",
+                  error, error_cap);
+  CurrentDevice current;
+  if (cudaGetDevice(&current.prev) != cudaSuccess) current.prev = -1;
+  PerDevice &pd = g_devices[device];
+  if (!pd.ready.load(std::memory_order_acquire)) {  // set-up, once per device
+    std::lock_guard<std::mutex> lock(g_setup);
+    if (!pd.ready.load(std::memory_order_relaxed)) {
+      fdc_status st = setup_device(device, pd, error, error_cap);
+      if (st != FDC_OK) return st;
+    }
+  }
   cudaError_t e = cudaSetDevice(device);
   if (e != cudaSuccess) return fail(FDC_DEVICE_ERROR, std::string("cudaSetDevice: ") + cudaGetErrorString(e), error, error_cap);
-  PerDevice &pd = g_devices[device];
-  if (!pd.ready) {  // set-up, once per device, with the device current
-    void *ptr = nullptr;
-    e = cudaGetSymbolAddress(&ptr, noalloc_scratch);
-    if (e != cudaSuccess) return fail(FDC_DEVICE_ERROR, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e), error, error_cap);
-    int sms = 0;
-    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    if (e != cudaSuccess) return fail(FDC_DEVICE_ERROR, std::string("device attribute: ") + cudaGetErrorString(e), error, error_cap);
-    pd.scratch = (unsigned char *)ptr;
-    pd.sm_count = sms;
-    pd.ready = true;
-  }
   cudaStream_t st = (cudaStream_t)stream;
   const bool ext = j.tier == FDC_TIER_SCALED, deriv = (j.flags & FDC_DERIVATIVE) != 0;
   fdk::Params p{};
@@ -209,14 +270,16 @@ extern "C" fdc_status fdc_render_noalloc(int device, const double *orbit, uint64
   if (e != cudaSuccess) return fail(FDC_DEVICE_ERROR, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e), error, error_cap);
   int variant = 0;
   void *fn = noalloc_kernel(ext, deriv, variant);
-  if (!pd.blocks_per_sm[variant]) {
+  int resident = pd.blocks_per_sm[variant].load(std::memory_order_relaxed);
+  if (!resident) {  // the same value whichever thread computes it first
     int b = 0;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, 128, 0);
     if (e != cudaSuccess) return fail(FDC_DEVICE_ERROR, std::string("occupancy: ") + cudaGetErrorString(e), error, error_cap);
-    pd.blocks_per_sm[variant] = b > 0 ? b : 1;
+    resident = b > 0 ? b : 1;
+    pd.blocks_per_sm[variant].store(resident, std::memory_order_relaxed);
   }
   void *args[] = {&p, &row_sums};
-  e = cudaLaunchKernel(fn, dim3(pd.sm_count * pd.blocks_per_sm[variant]), dim3(128), args, 0, st);
+  e = cudaLaunchKernel(fn, dim3(pd.sm_count * resident), dim3(128), args, 0, st);
   if (e != cudaSuccess) return fail(FDC_DEVICE_ERROR, std::string("launch: ") + cudaGetErrorString(e), error, error_cap);
   if (row_iterations || counters) {
     unsigned char head[HEADER_BYTES];

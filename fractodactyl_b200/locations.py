@@ -7,7 +7,7 @@ then the ladder nucleus next to it whose size is about width/30, found by the ba
 period and Newton in fixed point at the stated precision.
 
 The recipe takes minutes per centre beyond ~1e-300 (about 5 at 1e-1000), so the centres
-of configurations 3-5 are computed once by `python -m fractodactyl_b200.locations
+of configurations 2-5 are computed once by `python -m fractodactyl_b200.locations
 --write` (all cores) into locations.json beside this file and read from there; the same
 command with --check recomputes and compares them.
 """
@@ -63,14 +63,20 @@ def config1() -> Frame:
 
 def config2(seed: int = 2, nx: int = 1920, ny: int = 1080, tier: Optional[str] = "scaled") -> Frame:
     """Plain perturbation + BLA with floatexp deltas: 1920x1080 at the seeded 400-bit ladder
-    nucleus, 1e-100 wide, 1,000,000 iterations, BLA table from the CPU builder (eps 2^-50)."""
-    re_, im_, p, rel = nucleus(seed, -100.0, 400)
+    nucleus, 1e-100 wide, 1,000,000 iterations, BLA table from the CPU builder (eps 2^-50).
+    The benchmark seed's centre is read from locations.json; other seeds are computed."""
+    hit = [d for d in cached("c2") if d["seed"] == seed] if os.path.exists(CACHE) else []
+    if hit:
+        re_, im_, p, rel = hit[0]["re"], hit[0]["im"], hit[0]["period"], hit[0]["log10_size_over_width"]
+    else:
+        re_, im_, p, rel = nucleus(seed, -100.0, C2_BITS)
     return Frame(f"c2-{nx}x{ny}-1e-100-seed{seed}", View(re_, im_, "1e-100"),
                  Params(nx, ny, max_iter=1_000_000, escape_radius=1e10, columns=("nu", "de", "normal"), tier=tier),
                  EPS, p, rel)
 
 
 CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "locations.json")
+C2_BITS = 400  # configuration 2's stated precision for its nucleus
 
 
 def centre_bits(log10_width: float) -> int:
@@ -80,16 +86,17 @@ def centre_bits(log10_width: float) -> int:
 
 
 def specs() -> Dict[str, List[dict]]:
-    """The seeded centres configurations 3-5 need: C3 one nucleus 1e-300 wide (seed 3);
-    C4 one nucleus for the deepest film frame, 1e-500 (seed 4); C5 32 nuclei with widths
-    log-uniform on [1e-1000, 1e-20] (seeds 5000 + k)."""
+    """The seeded centres the configurations need: C2 the 1e-100 nucleus at 400 bits (seed
+    2); C3 one nucleus 1e-300 wide (seed 3); C4 one nucleus for the deepest film frame,
+    1e-500 (seed 4); C5 32 nuclei with widths log-uniform on [1e-1000, 1e-20] (seeds
+    5000 + k). Configuration 1's centre is given as a decimal and needs no recipe."""
     rng = np.random.default_rng(5)
     c5 = [dict(seed=5000 + k, log10_width=float(w)) for k, w in enumerate(rng.uniform(-1000.0, -20.0, 32))]
     out = {"c3": [dict(seed=3, log10_width=-300.0)], "c4": [dict(seed=4, log10_width=-500.0)], "c5": c5}
     for v in out.values():
         for d in v:
             d["bits"] = centre_bits(d["log10_width"])
-    return out
+    return {"c2": [dict(seed=2, log10_width=-100.0, bits=C2_BITS)], **out}
 
 
 def _compute(d):

@@ -492,6 +492,22 @@ class Batch:
             self.h = C.c_void_p()
 
 
+def _rust_f64(x: float) -> str:
+    """f64's Display in Rust for the values a refusal message prints."""
+    if math.isnan(x):
+        return "NaN"
+    if math.isinf(x):
+        return "inf" if x > 0 else "-inf"
+    return str(int(x)) if x == int(x) and abs(x) < 1e16 else repr(x)
+
+
+def _check_bla_escape_radius(radius: float):
+    """grid.rs:393-398: a BLA table needs an escape radius of at least 4 (NaN refused)."""
+    if math.isnan(radius) or radius < 4.0:
+        raise ValueError(f"escape radius {_rust_f64(radius)} is below 4: BLA blocks may only skip iterates with "
+                         "|z| <= 2 (1 + 2 eps), which needs escape radius >= 4")
+
+
 def _setup(view: View, p: Params):
     """grid.rs:779-799."""
     if p.ss == 0 or p.nx % p.ss or p.ny % p.ss:
@@ -600,8 +616,7 @@ def render_with(view: View, p: Params, orbit=None, bla: Optional[Bla] = None, de
     # refusals (grid.rs:392-411), which the device checks for uploaded tables, are checked here.
     table = bla if bla is not None and bla.levels > 0 else None
     if bla is not None and table is None:
-        if p.escape_radius < 4.0:
-            raise ValueError("escape radius is below 4: BLA blocks may only skip iterates with |z| <= 2 (1 + 2 eps)")
+        _check_bla_escape_radius(p.escape_radius)
         dc, e = bla_dc_bound(view, p)
         over = dc > bla.dc_max if e == bla.dc_exp else \
             math.log2(dc) + e > math.log2(bla.dc_max) + bla.dc_exp
@@ -689,8 +704,7 @@ def render_bla(view: View, p: Params, orbit=None, eps: float = EPS, **kw):
     view's largest |dc| (control.rs:344-360), then the BLA kernel."""
     if orbit is None:
         orbit = reference(view, p)
-    if p.escape_radius < 4.0:
-        raise ValueError("escape radius is below 4: BLA blocks may only skip iterates with |z| <= 2 (1 + 2 eps)")
+    _check_bla_escape_radius(p.escape_radius)
     dc, e = bla_dc_bound(view, p)
     t = time.perf_counter()
     table = Bla.build_scaled(orbit[0], eps, dc, e, p.threads)

@@ -204,9 +204,13 @@ void fdc_batch_free(fdc_ctx *ctx, fdc_batch *batch);
  * array of FDC_NOALLOC_SCRATCH_BYTES, which every GPU that loads the library holds until
  * the process exits. That fixes the row limit: a job renders at most
  * (FDC_NOALLOC_SCRATCH_BYTES - 256) / 8 = 8160 rows per call (job->rows, or ny when 0);
- * larger jobs are refused with FDC_INVALID and a message naming the limit. The first
- * call on a device looks up the array's device address (once per device); make that
- * first call before any stream capture. Every call shares the array and clears what it
+ * larger jobs are refused with FDC_INVALID and a message naming the limit, and so are
+ * an orbit or z / dz column off a 16-byte boundary and any other column off its element
+ * size. The first call on a device checks it as fdc_open does (FDC_NO_DEVICE unless a
+ * present sm_100 device) and looks up the array's device address (once per device, safe
+ * under concurrent first calls); make that first call before any stream capture. The
+ * calling thread's current device is the same after the call as before it. Every call
+ * shares the array and clears what it
  * uses before its kernel runs: calls that overlap on the GPU (other streams, other host
  * threads) race on it, so serialise them. row_iterations (optional, host, `rows`
  * entries) receives the iterations spent per rendered row; counters (optional) the

@@ -16,7 +16,7 @@ under tests/golden/ are what the tests read. Sources, all from junovhs/fractodac
                                            (format: crates/fd-kernel/examples/kernel_contract.rs:82-96)
                                            plus the bench/locations.txt rows that produced them
 
-usage: python tests/golden/make_golden.py [REFERENCE_ROOT]
+usage: python tests/golden/make_golden.py REFERENCE_ROOT
 """
 import gzip
 import json
@@ -119,4 +119,6 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} REFERENCE_CHECKOUT (the junovhs/fractodactyl source tree)")
+    main(sys.argv[1])

@@ -7,7 +7,7 @@ compare hashes, so the bytes mpmath passed stay the oracle's and (through the pr
 byte-equality tests) the route's.
 
 Runs only where the reference tree is present (the checker is not copied here).
-usage: python tests/golden/make_mpmath_checks.py [REFERENCE_ROOT]
+usage: python tests/golden/make_mpmath_checks.py REFERENCE_ROOT
 """
 import json
 import os
@@ -68,4 +68,6 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit(f"usage: python {sys.argv[0]} REFERENCE_CHECKOUT (the junovhs/fractodactyl source tree)")
+    main(sys.argv[1])

@@ -60,3 +60,38 @@ def test_cuda_arm_fails_without_device():
     assert r.returncode != 0
     assert not [ln for ln in r.stdout.splitlines() if ln.startswith("{")]
     assert "NO_DEVICE" in r.stderr or "CUDA" in r.stderr
+
+
+@pytest.mark.parametrize("config", [1, 2])
+def test_reference_arm_frame_is_the_bench_frame(config):
+    """The reference arm reads its frame with json alone; it is the frame the CUDA arm
+    renders (fractodactyl_b200.locations), field for field."""
+    sys.path.insert(0, ROOT)
+    import argparse
+
+    import bench
+    from fractodactyl_b200 import locations
+    for extra in ({}, dict(nx=64, ny=36, tier="scaled")):
+        a = argparse.Namespace(config=config, seed=2, nx=extra.get("nx", 0), ny=extra.get("ny", 0),
+                               tier=extra.get("tier"))
+        w, f = bench.workload(a), bench.frame_for(a)
+        assert (w.name, w.bla_eps, w.period) == (f.name, f.bla_eps, f.period)
+        assert vars(w.view) == {k: getattr(f.view, k) for k in ("center_re", "center_im", "width", "rotation")}
+        for k in ("nx", "ny", "max_iter", "escape_radius", "columns", "tier"):
+            assert getattr(w.params, k) == getattr(f.params, k), k
+
+
+def test_reference_arm_loads_no_repo_library():
+    """The CPU arm of configuration 2 (whose centre the route's recipe computes) runs the
+    oracle only: libfdcuda.so is never mapped into its process."""
+    code = ("import sys, runpy; sys.argv = ['bench.py', '--impl', 'reference', '--config', '2', '--steps', '1', "
+            "'--warmup', '3', '--cpu-seconds', '0.2'];\n"
+            "runpy.run_path('bench.py', run_name='__main__')\n"
+            "maps = open('/proc/self/maps').read()\n"
+            "assert 'liboracle.so' in maps\n"
+            "print('MAPPED_FDCUDA' if 'libfdcuda.so' in maps else 'CLEAN')\n")
+    r = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert r.stdout.strip().splitlines()[-1] == "CLEAN"
+    line = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][0])
+    assert line["impl"] == "reference" and line["config"]["workload"] == "c2-1920x1080-1e-100-seed2"

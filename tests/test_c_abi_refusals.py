@@ -1,8 +1,9 @@
 """The C-ABI's refusals, which need no device: every entry point that takes a context
 returns FDC_INVALID for a null one (no crash, no CUDA call), the no-op teardown calls
 accept null, and the allocation-free entry point checks every argument before it touches
-a device, each refusal with its own message; a valid job on a host without a GPU then
-fails with FDC_DEVICE_ERROR naming the CUDA call. The route maps each status to an
+a device, each refusal with its own message (pointers off their element boundary
+included); a valid job on a host without a GPU then fails with FDC_NO_DEVICE, as
+fdc_open does. The route maps each status to an
 exception and never falls back to the CPU (frame.rs:357-368 leaves the restart to the
 caller)."""
 import ctypes as C
@@ -51,11 +52,17 @@ def _job(**kw):
     return j
 
 
-def _noalloc(L, job, orbit_len=100, orbit=True, out=True, device=0):
-    z = np.zeros(2 * max(orbit_len, 3))
+_HOLD = np.zeros(64)  # 16-byte aligned host memory; the refusals never touch it
+
+
+def _noalloc(L, job, orbit_len=100, orbit=True, out=True, device=0, orbit_offset=0, columns=None):
+    z = np.zeros(2 * max(orbit_len, 3) + 2)
     err = C.create_string_buffer(256)
-    st = L.fdc_render_noalloc(device, z.ctypes.data if orbit else None, orbit_len, C.byref(job),
-                              C.byref(_lib.Out()) if out else None, None, None, None, err, 256)
+    o = _lib.Out()
+    for name, off in (columns or {}).items():
+        setattr(o, name, _HOLD.ctypes.data + off)
+    st = L.fdc_render_noalloc(device, (z.ctypes.data + orbit_offset) if orbit else None, orbit_len, C.byref(job),
+                              C.byref(o) if out else None, None, None, None, err, 256)
     return st, err.value.decode()
 
 
@@ -90,6 +97,14 @@ REFUSALS = [
     ({}, dict(first_col=64), "column range"),
     ({}, dict(first_col=60, cols=5), "column range"),
     ({}, dict(ny=8192), "rows per call"),
+    (dict(orbit_offset=8), {}, "orbit must be 16-byte aligned"),
+    (dict(columns=dict(z=8)), {}, "column z must be 16-byte aligned"),
+    (dict(columns=dict(dz=8)), {}, "column dz must be 16-byte aligned"),
+    (dict(columns=dict(nu=4)), {}, "column nu must be 8-byte aligned"),
+    (dict(columns=dict(dexp=4)), {}, "column dexp must be 8-byte aligned"),
+    (dict(columns=dict(n=2)), {}, "column n must be 4-byte aligned"),
+    (dict(columns=dict(de=2)), {}, "column de must be 4-byte aligned"),
+    (dict(columns=dict(normal=1)), {}, "column normal must be 2-byte aligned"),
 ]
 
 
@@ -106,7 +121,13 @@ def test_noalloc_valid_job_without_device(L):
     ok = dict(rows=8160, ny=16320)  # the largest window one call takes, then ragged windows
     for fields in (ok, dict(first_row=8, rows=24), dict(first_col=60, cols=4), {}):
         st, err = _noalloc(L, _job(**fields))
-        assert st == _lib.DEVICE_ERROR and err.startswith("cudaSetDevice"), (fields, err)
+        assert st == _lib.NO_DEVICE and err.startswith("no CUDA device"), (fields, err)
+    # aligned columns of every element size pass the checks and meet the same device test
+    st, err = _noalloc(L, _job(), columns=dict(z=16, dz=32, nu=8, dexp=8, n=4, de=4, normal=2, cls=1, status=3))
+    assert st == _lib.NO_DEVICE, err
+    # the same status fdc_open gives for a host without a usable device
+    h = C.c_void_p()
+    assert L.fdc_open(0, C.byref(h)) == _lib.NO_DEVICE
     # a short error buffer is truncated and terminated, never overrun
     err = (C.c_char * 8)()
     z = np.zeros(200)

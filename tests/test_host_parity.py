@@ -198,6 +198,25 @@ def test_route_flag_and_declines():
         fd.route._setup(fd.View("0", "1", "1e-300"), fd.Params(8, 8, tier="f64"))
 
 
+@pytest.mark.parametrize("radius,shown", [(float("nan"), "NaN"), (3.5, "3.5"), (2.0, "2")])
+def test_bla_escape_radius_refusals(radius, shown):
+    """A BLA table needs an escape radius of at least 4, NaN refused (grid.rs:393-398),
+    with the reference's message: for a table without levels the route checks this on the
+    host, and render_bla before it builds the table. Nothing reaches a device."""
+    msg = f"escape radius {shown} is below 4: BLA blocks may only skip iterates with |z| <= 2 (1 + 2 eps), " \
+          "which needs escape radius >= 4"
+    view = fd.View("-0.7453", "0.1127", "1e-3")
+    p = fd.Params(8, 8, max_iter=200, escape_radius=radius)
+    r = fd.Reference.new(-0.7453, 0.1127, 200, 1e10)
+    empty = fd.Bla(np.zeros((0, 7)), np.zeros(1, np.uint64), 2.0 ** -50, 1e-5, 0, len(r))
+    with pytest.raises(ValueError) as e:
+        fd.render_with(view, p, (r, 53), empty)
+    assert str(e.value) == msg
+    with pytest.raises(ValueError) as e:
+        fd.render_bla(view, p, (r, 53))
+    assert str(e.value) == msg
+
+
 @pytest.mark.parametrize("case", KATS["fnv_views"], ids=lambda c: c["width"])
 def test_fds_writer_and_host_encoder_bytes(case):
     """fds.encode over the oracle's raw outcomes encoded by fdh_encode equals the oracle's
