@@ -167,6 +167,88 @@ def barrier(world):
         dist.barrier()
 
 
+def parity_vs_oracle(gpu, want, exact):
+    """The CUDA route's frame (host arrays, raw state) against the oracle's render of the
+    same frame. exact (the plain form): class, escape count, z, dz/dc and its exponent must
+    be bit-exact; the fractions equal are reported either way."""
+    cls_g, cls_o = gpu["cls"] & 3, want["cls"] & 3
+    n_g, n_o = gpu["n"].astype(np.int64), want["n"].astype(np.int64)
+    esc_g, esc_o = cls_g == 0, cls_o == 0
+    same_cls = cls_g == cls_o
+    same_n = same_cls & (n_g == n_o)
+    out = {"samples": int(len(cls_o)), "class_equal": float(same_cls.mean()), "count_equal": float(same_n.mean()),
+           "within_one": float((same_cls & (np.abs(n_g - n_o) <= 1)).mean())}
+    both = esc_g & esc_o & (n_g == n_o)
+    if exact:
+        zb = lambda a: a.view(np.uint64).reshape(len(a), 2)
+        out["z_bit_equal"] = float((zb(gpu["z"])[both] == zb(want["z"])[both]).all(axis=1).mean()) if both.any() \
+            else 1.0
+        out["dz_bit_equal"] = float(((zb(gpu["dz"])[both] == zb(want["dz"])[both]).all(axis=1) &
+                                     (gpu["dexp"][both] == want["dexp"][both])).mean()) if both.any() else 1.0
+    if "nu" in gpu and both.any():
+        rel = np.abs(gpu["nu"][both] - want["nu"][both]) / np.abs(want["nu"][both])
+        out["nu_rel_err_max"] = float(rel.max())
+    return out
+
+
+def sample_offset(plane, tier, nx, ny, k, offsets=None):
+    """(ar, ai, offset_exp) of sample k as the kernel forms it (view.rs:118-122,
+    grid.rs:709-723): unit offset times h on the ordinary tiers, times h_m with exponent
+    h_e on the scaled tier; offsets: per-sample unit offsets (jittered frames)."""
+    if offsets is not None:
+        ux, uy = float(offsets[k, 0]), float(offsets[k, 1])
+    else:
+        i, j = k % nx, k // nx
+        x, y = i + 0.5 - nx / 2.0, j + 0.5 - ny / 2.0
+        ux, uy = plane.cos_rot * x + plane.sin_rot * y, plane.sin_rot * x - plane.cos_rot * y
+    if tier == 2:
+        return ux * plane.h_m, uy * plane.h_m, plane.h_e
+    h = plane.h_m * 2.0 ** plane.h_e
+    return ux * h, uy * h, 0
+
+
+def precision_vs_direct(fdref, cases, forms, seconds, threads):
+    """Each form's escape counts and smooth iteration against fd-fixed direct iteration at
+    the sample's exact c (the sample's offset added to the centre at the view's bits + 64):
+    cases = [(centre_re, centre_im, bits, max_iter, escape_radius, ar, ai, oe, {form: (cls,
+    n, nu)})], tried in order until `seconds` have passed. A form misses a sample when its
+    class differs from direct iteration's (escaped or not) or its count is off by more than
+    one; its exact-count mismatch rate and the relative nu error where counts agree are
+    reported too."""
+    import math
+    from concurrent.futures import ThreadPoolExecutor
+    t0 = time.perf_counter()
+
+    def one(c):
+        if time.perf_counter() - t0 > seconds:
+            return None
+        cre, cim, bits, mi, er, ar, ai, oe, _ = c
+        return fdref.direct(cre, cim, ar, ai, oe, bits, mi, er)
+
+    with ThreadPoolExecutor(threads) as pool:
+        got = list(pool.map(one, cases))
+    done = [(c, g) for c, g in zip(cases, got) if g is not None]
+    out = {"samples": len(done), "of": len(cases)}
+    for form in forms:
+        miss = exact = 0
+        rel = []
+        for c, (n, zr, zi) in done:
+            cls, ng, nu = c[8][form]
+            esc = cls == 0
+            if (n is None) != (not esc) or (esc and abs(ng - n) > 1):
+                miss += 1
+            if not ((n is None and not esc) or (esc and n is not None and ng == n)):
+                exact += 1
+            if esc and n is not None and ng == n:
+                nu_d = n + 1 - math.log2(math.log2(math.hypot(zr, zi)))
+                rel.append(abs(nu - nu_d) / abs(nu_d))
+        k = max(1, len(done))
+        out[form] = {"mismatch_rate": exact / k, "off_by_more_than_one": miss / k,
+                     "nu_rel_err_median": float(np.median(rel)) if rel else None,
+                     "nu_rel_err_max": float(max(rel)) if rel else None}
+    return out
+
+
 def reference_arm(args, fr):
     """The reference CPU kernel on the host cores over a bounded sample of the frame's rows."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -291,7 +373,7 @@ def run_ours(args):
             tot["launches"] += cnt.launches
         torch.cuda.synchronize()
         barrier(world)
-        snap = {c: bufs[c].cpu().numpy().copy() for c in ("cls", "n")}
+        snap = {c: bufs[c].cpu().numpy().copy() for c in ("cls", "n") + (("nu",) if "nu" in bufs else ())}
         return tot, snap
 
     clocks = Clocks(local)
@@ -343,6 +425,15 @@ def run_ours(args):
         precision_roofline = {"fp32": {"achieved": a32, "peak": f32.value / 1e12, "frac": a32 / (f32.value / 1e12)},
                               "fp64": {"achieved": a64, "peak": peak, "frac": a64 / peak}, "unit": "TFLOP/s"}
 
+    # each form's frame once more with its raw state, into host arrays (untimed), for the
+    # parity check against the oracle and the direct-iteration report below
+    raw, raw_counters = {}, {}
+    if rank == 0 and world == 1 and not args.no_cpu:
+        for name, extra in (("fp64_plain", 0), ("fp32_floatexp", _lib.F32)):
+            if name in forms:
+                j = fd.route.make_job(plane, tier, p, handle, nuc, flags | extra)
+                raw[name], raw_counters[name], _ = dev.render_job(j, raw=True, columns=p.columns)
+
     # e2e through the public API with host buffers: uploads (H2D), render, host columns (D2H)
     h2d = 16 * len(r) + (56 * len(bla.blocks) if bla is not None else 0)
     d2h = n * sum(OUT_BYTES[c] for c in cols)
@@ -363,13 +454,35 @@ def run_ours(args):
     e2e_s = allmax(e2e_s, world)
     e2e_value = e2e_eff * world / e2e_s
 
-    cpu = None
+    cpu = parity = direct = None
     if rank == 0 and world == 1 and not args.no_cpu:
+        # the oracle over the whole frame on the host cores: the CPU baseline, and the
+        # check that the CUDA route's frame is the reference algorithm's, sample by sample
         fdref, job_o, ref_o, bla_o, sample, step, setup, cores = reference_arm(args, fr)
-        eff_c, dt_c, n_c = sample(step)
-        rows = len(range(job_o.row_first, p.ny, step))
-        cpu = {"value": eff_c / dt_c, "unit": UNIT, "cores": cores, "kind": "port",
-               "sample": f"{rows} of {p.ny} rows (every {step}th) of the same frame, {dt_c:.1f} s"}
+        job_o.row_first, job_o.row_step = 0, 1
+        t0 = time.perf_counter()
+        want = fdref.render(job_o, ref_o, bla_o, raw=True)
+        dt_c = time.perf_counter() - t0
+        so = want["stats"]
+        cpu = {"value": (so["iterations"] - so["blocks"] + so["skipped"]) / dt_c, "unit": UNIT, "cores": cores,
+               "kind": "port", "sample": f"the whole frame ({p.ny} of {p.ny} rows), {dt_c:.1f} s"}
+        parity = {}
+        for name in raw:
+            parity[name] = parity_vs_oracle(raw[name], want, exact=name == "fp64_plain")
+            if name == "fp64_plain":
+                cnt = raw_counters[name]
+                parity[name]["counters_equal"] = bool(
+                    (cnt.iterations, cnt.blocks, cnt.skipped) == (so["iterations"], so["blocks"], so["skipped"]))
+        # both forms against fd-fixed direct iteration on a seeded subset of samples
+        pick = np.random.default_rng(args.seed + 100).choice(n, args.direct_samples, replace=False)
+        cases = []
+        for k in pick:
+            k = int(k)
+            ar, ai, oe = sample_offset(plane, tier, p.nx, p.ny, k)
+            cases.append((view.center_re, view.center_im, plane.bits + 64, p.max_iter, p.escape_radius, ar, ai, oe,
+                          {f: (int(raw[f]["cls"][k]) & 3, int(raw[f]["n"][k]), float(raw[f]["nu"][k])
+                               if "nu" in raw[f] else 0.0) for f in raw}))
+        direct = precision_vs_direct(fdref, cases, list(raw), args.direct_seconds, cores)
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_total / args.steps, "higher_is_better": True,
@@ -393,11 +506,17 @@ def run_ours(args):
                              "traffic_unit": "bytes per launch (DRAM, ncu)",
                              "peak_source": "measured live: unfused DMUL+DADD chains on all SMs (fdk_alu_peaks)"},
                 "roofline_precision_form": precision_roofline,
-                "cpu_baseline": cpu, "clocks": clk, "gpu_launches": sum(v["tot"]["launches"] for v in forms.values()),
+                "cpu_baseline": cpu, "parity": parity, "precision_vs_direct": direct, "clocks": clk,
+                "gpu_launches": sum(v["tot"]["launches"] for v in forms.values()),
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "steps": args.e2e_steps}}
         print(json.dumps(line), flush=True)
     dev.close()
+    pl = (parity or {}).get("fp64_plain")
+    if pl is not None and not (pl["class_equal"] == 1.0 and pl["count_equal"] == 1.0 and pl["z_bit_equal"] == 1.0
+                               and pl["counters_equal"]):
+        log(f"PARITY FAILURE: the plain form's frame differs from the oracle's: {pl}")
+        sys.exit(3)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
@@ -591,6 +710,9 @@ def main():
     ap.add_argument("--seed", type=int, default=2)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--direct-samples", type=int, default=256,
+                    help="seeded samples checked against fd-fixed direct iteration")
+    ap.add_argument("--direct-seconds", type=float, default=60.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--nx", type=int, default=0)
     ap.add_argument("--ny", type=int, default=0)

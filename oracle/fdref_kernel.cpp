@@ -466,6 +466,22 @@ static inline uint64_t next_pow2(uint64_t x) {
 // ---------------------------------------------------------------- sample.rs:170-581
 // The B (bounded) and trace/stripe features are outside the hot path (the GPU route
 // declines Bound/Stripe frames). A series start (Start, sample.rs:69-80) is supported.
+// Precision experiment (not the reference's algorithm): with g_delta_bits in [1, 52],
+// the delta is rounded to that many mantissa bits (round half to even) after every update
+// that writes it (plain step, block, rebase), everything else staying binary64. 24 bits
+// is an ideal FP32-mantissa delta: the accuracy ceiling of any FP32-delta kernel, free of
+// that kernel's own shortcuts. 0 (the default) leaves the reference's algorithm as it is.
+static std::atomic<int> g_delta_bits{0};
+// ... applied only to updates that leave the iteration count in [g_round_from, g_round_to)
+static std::atomic<uint64_t> g_round_from{0}, g_round_to{UINT64_MAX};
+
+static inline double round_bits(double x, int bits) {
+  if (x == 0.0 || !std::isfinite(x)) return x;
+  int e;
+  const double m = std::frexp(x, &e);  // x = m 2^e, 0.5 <= |m| < 1
+  return std::ldexp(std::nearbyint(std::ldexp(m, bits)), e - bits);
+}
+
 template <bool EXT, bool D, bool L, bool B>
 static Outcome iterate_t(const Reference &r, const Bla *bla, Skip &skip,
                          std::optional<std::pair<double, double>> c, double ar, double ai,
@@ -510,6 +526,15 @@ static Outcome iterate_t(const Reference &r, const Bla *bla, Skip &skip,
   double e = 0.0, ed = 0.0;
   const double rc = 16.0 * U * (std::fabs(ar) + std::fabs(ai)) + 1e-300;
   Contraction contraction;
+  const int delta_bits = g_delta_bits.load(std::memory_order_relaxed);
+  const uint64_t round_from = g_round_from.load(std::memory_order_relaxed);
+  const uint64_t round_to = g_round_to.load(std::memory_order_relaxed);
+  auto rounded = [&]() {
+    if (delta_bits > 0 && n >= round_from && n < round_to) {
+      xr = round_bits(xr, delta_bits);
+      xi = round_bits(xi, delta_bits);
+    }
+  };
   uint64_t limit = max_iter;
   while (n < limit) {
     const Block *b = nullptr;
@@ -561,6 +586,7 @@ static Outcome iterate_t(const Reference &r, const Bla *bla, Skip &skip,
       n += len;
       skip.blocks += 1;
       skip.skipped += len;
+      rounded();
     } else {
       double fr = zr[m] + scale * xr, fi = zi[m] + scale * xi;
       if (nucleus && n >= 1) contraction.multiply(2.0 * fr, 2.0 * fi, 0);
@@ -600,6 +626,7 @@ static Outcome iterate_t(const Reference &r, const Bla *bla, Skip &skip,
       xi = ni;
       m += 1;
       n += 1;
+      rounded();
     }
     double physical_r = scale * xr, physical_i = scale * xi;
     double fr = zr[m] + physical_r, fi = zi[m] + physical_i;
@@ -661,6 +688,7 @@ static Outcome iterate_t(const Reference &r, const Bla *bla, Skip &skip,
           m = 1;
           n = n + 1;
         }
+        rounded();
         double factor = exp2i(offset_exp - delta_exp);
         dc_r = ar * factor;
         dc_i = ai * factor;
@@ -668,6 +696,7 @@ static Outcome iterate_t(const Reference &r, const Bla *bla, Skip &skip,
         xr = fr;
         xi = fi;
         m = 0;
+        rounded();
       }
     } else if (EXT) {
       double magnitude = rmax(std::fabs(xr), std::fabs(xi));
@@ -804,3 +833,11 @@ Outcome iterate(bool extended, bool D, bool L, const Reference &r, const Bla *bl
 #pragma GCC diagnostic pop
 
 }  // namespace fdref
+
+extern "C" int fdref_set_delta_bits(int bits, uint64_t from_n, uint64_t to_n) {
+  if (bits < 0 || bits > 52 || from_n > to_n) return -1;
+  fdref::g_delta_bits.store(bits);
+  fdref::g_round_from.store(from_n);
+  fdref::g_round_to.store(to_n);
+  return 0;
+}

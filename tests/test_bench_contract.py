@@ -95,3 +95,47 @@ def test_reference_arm_loads_no_repo_library():
     assert r.stdout.strip().splitlines()[-1] == "CLEAN"
     line = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][0])
     assert line["impl"] == "reference" and line["config"]["workload"] == "c2-1920x1080-1e-100-seed2"
+
+
+@pytest.mark.parametrize("width,tier", [("0.0065", None), ("1e-20", None), ("1e-300", "scaled")])
+def test_bench_parity_helpers_on_oracle_frames(width, tier):
+    """bench.py's checks on the CPU: sample_offset gives each sample's offset as the grid
+    forms it (the oracle's per-sample iteration there equals its frame render), the
+    parity summary of a frame against itself is exact and catches a planted count error,
+    and the direct-iteration report finds no miss on a plain frame of a shallow view."""
+    sys.path.insert(0, ROOT)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+
+    import bench
+    import fdref
+    from fractodactyl_b200 import route
+    re_, im_, nx, ny, it = "-0.7453", "0.1127", 24, 16, 3000
+    view, p = route.View(re_, im_, width), route.Params(nx, ny, max_iter=it, tier=tier, columns=("nu",))
+    plane, t = route._setup(view, p)
+    job = fdref.make_job(re_, im_, width, nx, ny, it, columns=fdref.COL_NU, tier=t, threads=2)
+    ref = fdref.Ref.for_job(job)
+    want = fdref.render(job, ref, None, raw=True)
+    kinds = {"escaped": 0, "interior": 1, "unresolved": 2}
+    for k in range(0, nx * ny, 7):
+        ar, ai, oe = bench.sample_offset(plane, t, nx, ny, k)
+        o = fdref.iterate(ref, None, extended=t == 2, derivative=False, ar=ar, ai=ai, offset_exp=oe, max_iter=it,
+                          r2=1e20, c=(plane.c_re + ar, plane.c_im + ai) if t == 0 else None)
+        assert kinds[o["kind"]] == want["cls"][k] & 3, k
+        if o["kind"] == "escaped":
+            assert o["n"] == want["n"][k] and (o["zr"], o["zi"]) == tuple(want["z"][k]), k
+    same = bench.parity_vs_oracle(want, want, exact=True)
+    assert same["class_equal"] == same["count_equal"] == same["z_bit_equal"] == same["dz_bit_equal"] == 1.0
+    bad = dict(want, n=want["n"].copy())
+    esc = np.flatnonzero((want["cls"] & 3) == 0)
+    bad["n"][esc[0]] += 1
+    worse = bench.parity_vs_oracle(bad, want, exact=True)
+    assert worse["count_equal"] == 1.0 - 1.0 / (nx * ny) and worse["within_one"] == 1.0
+    if t != 2:  # direct iteration of a few escaping samples of the shallow views
+        cases = []
+        for k in esc[:6]:
+            ar, ai, oe = bench.sample_offset(plane, t, nx, ny, int(k))
+            cases.append((re_, im_, plane.bits + 64, it, 1e10, ar, ai, oe,
+                          {"plain": (0, int(want["n"][k]), float(want["nu"][k]))}))
+        rep = bench.precision_vs_direct(fdref, cases, ["plain"], 60.0, 2)
+        assert rep["samples"] == 6 and rep["plain"]["off_by_more_than_one"] == 0.0
