@@ -169,9 +169,10 @@ typedef struct {
 } fdref_columns;
 /* Precision experiment, not the reference's algorithm: bits in [1, 52] rounds every
  * delta the kernel writes to that many mantissa bits (24: an ideal FP32-mantissa delta)
- * when the write leaves the iteration count n in [from_n, to_n); bits 0 restores the
- * reference's binary64 kernel. Process-wide; -1 for arguments out of range. */
-int fdref_set_delta_bits(int bits, uint64_t from_n, uint64_t to_n);
+ * when the write leaves the iteration count n in [from_n, to_n); round_orbit also rounds
+ * the orbit point a plain step multiplies the delta by (an FP32 copy of Z); bits 0
+ * restores the reference's binary64 kernel. Process-wide; -1 for arguments out of range. */
+int fdref_set_delta_bits(int bits, uint64_t from_n, uint64_t to_n, int round_orbit);
 
 /* fdref_render / fdref_render_series with every output: series and mask may be NULL. */
 int fdref_render_columns(const fdref_job *job, const fdref_ref *ref, const fdref_bla *bla,

@@ -145,17 +145,18 @@ def lib():
         L.fdref_iterate_bounded.argtypes = [P, C.c_int, C.c_int, D, D, D, D, U64, D, I64, D, D, C.POINTER(Outcome)]
         L.fdref_render_columns.argtypes = [C.POINTER(Job), P, P, P, P, C.POINTER(Columns), C.POINTER(Stats),
                                            C.c_char_p, C.c_size_t]
-        L.fdref_set_delta_bits.argtypes = [C.c_int, C.c_uint64, C.c_uint64]
+        L.fdref_set_delta_bits.argtypes = [C.c_int, C.c_uint64, C.c_uint64, C.c_int]
         _lib = L
     return _lib
 
 
-def set_delta_bits(bits, from_n=0, to_n=2 ** 64 - 1):
+def set_delta_bits(bits, from_n=0, to_n=2 ** 64 - 1, round_orbit=False):
     """Precision experiment (not the reference's algorithm): round every delta the kernel
     writes to `bits` mantissa bits (24: an ideal FP32-mantissa delta) while the iteration
-    count it leaves lies in [from_n, to_n); 0 restores the reference's binary64 kernel.
-    Process-wide."""
-    if lib().fdref_set_delta_bits(int(bits), int(from_n), int(to_n)) != 0:
+    count it leaves lies in [from_n, to_n); round_orbit: the orbit point each plain step
+    multiplies the delta by too (an FP32 copy of Z); 0 restores the reference's binary64
+    kernel. Process-wide."""
+    if lib().fdref_set_delta_bits(int(bits), int(from_n), int(to_n), int(bool(round_orbit))) != 0:
         raise ValueError(f"delta bits must lie in [0, 52] and from_n <= to_n, got {bits}, {from_n}, {to_n}")
 
 

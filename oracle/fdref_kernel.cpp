@@ -474,6 +474,9 @@ static inline uint64_t next_pow2(uint64_t x) {
 static std::atomic<int> g_delta_bits{0};
 // ... applied only to updates that leave the iteration count in [g_round_from, g_round_to)
 static std::atomic<uint64_t> g_round_from{0}, g_round_to{UINT64_MAX};
+// ... and, when set, the orbit point a plain step multiplies the delta by is rounded to
+// the same width (an FP32 copy of Z, as any FP32 recurrence holds it)
+static std::atomic<bool> g_round_orbit{false};
 
 static inline double round_bits(double x, int bits) {
   if (x == 0.0 || !std::isfinite(x)) return x;
@@ -529,6 +532,7 @@ static Outcome iterate_t(const Reference &r, const Bla *bla, Skip &skip,
   const int delta_bits = g_delta_bits.load(std::memory_order_relaxed);
   const uint64_t round_from = g_round_from.load(std::memory_order_relaxed);
   const uint64_t round_to = g_round_to.load(std::memory_order_relaxed);
+  const bool round_orbit = g_round_orbit.load(std::memory_order_relaxed);
   auto rounded = [&]() {
     if (delta_bits > 0 && n >= round_from && n < round_to) {
       xr = round_bits(xr, delta_bits);
@@ -614,6 +618,10 @@ static Outcome iterate_t(const Reference &r, const Bla *bla, Skip &skip,
         }
       }
       double Zr = zr[m], Zi = zi[m];
+      if (round_orbit && delta_bits > 0 && n >= round_from && n < round_to) {
+        Zr = round_bits(Zr, delta_bits);
+        Zi = round_bits(Zi, delta_bits);
+      }
       double nr, ni;
       if (EXT) {  // number.rs:109-124
         nr = 2.0 * (Zr * xr - Zi * xi) + scale * (xr * xr - xi * xi) + dc_r;
@@ -834,8 +842,9 @@ Outcome iterate(bool extended, bool D, bool L, const Reference &r, const Bla *bl
 
 }  // namespace fdref
 
-extern "C" int fdref_set_delta_bits(int bits, uint64_t from_n, uint64_t to_n) {
+extern "C" int fdref_set_delta_bits(int bits, uint64_t from_n, uint64_t to_n, int round_orbit) {
   if (bits < 0 || bits > 52 || from_n > to_n) return -1;
+  fdref::g_round_orbit.store(round_orbit != 0);
   fdref::g_delta_bits.store(bits);
   fdref::g_round_from.store(from_n);
   fdref::g_round_to.store(to_n);

@@ -7,7 +7,8 @@ to `bits` mantissa bits, everything else (orbit, derivative, rebase test, bailou
 radii, periodicity) left in binary64. At 24 bits that is an ideal FP32-mantissa delta:
 no FP32 kernel can follow the binary64 deltas more closely, whatever its own shortcuts.
 The escape-count agreement of the rounded runs with the binary64 run is the ceiling of
-every FP32-delta form on that view.
+every FP32-delta form on that view. With --round-orbit the orbit point each plain step
+multiplies the delta by is rounded too, as an FP32 recurrence holds its copy of Z.
 
     python oracle/precision_ceiling.py [--samples 20000] [--bits 24 32 40 48]
 
@@ -58,7 +59,7 @@ def agreement(a, b, sel):
             "nu_rel_err_p99": float(np.quantile(rel, 0.99)) if rel.size else None}
 
 
-def run(v, samples, bits_list, seed=11):
+def run(v, samples, bits_list, seed=11, round_orbit=False):
     job = fdref.make_job(v["re"], v["im"], v["width"], v["nx"], v["ny"], v["max_iter"],
                          escape_radius=v["escape_radius"], columns=fdref.COL_NU, tier=v["tier"])
     ref = fdref.Ref.for_job(job)
@@ -76,12 +77,13 @@ def run(v, samples, bits_list, seed=11):
     base = fdref.render_columns(job, ref, bla, mask=mask)
     out = []
     for bits in bits_list:
-        fdref.set_delta_bits(bits)
+        fdref.set_delta_bits(bits, round_orbit=round_orbit)
         try:
             got = fdref.render_columns(job, ref, bla, mask=mask)
         finally:
             fdref.set_delta_bits(0)
-        out.append(dict(view=v["name"], samples=int(sel.sum()), delta_bits=bits, **agreement(base, got, sel)))
+        out.append(dict(view=v["name"], samples=int(sel.sum()), delta_bits=bits, orbit_rounded=round_orbit,
+                        **agreement(base, got, sel)))
     return out, time.perf_counter() - t
 
 
@@ -90,11 +92,13 @@ def main():
     ap.add_argument("--samples", type=int, default=20_000)
     ap.add_argument("--bits", type=int, nargs="+", default=[24, 32, 40, 48])
     ap.add_argument("--views", nargs="*", default=None, help="view names (default: all)")
+    ap.add_argument("--round-orbit", action="store_true",
+                    help="also round the orbit point each plain step multiplies the delta by (an FP32 copy of Z)")
     a = ap.parse_args()
     for v in views():
         if a.views and v["name"] not in a.views:
             continue
-        rows, dt = run(v, a.samples, a.bits)
+        rows, dt = run(v, a.samples, a.bits, round_orbit=a.round_orbit)
         for r in rows:
             print(json.dumps(dict(r, seconds=round(dt, 1))), flush=True)
 
