@@ -152,13 +152,24 @@ __device__ __forceinline__ void relimit(const Params &p, State<EXT> &s) {
 // The radii of the first two levels come with the orbit entry (r2a, r2b); those of the
 // next PRE levels are loaded together before the comparisons that would stop at them.
 template <bool EXT>
-__device__ __forceinline__ int find_block(const Params &p, const State<EXT> &s, uint32_t &at) {
+__device__ __forceinline__ double block_d2(const State<EXT> &s) {
+  return EXT ? (s.xr * s.xr + s.xi * s.xi) * s.scale * s.scale : s.xr * s.xr + s.xi * s.xi;
+}
+
+// Whether Bla::find finds any block at m: one test for the nucleus gate, the budget and
+// the level-1 block (r2a is -1 unless a block starts at m); every operand is evaluated,
+// which costs fewer branches than returning at the first that fails.
+template <bool EXT>
+__device__ __forceinline__ bool block_starts(const State<EXT> &s) {
   const uint32_t budget = s.lim > s.n ? s.lim - s.n : 0u;
-  const double d2 = EXT ? (s.xr * s.xr + s.xi * s.xi) * s.scale * s.scale : s.xr * s.xr + s.xi * s.xi;
-  // One test for the nucleus gate, the budget and the level-1 block (r2a is -1 unless a
-  // block starts at m): every operand is evaluated, which costs fewer branches than
-  // returning at the first that fails.
-  if (!((s.nucleus < 0 || s.m != 0) & (budget >= 2) & (d2 < s.r2a))) return -1;
+  return (s.nucleus < 0 || s.m != 0) & (budget >= 2) & (block_d2(s) < s.r2a);
+}
+
+// The rest of Bla::find once block_starts holds: the level of the longest valid block.
+template <bool EXT>
+__device__ __forceinline__ int block_level(const Params &p, const State<EXT> &s, uint32_t &at) {
+  const uint32_t budget = s.lim > s.n ? s.lim - s.n : 0u;
+  const double d2 = block_d2(s);
   const uint32_t k = s.m - 1u;     // m = 0 wraps: odd, no block
   at = k >> 1;
   if (budget < 4 || !(d2 < s.r2b)) return 0;
@@ -192,6 +203,11 @@ __device__ __forceinline__ int find_block(const Params &p, const State<EXT> &s, 
     at = a;
   }
   return lv;
+}
+
+template <bool EXT>
+__device__ __forceinline__ int find_block(const Params &p, const State<EXT> &s, uint32_t &at) {
+  return block_starts(s) ? block_level(p, s, at) : -1;
 }
 
 // A BLA block application (sample.rs:264-315): delta' = A delta + B dc, dz' = A dz + B.
@@ -306,32 +322,81 @@ __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res
   double fr = Z.x + pr, fi = Z.y + pi;
   double f2 = fr * fr + fi * fi;
   {
-    // Quiet iterations (no escape, nucleus gate, rebase, rescaling or periodicity event)
-    // leave only z for the next iteration: one test of every event, then the full
-    // sequence below only when one of them may fire. Same expressions as below.
+    // The common iterations leave through a short path: no escape, nucleus gate or
+    // near-return (the full sequence below handles those), and at most a rebase onto Z_0
+    // whose delta keeps binary64's range (f2 > SQUARE_OK on the extended tier), a +-32
+    // rescaling of the extended tier's delta, or a Brent save point of the extended tier.
+    // Each of those is the full sequence's own expressions in its own order, so the state
+    // after either path is the same; the divergent work per lane is a few instructions.
     const double delta2 = pr * pr + pi * pi;
     const bool rebase = EXT ? f2 <= delta2 : f2 < delta2;
-    bool quiet = !(f2 > p.r2) && !rebase && s.m != p.last && !(s.nucleus >= 0 && s.n == (uint32_t)s.nucleus + 1u);
-    if (EXT) {
-      const double magnitude = rmax(fabs(s.xr), fabs(s.xi));
-      quiet = quiet && !(magnitude > HI && s.delta_exp < 0) && !(magnitude < LO && magnitude != 0.0);
-    }
-    const double check_r = EXT ? pr : s.xr, check_i = EXT ? pi : s.xi;
+    const bool reb = rebase || s.m == p.last;
+    bool common = !(f2 > p.r2) && !(s.nucleus >= 0 && s.n == (uint32_t)s.nucleus + 1u);
+    if (B || (EXT && !(f2 > SQUARE_OK))) common = common && !reb;  // bounded radii; sum2 rebase
+    // the judge reads the delta after a rebase on the ordinary tiers (it is then z itself)
+    const double check_r = EXT ? pr : (reb ? fr : s.xr), check_i = EXT ? pi : (reb ? fi : s.xi);
     bool judge = check_r * check_r + check_i * check_i > RES2 * f2;
     if (EXT) judge = judge && s.returns < 4;
     const double dist = fabs(fr - s.sr) + fabs(fi - s.si);
     const double size = fabs(s.sr) + fabs(s.si);
-    bool calm;
     if (EXT) {
-      calm = s.n < s.chk && !(judge && dist < 1e-13 * size + 1e-300);
+      common = common && !(judge && dist < 1e-13 * size + 1e-300);
     } else {
       const bool held = s.hold > 0 && s.n - s.sn < s.hold;  // sn <= n while hold > 0
-      calm = judge ? !(dist < 1e-3 * size) && (s.hold > 0 ? held : !(s.pending || s.n >= s.chk))
-                   : (s.hold > 0 ? held : s.n < s.chk);
+      common = common && (judge ? !(dist < 1e-3 * size) && (s.hold > 0 ? held : !(s.pending || s.n >= s.chk))
+                                : (s.hold > 0 ? held : s.n < s.chk));
     }
-    if (__builtin_expect(quiet && calm, 1)) {
-      s.fr = fr;
-      s.fi = fi;
+    if (__builtin_expect(common, 1)) {
+      bool moved = false;
+      if (__builtin_expect(reb, 0)) {  // sample.rs:418-452 without sum2 or TINY (scale is 1)
+        moved = true;
+        s.xr = fr;
+        s.xi = fi;
+        s.m = 0;
+        s.Zr = p.z0r;
+        s.Zi = p.z0i;
+        s.r2a = -1.0;  // no block starts at Z_0 (bla.rs:235-236)
+        s.r2b = -1.0;
+        if (EXT) {
+          s.delta_exp = 0;
+          s.scale = exp2i(s.delta_exp);
+          double factor = exp2i(s.offset_exp - s.delta_exp);
+          s.dc_r = s.ar * factor;
+          s.dc_i = s.ai * factor;
+        }
+      } else if (EXT) {  // sample.rs:453-467
+        const double magnitude = rmax(fabs(s.xr), fabs(s.xi));
+        int32_t k = 0;
+        if (magnitude > HI && s.delta_exp < 0)
+          k = -s.delta_exp < 32 ? -s.delta_exp : 32;
+        else if (magnitude < LO && magnitude != 0.0)
+          k = -32;
+        if (__builtin_expect(k != 0, 0)) {
+          moved = true;
+          double factor = exp2i(-k);
+          s.xr = s.xr * factor;
+          s.xi = s.xi * factor;
+          s.delta_exp = s.delta_exp + k;
+          s.scale = exp2i(s.delta_exp);
+          double f = exp2i(s.offset_exp - s.delta_exp);
+          s.dc_r = s.ar * f;
+          s.dc_i = s.ai * f;
+        }
+      }
+      if (moved) {  // the next iteration's z (sample.rs:331; number.rs:113 on the extended tier)
+        s.fr = EXT ? s.Zr + s.scale * s.xr : s.Zr + s.xr;
+        s.fi = EXT ? s.Zi + s.scale * s.xi : s.Zi + s.xi;
+      } else {
+        s.fr = fr;
+        s.fi = fi;
+      }
+      if (EXT && __builtin_expect(s.n >= s.chk, 0)) {  // sample.rs:488-491 / :571-574
+        s.sr = fr;
+        s.si = fi;
+        s.sn = s.n;
+        s.chk = s.chk >= 0x80000000u ? 0xffffffffu : s.chk * 2;
+        relimit(p, s);
+      }
       return false;
     }
   }
@@ -597,11 +662,10 @@ __device__ __forceinline__ bool warp_step(const Params &p, State<EXT> &s, Result
       } else {
         Zn = __ldg(p.orbit + s.m + 1);
       }
-      int lv = -1;
-      if (L) lv = find_block(p, s, w.at);
-      if (lv >= 0) {
+      // a lane that finds a block waits; its level is searched when the waiting lanes
+      // apply their blocks together (nothing the search reads changes while it waits)
+      if (L && block_starts(s)) {
         w.on = true;
-        w.lv = lv;
       } else {
         plain_update<EXT, D, B>(s, p.q);
         upd = true;
@@ -618,6 +682,7 @@ __device__ __forceinline__ bool warp_step(const Params &p, State<EXT> &s, Result
     const uint32_t busy = (uint32_t)__popc(waiting | stepping);
     const uint32_t thr = max(1u, (busy * defer) >> 5);
     if (waiting && ((uint32_t)__popc(waiting) >= thr || !stepping) && w.on) {
+      w.lv = block_level(p, s, w.at);
       apply_block<EXT, D>(p, s, w.lv, w.at);
       w.on = false;
       upd = took = true;
