@@ -641,6 +641,32 @@ struct Waiting {
   uint32_t at;
 };
 
+// A warp's reserved queue slots [base, end): one atomic on the queue head takes 32
+// consecutive slots (one tile), which the warp then hands to its idle lanes in order, so
+// one round trip to the head serves a tile instead of each lane as it finishes. Every
+// lane holds the same copy.
+struct Reservation {
+  unsigned long long base = 0, end = 0;
+  // Slots for the `need` idle lanes (warp-uniform): false when the queue is spent;
+  // otherwise the lanes of need with rank < count take first + rank.
+  __device__ __forceinline__ bool take(unsigned long long *queue, unsigned long long total, unsigned need,
+                                       unsigned lane, unsigned long long &first, unsigned &count) {
+    if (base >= end) {
+      unsigned long long b = 0;
+      if (lane == 0) b = atomicAdd(queue, 32ull);
+      b = __shfl_sync(0xffffffffu, b, 0);
+      if (b >= total) return false;
+      base = b;
+      end = b + 32 < total ? b + 32 : total;
+    }
+    const unsigned long long left = end - base, want = (unsigned long long)__popc(need);
+    count = (unsigned)(want < left ? want : left);
+    first = base;
+    base += count;
+    return true;
+  }
+};
+
 // One iteration for the active lanes of a warp (every lane of the warp calls it). A lane
 // whose next operation is a BLA block waits until at least defer/32 of the warp's busy
 // lanes wait or no lane steps plainly; the waiting lanes then apply their blocks together. The warp
@@ -924,6 +950,7 @@ __global__ void __launch_bounds__(128, Occupancy<EXT>::blocks) perturb_kernel(Pa
   Result res;
   Waiting w{false, -1, 0};
   bool active = false, exhausted = false;
+  Reservation slots;
   uint64_t t0 = p.deadline_ns ? globaltimer() : 0;
   unsigned long long n_samples = 0, iters = 0, blocks = 0, skipped = 0, fallback = 0, closed = 0;
   double shift = 0.0;
@@ -961,16 +988,15 @@ __global__ void __launch_bounds__(128, Occupancy<EXT>::blocks) perturb_kernel(Pa
         }
       }
       unsigned long long base = 0;
-      int leader = __ffs((int)need) - 1;
-      if ((int)lane == leader) base = atomicAdd(p.queue, (unsigned long long)__popc(need));
-      base = __shfl_sync(FULL, base, leader);
-      if (base >= p.total) {
+      unsigned take = 0;
+      if (!slots.take(p.queue, p.total, need, lane, base, take)) {
         exhausted = true;
         break;
       }
       if (!active) {
-        uint64_t slot = base + __popc(need & lt);
-        if (slot < p.total) {
+        const unsigned rank = __popc(need & lt);
+        const uint64_t slot = base + rank;
+        if (rank < take) {
           int got = init<EXT, D, L, S, B>(p, slot, s, res);
           if (got == 1) {
             active = true;
@@ -1065,6 +1091,7 @@ __global__ void __launch_bounds__(128, Occupancy<EXT>::blocks)
   Waiting w{false, -1, 0};
   bool active = false, exhausted = false;
   uint32_t job = 0, counted = 0xffffffffu;
+  Reservation slots;
   LaneCounters lc;
   lc.clear();
   auto finish = [&](const Params &p, uint32_t idx, const Result &r, uint64_t nblocks, uint64_t nskipped) {
@@ -1089,16 +1116,15 @@ __global__ void __launch_bounds__(128, Occupancy<EXT>::blocks)
     unsigned need = __ballot_sync(FULL, !active);
     while (need && !exhausted) {
       unsigned long long base = 0;
-      int leader = __ffs((int)need) - 1;
-      if ((int)lane == leader) base = atomicAdd(queue, (unsigned long long)__popc(need));
-      base = __shfl_sync(FULL, base, leader);
-      if (base >= total) {
+      unsigned take = 0;
+      if (!slots.take(queue, total, need, lane, base, take)) {
         exhausted = true;
         break;
       }
       if (!active) {
-        unsigned long long slot = base + __popc(need & lt);
-        if (slot < total) {
+        const unsigned rank = __popc(need & lt);
+        const unsigned long long slot = base + rank;
+        if (rank < take) {
           job = job_of(starts, njobs, slot);
           const Params &p = jobs[job];
           int got = init<EXT, D, L>(p, slot - __ldg(starts + job), s, res);
