@@ -35,6 +35,38 @@ class Declined(RuntimeError):
     """The route does not take this frame; render it on the CPU from n = 0."""
 
 
+class Incomplete(Declined):
+    """A deadline ended the render with some samples unfinished (frame.rs:338-341): the
+    finished samples are the CPU kernel's, and only the samples where `mask` is true
+    need the CPU (render_with_masked from n = 0, grid.rs:175-182), then the two are
+    overlaid. Carries what render_with returns (header, samples, stats, bla_stats; the
+    unfinished samples hold zeroed columns and status 0, the counters cover the finished
+    ones) and the mask, one bool per sample in row-major order. A caller that treats it
+    as a plain Declined restarts the whole frame instead, which is also correct."""
+
+    def __init__(self, message, header, samples, stats, bla_stats, mask):
+        super().__init__(message)
+        self.header, self.samples, self.stats, self.bla_stats, self.mask = header, samples, stats, bla_stats, mask
+
+    def merge(self, cpu: "Samples", cpu_stats: "Stats"):
+        """The whole frame after the caller's CPU restart: `cpu` is its masked render of
+        the unfinished samples (every column the device wrote, the others unset); the
+        finished samples keep the device's values and the iterations add up, as
+        frame.rs:338-343 overlays and counts them. Returns (Samples, Stats)."""
+        out = dataclasses.replace(self.samples)
+        for name in ("cls", "nu", "de", "normal", "n", "z", "dz", "dexp", "bound", "ez", "ed"):
+            g, c = getattr(self.samples, name), getattr(cpu, name)
+            if g is not None and c is not None:
+                g = g.copy()
+                g[self.mask] = c[self.mask]
+                setattr(out, name, g)
+        if out.status is not None:
+            out.status = self.samples.status.copy()
+            out.status[self.mask] = 1
+        return out, Stats(self.stats.reference_len, self.stats.reference_seconds,
+                          self.stats.iterations + cpu_stats.iterations)
+
+
 class RouteError(RuntimeError):
     pass
 
@@ -576,13 +608,15 @@ def encode_host(plane: Plane, ss: int, s: "Samples", columns=("nu", "de", "norma
 
 def render_with(view: View, p: Params, orbit=None, bla: Optional[Bla] = None, dev: Optional[Device] = None,
                 raw=False, shift=True, report: Optional[RouteReport] = None, quiet=True, host_encode=False,
-                series: Optional["Series"] = None):
+                series: Optional["Series"] = None, deadline_ms: Optional[float] = None):
     """fd_kernel::render_with / render_bla (grid.rs:106-208) on the CUDA route; with
     `series`, every sample starts from it (Series::render_masked, grid.rs:341-373).
 
     Returns (Header, Samples, Stats, BlaStats or None). Refusals are the reference's
     (grid.rs:350-366, :378-413, :461-475); the Stripe column is declined (frame.rs:129-144);
     the Bound column renders through fdc_render_bounded on the F64 / Fixed tiers.
+    deadline_ms: the device stops taking samples once it has passed; if any sample is
+    left, Incomplete carries the finished ones and the mask of those the CPU must render.
     """
     started = time.perf_counter()
     if "stripe" in p.columns:
@@ -643,12 +677,30 @@ def render_with(view: View, p: Params, orbit=None, bla: Optional[Bla] = None, de
         if table is not None and shift and p.needs_derivative():
             flags |= _lib.SHIFT
         job = make_job(plane, tier, p, h, r.nucleus_period(), flags)
+        if deadline_ms:
+            job.deadline_ms = float(deadline_ms)
         g = time.perf_counter()
         arrays, cnt, status = dev.render_job(job, raw=raw or host_encode,
                                              columns=() if host_encode else p.columns, bounded=bound)
         gpu_seconds = time.perf_counter() - g
     finally:
         dev.free(h)
+    rep = report if report is not None else RouteReport()
+    rep.device = f"cuda:{dev.index}"
+    rep.gpu_seconds = gpu_seconds
+    rep.table_blocks = 0 if bla is None else len(bla.blocks)
+    return assemble(view, p, plane, tier, bla, table, series, flags, shift, host_encode, arrays, cnt, status,
+                    len(r), reference_seconds, rep, started, quiet)
+
+
+def assemble(view: View, p: Params, plane: Plane, tier: int, bla: Optional[Bla], table: Optional[Bla],
+             series: Optional["Series"], flags: int, shift: bool, host_encode: bool, arrays: dict,
+             cnt: "_lib.Counters", status: int, reference_len: int, reference_seconds: float, rep: RouteReport,
+             started: float, quiet: bool = True):
+    """The route's result from one fdc_render (its arrays, counters and status): header,
+    samples, Stats and BlaStats as render_with returns them, the report's counters, and on
+    FDC_TIMEOUT the Incomplete restart contract (frame.rs:338-341)."""
+    bound = "bound" in p.columns
     kernel = plane.kernel(tier) + (" bla/1" if bla is not None else "") + (" series/0" if series is not None else "") \
         + " gpu-perturb-cuda/1"
     cols = ("class",) + tuple(c for c in ("nu", "de", "normal") if c in p.columns) + \
@@ -659,7 +711,13 @@ def render_with(view: View, p: Params, orbit=None, bla: Optional[Bla] = None, de
                 status=arrays.get("status"), bound=arrays.get("bound"), ez=arrays.get("ez"), ed=arrays.get("ed"))
     if host_encode:
         encode_host(plane, p.ss, s, p.columns, p.threads)
-    stats = Stats(len(r), reference_seconds, int(cnt.iterations))
+    unfinished = None
+    if status == _lib.TIMEOUT:
+        unfinished = arrays["status"] == 0
+        for col in (s.nu, s.de, s.normal):  # the host encoder's values of unwritten samples
+            if col is not None:
+                col[unfinished] = 0
+    stats = Stats(reference_len, reference_seconds, int(cnt.iterations))
     bstats = None
     if table is not None:
         bstats = BlaStats(int(cnt.blocks), int(cnt.skipped), int(cnt.fallback_samples),
@@ -669,19 +727,16 @@ def render_with(view: View, p: Params, orbit=None, bla: Optional[Bla] = None, de
         closed = int((((arrays["cls"] & 3) == 1) & (arrays["n"] == 0) & (arrays["status"] != 0)).sum())
         bstats = BlaStats(0, 0, int(cnt.samples) - closed, closed,
                           0.0 if (shift and p.needs_derivative()) else None)
-    rep = report if report is not None else RouteReport()
-    rep.device = f"cuda:{dev.index}"
     rep.accepted = int(cnt.samples)
     rep.fallback = p.nx * p.ny - int(cnt.samples)
-    rep.gpu_seconds = gpu_seconds
     rep.kernel_ms = cnt.kernel_ms
     rep.launches = cnt.launches
-    rep.table_blocks = 0 if bla is None else len(bla.blocks)
     rep.total_seconds = time.perf_counter() - started
     if not quiet:
         print(rep.line(stats, bstats), file=sys.stderr)
-    if status == _lib.TIMEOUT:
-        raise Declined(f"deadline passed with {rep.fallback} samples unfinished; CPU restart from zero")
+    if unfinished is not None:
+        raise Incomplete(f"deadline passed with {rep.fallback} samples unfinished; CPU restart of those from zero",
+                         header, s, stats, bstats, unfinished)
     return header, s, stats, bstats
 
 

@@ -19,6 +19,7 @@ import pytest
 
 import fdref
 import fractodactyl_b200 as fd
+from fractodactyl_b200 import _lib
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -611,6 +612,60 @@ def test_deadline_stops_taking_samples(emu, case):
     for k in ("cls", "n", "nu", "z", "status"):
         assert np.array_equal(late[k], full[k]), k
     assert late["counters"] == full["counters"]
+
+
+@pytest.mark.parametrize("case", ["f64", "scaled-bla"])
+def test_route_restarts_only_unfinished_samples(emu, case):
+    """The route's deadline contract (frame.rs:338-341 -> grid.rs:175-182): a render the
+    deadline cut short raises Incomplete with the finished samples (the kernel's, here on
+    the emulated clock) and the mask of the unfinished ones; the caller's CPU render of
+    just those samples (the oracle's masked render standing in for fd_kernel's), merged in,
+    gives the whole frame and its iteration count. The host encoder's columns of
+    unfinished samples are zero, not values computed from unwritten state."""
+    if case == "f64":
+        view3, nx, ny, it, flags = ("-0.7453", "0.1127", "0.0065"), 40, 24, 4_000, 1
+    else:
+        view3, nx, ny, it, flags = ("0", "1", "1e-300"), 32, 16, 5_000, 3
+    cols = ("nu", "de", "normal")
+    v, p, plane, t, r = _setup(view3, nx, ny, it)
+    table = None
+    if flags & 2:
+        dc, e = fd.bla_dc_bound(v, p)
+        table = fd.Bla.build_scaled(r, fd.route.EPS, dc, e)
+    got = emulate(emu, r, plane, t, p, flags, bla=table, win=Window(0, 0, 0, 0, 3, 0, None, None, 1000 * 200),
+                  timed_out=True)
+    c = got["counters"]
+    cnt = _lib.Counters(samples=c["samples"], iterations=c["iterations"], blocks=c["blocks"], skipped=c["skipped"],
+                        fallback_samples=c["fallback_samples"], closed_form_samples=c["closed_form_samples"])
+    ref = fdref.Ref.arrays(r.re, r.im, r.bits)
+    ot = fdref.Bla(ref, fd.route.EPS, table.dc_max, table.dc_exp) if table is not None else None
+    job = _oracle_job(view3, p, t, fdref.COL_NU | fdref.COL_DE | fdref.COL_NORMAL)
+    whole = fdref.render(job, ref, ot, raw=True)
+    for host_encode in (False, True):
+        arrays = {k: got[k].copy() for k in ("cls", "n", "z", "dz", "dexp", "status")}
+        if not host_encode:
+            arrays.update({k: got[k].copy() for k in cols})
+        with pytest.raises(fd.Incomplete) as ex:
+            fd.route.assemble(v, p, plane, t, table, table, None, flags, True, host_encode, arrays, cnt,
+                              _lib.TIMEOUT, len(r), 0.0, fd.RouteReport(), 0.0)
+        inc = ex.value
+        assert isinstance(inc, fd.Declined)
+        assert np.array_equal(inc.mask, got["status"] == 0) and 0 < inc.mask.sum() < nx * ny
+        assert inc.stats.iterations == c["iterations"]
+        if table is not None:
+            assert (inc.bla_stats.blocks, inc.bla_stats.skipped) == (c["blocks"], c["skipped"])
+        for k in cols:
+            assert not getattr(inc.samples, k)[inc.mask].any(), k
+        # the caller's CPU restart of the masked samples only, then the overlay
+        part = fdref.render_columns(job, ref, ot, mask=inc.mask.astype(np.uint8))
+        cpu = fd.Samples(cls=part["cls"], nu=part["nu"], de=part["de"], normal=part["normal"],
+                         n=part["n"].astype(np.uint32), z=part["z"], dz=part["dz"], dexp=part["dexp"])
+        merged, st = inc.merge(cpu, fd.Stats(len(r), 0.0, part["stats"]["iterations"]))
+        assert np.array_equal(merged.cls, whole["cls"]) and np.array_equal(merged.n, whole["n"].astype(np.uint32))
+        esc = whole["cls"] == 0
+        assert np.array_equal(merged.z[esc], whole["z"][esc]) and merged.status.all()
+        assert np.array_equal(merged.nu[esc], whole["nu"][esc])
+        assert st.iterations == whole["stats"]["iterations"]
 
 
 @pytest.mark.parametrize("view3,it", [(("-0.7436438870371587", "0.1318259042053120", "1e-12"), 20_000),
