@@ -161,6 +161,16 @@ def allmax(x, world):
     return float(t.item())
 
 
+def allsum(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
 def barrier(world):
     if world > 1:
         import torch.distributed as dist
@@ -522,6 +532,94 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_shard(args):
+    """--shard: one frame of configuration 1 or 2 split over the N ranks' GPUs (strong
+    scaling): rank 0 computes the orbit and table and broadcasts them, each rank renders
+    its interleaved 4-row stripes (fractodactyl_b200.shard) and an all-gather of each
+    rank's own rows assembles the frame on every rank. value = the frame's effective
+    pixel-iterations / the slowest rank's kernel time; e2e = the same over the slowest
+    rank's wall time per frame with the upload, render, column read-back and gather."""
+    import datetime
+    import socket
+
+    import torch
+    import torch.distributed as dist
+
+    import fractodactyl_b200 as fd
+    from fractodactyl_b200 import _lib, shard
+
+    rank, world, local = dist_init(args.gpus)
+    if world == 1:  # a one-rank group, so the same gather code runs
+        with socket.socket() as sk:
+            sk.bind(("127.0.0.1", 0))
+            port = sk.getsockname()[1]
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        os.environ["MASTER_PORT"] = str(port)
+        dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    fr = frame_for(args)
+    view, p = fr.view, fr.params
+    plane, tier = fd.route._setup(view, p)
+    r = bla = None
+    if rank == 0:
+        r, bits = fd.reference(view, p)
+        r.bits = bits
+        if fr.bla_eps is not None:
+            dc, e = fd.bla_dc_bound(view, p)
+            bla = fd.Bla.build_scaled(r, fr.bla_eps, dc, e)
+            bla = bla if bla.levels else None
+    r, bla = shard.share_reference(r, bla)
+    dev = fd.Device(local)
+    flags = (_lib.DERIVATIVE if p.needs_derivative() else 0) | (_lib.BLA if bla is not None else 0)
+    nuc = r.nucleus_period()
+
+    def frame():
+        h = dev.upload(r, bla)
+        try:
+            job = fd.route.make_job(plane, tier, p, h, nuc, flags)
+            return shard.render_frame(p.nx, p.ny, shard.cuda_renderer(dev, job, p.columns))
+        finally:
+            dev.free(h)
+
+    for _ in range(args.warmup):
+        frame()
+    clocks = Clocks(local)
+    clocks.start()
+    eff = 0.0
+    kernel_ms = wall = 0.0
+    launches = 0
+    barrier(world)
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        _, c = frame()
+        dt = allmax(time.perf_counter() - t0, world)
+        wall += dt
+        kernel_ms += c["kernel_ms"]  # already the slowest rank's
+        eff += c["iterations"] - c["blocks"] + c["skipped"]
+        launches += int(c["launches"])
+    barrier(world)
+    clk = clocks.stop()
+    if rank == 0:
+        n = p.nx * p.ny
+        h2d = 16 * len(r) + (56 * len(bla.blocks) if bla is not None else 0) + n
+        d2h = n * sum(OUT_BYTES[k] for k in ["cls", "n", "status"] + [c for c in ("nu", "de", "normal")
+                                                                       if c in p.columns])
+        line = {"metric": METRIC, "value": eff / (kernel_ms * 1e-3), "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": kernel_ms / args.steps,
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded location)",
+                "config": {"workload": fr.name, "nx": p.nx, "ny": p.ny, "max_iter": p.max_iter,
+                           "bla_eps": fr.bla_eps, "tier": {0: "f64", 1: "fixed", 2: "scaled"}[tier],
+                           "form": "fp64_plain", "l2": "not flushed (one frame split over the ranks)",
+                           "parallelism": f"stripes x{world}"},
+                "clocks": clk, "gpu_launches": launches,
+                "e2e": {"value": eff / wall, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                        "steps": args.steps}}
+        print(json.dumps(line), flush=True)
+    dev.close()
+    dist.destroy_process_group()
+
+
 def run_set(args):
     """Configs 3-5: the jittered 4-spp frame (one fdc_render per step, offsets staged), the
     60-frame film and the 256 mixed-location tiles (one batch graph replay per step), in
@@ -556,10 +654,21 @@ def run_set(args):
     samples = sum(w[1] * w[3] for w in js.windows)
     log(f"{name}: {len(js.jobs)} jobs, {samples} samples; orbits {js.orbit_seconds:.1f} s, tables "
         f"{js.bla_seconds:.1f} s, set-up {time.perf_counter() - t_start:.1f} s")
+    # --shard: this rank runs jobs k % world == rank of the set (strong scaling); otherwise
+    # every rank runs the whole set (replicas, weak scaling)
+    sel = list(range(len(js.jobs)))
+    if args.shard:
+        if cfg == 3:
+            raise SystemExit("--shard splits the jobs of configurations 4 and 5")
+        from fractodactyl_b200 import shard
+        sel = shard.jobs_for(len(js.jobs), rank, world)
+    groups = [js.groups[k] for k in sel] if js.groups else None
+    loc_of = (lambda k: js.groups[k]) if js.groups else (lambda k: k)  # a job's orbit and table
+    whole_job = (lambda x: allsum(x, world)) if args.shard else (lambda x: x * world)
 
     def with_flag(extra):
         out = []
-        for j in js.jobs:
+        for j in (js.jobs[k] for k in sel):
             c = _lib.Job()
             C.memmove(C.byref(c), C.byref(j), C.sizeof(_lib.Job))
             c.flags = (j.flags & ~_lib.F32) | extra
@@ -588,7 +697,7 @@ def run_set(args):
 
             snap = lambda: {c: bufs[c].cpu().numpy().copy() for c in ("cls", "n")}
         else:
-            b = dev.batch(jobs, columns=("nu", "de", "normal"), groups=js.groups)
+            b = dev.batch(jobs, columns=("nu", "de", "normal"), groups=groups)
 
             def step():
                 total, _ = b.run()
@@ -616,7 +725,7 @@ def run_set(args):
         else:
             del bufs
         ms = allmax(tot["ms"], world)
-        forms[form] = dict(tot=tot, snap=sn, ms=ms, value=(tot["it"] - tot["blocks"] + tot["skipped"]) * world /
+        forms[form] = dict(tot=tot, snap=sn, ms=ms, value=whole_job(tot["it"] - tot["blocks"] + tot["skipped"]) /
                            (ms * 1e-3))
         torch.cuda.empty_cache()
     clk = clocks.stop()
@@ -630,17 +739,18 @@ def run_set(args):
     head = "fp32_floatexp" if ("fp32_floatexp" in forms and (agree is None or agree["count_match"] >= 0.999)) \
         else "fp64_plain"
     # e2e through the public API with host buffers, one step: uploads, render(s), columns to host
-    h2d = sum(16 * len(r) + (56 * len(bl.blocks) if bl is not None else 0) for r, bl in zip(js.refs, js.blas))
+    locs = sorted({loc_of(k) for k in sel})  # the orbits and tables this rank uploads
+    h2d = sum(16 * len(js.refs[k]) + (56 * len(js.blas[k].blocks) if js.blas[k] is not None else 0) for k in locs)
     if cfg == 3:
         h2d += 16 * samples
     d2h = samples * sum(OUT_BYTES[c] for c in cols)
-    old_handles = list(js.handles)
+    old_handles = [js.handles[k] for k in sel]
     js.free(dev)
     # the caller's host columns, allocated before the timed step as a film or tile service
     # reuses them frame after frame (one array per column over every frame)
     frame_px = {}
-    for j, key in zip(js.jobs, js.groups or range(len(js.jobs))):
-        frame_px.setdefault(key, j.nx * j.ny)
+    for k in sel:
+        frame_px.setdefault(loc_of(k) if js.groups else k, js.jobs[k].nx * js.jobs[k].ny)
     host_out = {c: np.empty(sum(frame_px.values()), fd.route._HOST_DTYPES[c])
                 for c in ("cls", "status", "n", "nu", "de", "normal")}
     for a in host_out.values():
@@ -657,31 +767,31 @@ def run_set(args):
     else:
         hs = {}
         jobs = with_flag(_lib.F32 if head == "fp32_floatexp" else 0)
-        for j, old in zip(jobs, old_handles):
-            if old not in hs:  # locations appear in order; a film has one
-                loc = 0 if len(js.refs) == 1 else len(hs)
-                hs[old] = dev.upload(js.refs[loc], js.blas[loc])
+        for k, j, old in zip(sel, jobs, old_handles):
+            if old not in hs:  # one upload per orbit (a film's frames each hold a table)
+                hs[old] = dev.upload(js.refs[loc_of(k)], js.blas[loc_of(k)])
             j.orbit = hs[old]
-        b = dev.batch(jobs, columns=("nu", "de", "normal"), groups=js.groups)
-        total, _ = b.run()
+        b = dev.batch(jobs, columns=("nu", "de", "normal"), groups=groups)
+        cnt, _ = b.run()
         host, _ = b.all_columns(host_out)
         b.free()
         for h in hs.values():
             dev.free(h)
-        eff = total.iterations - total.blocks + total.skipped
+        eff = cnt.iterations - cnt.blocks + cnt.skipped
     e2e_s = allmax(time.perf_counter() - t0, world)
-    e2e = {"value": eff * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+    e2e = {"value": whole_job(eff) / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
            "steps": 1}
     if rank == 0:
         rf = forms.get("fp64_plain", forms[head])
         line = {"metric": METRIC, "value": forms[head]["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": forms[head]["ms"] / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded locations)",
+                "scaling": "strong" if args.shard else "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded locations)",
                 "config": {"workload": name, "samples_per_step": samples, "jobs": len(js.jobs),
                            "locations": len(js.refs), "reference_points": [len(r) for r in js.refs][:4],
                            "bits": sorted({r.bits for r in js.refs})[-1], "form": head,
                            "l2": "inputs larger than L2 per step" if samples * 20 > (126 << 20) else "not flushed",
-                           "parallelism": f"replicas x{world}"},
+                           "parallelism": f"jobs interleaved x{world}" if args.shard else f"replicas x{world}"},
                 "forms": {k: {"value": v["value"], "ms_per_step": v["ms"] / args.steps,
                               "iterations": v["tot"]["it"] // args.steps, "blocks": v["tot"]["blocks"] // args.steps,
                               "skipped": v["tot"]["skipped"] // args.steps,
@@ -718,6 +828,8 @@ def main():
     ap.add_argument("--ny", type=int, default=0)
     ap.add_argument("--tier", choices=("fixed", "scaled"), default=None)
     ap.add_argument("--form", choices=("both", "fp64", "f32"), default="both")
+    ap.add_argument("--shard", action="store_true",
+                    help="configurations 1-2: one frame split over the ranks (strong scaling)")
     args = ap.parse_args()
     if args.impl == "reference":
         if args.config > 2:
@@ -725,6 +837,10 @@ def main():
                               "reference CPU arm runs configs 1 and 2"}))
             return
         run_reference(args)
+    elif args.shard:
+        if args.config > 2:
+            raise SystemExit("--shard splits the one frame of configuration 1 or 2")
+        run_shard(args)
     elif args.config > 2:
         run_set(args)
     else:
