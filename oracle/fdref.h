@@ -26,7 +26,14 @@ extern "C" {
 #endif
 
 /* Column bits, as fd-samples Column (crates/fd-samples/src/column.rs:7-24). */
-enum { FDREF_COL_CLASS = 1, FDREF_COL_NU = 2, FDREF_COL_DE = 4, FDREF_COL_NORMAL = 8, FDREF_COL_BOUND = 16 };
+enum {
+  FDREF_COL_CLASS = 1,
+  FDREF_COL_NU = 2,
+  FDREF_COL_DE = 4,
+  FDREF_COL_NORMAL = 8,
+  FDREF_COL_BOUND = 16,
+  FDREF_COL_STRIPE = 32
+};
 
 /* Tier (crates/fd-kernel/src/view.rs:7-14); -1 = cheapest valid. */
 enum { FDREF_TIER_AUTO = -1, FDREF_TIER_F64 = 0, FDREF_TIER_FIXED = 1, FDREF_TIER_SCALED = 2 };
@@ -44,6 +51,8 @@ typedef struct {
   int32_t threads;
   int32_t tier;
   uint32_t row_first, row_step; /* render rows row_first, +row_step, ... (0, 0 = all) */
+  uint32_t stripe_window;       /* Stripe column: iterates averaged (grid.rs:36-37; 0 = 16) */
+  double stripe_freq;           /* Stripe column: k of sin(k arg z) (0 = 5) */
 } fdref_job;
 
 typedef struct fdref_ref fdref_ref; /* Reference orbit (reference.rs:7-10) + bits */
@@ -115,6 +124,11 @@ int fdref_render(const fdref_job *job, const fdref_ref *ref, const fdref_bla *bl
 /* sample::iterate from a supplied state (Start, sample.rs:69-80, 186-228): start_n
  * iterates done, delta (start_xr, start_xi) and dz/dc (start_dr, start_di); start_n 0 is
  * fdref_iterate. Refused on the extended tier and at or past the orbit's last point. */
+/* sample::iterate with the Stripe recorder (stripe.rs; window, freq: StripeParams) for one
+ * sample from Z_0: the outcome and the sample's stripe value (0 unless escaped). */
+int fdref_iterate_stripe(const fdref_ref *r, const fdref_bla *bla, int extended, int derivative, double ar,
+                         double ai, int64_t offset_exp, uint64_t max_iter, double r2, int64_t nucleus,
+                         uint32_t window, double freq, fdref_outcome *out, float *value);
 int fdref_iterate_from(const fdref_ref *r, const fdref_bla *bla, int extended, int derivative,
                        int has_c, double cr, double ci, double ar, double ai, int64_t offset_exp,
                        uint64_t max_iter, double r2, int64_t nucleus, uint64_t start_n,
@@ -166,6 +180,7 @@ typedef struct {
   double *z, *dz;
   int64_t *dexp;
   double *ez, *ed;
+  float *stripe; /* FDREF_COL_STRIPE: the stripe average of escaped samples (stripe.rs) */
 } fdref_columns;
 /* Precision experiment, not the reference's algorithm: bits in [1, 52] rounds every
  * delta the kernel writes to that many mantissa bits (24: an ideal FP32-mantissa delta)

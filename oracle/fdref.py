@@ -12,7 +12,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "liboracle.so")
 
-COL_CLASS, COL_NU, COL_DE, COL_NORMAL, COL_BOUND = 1, 2, 4, 8, 16
+COL_CLASS, COL_NU, COL_DE, COL_NORMAL, COL_BOUND, COL_STRIPE = 1, 2, 4, 8, 16, 32
 TIER = {None: -1, "auto": -1, "f64": 0, "fx": 1, "fixed": 1, "scaled": 2}
 
 
@@ -32,6 +32,8 @@ class Job(C.Structure):
         ("tier", C.c_int32),
         ("row_first", C.c_uint32),
         ("row_step", C.c_uint32),
+        ("stripe_window", C.c_uint32),
+        ("stripe_freq", C.c_double),
     ]
 
 
@@ -65,7 +67,8 @@ class Stats(C.Structure):
 
 
 class Columns(C.Structure):  # fdref_columns
-    _fields_ = [(k, C.c_void_p) for k in ("cls", "nu", "de", "normal", "bound", "n", "z", "dz", "dexp", "ez", "ed")]
+    _fields_ = [(k, C.c_void_p) for k in ("cls", "nu", "de", "normal", "bound", "n", "z", "dz", "dexp", "ez", "ed",
+                                          "stripe")]
 
 
 class SeriesInfo(C.Structure):
@@ -132,6 +135,8 @@ def lib():
         L.fdref_render_fds.argtypes = [C.POINTER(Job), P, P, P, U64]
         L.fdref_iterate_from.argtypes = [P, P, C.c_int, C.c_int, C.c_int, D, D, D, D, I64, U64, D, I64,
                                          U64, D, D, D, D, C.POINTER(Outcome)]
+        L.fdref_iterate_stripe.argtypes = [P, P, C.c_int, C.c_int, D, D, I64, U64, D, I64, C.c_uint32, D,
+                                           C.POINTER(Outcome), C.POINTER(C.c_float)]
         L.fdref_series_build.restype = P
         L.fdref_series_build.argtypes = [P, D, D, U64, U64]
         L.fdref_series_get.argtypes = [P, C.POINTER(SeriesInfo), P]
@@ -165,7 +170,8 @@ def _err():
 
 
 def make_job(re, im, width, nx, ny, max_iter, rotation=0.0, ss=1, escape_radius=1e10,
-             columns=COL_NU | COL_DE | COL_NORMAL, threads=None, tier=None, row_first=0, row_step=1):
+             columns=COL_NU | COL_DE | COL_NORMAL, threads=None, tier=None, row_first=0, row_step=1,
+             stripe_window=16, stripe_freq=5.0):
     j = Job()
     j._keep = [s.encode() if isinstance(s, str) else s for s in (re, im, width)]
     j.center_re, j.center_im, j.width = j._keep
@@ -177,6 +183,7 @@ def make_job(re, im, width, nx, ny, max_iter, rotation=0.0, ss=1, escape_radius=
     j.threads = threads or os.cpu_count() or 1
     j.tier = TIER[tier] if not isinstance(tier, int) else tier
     j.row_first, j.row_step = row_first, row_step
+    j.stripe_window, j.stripe_freq = stripe_window, stripe_freq
     return j
 
 
@@ -356,7 +363,7 @@ def render_columns(job, ref=None, bla=None, series=None, mask=None):
     n = job.nx * job.ny
     out = dict(cls=np.zeros(n, np.uint8), nu=np.zeros(n), de=np.zeros(n, np.float32), normal=np.zeros(n, np.uint16),
                bound=np.zeros(n, np.float32), n=np.zeros(n, np.uint64), z=np.zeros((n, 2)), dz=np.zeros((n, 2)),
-               dexp=np.zeros(n, np.int64), ez=np.zeros(n), ed=np.zeros(n))
+               dexp=np.zeros(n, np.int64), ez=np.zeros(n), ed=np.zeros(n), stripe=np.zeros(n, np.float32))
     cols = Columns(**{k: v.ctypes.data for k, v in out.items()})
     m = None if mask is None else np.ascontiguousarray(mask, dtype=np.uint8)
     st = Stats()
@@ -402,6 +409,19 @@ def iterate(ref, bla=None, extended=False, derivative=True, c=None, ar=0.0, ai=0
     kind = {0: "escaped", 1: "interior", 2: "unresolved"}[o.kind]
     return dict(kind=kind, n=o.n, zr=o.zr, zi=o.zi, dr=o.dr, di=o.di, dexp=o.dexp, blocks=o.blocks,
                 skipped=o.skipped, shift=o.shift)
+
+
+def iterate_stripe(ref, bla=None, extended=False, derivative=False, ar=0.0, ai=0.0, offset_exp=0, max_iter=1000,
+                   r2=1e20, nucleus=-2, window=16, freq=5.0):
+    """One sample from Z_0 with the Stripe recorder (stripe.rs): (outcome dict, stripe value)."""
+    o, v = Outcome(), C.c_float()
+    rc = lib().fdref_iterate_stripe(ref.h, bla.h if bla else None, int(extended), int(derivative), ar, ai, offset_exp,
+                                    max_iter, r2, -1 if nucleus is None else nucleus, window, freq, C.byref(o),
+                                    C.byref(v))
+    if rc != 0:
+        raise ValueError(_err())
+    kind = {0: "escaped", 1: "interior", 2: "unresolved"}[o.kind]
+    return dict(kind=kind, n=o.n, zr=o.zr, zi=o.zi, blocks=o.blocks, skipped=o.skipped), v.value
 
 
 def render(job, ref=None, bla=None, raw=False):

@@ -43,6 +43,7 @@ struct Columns {
   double *z = nullptr, *dz = nullptr;
   int64_t *dexp = nullptr;
   double *ez = nullptr, *ed = nullptr;  // raw error radii of escaped samples (bounded renders)
+  float *stripe = nullptr;              // Stripe column (stripe.rs)
 };
 
 // store.rs:115-151: Bounded evidence for an escaped sample with |z| = az, |dz/dc| = ad
@@ -111,6 +112,9 @@ struct Stats {
 static std::pair<Plane, Tier> setup(const View &v, const Params &p) {
   if (p.ss == 0 || p.nx % p.ss != 0 || p.ny % p.ss != 0)
     throw std::runtime_error("grid must be a whole number of pixels");
+  if ((p.columns & FDREF_COL_STRIPE) &&
+      (p.stripe_window < 1 || p.stripe_window > 64 || !std::isfinite(p.stripe_freq)))
+    throw std::runtime_error("stripe window must be 1..=64 and the frequency finite");
   Plane plane = Plane::make(v, p.nx, p.ny);
   Tier tier = p.tier ? *p.tier : plane.tier;
   if (!plane.allows(tier)) throw std::runtime_error("tier is not valid at this depth");
@@ -147,7 +151,7 @@ static void bla_checks(const Plane &plane, Tier tier, const Params &p, const Ref
   if (std::isnan(dc) || over) throw std::runtime_error("view reaches |dc| beyond the BLA table's dc_max");
 }
 
-// grid.rs:446-535 + Job::one/one_from/fill (grid.rs:623-775), without stripe. series: a
+// grid.rs:446-535 + Job::one/one_from/fill (grid.rs:623-775), stripe included. series: a
 // start every sample takes (n > 0; Series::render_masked's refusals, grid.rs:341-373,
 // checked here); mask: render only samples with mask != 0 (the others keep their columns).
 static std::string run(const View &v, const Params &p, const Reference *supplied, const Bla *bla, Columns cols,
@@ -195,8 +199,13 @@ static std::string run(const View &v, const Params &p, const Reference *supplied
   std::optional<size_t> nucleus = ref->nucleus_period();
   std::atomic<uint32_t> next_row{0};
   std::mutex mu;
+  const bool striped = (p.columns & FDREF_COL_STRIPE) != 0;
   auto worker = [&]() {
     Stats local;
+    Stripe stripe;  // this thread's recorder (grid.rs:498), begun per sample
+    stripe.window = p.stripe_window;
+    stripe.freq = p.stripe_freq;
+    Stripe *trace = striped ? &stripe : nullptr;
     for (;;) {
       uint64_t jj = (uint64_t)p.row_first + (uint64_t)next_row.fetch_add(1) * p.row_step;
       if (jj >= p.ny) break;
@@ -213,24 +222,26 @@ static std::string run(const View &v, const Params &p, const Reference *supplied
             case Tier::F64: {
               double ar = ux * h, ai = uy * h;
               return iterate(false, D, L, *ref, bla, skip, std::make_pair(plane.c_re + ar, plane.c_im + ai), ar, ai,
-                             0, p.max_iter, r2, nucleus, start(ar, ai), qp);
+                             0, p.max_iter, r2, nucleus, start(ar, ai), qp, trace);
             }
             case Tier::Fixed:
               return iterate(false, D, L, *ref, bla, skip, std::nullopt, ux * h, uy * h, 0, p.max_iter, r2, nucleus,
-                             start(ux * h, uy * h), qp);
+                             start(ux * h, uy * h), qp, trace);
             case Tier::Scaled:
             default:
               return iterate(true, D, L, *ref, bla, skip, std::nullopt, ux * plane.h_m, uy * plane.h_m, plane.h_e,
-                             p.max_iter, r2, nucleus);
+                             p.max_iter, r2, nucleus, Start{}, nullptr, trace);
           }
         };
         // Job::one (grid.rs:623-648): the prefix is not counted; an unresolved series start
         // retries from zero (keeping the nucleus heuristic), counting both runs
+        if (trace) trace->begin();  // Job::one (grid.rs:630)
         const Outcome first = one_from(true);
         const uint64_t prefix = series && !(first.kind == Kind::Interior && first.n == 0) ? series->n : 0;
         uint64_t spent = first.iterations(p.max_iter) - prefix;
         Outcome o = first;
         if (prefix > 0 && first.kind == Kind::Unresolved) {
+          if (trace) trace->begin();  // grid.rs:638
           o = one_from(false);
           spent += o.iterations(p.max_iter);
         }
@@ -245,6 +256,7 @@ static std::string run(const View &v, const Params &p, const Reference *supplied
         }
         local.iterations += spent;
         put(plane, p.ss, p.columns, o, (size_t)j * p.nx + i, cols, p.max_iter);
+        if (trace && cols.stripe) cols.stripe[(size_t)j * p.nx + i] = trace->value;  // grid.rs:772
       }
     }
     std::lock_guard<std::mutex> g(mu);
@@ -291,7 +303,7 @@ struct Out {
 static std::vector<uint8_t> fds(const View &v, const Params &p, uint32_t colset, const std::string &kernel,
                                 const std::vector<uint8_t> &cls, const std::vector<double> &nu,
                                 const std::vector<float> &de, const std::vector<uint16_t> &normal,
-                                const std::vector<float> &bound) {
+                                const std::vector<float> &bound, const std::vector<float> &stripe) {
   Out o;
   o.bytes("FDSAMPLE", 8);
   o.u16(1);
@@ -325,6 +337,10 @@ static std::vector<uint8_t> fds(const View &v, const Params &p, uint32_t colset,
   }
   if (colset & FDREF_COL_BOUND) {  // column.rs:18-19, 42: f32, after normal in bit order
     o.bytes(bound.data(), bound.size() * 4);
+    o.pad8();
+  }
+  if (colset & FDREF_COL_STRIPE) {  // column.rs:20-22, 42: f32, last in bit order
+    o.bytes(stripe.data(), stripe.size() * 4);
     o.pad8();
   }
   return o.b;
@@ -374,6 +390,8 @@ static Params to_params(const fdref_job *j) {
   if (j->tier >= 0) p.tier = (Tier)j->tier;
   p.row_first = j->row_first;
   p.row_step = j->row_step ? j->row_step : 1;
+  p.stripe_window = j->stripe_window ? j->stripe_window : 16;
+  p.stripe_freq = j->stripe_freq != 0.0 ? j->stripe_freq : 5.0;
   return p;
 }
 
@@ -486,6 +504,38 @@ int fdref_bla_dc_bound(const fdref_job *job, double *dc, int64_t *e) {
   return -1;
 }
 
+int fdref_iterate_stripe(const fdref_ref *r, const fdref_bla *bla, int extended, int derivative, double ar,
+                         double ai, int64_t offset_exp, uint64_t max_iter, double r2, int64_t nucleus,
+                         uint32_t window, double freq, fdref_outcome *out, float *value) {
+  FDREF_TRY({
+    std::optional<size_t> nuc;
+    if (nucleus == -2) nuc = r->r.nucleus_period();
+    else if (nucleus >= 0) nuc = (size_t)nucleus;
+    Skip skip;
+    Stripe t;
+    t.window = window;
+    t.freq = freq;
+    t.begin();
+    Outcome o = iterate(extended != 0, derivative != 0, bla != nullptr, r->r, bla ? &bla->t : nullptr, skip,
+                        std::nullopt, ar, ai, offset_exp, max_iter, r2, nuc, Start{}, nullptr, &t);
+    out->kind = (int32_t)o.kind;
+    out->n = o.n;
+    out->zr = o.zr;
+    out->zi = o.zi;
+    out->dr = o.dr;
+    out->di = o.di;
+    out->dexp = o.dexp;
+    out->blocks = skip.blocks;
+    out->skipped = skip.skipped;
+    out->shift = skip.shift;
+    out->ez = o.ez;
+    out->ed = o.ed;
+    *value = t.value;
+    return 0;
+  })
+  return -1;
+}
+
 int fdref_iterate(const fdref_ref *r, const fdref_bla *bla, int extended, int derivative, int has_c, double cr,
                   double ci, double ar, double ai, int64_t offset_exp, uint64_t max_iter, double r2,
                   int64_t nucleus, fdref_outcome *out) {
@@ -581,6 +631,7 @@ int fdref_render_columns(const fdref_job *job, const fdref_ref *ref, const fdref
     c.dexp = out->dexp;
     c.ez = out->ez;
     c.ed = out->ed;
+    c.stripe = out->stripe;
     Stats st;
     std::string k = run(to_view(job), to_params(job), ref ? &ref->r : nullptr, bla ? &bla->t : nullptr, c, st,
                         nullptr, series ? &series->s : nullptr, mask);
@@ -751,15 +802,17 @@ int64_t fdref_render_fds(const fdref_job *job, const fdref_ref *ref, const fdref
     std::vector<float> de((p.columns & FDREF_COL_DE) ? n : 0, 0.0f);
     std::vector<uint16_t> normal((p.columns & FDREF_COL_NORMAL) ? n : 0, 0);
     std::vector<float> bound((p.columns & FDREF_COL_BOUND) ? n : 0, 0.0f);
+    std::vector<float> stripe((p.columns & FDREF_COL_STRIPE) ? n : 0, 0.0f);
     Columns c;
     c.cls = cls.data();
     c.nu = nu.empty() ? nullptr : nu.data();
     c.de = de.empty() ? nullptr : de.data();
     c.normal = normal.empty() ? nullptr : normal.data();
     c.bound = bound.empty() ? nullptr : bound.data();
+    c.stripe = stripe.empty() ? nullptr : stripe.data();
     Stats st;
     std::string k = run(v, p, ref ? &ref->r : nullptr, bla ? &bla->t : nullptr, c, st);
-    std::vector<uint8_t> bytes = fds(v, p, p.columns, k, cls, nu, de, normal, bound);
+    std::vector<uint8_t> bytes = fds(v, p, p.columns, k, cls, nu, de, normal, bound, stripe);
     if (buf && cap) std::memcpy(buf, bytes.data(), std::min<uint64_t>(cap, bytes.size()));
     return (int64_t)bytes.size();
   })

@@ -49,6 +49,8 @@ struct Params {
   int threads = 1;
   std::optional<Tier> tier;
   uint32_t row_first = 0, row_step = 1;
+  uint32_t stripe_window = 16;  // StripeParams (stripe.rs:20-36)
+  double stripe_freq = 5.0;
 };
 
 struct Plane {
@@ -120,12 +122,49 @@ struct Start {
   double xr = 0.0, xi = 0.0, dr = 0.0, di = 0.0;
 };
 
+// The loop state at the start of a BLA block, from which a stripe replay restarts
+// (stripe.rs:39-52).
+struct StripeSnap {
+  size_t m = 0;
+  uint64_t n = 0;
+  double xr = 0, xi = 0;
+  int64_t delta_exp = 0;
+  double scale = 0, dc_r = 0, dc_i = 0;
+  uint64_t valid = 0;  // first iterate of the recorded run that reached n
+};
+
+// stripe.rs:12-241: the Stripe column's recorder for one sample at a time. Iterates go
+// into a ring of the last RING; each block start is kept (the last SNAPS of them) so that
+// an escape whose window misses iterates can replay them plainly.
+struct Stripe {
+  static constexpr size_t RING = 128, SNAPS = 8;
+  uint32_t window = 16;
+  double freq = 5.0;
+  double ring_r[RING] = {}, ring_i[RING] = {};
+  uint64_t valid = UINT64_MAX;
+  StripeSnap snaps[SNAPS];
+  size_t count = 0;
+  float value = 0.0f;
+  void begin();
+  void start(uint64_t n) { valid = n + 1; }
+  void record(uint64_t n, double zr, double zi) {
+    ring_r[n % RING] = zr;
+    ring_i[n % RING] = zi;
+  }
+  void snap(StripeSnap s, uint64_t landed);
+  bool rewind(uint64_t n, StripeSnap &out);
+  void finish(uint64_t n, double zr, double zi, double r2);
+  double term(double zr, double zi) const;
+  bool complete(uint64_t n) const;
+};
+
 // q: the orbit's error radii (Reference::error_radius) to track the bounded variant
 // (B, ordinary tiers: no BLA, no nucleus gate, no series start); null otherwise.
+// trace: the Stripe column's recorder (begun by the caller), or null.
 Outcome iterate(bool extended, bool D, bool L, const Reference &r, const Bla *bla, Skip &skip,
                 std::optional<std::pair<double, double>> c, double ar, double ai, int64_t offset_exp,
                 uint64_t max_iter, double r2, std::optional<size_t> nucleus, const Start &start = Start{},
-                const double *q = nullptr);
+                const double *q = nullptr, Stripe *trace = nullptr);
 
 // series.rs:26-55
 struct SeriesConfig {

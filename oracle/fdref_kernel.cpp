@@ -463,9 +463,104 @@ static inline uint64_t next_pow2(uint64_t x) {
   return 1ull << (64 - __builtin_clzll(x - 1));
 }
 
-// ---------------------------------------------------------------- sample.rs:170-581
-// The B (bounded) and trace/stripe features are outside the hot path (the GPU route
-// declines Bound/Stripe frames). A series start (Start, sample.rs:69-80) is supported.
+// ---------------------------------------------------------------- stripe.rs
+// stripe.rs:164-168
+void Stripe::begin() {
+  valid = UINT64_MAX;
+  count = 0;
+  value = 0.0f;
+}
+
+// stripe.rs:180-187: keep the block start with the run it continues, the run restarts
+// at the iterate the block lands on
+void Stripe::snap(StripeSnap s, uint64_t landed) {
+  s.valid = valid;
+  snaps[count % SNAPS] = s;
+  count += 1;
+  valid = landed;
+}
+
+// stripe.rs:157-160: both windows ending at z_n recorded
+bool Stripe::complete(uint64_t n) const {
+  const uint64_t a = n > window ? n - window : 0;
+  return valid <= (a > 1 ? a : 1);
+}
+
+// stripe.rs:189-204: the latest kept block start at or before n - window, else the
+// oldest kept one; the replay records from its n + 1 on
+bool Stripe::rewind(uint64_t n, StripeSnap &out) {
+  if (count == 0 || complete(n)) return false;
+  const uint64_t need = n > window ? n - window : 0;
+  const size_t kept = count < SNAPS ? count : SNAPS;
+  const StripeSnap *pick = nullptr;
+  for (size_t j = 0; j < kept && !pick; ++j) {
+    const StripeSnap &c = snaps[(count - 1 - j) % SNAPS];
+    if (c.n <= need) pick = &c;
+  }
+  if (!pick) {  // the first of the equally oldest, in most-recent-first order
+    for (size_t j = 0; j < kept; ++j) {
+      const StripeSnap &c = snaps[(count - 1 - j) % SNAPS];
+      if (!pick || c.n < pick->n) pick = &c;
+    }
+  }
+  valid = pick->valid;
+  out = *pick;
+  return true;
+}
+
+// stripe.rs:132-152: 0.5 + 0.5 sin(k arg z); a whole k up to 16 as the sign of k times
+// Im (z / |z|)^|k|
+double Stripe::term(double zr, double zi) const {
+  const double k = freq;
+  double s;
+  if (k == std::trunc(k) && std::fabs(k) <= 16.0) {
+    const double h = std::hypot(zr, zi);
+    const double ur = zr / h, ui = zi / h;
+    double pr = 1.0, pi = 0.0;
+    const int reps = (int)std::fabs(k);
+    for (int q = 0; q < reps; ++q) {
+      const double nr = pr * ur - pi * ui, ni = pr * ui + pi * ur;
+      pr = nr;
+      pi = ni;
+    }
+    s = k < 0.0 ? -pi : pi;
+  } else {
+    s = std::sin(k * std::atan2(zi, zr));
+  }
+  return 0.5 + 0.5 * s;
+}
+
+// stripe.rs:206-240: the windows ending at z_n and z_{n-1}, interpolated by how far past
+// the escape radius z_n landed
+void Stripe::finish(uint64_t n, double zr, double zi, double r2) {
+  const uint64_t lo = n > window ? n - window : 0;
+  const uint64_t first = lo > 1 ? lo : 1;
+  double now = 0.0, before = 0.0;
+  uint32_t count_now = 0, count_before = 0;
+  for (uint64_t i = first; i <= n; ++i) {
+    if (i < valid) continue;
+    const double t = term(ring_r[i % RING], ring_i[i % RING]);
+    if (i > first || (first == 1 && n <= window)) {
+      now += t;
+      count_now += 1;
+    }
+    if (i < n) {
+      before += t;
+      count_before += 1;
+    }
+  }
+  if (count_now == 0) {
+    value = 0.0f;
+    return;
+  }
+  now /= (double)count_now;
+  before = count_before > 0 ? before / (double)count_before : now;
+  double frac = 1.0 - std::log2(std::log(zr * zr + zi * zi) / std::log(r2));
+  if (frac < 0.0) frac = 0.0;  // f64::clamp: NaN stays NaN
+  if (frac > 1.0) frac = 1.0;
+  value = (float)(before * (1.0 - frac) + now * frac);
+}
+
 // Precision experiment (not the reference's algorithm): with g_delta_bits in [1, 52],
 // the delta is rounded to that many mantissa bits (round half to even) after every update
 // that writes it (plain step, block, rebase), everything else staying binary64. 24 bits
@@ -485,11 +580,18 @@ static inline double round_bits(double x, int bits) {
   return std::ldexp(std::nearbyint(std::ldexp(m, bits)), e - bits);
 }
 
-template <bool EXT, bool D, bool L, bool B>
+// ---------------------------------------------------------------- sample.rs:170-581
+// The B (bounded) variant and the Stripe recorder (T) are template arguments, so the
+// plain kernel compiles without them. A series start (Start, sample.rs:69-80) is supported.
+// T: the Stripe column's recorder is on (sample.rs:231-236): each iterate is recorded,
+// each block start kept, and an escape whose window misses iterates replays them plainly
+// from a kept block start, the outcome staying the first escape's.
+template <bool EXT, bool D, bool L, bool B, bool T = false>
 static Outcome iterate_t(const Reference &r, const Bla *bla, Skip &skip,
                          std::optional<std::pair<double, double>> c, double ar, double ai,
                          int64_t offset_exp, uint64_t max_iter, double r2,
-                         std::optional<size_t> nucleus, const Start &start, const double *q) {
+                         std::optional<size_t> nucleus, const Start &start, const double *q,
+                         Stripe *trace = nullptr) {
   Outcome o;
   if (c && in_main_components(c->first, c->second)) {
     o.kind = Kind::Interior;
@@ -540,10 +642,15 @@ static Outcome iterate_t(const Reference &r, const Bla *bla, Skip &skip,
     }
   };
   uint64_t limit = max_iter;
+  bool replaying = false;
+  Outcome first;  // the escape the blocks found, while a replay re-walks its window
+  uint64_t first_at = 0;
+  double first_r = 0.0, first_i = 0.0;
+  if (T) trace->start(n);
   while (n < limit) {
     const Block *b = nullptr;
     size_t len = 0;
-    if (L && bla && (!nucleus || m != 0)) {
+    if (L && bla && !replaying && (!nucleus || m != 0)) {
       double d2 = EXT ? (xr * xr + xi * xi) * scale * scale : xr * xr + xi * xi;
       uint64_t cap = hold > 0 ? sn + hold : (pending ? UINT64_MAX : chk);
       uint64_t budget = std::min(max_iter, cap);
@@ -552,6 +659,7 @@ static Outcome iterate_t(const Reference &r, const Bla *bla, Skip &skip,
       b = bla->find(m, d2, budget, len);
     }
     if (b) {
+      if (T) trace->snap(StripeSnap{m, n, xr, xi, delta_exp, scale, dc_r, dc_i, 0}, n + len);
       double a_r = b->ar, a_i = b->ai, b_r = b->br, b_i = b->bi;
       if (nucleus && n >= 1) contraction.multiply(a_r, a_i, 0);
       if (!EXT && hold > 0) mu.multiply(a_r, a_i);
@@ -639,6 +747,7 @@ static Outcome iterate_t(const Reference &r, const Bla *bla, Skip &skip,
     double physical_r = scale * xr, physical_i = scale * xi;
     double fr = zr[m] + physical_r, fi = zi[m] + physical_i;
     double f2 = fr * fr + fi * fi;
+    if (T) trace->record(n, fr, fi);
     if (f2 > r2) {
       o.kind = Kind::Escaped;
       o.n = n;
@@ -651,9 +760,34 @@ static Outcome iterate_t(const Reference &r, const Bla *bla, Skip &skip,
         o.ez = e + q[m] + 4.0 * U * std::sqrt(f2);
         o.ed = ed;
       }
+      if (T) {  // sample.rs:387-403
+        if (replaying) {
+          trace->finish(n, fr, fi, r2);
+          return first;
+        }
+        StripeSnap sn;
+        if (trace->rewind(n, sn)) {
+          first = o;
+          first_at = n;
+          first_r = fr;
+          first_i = fi;
+          replaying = true;
+          limit = std::min<uint64_t>(max_iter, n + 64);
+          m = sn.m;
+          n = sn.n;
+          xr = sn.xr;
+          xi = sn.xi;
+          delta_exp = sn.delta_exp;
+          scale = sn.scale;
+          dc_r = sn.dc_r;
+          dc_i = sn.dc_i;
+          continue;
+        }
+        trace->finish(n, fr, fi, r2);
+      }
       return o;
     }
-    if (nucleus && n == (uint64_t)*nucleus + 1) {
+    if (!replaying && nucleus && n == (uint64_t)*nucleus + 1) {
       if (contraction.small()) {
         o.kind = Kind::Interior;
         o.n = n;
@@ -695,6 +829,7 @@ static Outcome iterate_t(const Reference &r, const Bla *bla, Skip &skip,
           scale = exp2i(delta_exp);
           m = 1;
           n = n + 1;
+          if (T) trace->start(n);  // this step's iterate is not recorded
         }
         rounded();
         double factor = exp2i(offset_exp - delta_exp);
@@ -724,6 +859,7 @@ static Outcome iterate_t(const Reference &r, const Bla *bla, Skip &skip,
         dc_i = ai * f;
       }
     }
+    if (T && replaying) continue;  // sample.rs:470-472: the replay only re-walks iterates
     double check_r = EXT ? physical_r : xr, check_i = EXT ? physical_i : xi;
     bool judge = EXT ? (returns < 4 && resolvable(check_r, check_i, f2)) : resolvable(check_r, check_i, f2);
     if (!judge) {
@@ -808,6 +944,10 @@ static Outcome iterate_t(const Reference &r, const Bla *bla, Skip &skip,
       chk = chk * 2;
     }
   }
+  if (T && replaying) {  // sample.rs:576-579: the replay gave up; from what was recorded
+    trace->finish(first_at, first_r, first_i, r2);
+    return first;
+  }
   o.kind = Kind::Unresolved;
   return o;
 }
@@ -819,17 +959,24 @@ static Outcome iterate_t(const Reference &r, const Bla *bla, Skip &skip,
 Outcome iterate(bool extended, bool D, bool L, const Reference &r, const Bla *bla, Skip &skip,
                 std::optional<std::pair<double, double>> c, double ar, double ai, int64_t offset_exp,
                 uint64_t max_iter, double r2, std::optional<size_t> nucleus, const Start &start,
-                const double *q) {
+                const double *q, Stripe *trace) {
   // sample.rs:226-229: a supplied state skipped the contraction's products, and a
   // bounded render has no proof for the heuristic, so both decline it
   if (start.n > 0 || q) nucleus = std::nullopt;
   if (q) {  // sample.rs:185-186, 246: the bounded variant is ordinary-tier, unblocked, from Z_0
     if (extended || start.n > 0) throw std::runtime_error("bounded iteration needs an ordinary tier and no series start");
+    if (trace)
+      return D ? iterate_t<false, true, false, true, true>(r, nullptr, skip, c, ar, ai, 0, max_iter, r2, nucleus,
+                                                           start, q, trace)
+               : iterate_t<false, false, false, true, true>(r, nullptr, skip, c, ar, ai, 0, max_iter, r2, nucleus,
+                                                            start, q, trace);
     return D ? iterate_t<false, true, false, true>(r, nullptr, skip, c, ar, ai, 0, max_iter, r2, nucleus, start, q)
              : iterate_t<false, false, false, true>(r, nullptr, skip, c, ar, ai, 0, max_iter, r2, nucleus, start, q);
   }
-#define FDREF_IT(E, DD, LL) \
-  iterate_t<E, DD, LL, false>(r, bla, skip, c, ar, ai, offset_exp, max_iter, r2, nucleus, start, nullptr)
+#define FDREF_IT(E, DD, LL)                                                                                     \
+  (trace ? iterate_t<E, DD, LL, false, true>(r, bla, skip, c, ar, ai, offset_exp, max_iter, r2, nucleus, start, \
+                                             nullptr, trace)                                                    \
+         : iterate_t<E, DD, LL, false>(r, bla, skip, c, ar, ai, offset_exp, max_iter, r2, nucleus, start, nullptr))
   if (extended) {
     if (D) return L ? FDREF_IT(true, true, true) : FDREF_IT(true, true, false);
     return L ? FDREF_IT(true, false, true) : FDREF_IT(true, false, false);
