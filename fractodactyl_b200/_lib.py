@@ -63,6 +63,10 @@ class BoundOut(C.Structure):  # fdc_bound_out
     _fields_ = [("bound", C.c_void_p), ("ez", C.c_void_p), ("ed", C.c_void_p)]
 
 
+class Stripe(C.Structure):  # fdc_stripe
+    _fields_ = [("window", C.c_uint32), ("freq", C.c_double)]
+
+
 class Out(C.Structure):
     _fields_ = [(name, C.c_void_p) for name in ("cls", "n", "nu", "de", "normal", "z", "dz", "dexp", "status")]
 
@@ -105,7 +109,7 @@ DEFAULT_DEFER = 0  # FDC_DEFAULT_DEFER: each kernel variant's measured default
 
 # Every symbol the headers declare, for the export check.
 FDC_SYMBOLS = ["fdc_abi_version", "fdc_open", "fdc_close", "fdc_last_error", "fdc_upload_orbit", "fdc_free_orbit",
-               "fdc_upload_bla", "fdc_upload_series", "fdc_upload_error_radius", "fdc_render_bounded", "fdc_render", "fdc_batch_create", "fdc_batch_run", "fdc_batch_free",
+               "fdc_upload_bla", "fdc_upload_series", "fdc_upload_error_radius", "fdc_render_bounded", "fdc_render_stripe", "fdc_render", "fdc_batch_create", "fdc_batch_run", "fdc_batch_free",
                "fdc_render_noalloc", "fdc_set_tuning", "fdc_get_tuning"]
 FDH_SYMBOLS = ["fdh_last_error", "fdh_plane_new", "fdh_orbit_fixed", "fdh_orbit_fixed_threads", "fdh_orbit_f64",
                "fdh_nucleus_period",
@@ -134,6 +138,7 @@ def lib():
     L.fdc_upload_series.argtypes = [P, I32, U64, U64, D, P, U32]
     L.fdc_render.argtypes = [P, C.POINTER(Job), C.POINTER(Out), C.POINTER(Counters)]
     L.fdc_render_bounded.argtypes = [P, C.POINTER(Job), C.POINTER(Out), C.POINTER(BoundOut), C.POINTER(Counters)]
+    L.fdc_render_stripe.argtypes = [P, C.POINTER(Job), C.POINTER(Out), C.POINTER(Stripe), P, C.POINTER(Counters)]
     L.fdc_upload_error_radius.argtypes = [P, I32, P, U64]
     L.fdc_batch_create.argtypes = [P, P, P, U32, C.POINTER(P)]
     L.fdc_batch_run.argtypes = [P, P, C.POINTER(Counters), P]

@@ -85,7 +85,7 @@ struct fdc_ctx {
   // staging for host outputs / inputs, grown on demand
   void *stage = nullptr;
   size_t stage_bytes = 0;
-  int blocks_per_sm[13] = {};
+  int blocks_per_sm[21] = {};
   int blocks_per_sm_f32[4] = {};
   int blocks_per_sm_batch[8] = {};
   int blocks_per_sm_batch_f32[4] = {};
@@ -296,17 +296,31 @@ __global__ void fuse_bla(const double2 *__restrict__ z, uint64_t len, const doub
 
 unsigned grid_for(uint64_t n) { return (unsigned)std::min<uint64_t>((n + 255) / 256, 148 * 16); }
 
-template <bool EXT, bool D, bool L, bool S = false, bool B = false>
+template <bool EXT, bool D, bool L, bool S = false, bool B = false, bool T = false>
 void *kernel_ptr() {
-  return (void *)fdk::perturb_kernel<EXT, D, L, S, B>;
+  return (void *)fdk::perturb_kernel<EXT, D, L, S, B, T>;
 }
 
 // series: a job starting from an admitted series (ordinary tiers only): variants 8-11;
-// bounded: the bounded variant (ordinary tiers, derivative, no BLA or series): 12
-void *pick_kernel(bool ext, bool d, bool l, bool series, bool bounded, int &variant) {
+// bounded: the bounded variant (ordinary tiers, derivative, no BLA or series): 12;
+// stripe: the Stripe recorder (no series, not bounded): 13-20
+void *pick_kernel(bool ext, bool d, bool l, bool series, bool bounded, int &variant, bool stripe = false) {
   if (bounded) {
     variant = 12;
     return kernel_ptr<false, true, false, false, true>();
+  }
+  if (stripe) {
+    variant = 13 + ((ext ? 4 : 0) | (d ? 2 : 0) | (l ? 1 : 0));
+    switch (variant - 13) {
+      case 0: return kernel_ptr<false, false, false, false, false, true>();
+      case 1: return kernel_ptr<false, false, true, false, false, true>();
+      case 2: return kernel_ptr<false, true, false, false, false, true>();
+      case 3: return kernel_ptr<false, true, true, false, false, true>();
+      case 4: return kernel_ptr<true, false, false, false, false, true>();
+      case 5: return kernel_ptr<true, false, true, false, false, true>();
+      case 6: return kernel_ptr<true, true, false, false, false, true>();
+      default: return kernel_ptr<true, true, true, false, false, true>();
+    }
   }
   variant = (ext ? 4 : 0) | (d ? 2 : 0) | (l ? 1 : 0);
   if (series && !ext) {
@@ -827,10 +841,11 @@ fdc_status fdc_upload_series(fdc_ctx *ctx, int32_t orbit, uint64_t points, uint6
 
 namespace {
 
-// fdc_render and fdc_render_bounded: bout (the Bound column and raw radii) is null for the
-// former; with it, ordinary-tier jobs run the bounded variant (derivative on).
+// fdc_render, fdc_render_bounded and fdc_render_stripe: bout (the Bound column and raw
+// radii) is null but for the second; with it, ordinary-tier jobs run the bounded variant
+// (derivative on). stripe (with its column stripe_out) is null but for the third.
 fdc_status render_impl(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, const fdc_bound_out *bout,
-                       fdc_counters *counters) {
+                       fdc_counters *counters, const fdc_stripe *stripe = nullptr, float *stripe_out = nullptr) {
   if (!ctx || !job || !out) return fail(ctx, FDC_INVALID, "null argument");
   auto it = ctx->orbits.find(job->orbit);
   if (it == ctx->orbits.end()) return fail(ctx, FDC_INVALID, "unknown orbit handle");
@@ -855,6 +870,14 @@ fdc_status render_impl(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, const fdc
     p.q = o.q;
     p.flags |= fdk::F_DERIV;
   }
+  if (stripe) {  // grid.rs:783-788; the route's own declines after
+    if (stripe->window < 1 || stripe->window > 64 || !std::isfinite(stripe->freq))
+      return fail(ctx, FDC_INVALID, "stripe window must be 1..=64 and the frequency finite");
+    if (j.flags & (FDC_SERIES | FDC_F32))
+      return fail(ctx, FDC_DECLINED, "the Stripe column renders on the plain form from Z_0 only");
+    p.stripe_window = stripe->window;
+    p.stripe_freq = stripe->freq;
+  }
   const bool deriv = (j.flags & FDC_DERIVATIVE) != 0 || bounded;
   CK(cudaSetDevice(ctx->device));
   // the window: rows x cols samples; outputs and inputs of full frame rows (pitch nx),
@@ -871,13 +894,14 @@ fdc_status render_impl(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, const fdc
   };
 
   // Device buffers: caller's (FDC_DEVICE_OUT) or staging for the rendered rows.
-  constexpr int NCOL = 12;
+  constexpr int NCOL = 13;
   struct Col {
     void *host;
     size_t width;
   } cols[NCOL] = {{out->cls, 1}, {out->n, 4}, {out->nu, 8}, {out->de, 4}, {out->normal, 2},
                   {out->z, 16}, {out->dz, 16}, {out->dexp, 8}, {out->status, 1},
-                  {bout ? bout->bound : nullptr, 4}, {bout ? bout->ez : nullptr, 8}, {bout ? bout->ed : nullptr, 8}};
+                  {bout ? bout->bound : nullptr, 4}, {bout ? bout->ez : nullptr, 8}, {bout ? bout->ed : nullptr, 8},
+                  {stripe ? stripe_out : nullptr, 4}};
   size_t need = 0;
   size_t offs[NCOL + 2];
   for (int c = 0; c < NCOL; ++c) {
@@ -915,6 +939,7 @@ fdc_status render_impl(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, const fdc
   p.bound_out = (float *)dptr[9];
   p.ez_out = (double *)dptr[10];
   p.ed_out = (double *)dptr[11];
+  p.stripe_out = (float *)dptr[12];
   p.out_pitch = dev_out ? j.nx : p.cols;
   if (j.mask) {
     p.mask = (const uint8_t *)(stage + offs[NCOL]);
@@ -945,7 +970,7 @@ fdc_status render_impl(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, const fdc
                        ctx->blocks_per_sm_f32));
   } else {
     int variant = 0;
-    void *fn = pick_kernel(ext, deriv, bla, p.series_n > 0, bounded, variant);
+    void *fn = pick_kernel(ext, deriv, bla, p.series_n > 0, bounded, variant, stripe != nullptr);
     if (!ctx->blocks_per_sm[variant]) {
       int b = 0;
       CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, 128, 0));
@@ -999,6 +1024,12 @@ fdc_status fdc_render_bounded(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, co
                               fdc_counters *counters) {
   if (!bound) return fail(ctx, FDC_INVALID, "null argument");
   return render_impl(ctx, job, out, bound, counters);
+}
+
+fdc_status fdc_render_stripe(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, const fdc_stripe *stripe,
+                             float *stripe_out, fdc_counters *counters) {
+  if (!stripe || !stripe_out) return fail(ctx, FDC_INVALID, "null argument");
+  return render_impl(ctx, job, out, nullptr, counters, stripe, stripe_out);
 }
 
 fdc_status fdc_upload_error_radius(fdc_ctx *ctx, int32_t orbit, const double *q, uint64_t len) {

@@ -95,6 +95,10 @@ struct Params {
   const double *__restrict__ q;
   float *bound_out;
   double *ez_out, *ed_out;
+  // Stripe variant (T): the column (stripe.rs) and its settings (window 1..64, frequency)
+  float *stripe_out;
+  uint32_t stripe_window;
+  double stripe_freq;
 };
 
 constexpr double SAFE = 1.0 + 8.0 * U;  // sample.rs:56
@@ -123,6 +127,8 @@ struct State {
   uint32_t m, idx;
   int returns;
   bool pending, predicted;
+  bool replaying;  // T: re-walking a stripe window plainly (sample.rs:231-236) ...
+  uint32_t limit;  // ... up to this iterate
 };
 
 // Result of a finished sample (sample.rs:21-40): kind 0 escaped, 1 interior, 2 unresolved.
@@ -132,6 +138,117 @@ struct Result {
   double zr, zi, dr, di;
   int64_t dexp;
   double ez, ed;  // B: error radii of an escaped sample (sample.rs:373-377)
+};
+
+// The loop state at the start of a BLA block, from which a stripe replay restarts
+// (stripe.rs:39-52).
+struct StripeSnap {
+  uint32_t m, n;
+  double xr, xi;
+  int32_t delta_exp;
+  double scale, dc_r, dc_i;
+  uint64_t valid;  // first iterate of the recorded run that reached n
+};
+
+// The Stripe column's recorder for one lane (stripe.rs:12-241): the last 128 iterates, the
+// last 8 block starts, and the escape the blocks found while a replay re-walks its window.
+// Only the stripe variants (T) hold one; it lives in local memory (~2.6 KB per lane).
+struct StripeTrace {
+  static constexpr uint32_t RING = 128, SNAPS = 8;
+  double2 ring[RING];
+  StripeSnap snaps[SNAPS];
+  Result first;
+  double first_r, first_i;
+  uint64_t first_at;
+  uint64_t valid;
+  uint32_t count;
+  float value;
+
+  __device__ __forceinline__ void begin() {  // stripe.rs:164-168
+    valid = ~0ull;
+    count = 0;
+    value = 0.0f;
+  }
+  __device__ __forceinline__ void start(uint64_t n) { valid = n + 1; }
+  __device__ __forceinline__ void record(uint64_t n, double zr, double zi) { ring[n % RING] = make_double2(zr, zi); }
+  __device__ __forceinline__ void snap(StripeSnap s, uint64_t landed) {  // stripe.rs:180-187
+    s.valid = valid;
+    snaps[count % SNAPS] = s;
+    count += 1;
+    valid = landed;
+  }
+  // stripe.rs:157-160 and 189-204: a kept block start to replay from when the windows
+  // ending at z_n miss iterates (the latest at or before n - window, else the oldest)
+  __device__ bool rewind(uint64_t n, uint32_t window, StripeSnap &out) {
+    const uint64_t need = n > window ? n - window : 0;
+    if (count == 0 || valid <= (need > 1 ? need : 1)) return false;
+    const uint32_t kept = count < SNAPS ? count : SNAPS;
+    int pick = -1;
+    for (uint32_t j = 0; j < kept && pick < 0; ++j) {
+      const uint32_t k = (count - 1 - j) % SNAPS;
+      if (snaps[k].n <= need) pick = (int)k;
+    }
+    if (pick < 0) {
+      for (uint32_t j = 0; j < kept; ++j) {
+        const uint32_t k = (count - 1 - j) % SNAPS;
+        if (pick < 0 || snaps[k].n < snaps[pick].n) pick = (int)k;
+      }
+    }
+    valid = snaps[pick].valid;
+    out = snaps[pick];
+    return true;
+  }
+  // stripe.rs:132-152: 0.5 + 0.5 sin(k arg z); a whole k up to 16 as the sign of k times
+  // Im (z / |z|)^|k|
+  __device__ static double term(double zr, double zi, double k) {
+    double s;
+    if (k == trunc(k) && fabs(k) <= 16.0) {
+      const double h = hypot(zr, zi);
+      const double ur = zr / h, ui = zi / h;
+      double pr = 1.0, pi = 0.0;
+      const int reps = (int)fabs(k);
+      for (int q = 0; q < reps; ++q) {
+        const double nr = pr * ur - pi * ui, ni = pr * ui + pi * ur;
+        pr = nr;
+        pi = ni;
+      }
+      s = k < 0.0 ? -pi : pi;
+    } else {
+      s = sin(k * atan2(zi, zr));
+    }
+    return 0.5 + 0.5 * s;
+  }
+  // stripe.rs:206-240: the windows ending at z_n and z_{n-1}, interpolated by how far
+  // past the escape radius z_n landed
+  __device__ void finish(uint64_t n, double zr, double zi, double r2, uint32_t window, double k) {
+    const uint64_t lo = n > window ? n - window : 0;
+    const uint64_t first_i = lo > 1 ? lo : 1;
+    double now = 0.0, before = 0.0;
+    uint32_t cn = 0, cb = 0;
+    for (uint64_t i = first_i; i <= n; ++i) {
+      if (i < valid) continue;
+      const double2 z = ring[i % RING];
+      const double t = term(z.x, z.y, k);
+      if (i > first_i || (first_i == 1 && n <= window)) {
+        now += t;
+        cn += 1;
+      }
+      if (i < n) {
+        before += t;
+        cb += 1;
+      }
+    }
+    if (cn == 0) {
+      value = 0.0f;
+      return;
+    }
+    now /= (double)cn;
+    before = cb > 0 ? before / (double)cb : now;
+    double frac = 1.0 - log2(log(zr * zr + zi * zi) / log(r2));
+    if (frac < 0.0) frac = 0.0;  // f64::clamp keeps NaN
+    if (frac > 1.0) frac = 1.0;
+    value = (float)(before * (1.0 - frac) + now * frac);
+  }
 };
 
 // The iteration limit behind Bla::find's budget (sample.rs:246-263) with n left out:
@@ -304,9 +421,11 @@ __device__ __forceinline__ void plain_update(State<EXT> &s, const double *__rest
 // bailout, nucleus gate, rebase, rescaling and periodicity. Zn/Rn hold the prefetched
 // entry m + 1 of the iteration's start, right after a plain step; after a block (took)
 // the entry at the new m is loaded here. Returns true when the sample has an outcome.
-template <bool EXT, bool D, bool L, bool B = false>
+// T: the Stripe recorder tr records the iterate, and an escape whose window misses
+// iterates replays them from a kept block start (sample.rs:369-403).
+template <bool EXT, bool D, bool L, bool B = false, bool T = false>
 __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res, bool took, double2 Zn,
-                                     double2 Rn) {
+                                     double2 Rn, StripeTrace *tr = nullptr) {
   double2 Z = Zn;
   if (L) {
     if (took) {  // a block moved m by its length
@@ -321,6 +440,8 @@ __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res
   double pr = EXT ? s.scale * s.xr : s.xr, pi = EXT ? s.scale * s.xi : s.xi;
   double fr = Z.x + pr, fi = Z.y + pi;
   double f2 = fr * fr + fi * fi;
+  if (T) tr->record(s.n, fr, fi);
+  const bool replaying = T && s.replaying;  // no nucleus gate or periodicity while replaying
   {
     // The common iterations leave through a short path: no escape, nucleus gate or
     // near-return (the full sequence below handles those), and at most a rebase onto Z_0
@@ -331,7 +452,7 @@ __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res
     const double delta2 = pr * pr + pi * pi;
     const bool rebase = EXT ? f2 <= delta2 : f2 < delta2;
     const bool reb = rebase || s.m == p.last;
-    bool common = !(f2 > p.r2) && !(s.nucleus >= 0 && s.n == (uint32_t)s.nucleus + 1u);
+    bool common = !(f2 > p.r2) && !(!replaying && s.nucleus >= 0 && s.n == (uint32_t)s.nucleus + 1u);
     if (B || (EXT && !(f2 > SQUARE_OK))) common = common && !reb;  // bounded radii; sum2 rebase
     // the judge reads the delta after a rebase on the ordinary tiers (it is then z itself)
     const double check_r = EXT ? pr : (reb ? fr : s.xr), check_i = EXT ? pi : (reb ? fi : s.xi);
@@ -339,7 +460,8 @@ __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res
     if (EXT) judge = judge && s.returns < 4;
     const double dist = fabs(fr - s.sr) + fabs(fi - s.si);
     const double size = fabs(s.sr) + fabs(s.si);
-    if (EXT) {
+    if (replaying) {
+    } else if (EXT) {
       common = common && !(judge && dist < 1e-13 * size + 1e-300);
     } else {
       const bool held = s.hold > 0 && s.n - s.sn < s.hold;  // sn <= n while hold > 0
@@ -390,7 +512,7 @@ __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res
         s.fr = fr;
         s.fi = fi;
       }
-      if (EXT && __builtin_expect(s.n >= s.chk, 0)) {  // sample.rs:488-491 / :571-574
+      if (EXT && !replaying && __builtin_expect(s.n >= s.chk, 0)) {  // sample.rs:488-491 / :571-574
         s.sr = fr;
         s.si = fi;
         s.sn = s.n;
@@ -412,9 +534,41 @@ __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res
       res.ez = s.e + __ldg(p.q + s.m) + 4.0 * U * sqrt(f2);
       res.ed = s.ed;
     }
+    if (T) {  // sample.rs:387-403
+      if (replaying) {  // the replay reached an escape: the blocks' outcome, this window
+        tr->finish(s.n, fr, fi, p.r2, p.stripe_window, p.stripe_freq);
+        res = tr->first;
+        return true;
+      }
+      StripeSnap sn;
+      if (tr->rewind(s.n, p.stripe_window, sn)) {
+        tr->first = res;
+        tr->first_at = s.n;
+        tr->first_r = fr;
+        tr->first_i = fi;
+        s.replaying = true;
+        const uint64_t give_up = (uint64_t)s.n + 64;  // sample.rs:397
+        s.limit = (uint32_t)(give_up < p.max_iter ? give_up : p.max_iter);
+        s.m = sn.m;
+        s.n = sn.n;
+        s.xr = sn.xr;
+        s.xi = sn.xi;
+        s.delta_exp = sn.delta_exp;
+        s.scale = sn.scale;
+        s.dc_r = sn.dc_r;
+        s.dc_i = sn.dc_i;
+        const double2 Zm = __ldg(p.orbit + s.m);  // z of the replay's first step
+        s.Zr = Zm.x;
+        s.Zi = Zm.y;
+        s.fr = EXT ? s.Zr + s.scale * s.xr : s.Zr + s.xr;
+        s.fi = EXT ? s.Zi + s.scale * s.xi : s.Zi + s.xi;
+        return false;
+      }
+      tr->finish(s.n, fr, fi, p.r2, p.stripe_window, p.stripe_freq);
+    }
     return true;
   }
-  if (__builtin_expect(s.nucleus >= 0, 0) && s.n == (uint32_t)s.nucleus + 1u) {
+  if (!replaying && __builtin_expect(s.nucleus >= 0, 0) && s.n == (uint32_t)s.nucleus + 1u) {
     if (s.ct.small()) {
       res.kind = 1;
       res.n = s.n;
@@ -465,6 +619,7 @@ __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res
         s.scale = exp2i(s.delta_exp);
         s.m = 1;
         s.n = s.n + 1;
+        if (T) tr->start(s.n);  // this step's iterate is not recorded (sample.rs:444-446)
         double2 Z1 = __ldg(p.orbit + 1);
         s.Zr = Z1.x;
         s.Zi = Z1.y;
@@ -512,6 +667,7 @@ __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res
     s.fr = fr;
     s.fi = fi;
   }
+  if (replaying) return false;  // sample.rs:470-472: the replay only re-walks iterates
   double check_r = EXT ? pr : s.xr, check_i = EXT ? pi : s.xi;
   bool judge = check_r * check_r + check_i * check_i > RES2 * f2;
   if (EXT) judge = judge && s.returns < 4;
@@ -672,14 +828,19 @@ struct Reservation {
 // lanes wait or no lane steps plainly; the waiting lanes then apply their blocks together. The warp
 // runs the block path for many lanes at a time instead of for one or two lanes on
 // nearly every iteration, and each lane's own sequence of operations is unchanged.
-template <bool EXT, bool D, bool L, bool B = false>
+template <bool EXT, bool D, bool L, bool B = false, bool T = false>
 __device__ __forceinline__ bool warp_step(const Params &p, State<EXT> &s, Result &res, bool active, Waiting &w,
-                                          uint32_t defer) {
+                                          uint32_t defer, StripeTrace *tr = nullptr) {
   bool upd = false, took = false, done = false;
   double2 Zn = make_double2(0.0, 0.0), Rn = make_double2(-1.0, -1.0);
   if (active && !w.on) {
-    if (s.n >= p.max_iter) {
-      res.kind = 2;
+    if (s.n >= (T ? s.limit : p.max_iter)) {
+      if (T && s.replaying) {  // sample.rs:576-579: the replay gave up; from what was recorded
+        tr->finish(tr->first_at, tr->first_r, tr->first_i, p.r2, p.stripe_window, p.stripe_freq);
+        res = tr->first;
+      } else {
+        res.kind = 2;
+      }
       done = true;
     } else {
       if (L) {
@@ -690,7 +851,7 @@ __device__ __forceinline__ bool warp_step(const Params &p, State<EXT> &s, Result
       }
       // a lane that finds a block waits; its level is searched when the waiting lanes
       // apply their blocks together (nothing the search reads changes while it waits)
-      if (L && block_starts(s)) {
+      if (L && !(T && s.replaying) && block_starts(s)) {
         w.on = true;
       } else {
         plain_update<EXT, D, B>(s, p.q);
@@ -709,12 +870,14 @@ __device__ __forceinline__ bool warp_step(const Params &p, State<EXT> &s, Result
     const uint32_t thr = max(1u, (busy * defer) >> 5);
     if (waiting && ((uint32_t)__popc(waiting) >= thr || !stepping) && w.on) {
       w.lv = block_level(p, s, w.at);
+      if (T)  // sample.rs:267-281: the block start, for a later replay
+        tr->snap(StripeSnap{s.m, s.n, s.xr, s.xi, s.delta_exp, s.scale, s.dc_r, s.dc_i, 0}, s.n + (2u << w.lv));
       apply_block<EXT, D>(p, s, w.lv, w.at);
       w.on = false;
       upd = took = true;
     }
   }
-  if (upd) done = post<EXT, D, L, B>(p, s, res, took, Zn, Rn);
+  if (upd) done = post<EXT, D, L, B, T>(p, s, res, took, Zn, Rn, tr);
   return done;
 }
 
@@ -825,6 +988,8 @@ __device__ __forceinline__ void start_sample(const Params &p, State<EXT> &s, boo
   s.sr = 0.0;
   s.si = 0.0;
   s.chk = 16;
+  s.replaying = false;
+  s.limit = (uint32_t)p.max_iter;
   s.sn = EXT ? 0 : 8;
   s.returns = 0;
   s.pending = false;
@@ -896,11 +1061,12 @@ __device__ __forceinline__ bool bounds(uint64_t n, double az, double ez, double 
   return true;
 }
 
-template <bool B = false>
-__device__ __forceinline__ void put(const Params &p, uint32_t sample, const Result &r) {
+template <bool B = false, bool T = false>
+__device__ __forceinline__ void put(const Params &p, uint32_t sample, const Result &r, float stripe = 0.0f) {
   const uint32_t j = sample / p.nx, i = sample - j * p.nx;
   const uint64_t idx = (uint64_t)(j - p.first_row) * p.out_pitch + (i - p.first_col);
   if (p.status) p.status[idx] = 1;
+  if (T && p.stripe_out) p.stripe_out[idx] = stripe;  // grid.rs:772: 0 unless escaped
   if (p.n_out) p.n_out[idx] = (uint32_t)(r.kind == 2 ? p.max_iter : r.n);
   if (r.kind != 0) {
     if (p.cls) p.cls[idx] = (uint8_t)(r.kind == 2 ? 2 : 1);
@@ -941,7 +1107,18 @@ __device__ __forceinline__ void put(const Params &p, uint32_t sample, const Resu
 // compile without the series start and its retry.
 // B: the bounded variant (ordinary tiers, derivative on, no BLA or series): error radii,
 // Bounded evidence and the Bound column.
-template <bool EXT, bool D, bool L, bool S = false, bool B = false>
+// T: the stripe variant: every lane holds a Stripe recorder and writes the Stripe column.
+template <bool T>
+struct TraceSlot {
+  __device__ __forceinline__ StripeTrace *get() { return nullptr; }
+};
+template <>
+struct TraceSlot<true> {
+  StripeTrace t;
+  __device__ __forceinline__ StripeTrace *get() { return &t; }
+};
+
+template <bool EXT, bool D, bool L, bool S = false, bool B = false, bool T = false>
 __global__ void __launch_bounds__(128, Occupancy<EXT>::blocks) perturb_kernel(Params p) {
   const unsigned FULL = 0xffffffffu;
   const unsigned lane = threadIdx.x & 31u;
@@ -951,6 +1128,8 @@ __global__ void __launch_bounds__(128, Occupancy<EXT>::blocks) perturb_kernel(Pa
   Waiting w{false, -1, 0};
   bool active = false, exhausted = false;
   Reservation slots;
+  TraceSlot<T> trace;
+  StripeTrace *tr = trace.get();
   uint64_t t0 = p.deadline_ns ? globaltimer() : 0;
   unsigned long long n_samples = 0, iters = 0, blocks = 0, skipped = 0, fallback = 0, closed = 0;
   double shift = 0.0;
@@ -959,7 +1138,7 @@ __global__ void __launch_bounds__(128, Occupancy<EXT>::blocks) perturb_kernel(Pa
   // prefix - max_iter, so that the first run counts max_iter - prefix.
   int64_t bias = 0;
   auto finish = [&](uint32_t idx, const Result &r, uint64_t nblocks, uint64_t nskipped, double sh) {
-    put<B>(p, idx, r);
+    put<B, T>(p, idx, r, T && r.kind == 0 ? tr->value : 0.0f);
     uint64_t spent = (uint64_t)((int64_t)(r.kind == 2 ? p.max_iter : r.n) - bias);
     bias = 0;
     if (L) {
@@ -1001,6 +1180,10 @@ __global__ void __launch_bounds__(128, Occupancy<EXT>::blocks) perturb_kernel(Pa
           if (got == 1) {
             active = true;
             if (S) bias = p.series_n;
+            if (T) {  // Job::one (grid.rs:630) and the loop's start (sample.rs:235)
+              tr->begin();
+              tr->start(s.n);
+            }
           } else if (got == 2) {
             finish(s.idx, res, 0, 0, 0.0);
           }
@@ -1009,12 +1192,16 @@ __global__ void __launch_bounds__(128, Occupancy<EXT>::blocks) perturb_kernel(Pa
       need = __ballot_sync(FULL, !active);
     }
     if (!__any_sync(FULL, active)) break;
-    if (warp_step<EXT, D, L, B>(p, s, res, active, w, p.defer)) {
+    if (warp_step<EXT, D, L, B, T>(p, s, res, active, w, p.defer, tr)) {
       if (S && bias > 0 && res.kind == 2) {
         // an unresolved series start retries from zero, keeping the nucleus heuristic
         // (grid.rs:637-642); its count and blocks carry over
         bias -= (int64_t)p.max_iter;
         start_sample<EXT, D, L, B>(p, s, false, true);
+        if (T) {  // grid.rs:638
+          tr->begin();
+          tr->start(s.n);
+        }
       } else {
         finish(s.idx, res, s.blocks, s.skipped, s.shift);
         active = false;

@@ -2,14 +2,15 @@
 little-endian header (magic FDSAMPLE, major 1, minor, column bits, grid, iteration cap,
 escape radius, rotation, the view strings and the kernel id, padded to 8 bytes), then each
 present column in bit order, each padded to 8 bytes. Columns the route fills: class (u8),
-nu (f64), de (f32), normal (u16), bound (f32, crates/fd-samples/src/column.rs:18-19)."""
+nu (f64), de (f32), normal (u16), bound (f32), stripe (f32; crates/fd-samples/src/
+column.rs:18-22)."""
 import struct
 
 import numpy as np
 
 MAGIC = b"FDSAMPLE"
 MAJOR, MINOR = 1, 1
-BITS = {"class": 1, "nu": 2, "de": 4, "normal": 8, "bound": 16}
+BITS = {"class": 1, "nu": 2, "de": 4, "normal": 8, "bound": 16, "stripe": 32}
 
 
 def _pad8(b: bytearray):
@@ -25,7 +26,7 @@ def _str(b: bytearray, s: str):
 
 def encode(header, samples, minor=MINOR) -> bytes:
     """Header::encode (header.rs:62-81) + write (write.rs:8-53)."""
-    cols = ("class",) + tuple(c for c in ("nu", "de", "normal", "bound") if c in header.columns)
+    cols = ("class",) + tuple(c for c in ("nu", "de", "normal", "bound", "stripe") if c in header.columns)
     n = header.nx * header.ny
     b = bytearray(MAGIC)
     b += struct.pack("<HHIIIII", MAJOR, minor, sum(BITS[c] for c in cols), header.nx, header.ny, header.ss, 0)
@@ -34,7 +35,8 @@ def encode(header, samples, minor=MINOR) -> bytes:
         _str(b, s)
     _pad8(b)
     arrays = {"class": (samples.cls, np.uint8), "nu": (samples.nu, "<f8"), "de": (samples.de, "<f4"),
-              "normal": (samples.normal, "<u2"), "bound": (samples.bound, "<f4")}
+              "normal": (samples.normal, "<u2"), "bound": (samples.bound, "<f4"),
+              "stripe": (samples.stripe, "<f4")}
     for c in cols:
         a, dt = arrays[c]
         if a is None or len(a) != n:

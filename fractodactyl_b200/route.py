@@ -54,7 +54,7 @@ class Incomplete(Declined):
         finished samples keep the device's values and the iterations add up, as
         frame.rs:338-343 overlays and counts them. Returns (Samples, Stats)."""
         out = dataclasses.replace(self.samples)
-        for name in ("cls", "nu", "de", "normal", "n", "z", "dz", "dexp", "bound", "ez", "ed"):
+        for name in ("cls", "nu", "de", "normal", "n", "z", "dz", "dexp", "bound", "ez", "ed", "stripe"):
             g, c = getattr(self.samples, name), getattr(cpu, name)
             if g is not None and c is not None:
                 g = g.copy()
@@ -99,6 +99,8 @@ class Params:
     columns: tuple = ("nu", "de", "normal")
     threads: int = 0
     tier: Optional[str] = None
+    stripe_window: int = 16   # StripeParams (crates/fd-kernel/src/stripe.rs:20-36, grid.rs:36-37)
+    stripe_freq: float = 5.0
 
     def needs_derivative(self):
         return "de" in self.columns or "normal" in self.columns
@@ -274,6 +276,7 @@ class Samples:
     dexp: Optional[np.ndarray] = None
     status: Optional[np.ndarray] = None
     bound: Optional[np.ndarray] = None  # Bound column (f32 nu error bound; bounded renders)
+    stripe: Optional[np.ndarray] = None  # Stripe column (f32 stripe average of escaped samples)
     ez: Optional[np.ndarray] = None     # raw error radii of escaped samples (bounded renders)
     ed: Optional[np.ndarray] = None
 
@@ -373,11 +376,13 @@ class Device:
         q = np.ascontiguousarray(q, dtype=np.float64)
         _check(lib().fdc_upload_error_radius(self.h, orbit, q.ctypes.data, len(q)), self, "upload error radii")
 
-    def render_job(self, job: _lib.Job, raw=False, columns=COLUMNS, device_out=None, host_out=None, bounded=False):
+    def render_job(self, job: _lib.Job, raw=False, columns=COLUMNS, device_out=None, host_out=None, bounded=False,
+                   stripe=None):
         """fdc_render into fresh host arrays, into the caller's host arrays (host_out: the
         dict an earlier call returned, reused frame after frame) or into caller device
         buffers (device_out). bounded: fdc_render_bounded, adding the host arrays
-        "bound", "ez" and "ed"."""
+        "bound", "ez" and "ed". stripe: (window, freq) for fdc_render_stripe, adding the
+        array "stripe" (a device pointer under device_out["stripe"])."""
         n = job.nx * job.ny
         out = _lib.Out()
         arrays = {}
@@ -405,7 +410,16 @@ class Device:
             for k, a in arrays.items():
                 setattr(out, k, a.ctypes.data)
         cnt = _lib.Counters()
-        if bounded:
+        if stripe is not None:
+            if device_out is not None:
+                sp = device_out["stripe"]
+            else:
+                if "stripe" not in arrays:
+                    arrays["stripe"] = np.zeros(n, np.float32)
+                sp = arrays["stripe"].ctypes.data
+            st = lib().fdc_render_stripe(self.h, C.byref(job), C.byref(out),
+                                         C.byref(_lib.Stripe(int(stripe[0]), float(stripe[1]))), sp, C.byref(cnt))
+        elif bounded:
             for k, dt in (("bound", np.float32), ("ez", np.float64), ("ed", np.float64)):
                 if k not in arrays:
                     arrays[k] = np.zeros(n, dt)
@@ -613,15 +627,19 @@ def render_with(view: View, p: Params, orbit=None, bla: Optional[Bla] = None, de
     `series`, every sample starts from it (Series::render_masked, grid.rs:341-373).
 
     Returns (Header, Samples, Stats, BlaStats or None). Refusals are the reference's
-    (grid.rs:350-366, :378-413, :461-475); the Stripe column is declined (frame.rs:129-144);
-    the Bound column renders through fdc_render_bounded on the F64 / Fixed tiers.
+    (grid.rs:350-366, :378-413, :461-475, :783-788); the Bound column renders through
+    fdc_render_bounded on the F64 / Fixed tiers, the Stripe column through
+    fdc_render_stripe (declined, for a CPU restart, with the Bound column or a series start).
     deadline_ms: the device stops taking samples once it has passed; if any sample is
     left, Incomplete carries the finished ones and the mask of those the CPU must render.
     """
     started = time.perf_counter()
-    if "stripe" in p.columns:
-        raise Declined("frame declined (stripe); CPU restart from zero")
+    striped = "stripe" in p.columns
+    if striped and not (1 <= p.stripe_window <= 64 and math.isfinite(p.stripe_freq)):  # grid.rs:783-788
+        raise ValueError("stripe window must be 1..=64 and the frequency finite")
     bound = "bound" in p.columns
+    if striped and (bound or series is not None):
+        raise Declined("frame declined (stripe with bound or a series start); CPU restart from zero")
     if bound and bla is not None:  # grid.rs:379-384
         raise ValueError("--columns bound certifies every step; BLA remainders are not certified (ACC-02)")
     if bound and series is not None:  # grid.rs:354
@@ -681,7 +699,8 @@ def render_with(view: View, p: Params, orbit=None, bla: Optional[Bla] = None, de
             job.deadline_ms = float(deadline_ms)
         g = time.perf_counter()
         arrays, cnt, status = dev.render_job(job, raw=raw or host_encode,
-                                             columns=() if host_encode else p.columns, bounded=bound)
+                                             columns=() if host_encode else p.columns, bounded=bound,
+                                             stripe=(p.stripe_window, p.stripe_freq) if striped else None)
         gpu_seconds = time.perf_counter() - g
     finally:
         dev.free(h)
@@ -704,11 +723,12 @@ def assemble(view: View, p: Params, plane: Plane, tier: int, bla: Optional[Bla],
     kernel = plane.kernel(tier) + (" bla/1" if bla is not None else "") + (" series/0" if series is not None else "") \
         + " gpu-perturb-cuda/1"
     cols = ("class",) + tuple(c for c in ("nu", "de", "normal") if c in p.columns) + \
-        (("bound",) if bound else ())
+        (("bound",) if bound else ()) + (("stripe",) if "stripe" in p.columns else ())
     header = Header(cols, p.nx, p.ny, p.ss, p.max_iter, p.escape_radius, view, kernel)
     s = Samples(cls=arrays["cls"], nu=arrays.get("nu"), de=arrays.get("de"), normal=arrays.get("normal"),
                 n=arrays.get("n"), z=arrays.get("z"), dz=arrays.get("dz"), dexp=arrays.get("dexp"),
-                status=arrays.get("status"), bound=arrays.get("bound"), ez=arrays.get("ez"), ed=arrays.get("ed"))
+                status=arrays.get("status"), bound=arrays.get("bound"), ez=arrays.get("ez"), ed=arrays.get("ed"),
+                stripe=arrays.get("stripe"))
     if host_encode:
         encode_host(plane, p.ss, s, p.columns, p.threads)
     unfinished = None

@@ -153,6 +153,23 @@ fdc_status fdc_upload_error_radius(fdc_ctx *ctx, int32_t orbit, const double *q,
 fdc_status fdc_render_bounded(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, const fdc_bound_out *bound,
                               fdc_counters *counters);
 
+/* The Stripe column (crates/fd-kernel/src/stripe.rs; the column grid.rs:493-498, 772
+ * writes, the refusal of grid.rs:783-788). fdc_render_stripe renders like fdc_render
+ * and also records each sample's last 128 iterates and last 8 BLA block starts; an escape
+ * whose window misses iterates replays them plainly from a kept block start, as the CPU
+ * kernel does (sample.rs:231-236, 387-403), so every output of fdc_render is unchanged.
+ * stripe_out receives the stripe average of escaped samples (0 elsewhere; f32, fdc_out's
+ * layout, FDC_DEVICE_OUT included); the average's terms use CUDA's hypot / sin / atan2 /
+ * log, so values are within a few ulps of the CPU's. FDC_INVALID: window outside 1..64 or
+ * a frequency that is not finite. FDC_DECLINED (render on the CPU): FDC_SERIES, FDC_F32.
+ * Each sample's recorder lives in local memory (~2.6 KB per resident lane). */
+typedef struct {
+  uint32_t window; /* iterates averaged before escape, 1..64 (StripeParams, stripe.rs:20-36) */
+  double freq;     /* k of 0.5 + 0.5 sin(k arg z) */
+} fdc_stripe;
+fdc_status fdc_render_stripe(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, const fdc_stripe *stripe,
+                             float *stripe_out, fdc_counters *counters);
+
 /* Launch tuning (no counterpart in the reference; the reference's shader has fixed
  * workgroups). defer: lanes of a warp whose next operation is a BLA block wait until
  * defer/32 of the warp's busy lanes wait, or no lane steps plainly, and then apply their

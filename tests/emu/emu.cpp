@@ -83,12 +83,18 @@ struct Setup {
   bool ext = false, deriv = false, bla = false;
 };
 
-template <bool EXT, bool D, bool L, bool S, bool B>
+template <bool EXT, bool D, bool L, bool S, bool B, bool T = false>
 void launch(fdk::Params &p) {
   threadIdx.x = 0;
   blockIdx.x = 0;
-  fdk::perturb_kernel<EXT, D, L, S, B>(p);
+  fdk::perturb_kernel<EXT, D, L, S, B, T>(p);
 }
+
+// The Stripe column of the next emu_render call that sets flag bit 5 (the stripe variant):
+// its window, frequency and the whole-frame f32 output.
+uint32_t g_stripe_window = 16;
+double g_stripe_freq = 5.0;
+float *g_stripe_out = nullptr;
 
 template <bool D, bool L>
 void launch_f32(fdk::Params &p, const fdk::Entry32 *orbit) {
@@ -283,8 +289,9 @@ int emu_render_window(const double *re, const double *im, uint64_t len, const do
                       int64_t *dexp_out, uint8_t *status, float *bound, double *ez, double *ed, uint64_t *counters,
                       const EmuWindow *win) {
   const bool ext = tier == 2, deriv = flags & 1, bla = (flags & 2) != 0, series = (flags & 4) && series_n > 0,
-             bounded = (flags & 8) && !ext, f32 = flags & 16;
-  if (len < 3 || (bla && bounded) || (series && (ext || bounded)) || (f32 && (series || bounded)))
+             bounded = (flags & 8) && !ext, f32 = flags & 16, striped = (flags & 32) != 0;
+  if (len < 3 || (bla && bounded) || (series && (ext || bounded)) || (f32 && (series || bounded)) ||
+      (striped && (series || bounded || f32)))
     return -1;  // the route's refusals
   Setup s;
   s.ext = ext;
@@ -320,7 +327,20 @@ int emu_render_window(const double *re, const double *im, uint64_t len, const do
     p.ed_out = ed ? ed + origin : nullptr;
   }
   const bool d = s.deriv;
-  if (f32) {
+  if (striped) {
+    p.stripe_out = g_stripe_out ? g_stripe_out + (uint64_t)p.first_row * nx + p.first_col : nullptr;
+    p.stripe_window = g_stripe_window;
+    p.stripe_freq = g_stripe_freq;
+  }
+  if (striped) {
+    if (ext) {
+      if (d) bla ? launch<true, true, true, false, false, true>(p) : launch<true, true, false, false, false, true>(p);
+      else bla ? launch<true, false, true, false, false, true>(p) : launch<true, false, false, false, false, true>(p);
+    } else {
+      if (d) bla ? launch<false, true, true, false, false, true>(p) : launch<false, true, false, false, false, true>(p);
+      else bla ? launch<false, false, true, false, false, true>(p) : launch<false, false, false, false, false, true>(p);
+    }
+  } else if (f32) {
     const fdk::Entry32 *o = s.z32.data();
     if (d) bla ? launch_f32<true, true>(p, o) : launch_f32<true, false>(p, o);
     else bla ? launch_f32<false, true>(p, o) : launch_f32<false, false>(p, o);
@@ -409,6 +429,12 @@ int emu_render_batch(EmuJob *jobs, uint32_t njobs) {
     for (size_t i = 0; i < order.size(); ++i) copy_counters(cnt[i], jobs[order[i]].counters);
   }
   return 0;
+}
+
+void emu_set_stripe(uint32_t window, double freq, float *out) {
+  g_stripe_window = window;
+  g_stripe_freq = freq;
+  g_stripe_out = out;
 }
 
 }  // extern "C"

@@ -37,6 +37,10 @@ def test_null_context_refused(L):
     assert L.fdc_render(None, C.byref(job), C.byref(out), C.byref(c)) == _lib.INVALID
     assert L.fdc_render_bounded(None, C.byref(job), C.byref(out), None, C.byref(c)) == _lib.INVALID
     assert L.fdc_render_bounded(None, C.byref(job), C.byref(out), C.byref(_lib.BoundOut()), C.byref(c)) == _lib.INVALID
+    col = np.zeros(4, np.float32)
+    assert L.fdc_render_stripe(None, C.byref(job), C.byref(out), C.byref(_lib.Stripe(16, 5.0)), col.ctypes.data,
+                               C.byref(c)) == _lib.INVALID
+    assert L.fdc_render_stripe(None, C.byref(job), C.byref(out), None, None, C.byref(c)) == _lib.INVALID
     assert L.fdc_set_tuning(None, C.byref(t)) == _lib.INVALID
     assert L.fdc_get_tuning(None, C.byref(t)) == _lib.INVALID
     b = C.c_void_p()

@@ -187,8 +187,14 @@ def test_route_flag_and_declines():
     assert fd.enabled(None) is False and fd.enabled("cuda") and fd.enabled("cuda-bla") and fd.enabled("bla")
     with pytest.raises(ValueError):
         fd.enabled("fast")
-    with pytest.raises(fd.Declined):  # the Stripe column stays on the CPU
-        fd.render(fd.View("0", "1", "1e-3"), fd.Params(8, 8, columns=("nu", "stripe")))
+    # the Stripe column: the reference's refusal (grid.rs:783-788), and the combinations the
+    # route leaves to the CPU (with the Bound column or a series start)
+    with pytest.raises(ValueError, match="stripe window"):
+        fd.render(fd.View("0", "1", "1e-3"), fd.Params(8, 8, columns=("nu", "stripe"), stripe_window=65))
+    with pytest.raises(ValueError, match="stripe window"):
+        fd.render(fd.View("0", "1", "1e-3"), fd.Params(8, 8, columns=("nu", "stripe"), stripe_freq=float("inf")))
+    with pytest.raises(fd.Declined):
+        fd.render(fd.View("0", "1", "1e-3"), fd.Params(8, 8, columns=("nu", "stripe", "bound")))
     # the Bound column certifies every step: no BLA (grid.rs:379-384), no series start
     r = fd.Reference.new(-0.7453, 0.1127, 2_000, 1e10)
     table = fd.Bla.build_scaled(r, 2.0 ** -50, 1e-5)

@@ -47,6 +47,7 @@ def emu():
     L.emu_render_window.argtypes = L.emu_render.argtypes + [C.POINTER(Window)]
     L.emu_render_batch.restype = C.c_int
     L.emu_render_batch.argtypes = [C.POINTER(Job), U32]
+    L.emu_set_stripe.argtypes = [U32, D, P]
     return L
 
 
@@ -688,3 +689,49 @@ def test_bla_kernel_with_a_table_without_levels(emu, view3, it):
                         fdref.Bla(ref, fd.route.EPS, table.dc_max, table.dc_exp))["stats"]
     for k in ("iterations", "blocks", "skipped", "fallback_samples", "closed_form_samples"):
         assert got["counters"][k] == want[k], k
+
+
+STRIPE_FRAMES = [
+    # view, grid, iterations, BLA, tier
+    (("-0.7453", "0.1127", "0.0065"), 40, 24, 3000, False, None),
+    (("-0.743643887037158704752191506114774", "0.131825904205311970493132056385139", "1e-28"), 40, 24, 30_000, True,
+     None),
+    (("0", "1", "1e-300"), 32, 24, 5000, True, None),
+    (("0", "1", "1e-300"), 32, 24, 5000, True, "scaled"),
+]
+
+
+@pytest.mark.parametrize("frame", STRIPE_FRAMES, ids=lambda f: f"{f[0][2]}-{f[4]}-{f[5]}")
+@pytest.mark.parametrize("window,freq,deriv", [(16, 5.0, True), (64, 2.5, False), (3, -7.0, True)])
+def test_stripe_kernel_equals_oracle(emu, frame, window, freq, deriv):
+    """The stripe variant of the kernel (perturb_kernel<..., T>: every iterate recorded in a
+    128-entry ring, the last 8 block starts kept, a plain replay of an incomplete window
+    from a kept block start, sample.rs:231-236, 387-403) equals the oracle's Stripe column
+    bit for bit on the host (same libm), and its class, count and z are the untraced
+    kernel's: on the F64 and Fixed tiers with and without BLA and on the Scaled tier."""
+    view3, nx, ny, it, use_bla, tier = frame
+    v, p, plane, t, r = _setup(view3, nx, ny, it, tier=tier, columns=("nu", "de") if deriv else ("nu",))
+    table = None
+    if use_bla:
+        dc, e = fd.bla_dc_bound(v, p)
+        table = fd.Bla.build_scaled(r, fd.route.EPS, dc, e)
+        assert table.levels > 0
+    flags = (1 if deriv else 0) | (2 if table is not None else 0)
+    plain = emulate(emu, r, plane, t, p, flags, bla=table)
+    stripe = np.zeros(nx * ny, np.float32)
+    emu.emu_set_stripe(window, freq, stripe.ctypes.data)
+    try:
+        got = emulate(emu, r, plane, t, p, flags | 32, bla=table)
+    finally:
+        emu.emu_set_stripe(16, 5.0, None)
+    for k in ("cls", "n", "z", "dz", "dexp", "status"):
+        assert np.array_equal(got[k], plain[k]), k
+    assert got["counters"] == plain["counters"]
+    ref = fdref.Ref.arrays(r.re, r.im, r.bits)
+    job = fdref.make_job(*view3, nx, ny, it, columns=fdref.COL_NU | fdref.COL_STRIPE, tier=t, threads=2,
+                         stripe_window=window, stripe_freq=freq)
+    ot = fdref.Bla(ref, fd.route.EPS, table.dc_max, table.dc_exp) if table is not None else None
+    want = fdref.render_columns(job, ref, ot)
+    assert np.array_equal(got["cls"], want["cls"])
+    esc = want["cls"] == 0
+    assert esc.any() and np.array_equal(stripe, want["stripe"]), np.abs(stripe - want["stripe"]).max()
