@@ -829,7 +829,7 @@ def main():
     ap.add_argument("--tier", choices=("fixed", "scaled"), default=None)
     ap.add_argument("--form", choices=("both", "fp64", "f32"), default="both")
     ap.add_argument("--shard", action="store_true",
-                    help="configurations 1-2: one frame split over the ranks (strong scaling)")
+                    help="one frame (configurations 1-2) or the jobs (4-5) split over the ranks (strong scaling)")
     args = ap.parse_args()
     if args.impl == "reference":
         if args.config > 2:
@@ -837,9 +837,7 @@ def main():
                               "reference CPU arm runs configs 1 and 2"}))
             return
         run_reference(args)
-    elif args.shard:
-        if args.config > 2:
-            raise SystemExit("--shard splits the one frame of configuration 1 or 2")
+    elif args.shard and args.config <= 2:
         run_shard(args)
     elif args.config > 2:
         run_set(args)
