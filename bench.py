@@ -620,6 +620,41 @@ def run_shard(args):
     dist.destroy_process_group()
 
 
+def set_vs_direct(args, cfg, js, sel, frames, loc_of, forms):
+    """Both forms of a job set against fd-fixed direct iteration on seeded samples: the
+    frames the snapshots hold (in the batch's frame order), samples that escaped in both
+    forms within --direct-cap iterations (direct iteration at 1,100-3,500 bits costs a few
+    microseconds per step), each iterated at its exact c."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import fdref
+    fl, seen = [], {}
+    for k in sel:
+        key = js.groups[k] if js.groups else k
+        if key not in seen:
+            seen[key] = len(fl)
+            f = frames[loc_of(k)] if cfg != 3 else frames[0]
+            fl.append((f.view, js.planes[k], js.tiers[k], f.params, js.keep[0] if cfg == 3 else None))
+    starts = np.cumsum([0] + [t[3].nx * t[3].ny for t in fl])
+    snaps = {f: forms[f]["snap"] for f in forms}
+    ok = np.ones(int(starts[-1]), bool)
+    for sn in snaps.values():
+        ok &= ((sn["cls"] & 3) == 0) & (sn["n"].astype(np.int64) <= args.direct_cap)
+    cand = np.flatnonzero(ok)
+    pick = np.random.default_rng(args.seed + 200).choice(cand, min(max(1, args.direct_samples // 4), len(cand)),
+                                                         replace=False)
+    cases = []
+    for g in pick:
+        fi = int(np.searchsorted(starts, g, side="right")) - 1
+        view, plane, tier, p, offs = fl[fi]
+        ar, ai, oe = sample_offset(plane, tier, p.nx, p.ny, int(g - starts[fi]), offs)
+        cases.append((view.center_re, view.center_im, plane.bits + 64, p.max_iter, p.escape_radius, ar, ai, oe,
+                      {f: (0, int(sn["n"][g]), float(sn["nu"][g])) for f, sn in snaps.items()}))
+    out = precision_vs_direct(fdref, cases, list(snaps), args.direct_seconds, os.cpu_count() or 1)
+    out["selection"] = (f"seeded samples escaping in both forms within {args.direct_cap} iterations "
+                        f"({len(cand)} of {int(starts[-1])} qualify)")
+    return out
+
+
 def run_set(args):
     """Configs 3-5: the jittered 4-spp frame (one fdc_render per step, offsets staged), the
     60-frame film and the 256 mixed-location tiles (one batch graph replay per step), in
@@ -695,7 +730,7 @@ def run_set(args):
                 _, cnt, _ = dev.render_job(j, device_out={c: bufs[c].data_ptr() for c in cols})
                 return cnt
 
-            snap = lambda: {c: bufs[c].cpu().numpy().copy() for c in ("cls", "n")}
+            snap = lambda: {c: bufs[c].cpu().numpy().copy() for c in ("cls", "n", "nu")}
         else:
             b = dev.batch(jobs, columns=("nu", "de", "normal"), groups=groups)
 
@@ -704,7 +739,7 @@ def run_set(args):
                 return total
 
             # every frame's samples once (tiles of one location share its frame)
-            snap = lambda: {c: a.copy() for c, a in b.all_columns()[1].items() if c in ("cls", "n")}
+            snap = lambda: {c: a.copy() for c, a in b.all_columns()[1].items() if c in ("cls", "n", "nu")}
         for _ in range(args.warmup):
             cnt = step()
             log(f"{form} warm-up step: {cnt.kernel_ms:.1f} ms device")
@@ -738,6 +773,9 @@ def run_set(args):
                  "within_one": float(((ea == eb) & (~ea | (dn <= 1))).mean())}
     head = "fp32_floatexp" if ("fp32_floatexp" in forms and (agree is None or agree["count_match"] >= 0.999)) \
         else "fp64_plain"
+    direct = None
+    if rank == 0 and not args.no_cpu and args.direct_samples > 0:
+        direct = set_vs_direct(args, cfg, js, sel, frames, loc_of, forms)
     # e2e through the public API with host buffers, one step: uploads, render(s), columns to host
     locs = sorted({loc_of(k) for k in sel})  # the orbits and tables this rank uploads
     h2d = sum(16 * len(js.refs[k]) + (56 * len(js.blas[k].blocks) if js.blas[k] is not None else 0) for k in locs)
@@ -779,8 +817,11 @@ def run_set(args):
             dev.free(h)
         eff = cnt.iterations - cnt.blocks + cnt.skipped
     e2e_s = allmax(time.perf_counter() - t0, world)
+    # the same step with the host set-up of its orbits and tables (serial fixed-point work,
+    # configurations 4-5's largest cost) added, as a caller computing them per step pays it
+    setup_s = js.orbit_seconds + js.bla_seconds
     e2e = {"value": whole_job(eff) / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-           "steps": 1}
+           "steps": 1, "value_with_host_setup": whole_job(eff) / (e2e_s + setup_s), "host_setup_seconds": setup_s}
     if rank == 0:
         rf = forms.get("fp64_plain", forms[head])
         line = {"metric": METRIC, "value": forms[head]["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -800,7 +841,7 @@ def run_set(args):
                                  if len(forms) == 2 else None),
                 "agreement_fp32_vs_fp64": agree,
                 "setup_seconds": {"orbit": js.orbit_seconds, "bla": js.bla_seconds},
-                "cpu_baseline": None, "clocks": clk,
+                "cpu_baseline": None, "precision_vs_direct": direct, "clocks": clk,
                 "gpu_launches": sum(v["tot"]["launches"] for v in forms.values()), "e2e": e2e}
         print(json.dumps(line), flush=True)
     dev.close()
@@ -818,11 +859,13 @@ def main():
     ap.add_argument("--config", type=int, choices=(1, 2, 3, 4, 5), default=2)
     ap.add_argument("--frames", type=int, default=0, help="configs 4/5: first N frames / locations only")
     ap.add_argument("--seed", type=int, default=2)
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--direct-samples", type=int, default=256,
                     help="seeded samples checked against fd-fixed direct iteration")
     ap.add_argument("--direct-seconds", type=float, default=60.0)
+    ap.add_argument("--direct-cap", type=int, default=200_000,
+                    help="configurations 3-5: direct iteration only of samples escaping within this many steps")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--nx", type=int, default=0)
     ap.add_argument("--ny", type=int, default=0)
