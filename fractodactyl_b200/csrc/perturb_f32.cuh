@@ -155,10 +155,15 @@ __device__ __forceinline__ void relimit_f32(const Params &p, StateF &s) {
   s.lim = (uint32_t)b;
 }
 
-// Bla::find on the FP64 |delta|^2 of the iteration's start (s.d2).
-__device__ __forceinline__ int find_block_f32(const Params &p, const StateF &s, uint32_t &at) {
+// Whether Bla::find (on the FP64 |delta|^2 of the iteration's start, s.d2) finds a block.
+__device__ __forceinline__ bool block_starts_f32(const StateF &s) {
   const uint32_t budget = s.lim > s.n ? s.lim - s.n : 0u;
-  if (!((s.nucleus < 0 || s.m != 0) & (budget >= 2) & (s.d2 < s.r2a))) return -1;
+  return (s.nucleus < 0 || s.m != 0) & (budget >= 2) & (s.d2 < s.r2a);
+}
+
+// The rest of Bla::find once block_starts_f32 holds: the level of the longest valid block.
+__device__ __forceinline__ int block_level_f32(const Params &p, const StateF &s, uint32_t &at) {
+  const uint32_t budget = s.lim > s.n ? s.lim - s.n : 0u;
   const double d2 = s.d2;
   const uint32_t k = s.m - 1u;
   at = k >> 1;
@@ -426,11 +431,10 @@ __device__ __forceinline__ bool warp_step_f32(const Params &p, const Entry32 *__
       const double2 *e2 = reinterpret_cast<const double2 *>(orbit + s.m + 1);
       nz = __ldg(e2);
       nr = __ldg(e2 + 1);
-      int lv = -1;
-      if (L) lv = find_block_f32(p, s, w.at);
-      if (lv >= 0) {
+      // a lane that finds a block waits; its level is searched when the waiting lanes
+      // apply their blocks together (nothing the search reads changes while it waits)
+      if (L && block_starts_f32(s)) {
         w.on = true;
-        w.lv = lv;
       } else {
         plain_update_f32<D>(s);
         upd = true;
@@ -447,6 +451,7 @@ __device__ __forceinline__ bool warp_step_f32(const Params &p, const Entry32 *__
     const uint32_t busy = (uint32_t)__popc(waiting | stepping);
     const uint32_t thr = max(1u, (busy * defer) >> 5);
     if (waiting && ((uint32_t)__popc(waiting) >= thr || !stepping) && w.on) {
+      w.lv = block_level_f32(p, s, w.at);
       apply_block_f32<D>(p, s, w.lv, w.at);
       w.on = false;
       upd = took = true;
