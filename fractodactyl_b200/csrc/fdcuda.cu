@@ -902,11 +902,21 @@ fdc_status render_impl(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, const fdc
                   {out->z, 16}, {out->dz, 16}, {out->dexp, 8}, {out->status, 1},
                   {bout ? bout->bound : nullptr, 4}, {bout ? bout->ez : nullptr, 8}, {bout ? bout->ed : nullptr, 8},
                   {stripe ? stripe_out : nullptr, 4}};
+  // The BLA kernels outside the bounded and stripe variants store finished samples' raw
+  // state and encode_kernel computes nu / de / normal from it afterwards: class, count,
+  // status, z, dz/dc and its exponent must all exist, as scratch where the caller asked
+  // for none (never copied back; at the outputs' pitch).
+  const bool encode_later = !(j.flags & FDC_F32) && !bounded && !stripe && bla;
+  bool scratch[NCOL] = {};
+  if (encode_later)
+    for (int c : {0, 1, 5, 6, 7, 8}) scratch[c] = cols[c].host == nullptr;
+  const uint64_t scratch_rows = (uint64_t)rows * (dev_out ? j.nx : p.cols);
   size_t need = 0;
   size_t offs[NCOL + 2];
   for (int c = 0; c < NCOL; ++c) {
     offs[c] = need;
-    if (cols[c].host && !dev_out) need += (n_rows * cols[c].width + 255) & ~(size_t)255;
+    if (scratch[c]) need += (scratch_rows * cols[c].width + 255) & ~(size_t)255;
+    else if (cols[c].host && !dev_out) need += (n_rows * cols[c].width + 255) & ~(size_t)255;
   }
   offs[NCOL] = need;  // mask
   if (j.mask) need += (n_rows + 255) & ~(size_t)255;
@@ -923,7 +933,8 @@ fdc_status render_impl(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, const fdc
   char *stage = (char *)ctx->stage;
   void *dptr[NCOL];
   for (int c = 0; c < NCOL; ++c) {
-    if (!cols[c].host) dptr[c] = nullptr;
+    if (scratch[c]) dptr[c] = stage + offs[c];
+    else if (!cols[c].host) dptr[c] = nullptr;
     else if (dev_out) dptr[c] = (char *)cols[c].host + origin * cols[c].width;
     else dptr[c] = stage + offs[c];
   }
@@ -954,7 +965,9 @@ fdc_status render_impl(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, const fdc
   for (int c = 0; c < NCOL; ++c) {
     if (!dptr[c]) continue;
     const size_t w = cols[c].width;
-    if (!dev_out || full)
+    if (scratch[c])
+      CK(cudaMemsetAsync(dptr[c], 0, scratch_rows * w, ctx->stream));
+    else if (!dev_out || full)
       CK(cudaMemsetAsync(dptr[c], 0, n_rows * w, ctx->stream));
     else
       CK(cudaMemset2DAsync(dptr[c], j.nx * w, 0, p.cols * w, rows, ctx->stream));
@@ -964,6 +977,7 @@ fdc_status render_impl(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, const fdc
   p.timed_out = &ctx->scratch->timed_out;
   CK(cudaMemsetAsync(ctx->scratch, 0, sizeof(Scratch), ctx->stream));
 
+  uint32_t launches = 1;
   CK(cudaEventRecord(ctx->ev0, ctx->stream));
   if (j.flags & FDC_F32) {
     CK(fdk::launch_f32(p, o.z32, deriv, bla, ctx->sm_count, (int)ctx->tune.blocks_per_sm, ctx->stream,
@@ -980,6 +994,11 @@ fdc_status render_impl(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, const fdc
     void *args[] = {&p};
     CK(cudaLaunchKernel(fn, grid, block, args, 0, ctx->stream));
     CK(cudaGetLastError());
+    if (encode_later && (p.nu || p.de || p.normal)) {
+      fdk::encode_kernel<0><<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(p);
+      CK(cudaGetLastError());
+      launches += 1;
+    }
   }
   CK(cudaEventRecord(ctx->ev1, ctx->stream));
   if (!dev_out) {
@@ -1006,7 +1025,7 @@ fdc_status render_impl(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, const fdc
     std::memcpy(&sh, &sc.counters.shift_bits, 8);
     counters->shift = sh;
     counters->kernel_ms = ms;
-    counters->launches = 1;
+    counters->launches = launches;
   }
   if (sc.timed_out) return fail(ctx, FDC_TIMEOUT, "deadline passed; unfinished samples have status 0");
   return FDC_OK;

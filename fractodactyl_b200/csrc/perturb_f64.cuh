@@ -1061,31 +1061,10 @@ __device__ __forceinline__ bool bounds(uint64_t n, double az, double ez, double 
   return true;
 }
 
-template <bool B = false, bool T = false>
-__device__ __forceinline__ void put(const Params &p, uint32_t sample, const Result &r, float stripe = 0.0f) {
-  const uint32_t j = sample / p.nx, i = sample - j * p.nx;
-  const uint64_t idx = (uint64_t)(j - p.first_row) * p.out_pitch + (i - p.first_col);
-  if (p.status) p.status[idx] = 1;
-  if (T && p.stripe_out) p.stripe_out[idx] = stripe;  // grid.rs:772: 0 unless escaped
-  if (p.n_out) p.n_out[idx] = (uint32_t)(r.kind == 2 ? p.max_iter : r.n);
-  if (r.kind != 0) {
-    if (p.cls) p.cls[idx] = (uint8_t)(r.kind == 2 ? 2 : 1);
-    return;
-  }
-  if (p.z_out) p.z_out[idx] = make_double2(r.zr, r.zi);
-  if (p.dz_out) p.dz_out[idx] = make_double2(r.dr, r.di);
-  if (p.dexp_out) p.dexp_out[idx] = r.dexp;
-  double z2 = r.zr * r.zr + r.zi * r.zi;
-  double log2z = 0.5 * log2(z2);
-  double de_lo = 0.0, bnd = 0.0;
-  bool bounded = false;
-  if (B) {  // store.rs:88-106
-    bounded = bounds(r.n, sqrt(z2), r.ez, hypot(r.dr, r.di), r.ed, de_lo, bnd);
-    if (p.bound_out) p.bound_out[idx] = bounded ? (float)bnd : 0.0f;
-    if (p.ez_out) p.ez_out[idx] = r.ez;
-    if (p.ed_out) p.ed_out[idx] = r.ed;
-  }
-  if (p.cls) p.cls[idx] = bounded ? 4 : 0;  // Escaped | Bounded << 2
+// nu, de and normal of an escaped sample (store.rs:66-112, 145-150; samples.rs:45-48):
+// the Bounded evidence's lower DE factor de_lo scales de when bounded.
+__device__ __forceinline__ void encode_columns(const Params &p, uint64_t idx, const Result &r, double z2,
+                                               double log2z, bool bounded, double de_lo) {
   if (p.nu) p.nu[idx] = (double)r.n + 1.0 - log2(log2z);
   if (p.de) {  // store.rs:145-150
     double lnz = log2z * LN_2;
@@ -1100,6 +1079,66 @@ __device__ __forceinline__ void put(const Params &p, uint32_t sample, const Resu
     double x = p.cosr * re + p.sinr * im, y = p.sinr * re - p.cosr * im;
     double t = atan2(y, x) * (65536.0 / TAU);
     p.normal[idx] = (uint16_t)(int64_t)round(t);
+  }
+}
+
+// A finished sample's outputs. R: only the raw state (status, count, class, z, dz/dc and
+// its exponent, every pointer present) is stored here, and encode_kernel computes the
+// columns of escaped samples afterwards from it, with all threads of a warp busy instead of
+// the one lane that finishes.
+template <bool B = false, bool T = false, bool R = false>
+__device__ __forceinline__ void put(const Params &p, uint32_t sample, const Result &r, float stripe = 0.0f) {
+  const uint32_t j = sample / p.nx, i = sample - j * p.nx;
+  const uint64_t idx = (uint64_t)(j - p.first_row) * p.out_pitch + (i - p.first_col);
+  if (p.status) p.status[idx] = 1;
+  if (T && p.stripe_out) p.stripe_out[idx] = stripe;  // grid.rs:772: 0 unless escaped
+  if (p.n_out) p.n_out[idx] = (uint32_t)(r.kind == 2 ? p.max_iter : r.n);
+  if (r.kind != 0) {
+    if (p.cls) p.cls[idx] = (uint8_t)(r.kind == 2 ? 2 : 1);
+    return;
+  }
+  if (p.z_out) p.z_out[idx] = make_double2(r.zr, r.zi);
+  if (p.dz_out) p.dz_out[idx] = make_double2(r.dr, r.di);
+  if (p.dexp_out) p.dexp_out[idx] = r.dexp;
+  if (R) {
+    p.cls[idx] = 0;  // Escaped, heuristic evidence
+    return;
+  }
+  double z2 = r.zr * r.zr + r.zi * r.zi;
+  double log2z = 0.5 * log2(z2);
+  double de_lo = 0.0, bnd = 0.0;
+  bool bounded = false;
+  if (B) {  // store.rs:88-106
+    bounded = bounds(r.n, sqrt(z2), r.ez, hypot(r.dr, r.di), r.ed, de_lo, bnd);
+    if (p.bound_out) p.bound_out[idx] = bounded ? (float)bnd : 0.0f;
+    if (p.ez_out) p.ez_out[idx] = r.ez;
+    if (p.ed_out) p.ed_out[idx] = r.ed;
+  }
+  if (p.cls) p.cls[idx] = bounded ? 4 : 0;  // Escaped | Bounded << 2
+  encode_columns(p, idx, r, z2, log2z, bounded, de_lo);
+}
+
+// The columns of the escaped samples of a window whose persistent kernel stored only their
+// raw state (put with R): one thread per sample, the same expressions as put. (A template,
+// so that every translation unit including this header may hold it.)
+template <int V = 0>
+__global__ void encode_kernel(Params p) {
+  const uint64_t total = (uint64_t)p.rows * p.cols;
+  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t jj = t / p.cols, ii = t - jj * p.cols;
+    const uint64_t idx = jj * p.out_pitch + ii;
+    if (!p.status[idx] || p.cls[idx] != 0) continue;
+    Result r;
+    r.kind = 0;
+    r.n = p.n_out[idx];
+    const double2 z = p.z_out[idx], dz = p.dz_out[idx];
+    r.zr = z.x;
+    r.zi = z.y;
+    r.dr = dz.x;
+    r.di = dz.y;
+    r.dexp = p.dexp_out[idx];
+    const double z2 = r.zr * r.zr + r.zi * r.zi;
+    encode_columns(p, idx, r, z2, 0.5 * log2(z2), false, 0.0);
   }
 }
 
@@ -1118,6 +1157,10 @@ struct TraceSlot<true> {
   __device__ __forceinline__ StripeTrace *get() { return &t; }
 };
 
+// The BLA variants outside B and T store finished samples' raw state only (put's R: every
+// raw pointer present) and encode_kernel fills nu, de and normal afterwards (measured:
+// config 2 40.1 -> 39.2 ms, its fixed-tier variant 35.7 -> 33.8 ms; without BLA, config 1's
+// short frame ran 3% slower, so the plain variants encode as they finish).
 template <bool EXT, bool D, bool L, bool S = false, bool B = false, bool T = false>
 __global__ void __launch_bounds__(128, Occupancy<EXT>::blocks) perturb_kernel(Params p) {
   const unsigned FULL = 0xffffffffu;
@@ -1138,7 +1181,7 @@ __global__ void __launch_bounds__(128, Occupancy<EXT>::blocks) perturb_kernel(Pa
   // prefix - max_iter, so that the first run counts max_iter - prefix.
   int64_t bias = 0;
   auto finish = [&](uint32_t idx, const Result &r, uint64_t nblocks, uint64_t nskipped, double sh) {
-    put<B, T>(p, idx, r, T && r.kind == 0 ? tr->value : 0.0f);
+    put<B, T, L && !B && !T>(p, idx, r, T && r.kind == 0 ? tr->value : 0.0f);
     uint64_t spent = (uint64_t)((int64_t)(r.kind == 2 ? p.max_iter : r.n) - bias);
     bias = 0;
     if (L) {
