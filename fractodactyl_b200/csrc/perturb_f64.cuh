@@ -115,6 +115,7 @@ struct State {
   double ar, ai;  // sample offset (mantissa on the extended tier)
   double dc_r, dc_i, scale, inverse;
   double sr, si, qr, qi, qstep;
+  double near;  // save_point(): the near-return bound of the save point (sr, si)
   Multiplier mu;
   Contraction ct;
   double adc, shift;
@@ -250,6 +251,18 @@ struct StripeTrace {
     value = (float)(before * (1.0 - frac) + now * frac);
   }
 };
+
+// A periodicity save point (sample.rs:488-491, 522-575): the point and the bound that a
+// later z's distance from it is compared with, fabs(sr) + fabs(si) scaled as each tier's
+// near-return test scales it. The reference evaluates the bound every iteration from the
+// same two values, so evaluating it once here gives the same double.
+template <bool EXT>
+__device__ __forceinline__ void save_point(State<EXT> &s, double r, double i) {
+  s.sr = r;
+  s.si = i;
+  const double size = fabs(r) + fabs(i);
+  s.near = EXT ? 1e-13 * size + 1e-300 : 1e-3 * size;
+}
 
 // The iteration limit behind Bla::find's budget (sample.rs:246-263) with n left out:
 // min(max_iter, the next periodicity save point, nucleus + 1), kept in the state and
@@ -459,13 +472,12 @@ __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res
     bool judge = check_r * check_r + check_i * check_i > RES2 * f2;
     if (EXT) judge = judge && s.returns < 4;
     const double dist = fabs(fr - s.sr) + fabs(fi - s.si);
-    const double size = fabs(s.sr) + fabs(s.si);
     if (replaying) {
     } else if (EXT) {
-      common = common && !(judge && dist < 1e-13 * size + 1e-300);
+      common = common && !(judge && dist < s.near);
     } else {
       const bool held = s.hold > 0 && s.n - s.sn < s.hold;  // sn <= n while hold > 0
-      common = common && (judge ? !(dist < 1e-3 * size) && (s.hold > 0 ? held : !(s.pending || s.n >= s.chk))
+      common = common && (judge ? !(dist < s.near) && (s.hold > 0 ? held : !(s.pending || s.n >= s.chk))
                                 : (s.hold > 0 ? held : s.n < s.chk));
     }
     if (__builtin_expect(common, 1)) {
@@ -513,8 +525,7 @@ __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res
         s.fi = fi;
       }
       if (EXT && !replaying && __builtin_expect(s.n >= s.chk, 0)) {  // sample.rs:488-491 / :571-574
-        s.sr = fr;
-        s.si = fi;
+        save_point(s, fr, fi);
         s.sn = s.n;
         s.chk = s.chk >= 0x80000000u ? 0xffffffffu : s.chk * 2;
         relimit(p, s);
@@ -674,8 +685,7 @@ __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res
   if (!judge) {
     if (EXT) {
       if (s.n >= s.chk) {
-        s.sr = fr;
-        s.si = fi;
+        save_point(s, fr, fi);
         s.sn = s.n;
         s.chk = s.chk >= 0x80000000u ? 0xffffffffu : s.chk * 2;
         relimit(p, s);
@@ -694,9 +704,8 @@ __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res
     return false;
   }
   double dist = fabs(fr - s.sr) + fabs(fi - s.si);
-  double size = fabs(s.sr) + fabs(s.si);
   if (EXT) {
-    if (s.returns < 4 && dist < 1e-13 * size + 1e-300) {
+    if (s.returns < 4 && dist < s.near) {
       if (contracting(p.orbit, p.last, s.m, check_r, check_i, s.ar * exp2i(s.offset_exp),
                       s.ai * exp2i(s.offset_exp), (uint64_t)(s.n - s.sn))) {
         res.kind = 2;
@@ -705,15 +714,14 @@ __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res
       s.returns += 1;
     }
     if (s.n >= s.chk) {
-      s.sr = fr;
-      s.si = fi;
+      save_point(s, fr, fi);
       s.sn = s.n;
       s.chk = s.chk >= 0x80000000u ? 0xffffffffu : s.chk * 2;
       relimit(p, s);
     }
     return false;
   }
-  if (dist < 1e-3 * size) {
+  if (dist < s.near) {
     uint32_t period = s.n - s.sn;
     if (s.hold == period && s.mu.below_one()) {
       double mr, mi;
@@ -723,7 +731,7 @@ __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res
       double den = er * er + ei * ei;
       double qpr = s.sr - (gr * er + gi * ei) / den;
       double qpi = s.si - (gi * er - gr * ei) / den;
-      double tol = rmin(0.1 * sqrt(den), 1e-2) * s.qstep + 16.0 * U * size;
+      double tol = rmin(0.1 * sqrt(den), 1e-2) * s.qstep + 16.0 * U * (fabs(s.sr) + fabs(s.si));
       if (s.predicted && fabs(qpr - s.qr) + fabs(qpi - s.qi) <= tol) {
         res.kind = 1;
         res.n = s.n;
@@ -737,8 +745,7 @@ __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res
       s.predicted = false;
     }
     s.hold = period;
-    s.sr = fr;
-    s.si = fi;
+    save_point(s, fr, fi);
     s.sn = s.n;
     s.pending = false;
     s.mu.reset();
@@ -755,8 +762,7 @@ __device__ __forceinline__ bool post(const Params &p, State<EXT> &s, Result &res
     uint64_t np = next_pow2((uint64_t)s.n + 1);
     uint32_t np32 = np > 0xffffffffull ? 0xffffffffu : (uint32_t)np;
     s.chk = s.chk > np32 ? s.chk : np32;
-    s.sr = fr;
-    s.si = fi;
+    save_point(s, fr, fi);
     s.sn = s.n;
     s.pending = false;
   }
@@ -799,21 +805,27 @@ struct Waiting {
 
 // A warp's reserved queue slots [base, end): one atomic on the queue head takes 32
 // consecutive slots (one tile), which the warp then hands to its idle lanes in order, so
-// one round trip to the head serves a tile instead of each lane as it finishes. Every
-// lane holds the same copy.
+// one round trip to the head serves a tile instead of each lane as it finishes, and
+// neighbouring samples share a warp. Held slots start only as the warp's own lanes finish,
+// so over the last eighth of the queue a warp takes just the slots its idle lanes need:
+// there a long sample left waiting behind busy lanes would lengthen the launch's tail.
+// Every lane holds the same copy.
 struct Reservation {
   unsigned long long base = 0, end = 0;
+  bool tail = false;  // within the last eighth of the queue
   // Slots for the `need` idle lanes (warp-uniform): false when the queue is spent;
   // otherwise the lanes of need with rank < count take first + rank.
   __device__ __forceinline__ bool take(unsigned long long *queue, unsigned long long total, unsigned need,
                                        unsigned lane, unsigned long long &first, unsigned &count) {
     if (base >= end) {
+      const unsigned long long grab = tail ? (unsigned long long)__popc(need) : 32ull;
       unsigned long long b = 0;
-      if (lane == 0) b = atomicAdd(queue, 32ull);
+      if (lane == 0) b = atomicAdd(queue, grab);
       b = __shfl_sync(0xffffffffu, b, 0);
       if (b >= total) return false;
       base = b;
-      end = b + 32 < total ? b + 32 : total;
+      end = b + grab < total ? b + grab : total;
+      tail = total - b <= total / 8;
     }
     const unsigned long long left = end - base, want = (unsigned long long)__popc(need);
     count = (unsigned)(want < left ? want : left);
@@ -985,8 +997,7 @@ __device__ __forceinline__ void start_sample(const Params &p, State<EXT> &s, boo
   s.r2b = -1.0;
   s.fr = EXT ? p.z0r + s.scale * 0.0 : p.z0r + 0.0;  // z of the first iteration
   s.fi = EXT ? p.z0i + s.scale * 0.0 : p.z0i + 0.0;
-  s.sr = 0.0;
-  s.si = 0.0;
+  save_point(s, 0.0, 0.0);
   s.chk = 16;
   s.replaying = false;
   s.limit = (uint32_t)p.max_iter;
@@ -1027,8 +1038,7 @@ __device__ __forceinline__ void start_sample(const Params &p, State<EXT> &s, boo
     }
     s.fr = s.Zr + s.xr;
     s.fi = s.Zi + s.xi;
-    s.sr = s.Zr + s.xr;
-    s.si = s.Zi + s.xi;
+    save_point(s, s.Zr + s.xr, s.Zi + s.xi);
     s.sn = m;
     const uint64_t np = next_pow2((uint64_t)m + 1);
     s.chk = np > 16 ? (uint32_t)np : 16u;
