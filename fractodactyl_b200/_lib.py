@@ -109,7 +109,7 @@ DEFAULT_DEFER = 0  # FDC_DEFAULT_DEFER: each kernel variant's measured default
 
 # Every symbol the headers declare, for the export check.
 FDC_SYMBOLS = ["fdc_abi_version", "fdc_open", "fdc_close", "fdc_last_error", "fdc_upload_orbit", "fdc_free_orbit",
-               "fdc_upload_bla", "fdc_upload_series", "fdc_upload_error_radius", "fdc_render_bounded", "fdc_render_stripe", "fdc_render", "fdc_batch_create", "fdc_batch_run", "fdc_batch_free",
+               "fdc_upload_bla", "fdc_build_bla", "fdc_upload_series", "fdc_upload_error_radius", "fdc_render_bounded", "fdc_render_stripe", "fdc_render", "fdc_batch_create", "fdc_batch_run", "fdc_batch_free",
                "fdc_render_noalloc", "fdc_set_tuning", "fdc_get_tuning"]
 FDH_SYMBOLS = ["fdh_last_error", "fdh_plane_new", "fdh_orbit_fixed", "fdh_orbit_fixed_threads", "fdh_orbit_f64",
                "fdh_nucleus_period",
@@ -135,6 +135,7 @@ def lib():
     L.fdc_upload_orbit.argtypes = [P, P, P, U64, U32, C.POINTER(I32)]
     L.fdc_free_orbit.argtypes = [P, I32]
     L.fdc_upload_bla.argtypes = [P, I32, P, P, U32, D, D, I64]
+    L.fdc_build_bla.argtypes = [P, I32, D, D, I64, C.POINTER(U32), P]
     L.fdc_upload_series.argtypes = [P, I32, U64, U64, D, P, U32]
     L.fdc_render.argtypes = [P, C.POINTER(Job), C.POINTER(Out), C.POINTER(Counters)]
     L.fdc_render_bounded.argtypes = [P, C.POINTER(Job), C.POINTER(Out), C.POINTER(BoundOut), C.POINTER(Counters)]

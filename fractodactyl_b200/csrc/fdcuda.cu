@@ -20,6 +20,7 @@
 
 #include "../../include/fdcuda.h"
 #include "launch.hpp"
+#include "bla_build.cuh"
 #include "perturb_f64.cuh"
 #include "route_internal.hpp"
 
@@ -803,6 +804,106 @@ fdc_status fdc_upload_bla(fdc_ctx *ctx, int32_t orbit, const double *blocks7, co
   free_bla(ctx, o.bla);
   o.bla = d;
   o.has_bla = true;
+  return FDC_OK;
+}
+
+// The table built on the device over the uploaded orbit (Bla::build_scaled, bla.rs:161-216):
+// every possible level is queued at once (bla_level skips a level after one without a
+// valid block), one read of the level flags gives the kept levels, and the table then takes
+// the upload's path (pack_bla's value checks, fuse_bla). export7: optional host copy of
+// the kept levels in the export form.
+fdc_status fdc_build_bla(fdc_ctx *ctx, int32_t orbit, double eps, double dc_max, int64_t dc_exp, uint32_t *levels,
+                         double *export7) {
+  if (!ctx) return FDC_INVALID;
+  auto it = ctx->orbits.find(orbit);
+  if (it == ctx->orbits.end()) return fail(ctx, FDC_INVALID, "unknown orbit handle");
+  OrbitDev &o = it->second;
+  if (o.batch_refs) return fail(ctx, FDC_INVALID, "orbit is read by a live batch: free the batch first");
+  if (!(eps > 0.0 && eps <= 1.0 / (double)(1u << 24) && dc_max > 0.0 && std::isfinite(dc_max)))
+    return fail(ctx, FDC_INVALID, "BLA needs 0 < eps <= 2^-24 and a finite dc_max > 0");
+  CK(cudaSetDevice(ctx->device));
+  const uint64_t steps = o.len >= 2 ? o.len - 2 : 0;
+  uint64_t size[fdk::MAX_LEVELS] = {}, at[fdk::MAX_LEVELS] = {}, room = 0;
+  uint32_t built = 0;  // levels with at least one block (orbits of at most 2^20 points: <= 19)
+  for (uint64_t n = steps / 2; n > 0 && built < (uint32_t)fdk::MAX_LEVELS; n /= 2) {
+    at[built] = room;
+    size[built++] = n;
+    room += n;
+  }
+  const size_t flag_bytes = 256;
+  char *buf = (char *)pool_get(ctx, flag_bytes + 56 * room);
+  if (!buf) return fail(ctx, FDC_DEVICE_ERROR, "device memory for the BLA build");
+  unsigned *valid = (unsigned *)buf;
+  double *raw = (double *)(buf + flag_bytes);
+  cudaError_t e = cudaMemsetAsync(valid, 0, flag_bytes, ctx->stream);
+  for (uint32_t i = 0; e == cudaSuccess && i < built; ++i) {
+    fdk::bla_level<<<grid_for(size[i]), 256, 0, ctx->stream>>>(
+        o.z, i > 0 ? raw + 7 * at[i - 1] : nullptr, size[i], i, eps, dc_max, dc_exp, raw + 7 * at[i], valid);
+    e = cudaGetLastError();
+  }
+  unsigned flags[fdk::MAX_LEVELS] = {};
+  if (e == cudaSuccess) e = cudaMemcpyAsync(flags, valid, sizeof flags, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) {
+    pool_put(ctx, buf, flag_bytes + 56 * room);
+    return fail(ctx, FDC_DEVICE_ERROR, std::string("BLA build: ") + cudaGetErrorString(e));
+  }
+  uint32_t kept = 0;
+  while (kept < built && flags[kept]) ++kept;
+  if (kept >= (uint32_t)fdk::MAX_LEVELS) {
+    pool_put(ctx, buf, flag_bytes + 56 * room);
+    return fail(ctx, FDC_INVALID, "too many BLA levels");
+  }
+  const uint64_t total = kept ? at[kept - 1] + size[kept - 1] : 0;
+  BlaDev d;
+  d.levels = kept;
+  d.eps = eps;
+  d.dc_max = dc_max;
+  d.dc_exp = dc_exp;
+  d.points = o.len;
+  d.blocks = total;
+  for (uint32_t i = 0; i < kept; ++i) {
+    d.off[i] = (uint32_t)at[i];
+    d.count[i] = (uint32_t)size[i];
+  }
+  d.fused = (double *)pool_get(ctx, 32 * o.len);
+  d.r2 = (double *)pool_get(ctx, 8 * total);
+  d.coef = (double2 *)pool_get(ctx, 32 * total);
+  d.ab = (double2 *)pool_get(ctx, 16 * total);
+  if (!d.fused || (total && (!d.r2 || !d.coef || !d.ab))) {
+    pool_put(ctx, buf, flag_bytes + 56 * room);
+    free_bla(ctx, d);
+    return fail(ctx, FDC_DEVICE_ERROR, "device memory for the BLA table");
+  }
+  unsigned *bad = &ctx->scratch->bad;
+  e = cudaMemsetAsync(bad, 0, sizeof(unsigned), ctx->stream);
+  if (e == cudaSuccess && total) {
+    pack_bla<<<grid_for(total), 256, 0, ctx->stream>>>(raw, total, d.r2, d.coef, d.ab, bad);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess && export7 && total) e = download(ctx, export7, raw, 56 * total);
+  unsigned badf = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&badf, bad, sizeof badf, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  pool_put(ctx, buf, flag_bytes + 56 * room);
+  if (e != cudaSuccess || badf) {
+    free_bla(ctx, d);
+    if (e != cudaSuccess) return fail(ctx, FDC_DEVICE_ERROR, std::string("BLA build: ") + cudaGetErrorString(e));
+    return fail(ctx, FDC_INVALID, (badf & 1) ? "BLA level holds a non-finite value"
+                                             : "BLA level holds a negative radius");
+  }
+  fuse_bla<<<grid_for(o.len), 256, 0, ctx->stream>>>(o.z, o.len, d.r2, kept, kept > 0 ? d.off[0] : 0,
+                                                     kept > 0 ? d.count[0] : 0, kept > 1 ? d.off[1] : 0,
+                                                     kept > 1 ? d.count[1] : 0, d.fused, o.z32);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    free_bla(ctx, d);
+    return fail(ctx, FDC_DEVICE_ERROR, std::string("BLA build: ") + cudaGetErrorString(e));
+  }
+  free_bla(ctx, o.bla);
+  o.bla = d;
+  o.has_bla = true;
+  if (levels) *levels = kept;
   return FDC_OK;
 }
 

@@ -221,6 +221,19 @@ class Bla:
 
 
 @dataclasses.dataclass
+class DeviceTable:
+    """The BLA table Bla.build_scaled(orbit, eps, dc_max, dc_exp) would build, built on the
+    device over the uploaded orbit instead (fdc_build_bla): no host build, no table upload.
+    render_with fills in levels and blocks (the kept level and block counts) after the build."""
+    eps: float
+    dc_max: float
+    dc_exp: int
+    points: int
+    levels: int = 0
+    blocks: int = 0
+
+
+@dataclasses.dataclass
 class Series:
     """A parameter-series start (crates/fd-kernel/src/series.rs:57-84): every sample with
     |dc| <= rho may start at iterate n from delta = sum_k b_k (dc / rho)^k. n = 0: none
@@ -336,6 +349,7 @@ class Device:
             raise RouteError(f"fdc_open({index}): {_lib.STATUS_NAMES.get(st, st)}")
         self.index = index
         self._orbits = {}
+        self._orbit_len = {}  # handle -> points, for build_bla's export size
 
     def close(self):
         if self.h:
@@ -353,6 +367,7 @@ class Device:
         h = C.c_int32()
         _check(lib().fdc_upload_orbit(self.h, re.ctypes.data, im.ctypes.data, len(re), r.bits, C.byref(h)), self,
                "upload orbit")
+        self._orbit_len[h.value] = len(re)
         if bla is not None:
             b = np.ascontiguousarray(bla.blocks)
             offs = np.ascontiguousarray(bla.level_offsets)
@@ -360,6 +375,23 @@ class Device:
                                         offs.ctypes.data, bla.levels, bla.eps, bla.dc_max, bla.dc_exp), self,
                    "upload BLA")
         return h.value
+
+    def build_bla(self, orbit: int, eps: float, dc_max: float, dc_exp: int = 0, export: bool = False):
+        """fdc_build_bla: the BLA table of Bla.build_scaled(orbit, eps, dc_max, dc_exp) built on
+        the device over the uploaded orbit, in place of an uploaded one. Returns the kept level
+        count, and with export the blocks in the export form ([f64; 7] rows, level-major)."""
+        levels = C.c_uint32()
+        out = None
+        if export:
+            cap = max(self._orbit_len[orbit] - 3, 0)
+            out = np.empty((max(cap, 1), 7))
+        _check(lib().fdc_build_bla(self.h, orbit, eps, dc_max, dc_exp, C.byref(levels),
+                                   out.ctypes.data if out is not None else None), self, "build BLA")
+        if not export:
+            return levels.value
+        steps = max(self._orbit_len[orbit] - 2, 0)
+        total = sum(steps >> (i + 1) for i in range(levels.value))
+        return levels.value, out[:total].copy()
 
     def upload_series(self, orbit: int, series: "Series"):
         """fdc_upload_series: the series start for jobs on `orbit` with the SERIES flag."""
@@ -663,10 +695,13 @@ def render_with(view: View, p: Params, orbit=None, bla: Optional[Bla] = None, de
     reference_seconds = time.perf_counter() - t
     if bla is not None and bla.points != len(r):
         raise ValueError(f"BLA table covers a {bla.points}-point orbit, not this {len(r)}-point one")
+    on_device = isinstance(bla, DeviceTable)
+    if on_device and (bound or series is not None):
+        raise ValueError("a device-built table serves the BLA kernel only (no Bound column, no series start)")
     # A table without levels skips nothing: its samples are the plain kernel's, so it is not
     # uploaded; the header and BlaStats stay render_bla's (grid.rs:526-529), and its
     # refusals (grid.rs:392-411), which the device checks for uploaded tables, are checked here.
-    table = bla if bla is not None and bla.levels > 0 else None
+    table = bla if bla is not None and (on_device or bla.levels > 0) else None
     if bla is not None and table is None:
         _check_bla_escape_radius(p.escape_radius)
         dc, e = bla_dc_bound(view, p)
@@ -683,8 +718,13 @@ def render_with(view: View, p: Params, orbit=None, bla: Optional[Bla] = None, de
         if math.isnan(dc) or dc > series.rho:
             raise ValueError(f"view reaches |dc| = {dc:e}, beyond the series radius {series.rho:e}")
     dev = dev or device(0)
-    h = dev.upload(r, table)
+    h = dev.upload(r, None if on_device else table)
     try:
+        if on_device:  # built over the uploaded orbit; without levels it skips nothing, as above
+            bla.levels = dev.build_bla(h, bla.eps, bla.dc_max, bla.dc_exp)
+            steps = max(len(r) - 2, 0)
+            bla.blocks = sum(steps >> (i + 1) for i in range(bla.levels))
+            table = bla if bla.levels > 0 else None
         flags = (_lib.DERIVATIVE if p.needs_derivative() or (bound and tier != 2) else 0) | \
             (_lib.BLA if table is not None else 0)
         if series is not None:
@@ -707,9 +747,16 @@ def render_with(view: View, p: Params, orbit=None, bla: Optional[Bla] = None, de
     rep = report if report is not None else RouteReport()
     rep.device = f"cuda:{dev.index}"
     rep.gpu_seconds = gpu_seconds
-    rep.table_blocks = 0 if bla is None else len(bla.blocks)
+    rep.table_blocks = 0 if bla is None else (bla.blocks if on_device else len(bla.blocks))
     return assemble(view, p, plane, tier, bla, table, series, flags, shift, host_encode, arrays, cnt, status,
                     len(r), reference_seconds, rep, started, quiet)
+
+
+def _f64_div(a: float, b: float) -> float:
+    """a / b as binary64 divides (grid.rs:532-533 in Rust): +-inf or NaN for b == 0, where
+    h underflows on the deepest views, instead of Python's ZeroDivisionError."""
+    with np.errstate(divide="ignore", invalid="ignore"):
+        return float(np.float64(a) / np.float64(b))
 
 
 def assemble(view: View, p: Params, plane: Plane, tier: int, bla: Optional[Bla], table: Optional[Bla],
@@ -742,7 +789,7 @@ def assemble(view: View, p: Params, plane: Plane, tier: int, bla: Optional[Bla],
     if table is not None:
         bstats = BlaStats(int(cnt.blocks), int(cnt.skipped), int(cnt.fallback_samples),
                           int(cnt.closed_form_samples),
-                          cnt.shift / (plane.h() * p.ss) if (flags & _lib.SHIFT) else None)
+                          _f64_div(cnt.shift, plane.h() * p.ss) if (flags & _lib.SHIFT) else None)
     elif bla is not None:  # no block anywhere: closed-form interiors, every other sample a fallback
         closed = int((((arrays["cls"] & 3) == 1) & (arrays["n"] == 0) & (arrays["status"] != 0)).sum())
         bstats = BlaStats(0, 0, int(cnt.samples) - closed, closed,
@@ -773,14 +820,19 @@ def render_series(view: View, p: Params, orbit, series: "Series", bla: Optional[
     return render_with(view, p, orbit, bla, series=series, **kw)
 
 
-def render_bla(view: View, p: Params, orbit=None, eps: float = EPS, **kw):
+def render_bla(view: View, p: Params, orbit=None, eps: float = EPS, device_table: bool = False, **kw):
     """perturb_gpu::render_bla (frame.rs:78-84) on the CUDA route: the reference orbit
-    (computed unless supplied) and a BLA table built over it by the CPU builder for the
-    view's largest |dc| (control.rs:344-360), then the BLA kernel."""
+    (computed unless supplied) and a BLA table built over it for the view's largest |dc|
+    (control.rs:344-360), then the BLA kernel. The table is the CPU builder's, or with
+    device_table the same table built on the GPU over the uploaded orbit (fdc_build_bla)."""
     if orbit is None:
         orbit = reference(view, p)
     _check_bla_escape_radius(p.escape_radius)
     dc, e = bla_dc_bound(view, p)
+    if device_table:
+        if not (0.0 < eps <= 2.0 ** -24 and 0.0 < dc < math.inf):  # bla.rs:26-33, the host builder's refusal
+            raise ValueError("BLA needs 0 < eps <= 2^-24 and a finite dc_max > 0")
+        return render_with(view, p, orbit, DeviceTable(eps, dc, e, len(orbit[0])), **kw)
     t = time.perf_counter()
     table = Bla.build_scaled(orbit[0], eps, dc, e, p.threads)
     report = kw.pop("report", None) or RouteReport()

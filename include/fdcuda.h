@@ -118,6 +118,16 @@ fdc_status fdc_free_orbit(fdc_ctx *ctx, int32_t orbit);
 fdc_status fdc_upload_bla(fdc_ctx *ctx, int32_t orbit, const double *blocks7, const uint64_t *level_offsets,
                           uint32_t levels, double eps, double dc_max, int64_t dc_exp);
 
+/* Build that table on the device from the uploaded orbit instead of uploading it:
+ * Bla::build_scaled(reference, eps, dc_max, dc_exp) (bla.rs:161-216, called by
+ * frame.rs:119-140 before pack_bla), with the same blocks bit for bit and the same refusals
+ * as fdc_upload_bla. *levels (optional) receives the kept level count; export7 (optional,
+ * host memory for len - 3 blocks) receives the kept levels in the export form above,
+ * level i at offset sum_{j<i} (len - 2) >> (j + 1). Replaces the host build and the
+ * 56-byte-per-block upload. */
+fdc_status fdc_build_bla(fdc_ctx *ctx, int32_t orbit, double eps, double dc_max, int64_t dc_exp, uint32_t *levels,
+                         double *export7);
+
 /* Upload a parameter-series start built over that orbit (Series, series.rs:57-84, e.g. by
  * fdh_series_build): jobs with FDC_SERIES start every sample at iterate n from delta =
  * sum_k b_k (dc / rho)^k, coeffs = b_1..b_order as (re, im) pairs (order <= 64), on the

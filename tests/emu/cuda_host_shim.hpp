@@ -19,6 +19,7 @@
 #define __align__(n) alignas(n)
 
 using std::isfinite;
+using std::isinf;
 using std::isnan;
 
 struct double2 {

@@ -24,6 +24,7 @@ inline uint64_t now() { return ticks += 1000; }
 #define FDK_HOST_TIMER() emu_clock::now()
 
 #include "perturb_f32.cuh"
+#include "bla_build.cuh"
 
 extern "C" {
 
@@ -440,6 +441,50 @@ void emu_set_stripe(uint32_t window, double freq, float *out) {
   g_stripe_window = window;
   g_stripe_freq = freq;
   g_stripe_out = out;
+}
+
+
+// fdk::libm_hypot over n pairs against the host C library's hypot: how many differ (two
+// NaN results count as equal).
+uint64_t emu_hypot_check(const double *x, const double *y, uint64_t n) {
+  uint64_t bad = 0;
+  for (uint64_t k = 0; k < n; ++k) {
+    const double a = fdk::libm_hypot(x[k], y[k]), b = std::hypot(x[k], y[k]);
+    bad += !(std::memcmp(&a, &b, 8) == 0 || (std::isnan(a) && std::isnan(b)));
+  }
+  return bad;
+}
+
+// The device table builder (fdk::bla_level, one host thread per level) over an orbit, as
+// fdc_build_bla queues it: every possible level, each skipped after a level without a
+// valid block. out7: room for len - 3 blocks; the kept levels are written level-major.
+// Returns the kept level count.
+uint32_t emu_bla_build(const double *re, const double *im, uint64_t len, double eps, double dc_max, int64_t dc_exp,
+                       double *out7) {
+  std::vector<double2> z(len);
+  for (uint64_t k = 0; k < len; ++k) z[k] = make_double2(re[k], im[k]);
+  const uint64_t steps = len >= 2 ? len - 2 : 0;
+  std::vector<uint64_t> size, at;
+  uint64_t room = 0;
+  for (uint64_t n = steps / 2; n > 0 && size.size() < (size_t)fdk::MAX_LEVELS; n /= 2) {
+    at.push_back(room);
+    size.push_back(n);
+    room += n;
+  }
+  std::vector<double> raw(7 * std::max<uint64_t>(room, 1));
+  std::vector<unsigned> valid(fdk::MAX_LEVELS, 0);
+  blockIdx.x = 0;
+  threadIdx.x = 0;
+  blockDim.x = 1;
+  gridDim.x = 1;
+  for (uint32_t i = 0; i < size.size(); ++i)
+    fdk::bla_level(z.data(), i > 0 ? raw.data() + 7 * at[i - 1] : nullptr, size[i], i, eps, dc_max, dc_exp,
+                   raw.data() + 7 * at[i], valid.data());
+  uint32_t kept = 0;
+  while (kept < size.size() && valid[kept]) ++kept;
+  const uint64_t total = kept ? at[kept - 1] + size[kept - 1] : 0;
+  std::copy(raw.begin(), raw.begin() + 7 * total, out7);
+  return kept;
 }
 
 }  // extern "C"

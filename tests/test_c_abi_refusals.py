@@ -32,6 +32,8 @@ def test_null_context_refused(L):
     assert orbit.value == 7  # untouched
     assert L.fdc_free_orbit(None, 0) == _lib.INVALID
     assert L.fdc_upload_bla(None, 0, a.ctypes.data, a.ctypes.data, 1, 1e-15, 1.0, 0) == _lib.INVALID
+    lv = C.c_uint32(5)
+    assert L.fdc_build_bla(None, 0, 1e-15, 1.0, 0, C.byref(lv), None) == _lib.INVALID and lv.value == 5
     assert L.fdc_upload_series(None, 0, 8, 4, 1.0, a.ctypes.data, 2) == _lib.INVALID
     assert L.fdc_upload_error_radius(None, 0, a.ctypes.data, 8) == _lib.INVALID
     assert L.fdc_render(None, C.byref(job), C.byref(out), C.byref(c)) == _lib.INVALID

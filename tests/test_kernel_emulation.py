@@ -33,7 +33,8 @@ def emu():
     src = [os.path.join(HERE, "emu", "emu.cpp"), os.path.join(HERE, "emu", "cuda_host_shim.hpp"),
            os.path.join(ROOT, "fractodactyl_b200", "csrc", "perturb_f64.cuh"),
            os.path.join(ROOT, "fractodactyl_b200", "csrc", "perturb_f32.cuh"),
-           os.path.join(ROOT, "fractodactyl_b200", "csrc", "fd_device.cuh")]
+           os.path.join(ROOT, "fractodactyl_b200", "csrc", "fd_device.cuh"),
+           os.path.join(ROOT, "fractodactyl_b200", "csrc", "bla_build.cuh")]
     if not os.path.exists(LIB) or os.path.getmtime(LIB) < max(os.path.getmtime(s) for s in src):
         subprocess.run(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-ffp-contract=off", "-Wno-unknown-pragmas",
                         "-I", os.path.join(HERE, "emu"), "-I", os.path.join(ROOT, "fractodactyl_b200", "csrc"),
@@ -48,6 +49,10 @@ def emu():
     L.emu_render_batch.restype = C.c_int
     L.emu_render_batch.argtypes = [C.POINTER(Job), U32]
     L.emu_set_stripe.argtypes = [U32, D, P]
+    L.emu_hypot_check.restype = U64
+    L.emu_hypot_check.argtypes = [P, P, U64]
+    L.emu_bla_build.restype = U32
+    L.emu_bla_build.argtypes = [P, P, U64, D, D, I64, P]
     return L
 
 
@@ -735,3 +740,80 @@ def test_stripe_kernel_equals_oracle(emu, frame, window, freq, deriv):
     assert np.array_equal(got["cls"], want["cls"])
     esc = want["cls"] == 0
     assert esc.any() and np.array_equal(stripe, want["stripe"]), np.abs(stripe - want["stripe"]).max()
+
+
+def hypot_pairs(n, seed):
+    """Seeded pairs across the whole binary64 range (subnormals, overflowing squares and
+    the infinities that ldexp makes at the top): independent exponents, exponents within 70
+    of each other, near-equal pairs and pairs near a ratio of 2 (the two correction cases)."""
+    g = np.random.default_rng(seed)
+    with np.errstate(over="ignore"):
+        x = np.ldexp(g.uniform(-1, 1, n), g.integers(-1080, 1031, n))
+        kind = g.integers(0, 4, n)
+        y = np.ldexp(g.uniform(-1, 1, n), g.integers(-1080, 1031, n))
+        close = np.ldexp(g.uniform(-1, 1, n), np.frexp(x)[1] + g.integers(-70, 71, n))
+        near = x * (1 + 1e-3 * g.uniform(-1, 1, n))
+        half = x * (0.5 + 1e-2 * g.uniform(-1, 1, n))
+    return x, np.where(kind == 1, close, np.where(kind == 2, near, np.where(kind == 3, half, y)))
+
+
+def test_device_hypot_equals_host_libm(emu):
+    """The device table builder's hypot (Borges' corrected square root with power-of-two
+    scaling) returns the host C library's hypot bit for bit: 4M seeded pairs over the whole
+    range and every pair of special values (zeros, subnormals, the largest finite value,
+    infinities, NaN, the scaling thresholds)."""
+    x, y = hypot_pairs(4_000_000, 5)
+    assert emu.emu_hypot_check(x.ctypes.data, y.ctypes.data, len(x)) == 0
+    sp = np.array([0.0, -0.0, 1.0, -3.0, 4.0, np.inf, -np.inf, np.nan, 5e-324, 2.2250738585072014e-308,
+                   1.7976931348623157e308, 2.0 ** 1023, 2.0 ** -537, 2.0 ** 511, 2.0 ** 500, 2.0 ** -500,
+                   2.0 ** -400, np.nextafter(2.0 ** 500, np.inf), np.nextafter(2.0 ** -500, 0.0)])
+    a, b = np.meshgrid(sp, sp)
+    a, b = np.ascontiguousarray(a.ravel()), np.ascontiguousarray(b.ravel())
+    assert emu.emu_hypot_check(a.ctypes.data, b.ctypes.data, len(a)) == 0
+
+
+TABLE_VIEWS = [
+    # view, iterations, tier; the dc bound's exponent ranges from 0 to far below -1022
+    # (the first view's orbit escapes early: a table without levels)
+    (SEAHORSE + ("1e-14",), 20_000, None),
+    (("-0.743643887037158704752191506114774", "0.131825904205311970493132056385139", "1e-20"), 20_000, None),
+    (("0", "1", "1e-300"), 5000, "scaled"),
+    (("0", "1", "1e-400"), 5000, "scaled"),
+    (("-0.743643887037158704752191506114774", "0.131825904205311970493132056385139", "1e-28"), 50_000, None),
+]
+
+
+@pytest.mark.parametrize("view3,it,tier", TABLE_VIEWS, ids=lambda v: str(v)[:24])
+def test_device_table_builder_equals_host_and_oracle(emu, view3, it, tier):
+    """fdc_build_bla's level kernel (fdk::bla_level, Block::single / merge, bla.rs:72-112,
+    161-216), run on the host, builds the host builder's table and the oracle's: the same
+    kept levels and every block's seven fields bit for bit."""
+    v, p, plane, t, r = _setup(view3, 64, 36, it, tier=tier)
+    dc, e = fd.bla_dc_bound(v, p)
+    host = fd.Bla.build_scaled(r, fd.route.EPS, dc, e)
+    re, im = np.ascontiguousarray(r.re), np.ascontiguousarray(r.im)
+    out = np.zeros((max(len(re) - 3, 1), 7))
+    levels = emu.emu_bla_build(re.ctypes.data, im.ctypes.data, len(re), fd.route.EPS, dc, e, out.ctypes.data)
+    assert levels == host.levels and (levels > 0 or view3[2] == "1e-14")
+    total = len(host.blocks)
+    assert np.array_equal(out[:total].view(np.uint64), np.asarray(host.blocks).reshape(-1, 7).view(np.uint64))
+    ref = fdref.Ref.arrays(r.re, r.im, r.bits)
+    blocks, offs = fdref.Bla(ref, fd.route.EPS, dc, e).export()
+    assert np.array_equal(out[:total].reshape(-1).view(np.uint64), np.asarray(blocks).reshape(-1).view(np.uint64))
+
+
+def test_device_table_builder_on_the_nucleus_orbit(emu):
+    """The same on configuration 2's orbit (the seeded 1e-100 nucleus, 10^6 points, a
+    999,016-block table over 10 levels) against the host builder."""
+    from fractodactyl_b200 import locations
+    fr = locations.config2()
+    r, bits = fd.reference(fr.view, fr.params)
+    dc, e = fd.bla_dc_bound(fr.view, fr.params)
+    host = fd.Bla.build_scaled(r, fr.bla_eps, dc, e)
+    re, im = np.ascontiguousarray(r.re), np.ascontiguousarray(r.im)
+    out = np.zeros((len(re) - 3, 7))
+    levels = emu.emu_bla_build(re.ctypes.data, im.ctypes.data, len(re), fr.bla_eps, dc, e, out.ctypes.data)
+    assert levels == host.levels
+    total = len(host.blocks)
+    assert total > 900_000
+    assert np.array_equal(out[:total].view(np.uint64), np.asarray(host.blocks).reshape(-1, 7).view(np.uint64))
