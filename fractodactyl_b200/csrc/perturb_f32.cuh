@@ -16,9 +16,13 @@
 
 namespace fdk {
 
-// Resident 128-thread blocks per SM the precision-form kernels are compiled for.
+// Resident 128-thread blocks per SM the precision-form kernels are compiled for. The loop
+// body carries both arithmetics, and instruction fetch bounded it: the rare paths below
+// (delta renormalisation, wide-exponent sums, multiplier rescaling, the block's derivative
+// renormalisation, Newton's cycle prediction) are out-of-line functions, one copy each
+// instead of one per call site, which leaves 126 registers without spills at 4 blocks.
 #ifndef FDK_MIN_BLOCKS_F32
-#define FDK_MIN_BLOCKS_F32 5
+#define FDK_MIN_BLOCKS_F32 4
 #endif
 
 // 32-byte orbit entry of the precision form: Z in f64, Z in f32 (NaN where |Z| < 2^-60),
@@ -47,26 +51,30 @@ struct MulF {
     re = nr;
     im = ni;
     float a = fmaxf(fabsf(re), fabsf(im));
-    if (!(a > 1e-18f && a < 1e18f) && a > 0.0f && isfinite(a)) {
-      int e = ilogbf(a);
-      re = scalbnf(re, -e);
-      im = scalbnf(im, -e);
-      exp += e;
-    }
+    if (!(a > 1e-18f && a < 1e18f) && a > 0.0f && isfinite(a)) *this = renorm(*this, a);
+  }
+  static __device__ __noinline__ MulF renorm(MulF m, float a) {
+    int e = ilogbf(a);
+    m.re = scalbnf(m.re, -e);
+    m.im = scalbnf(m.im, -e);
+    m.exp += e;
+    return m;
   }
   // The same for an FP64 factor of any size (a BLA block's multiplier A can exceed f32's
   // range): scaled by a power of two into [1, 2) before the f32 product, the power carried
   // in the exponent, as Contraction::multiply scales its factors (sample.rs:672-681).
-  __device__ __forceinline__ void multiply_wide(double r, double i) {
+  __device__ __forceinline__ void multiply_wide(double r, double i) { *this = times_wide(*this, r, i); }
+  static __device__ __noinline__ MulF times_wide(MulF m, double r, double i) {
     const double a = fmax(fabs(r), fabs(i));
     if (a == 0.0 || !isfinite(a)) {
-      multiply((float)r, (float)i);
-      return;
+      m.multiply((float)r, (float)i);
+      return m;
     }
     const int k = floor_log2(a);
     const double h = exp2i(-(k / 2)), l = exp2i(-(k - k / 2));
-    multiply((float)(r * h * l), (float)(i * h * l));
-    exp += k;
+    m.multiply((float)(r * h * l), (float)(i * h * l));
+    m.exp += k;
+    return m;
   }
   __device__ __forceinline__ bool below(float lim) const {  // |v|^2 < lim
     return isfinite(re) && isfinite(im) &&
@@ -99,28 +107,49 @@ struct StateF {
 
 // delta = (re, im) 2^k (f64 mantissas, any k) into the f32 form, the exponent kept at or
 // above oe - 64 so that dc 2^-e stays representable.
-__device__ __forceinline__ void set_delta(StateF &s, double re, double im, int64_t k) {
+// The delta's f32 form as set_delta stores it (an out-of-line function: set_delta has
+// several call sites, all rare).
+struct DeltaF {
+  float wr, wi, s32, dcr, dci;
+  int e;
+  double s64;
+};
+
+static __device__ __noinline__ DeltaF make_delta(double re, double im, int64_t k, int oe, double ar, double ai) {
   double a = fmax(fabs(re), fabs(im));
   int64_t e = k;
   if (a != 0.0 && isfinite(a)) e = k + ilogb(a);
-  if (e < (int64_t)s.oe - 64) e = (int64_t)s.oe - 64;
+  if (e < (int64_t)oe - 64) e = (int64_t)oe - 64;
   int64_t sh = k - e;  // re 2^k = (re 2^sh) 2^e, 2^sh applied in two factors
   double f1 = exp2i(sh / 2), f2 = exp2i(sh - sh / 2);
-  s.wr = (float)(re * f1 * f2);
-  s.wi = (float)(im * f1 * f2);
-  s.e = (int)e;
-  s.s32 = exp2f_int(s.e);
-  s.s64 = exp2i(s.e);
-  double g = exp2i((int64_t)s.oe - s.e);
-  s.dcr = (float)(s.ar * g);
-  s.dci = (float)(s.ai * g);
+  DeltaF d;
+  d.wr = (float)(re * f1 * f2);
+  d.wi = (float)(im * f1 * f2);
+  d.e = (int)e;
+  d.s32 = exp2f_int(d.e);
+  d.s64 = exp2i(d.e);
+  double g = exp2i((int64_t)oe - d.e);
+  d.dcr = (float)(ar * g);
+  d.dci = (float)(ai * g);
+  return d;
+}
+
+__device__ __forceinline__ void set_delta(StateF &s, double re, double im, int64_t k) {
+  const DeltaF d = make_delta(re, im, k, s.oe, s.ar, s.ai);
+  s.wr = d.wr;
+  s.wi = d.wi;
+  s.e = d.e;
+  s.s32 = d.s32;
+  s.s64 = d.s64;
+  s.dcr = d.dcr;
+  s.dci = d.dci;
 }
 
 // Sum of two wide-exponent complex terms (as sum2, sample.rs:1094-1114), with a zero
 // term passed over: sum2 scales every term by 2^(e - top), and a zero term whose
 // exponent lies more than 2046 above the other's (an orbit point that is 0 in f64 next
 // to a delta far below f64's range) would give 0 * inf.
-__device__ __forceinline__ Cx3 add3(Cx3 a, Cx3 b) {
+static __device__ __noinline__ Cx3 add3(Cx3 a, Cx3 b) {
   if (a.re == 0.0 && a.im == 0.0) return b;
   if (b.re == 0.0 && b.im == 0.0) return a;
   return sum2(a, b, a.e);
@@ -198,6 +227,22 @@ __device__ __forceinline__ int block_level_f32(const Params &p, const StateF &s,
   return lv;
 }
 
+// dz' = A dz + B with the renormalisations around it (sample.rs:296-323), out of line.
+struct DzF {
+  double dr, di, inverse;
+  int64_t dexp;
+};
+
+static __device__ __noinline__ DzF block_dz(double dr, double di, int64_t dexp, double2 A, double2 B) {
+  normalise(dr, di, dexp, INT64_MAX / 4);
+  double inverse = exp2i(-dexp);
+  double t = A.x * dr - A.y * di + B.x * inverse;
+  di = A.x * di + A.y * dr + B.y * inverse;
+  dr = t;
+  normalise(dr, di, dexp, INT64_MAX / 4);
+  return DzF{dr, di, exp2i(-dexp), dexp};
+}
+
 // delta' = A delta + B dc with wide exponents, dz' = A dz + B in FP64.
 template <bool D>
 __device__ __forceinline__ void apply_block_f32(const Params &p, StateF &s, int lv, uint32_t at) {
@@ -210,13 +255,11 @@ __device__ __forceinline__ void apply_block_f32(const Params &p, StateF &s, int 
   }
   if (s.hold > 0) s.mu.multiply_wide(A.x, A.y);
   if (D) {
-    normalise(s.dr, s.di, s.dexp, INT64_MAX / 4);
-    s.inverse = exp2i(-s.dexp);
-    double t = A.x * s.dr - A.y * s.di + B.x * s.inverse;
-    s.di = A.x * s.di + A.y * s.dr + B.y * s.inverse;
-    s.dr = t;
-    normalise(s.dr, s.di, s.dexp, INT64_MAX / 4);
-    s.inverse = exp2i(-s.dexp);
+    DzF z = block_dz(s.dr, s.di, s.dexp, A, B);
+    s.dr = z.dr;
+    s.di = z.di;
+    s.dexp = z.dexp;
+    s.inverse = z.inverse;
   }
   const double wr = s.wr, wi = s.wi;
   Cx3 ad{A.x * wr - A.y * wi, A.x * wi + A.y * wr, s.e};
@@ -269,6 +312,31 @@ __device__ __forceinline__ void plain_update_f32(StateF &s) {
   }
   s.m += 1;
   s.n += 1;
+}
+
+// Newton's prediction of the cycle's point from a near return (sample.rs:524-552 in FP32),
+// out of line: the prediction, its step, and whether it lands within tolerance of the last.
+struct Newton {
+  float qr, qi, qstep;
+  bool hit;
+};
+
+static __device__ __noinline__ Newton newton(MulF mu, float gr, float gi, float sr, float si, float oqr, float oqi,
+                                             float oqstep, float size) {
+  float sc = mu.exp < -60 ? 0.0f : exp2f_int(mu.exp < 60 ? mu.exp : 60);
+  float mr = mu.re * sc, mi = mu.im * sc;
+  float hr = gr - sr, hi = gi - si;
+  float er = mr - 1.0f, ei = mi;
+  float den = er * er + ei * ei;
+  float qpr = sr - (hr * er + hi * ei) / den;
+  float qpi = si - (hi * er - hr * ei) / den;
+  float tol = fminf(0.1f * sqrtf(den), 1e-2f) * oqstep + 16.0f * 5.96e-8f * size;
+  Newton n;
+  n.hit = fabsf(qpr - oqr) + fabsf(qpi - oqi) <= tol;
+  n.qr = qpr;
+  n.qi = qpi;
+  n.qstep = (fabsf(hr) + fabsf(hi)) / sqrtf(den);
+  return n;
 }
 
 // After the update: next entry, FP64 bailout and rebase test, FP32 periodicity. nz/nr
@@ -368,22 +436,15 @@ __device__ __forceinline__ bool post_f32(const Params &p, const Entry32 *__restr
   if (dist < 1e-3f * size) {
     uint32_t period = s.n - s.sn;
     if (s.hold == period && s.mu.below(1.0f)) {
-      float sc = s.mu.exp < -60 ? 0.0f : exp2f_int(s.mu.exp < 60 ? s.mu.exp : 60);
-      float mr = s.mu.re * sc, mi = s.mu.im * sc;
-      float hr = gr - s.sr, hi = gi - s.si;
-      float er = mr - 1.0f, ei = mi;
-      float den = er * er + ei * ei;
-      float qpr = s.sr - (hr * er + hi * ei) / den;
-      float qpi = s.si - (hi * er - hr * ei) / den;
-      float tol = fminf(0.1f * sqrtf(den), 1e-2f) * s.qstep + 16.0f * 5.96e-8f * size;
-      if (s.predicted && fabsf(qpr - s.qr) + fabsf(qpi - s.qi) <= tol) {
+      const Newton nw = newton(s.mu, gr, gi, s.sr, s.si, s.qr, s.qi, s.qstep, size);
+      if (s.predicted && nw.hit) {
         res.kind = 1;
         res.n = s.n;
         return true;
       }
-      s.qr = qpr;
-      s.qi = qpi;
-      s.qstep = (fabsf(hr) + fabsf(hi)) / sqrtf(den);
+      s.qr = nw.qr;
+      s.qi = nw.qi;
+      s.qstep = nw.qstep;
       s.predicted = true;
     } else {
       s.predicted = false;
