@@ -790,7 +790,8 @@ def run_set(args):
     direct = None
     if rank == 0 and not args.no_cpu and args.direct_samples > 0:
         direct = set_vs_direct(args, cfg, js, sel, frames, loc_of, forms)
-    # e2e through the public API with host buffers, one step: uploads, render(s), columns to host
+    # e2e through the public API with host buffers: uploads, tables built on the device, render(s),
+    # columns to host
     locs = sorted({loc_of(k) for k in sel})  # the orbits and tables this rank uploads
     h2d = sum(16 * len(js.refs[k]) for k in locs)  # orbits; tables are built on the device (fdc_build_bla)
     if cfg == 3:
@@ -807,8 +808,6 @@ def run_set(args):
                 for c in ("cls", "status", "n", "nu", "de", "normal")}
     for a in host_out.values():
         a.fill(0)  # resident, as reused arrays are
-    barrier(world)
-    t0 = time.perf_counter()
     def upload_and_build(k):
         h = dev.upload(js.refs[k])
         if js.blas[k] is not None:
@@ -816,34 +815,51 @@ def run_set(args):
             dev.build_bla(h, t.eps, t.dc_max, t.dc_exp)
         return h
 
-    if cfg == 3:
-        h = upload_and_build(0)
-        j = with_flag(_lib.F32 if head == "fp32_floatexp" else 0)[0]
-        j.orbit = h
-        _, cnt, _ = dev.render_job(j, columns=("nu", "de", "normal"))
-        dev.free(h)
-        eff = cnt.iterations - cnt.blocks + cnt.skipped
-    else:
-        hs = {}
-        jobs = with_flag(_lib.F32 if head == "fp32_floatexp" else 0)
-        for k, j, old in zip(sel, jobs, old_handles):
-            if old not in hs:  # one upload per orbit (a film's frames each hold a table)
-                hs[old] = upload_and_build(loc_of(k))
-            j.orbit = hs[old]
-        b = dev.batch(jobs, columns=("nu", "de", "normal"), groups=groups)
-        cnt, _ = b.run()
-        host, _ = b.all_columns(host_out)
-        b.free()
-        for h in hs.values():
+    host3 = None  # configuration 3's host columns, reused step after step
+
+    def e2e_step():
+        nonlocal host3
+        if cfg == 3:
+            h = upload_and_build(0)
+            j = with_flag(_lib.F32 if head == "fp32_floatexp" else 0)[0]
+            j.orbit = h
+            host3, cnt, _ = dev.render_job(j, columns=("nu", "de", "normal"), host_out=host3)
             dev.free(h)
-        eff = cnt.iterations - cnt.blocks + cnt.skipped
-    e2e_s = allmax(time.perf_counter() - t0, world)
+        else:
+            hs = {}
+            jobs = with_flag(_lib.F32 if head == "fp32_floatexp" else 0)
+            for k, j, old in zip(sel, jobs, old_handles):
+                if old not in hs:  # one upload per orbit (a film's frames each hold a table)
+                    hs[old] = upload_and_build(loc_of(k))
+                j.orbit = hs[old]
+            b = dev.batch(jobs, columns=("nu", "de", "normal"), groups=groups)
+            cnt, _ = b.run()
+            b.all_columns(host_out)
+            b.free()
+            for h in hs.values():
+                dev.free(h)
+        return cnt.iterations - cnt.blocks + cnt.skipped
+
+    # one untimed step (first-use allocations of staging and batch buffers), then timed ones
+    e2e_steps = max(1, min(args.e2e_steps, 3))
+    eff, e2e_s = 0, 0.0
+    for i in range(1 + e2e_steps):
+        barrier(world)
+        t0 = time.perf_counter()
+        e = e2e_step()
+        el = time.perf_counter() - t0
+        if i >= 1:
+            eff += e
+            e2e_s += el
+    e2e_s = allmax(e2e_s, world) / e2e_steps
+    eff //= e2e_steps
     # the same step with the host set-up of its orbits (serial fixed-point work, configurations
     # 4-5's largest cost) added, as a caller computing them per step pays it; the tables are
     # built inside the step
     setup_s = js.orbit_seconds
     e2e = {"value": whole_job(eff) / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-           "steps": 1, "value_with_host_setup": whole_job(eff) / (e2e_s + setup_s), "host_setup_seconds": setup_s,
+           "steps": e2e_steps, "warmup": 1, "value_with_host_setup": whole_job(eff) / (e2e_s + setup_s),
+           "host_setup_seconds": setup_s,
            "tables": "built on the device over the uploaded orbits (fdc_build_bla)"}
     if rank == 0:
         rf = forms.get("fp64_plain", forms[head])
