@@ -1003,11 +1003,11 @@ fdc_status render_impl(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, const fdc
                   {out->z, 16}, {out->dz, 16}, {out->dexp, 8}, {out->status, 1},
                   {bout ? bout->bound : nullptr, 4}, {bout ? bout->ez : nullptr, 8}, {bout ? bout->ed : nullptr, 8},
                   {stripe ? stripe_out : nullptr, 4}};
-  // The BLA kernels outside the bounded and stripe variants store finished samples' raw
-  // state and encode_kernel computes nu / de / normal from it afterwards: class, count,
-  // status, z, dz/dc and its exponent must all exist, as scratch where the caller asked
-  // for none (never copied back; at the outputs' pitch).
-  const bool encode_later = !(j.flags & FDC_F32) && !bounded && !stripe && bla;
+  // The BLA kernels of both forms outside the bounded and stripe variants store finished
+  // samples' raw state and encode_kernel computes nu / de / normal from it afterwards:
+  // class, count, status, z, dz/dc and its exponent must all exist, as scratch where the
+  // caller asked for none (never copied back; at the outputs' pitch).
+  const bool encode_later = !bounded && !stripe && bla;
   bool scratch[NCOL] = {};
   if (encode_later)
     for (int c : {0, 1, 5, 6, 7, 8}) scratch[c] = cols[c].host == nullptr;
@@ -1083,6 +1083,11 @@ fdc_status render_impl(fdc_ctx *ctx, const fdc_job *job, fdc_out *out, const fdc
   if (j.flags & FDC_F32) {
     CK(fdk::launch_f32(p, o.z32, deriv, bla, ctx->sm_count, (int)ctx->tune.blocks_per_sm, ctx->stream,
                        ctx->blocks_per_sm_f32));
+    if (encode_later && (p.nu || p.de || p.normal)) {
+      fdk::encode_kernel<0><<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(p);
+      CK(cudaGetLastError());
+      launches += 1;
+    }
   } else {
     int variant = 0;
     void *fn = pick_kernel(ext, deriv, bla, p.series_n > 0, bounded, variant, stripe != nullptr);

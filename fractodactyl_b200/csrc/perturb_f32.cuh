@@ -600,8 +600,10 @@ __global__ void __launch_bounds__(128, FDK_MIN_BLOCKS_F32) perturb_f32_kernel(Pa
   bool active = false, exhausted = false;
   uint64_t t0 = p.deadline_ns ? globaltimer() : 0;
   unsigned long long n_samples = 0, iters = 0, blocks = 0, skipped = 0, fallback = 0, closed = 0;
+  // the BLA variants store a finished sample's raw state; encode_kernel computes its nu, de
+  // and normal afterwards with full warps (the column code stays out of this loop)
   auto finish = [&](uint32_t idx, const Result &r, uint64_t nblocks, uint64_t nskipped) {
-    put(p, idx, r);
+    put<false, false, L>(p, idx, r);
     uint64_t spent = r.kind == 2 ? p.max_iter : r.n;
     if (L) {
       spent = spent - nskipped + nblocks;

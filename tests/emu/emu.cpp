@@ -356,7 +356,7 @@ int emu_render_window(const double *re, const double *im, uint64_t len, const do
     if (d) bla ? launch<false, true, true, false, false>(p) : launch<false, true, false, false, false>(p);
     else bla ? launch<false, false, true, false, false>(p) : launch<false, false, false, false, false>(p);
   }
-  if (!f32 && !bounded && !striped && bla) {  // the columns from the raw state, as fdc_render does
+  if (!bounded && !striped && bla) {  // the columns from the raw state, as fdc_render does
     threadIdx.x = 0;
     blockIdx.x = 0;
     fdk::encode_kernel<0>(p);
