@@ -15,9 +15,10 @@ constexpr int MAX_LEVELS = 40;
 
 // Resident 128-thread blocks per SM each kernel variant is compiled for (caps registers
 // at 65536 / (128 * blocks)): floatexp-tier variants (EXT) and ordinary-tier variants;
-// chosen by measurement.
+// chosen by measurement (5 floatexp blocks at 96 registers: the 1920x1080 frame at a 1e-100
+// nucleus, 10^6 iterations, 37.95 -> 37.53 ms).
 #ifndef FDK_MIN_BLOCKS_EXT
-#define FDK_MIN_BLOCKS_EXT 4
+#define FDK_MIN_BLOCKS_EXT 5
 #endif
 #ifndef FDK_MIN_BLOCKS_FIX
 #define FDK_MIN_BLOCKS_FIX 4
@@ -1168,9 +1169,10 @@ struct TraceSlot<true> {
 };
 
 // The BLA variants outside B and T store finished samples' raw state only (put's R: every
-// raw pointer present) and encode_kernel fills nu, de and normal afterwards (measured:
-// config 2 40.1 -> 39.2 ms, its fixed-tier variant 35.7 -> 33.8 ms; without BLA, config 1's
-// short frame ran 3% slower, so the plain variants encode as they finish).
+// raw pointer present) and encode_kernel fills nu, de and normal afterwards (measured on the
+// 1920x1080 frame at a 1e-100 nucleus: 40.1 -> 39.2 ms, its fixed-tier variant 35.7 -> 33.8
+// ms; without BLA the 480x270 1e-12 frame ran 3% slower, so those variants encode as they
+// finish).
 template <bool EXT, bool D, bool L, bool S = false, bool B = false, bool T = false>
 __global__ void __launch_bounds__(128, Occupancy<EXT>::blocks) perturb_kernel(Params p) {
   const unsigned FULL = 0xffffffffu;
