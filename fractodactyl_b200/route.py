@@ -348,7 +348,6 @@ class Device:
         if st != _lib.OK:
             raise RouteError(f"fdc_open({index}): {_lib.STATUS_NAMES.get(st, st)}")
         self.index = index
-        self._orbits = {}
         self._orbit_len = {}  # handle -> points, for build_bla's export size
 
     def close(self):
@@ -402,6 +401,7 @@ class Device:
     def free(self, orbit: int):
         """fdc_free_orbit; refused (RouteError) while a live batch reads the orbit."""
         _check(lib().fdc_free_orbit(self.h, orbit), self, "free orbit")
+        self._orbit_len.pop(orbit, None)
 
     def upload_error_radius(self, orbit: int, q: np.ndarray):
         """fdc_upload_error_radius: the orbit's error radii for bounded renders."""
