@@ -136,6 +136,13 @@ struct Contraction {
     exp = 0;
     started = false;
   }
+  // (r, i) 2^-k with k = floor(log2 max(|r|, |i|)) (0 for a non-finite a), and k: the
+  // rescaling of multiply, out of line (one copy for its two uses and their call sites)
+  static __device__ __noinline__ Cx3 scaled(double r, double i, double a) {
+    int64_t k = isfinite(a) ? floor_log2(a) : 0;
+    double s = exp2i(-k);
+    return Cx3{r * s, i * s, k};
+  }
   __device__ __forceinline__ void multiply(double r, double i) {
     if (!started) {
       re = 1.0;
@@ -144,11 +151,10 @@ struct Contraction {
     int64_t e = 0;
     double a = rmax(fabs(r), fabs(i));
     if (a != 0.0 && !(LO <= a && a <= HI)) {
-      int64_t k = isfinite(a) ? floor_log2(a) : 0;
-      double s = exp2i(-k);
-      r *= s;
-      i *= s;
-      e += k;
+      const Cx3 t = scaled(r, i, a);
+      r = t.re;
+      i = t.im;
+      e += t.e;
     }
     double nr = re * r - im * i, ni = re * i + im * r;
     re = nr;
@@ -156,11 +162,10 @@ struct Contraction {
     exp += e;
     a = rmax(fabs(re), fabs(im));
     if (a != 0.0 && !(LO <= a && a <= HI)) {
-      int64_t k = isfinite(a) ? floor_log2(a) : 0;
-      double s = exp2i(-k);
-      re *= s;
-      im *= s;
-      exp += k;
+      const Cx3 t = scaled(re, im, a);
+      re = t.re;
+      im = t.im;
+      exp += t.e;
     }
   }
   __device__ __forceinline__ bool small() const {
