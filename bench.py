@@ -449,9 +449,14 @@ def run_ours(args):
     # the render and the host columns (D2H); and the same with the host-built table uploaded
     h2d = 16 * len(r)
     h2d_host_table = h2d + (56 * len(bla.blocks) if bla is not None else 0)
-    d2h = n * sum(OUT_BYTES[c] for c in cols)
+    # the caller's host columns, reused frame after frame: the reference's Samples (class and
+    # the requested nu / de / normal, fd-samples samples.rs:8-20) and the status byte that the
+    # route's shim reads
+    host_cols = {c: np.zeros(n, dt) for c, dt in (("cls", np.uint8), ("status", np.uint8), ("nu", np.float64),
+                                                  ("de", np.float32), ("normal", np.uint16))
+                 if c in ("cls", "status") or c in p.columns}
+    d2h = n * sum(OUT_BYTES[c] for c in host_cols)
     dev.free(handle)
-    host_cols = None  # the caller's host columns, reused frame after frame
 
     def e2e_run(device_table):
         nonlocal host_cols
