@@ -153,6 +153,8 @@ static int grid_blocks(const fdc_ctx *ctx, int occupancy) {
 struct fdc_batch {
   struct Group {
     bool f32, ext, deriv, bla;
+    bool encode = false;      // BLA group with columns to encode after its kernel
+    uint64_t max_window = 0;  // samples of its largest job window
     std::vector<uint32_t> order;  // original job index of each position
     fdk::Params *jobs = nullptr;
     unsigned long long *starts = nullptr;
@@ -164,6 +166,8 @@ struct fdc_batch {
   uint32_t njobs = 0;
   fdk::Counters *counters = nullptr;   // njobs, in group order
   unsigned long long *queues = nullptr;  // one per group
+  void *raw = nullptr;  // raw-state scratch of BLA jobs the caller gave no z / dz / ... column
+  size_t raw_bytes = 0;  // (from the context's pool, returned to it by fdc_batch_free)
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
 };
@@ -369,6 +373,7 @@ void free_batch(fdc_batch *b) {
   }
   cudaFree(b->counters);
   cudaFree(b->queues);
+  cudaFree(b->raw);
   delete b;
 }
 
@@ -1231,6 +1236,53 @@ fdc_status fdc_batch_create(fdc_ctx *ctx, const fdc_job *jobs, const fdc_out *ou
   }
   fdc_batch *b = new fdc_batch;
   b->njobs = njobs;
+  // The BLA kernels store a finished sample's raw state (class, count, status, z, dz/dc, its
+  // exponent) and encode_jobs_kernel computes nu / de / normal afterwards: columns the caller
+  // did not ask for get scratch at the job's output pitch (one allocation for the batch).
+  {
+    struct Need {
+      uint32_t k;
+      int col;
+      size_t bytes;
+    };
+    std::vector<Need> need;
+    size_t total_bytes = 0;
+    for (uint32_t k = 0; k < njobs; ++k) {
+      if (!(jobs[k].flags & FDC_BLA)) continue;
+      const fdk::Params &p = params[k];
+      if (p.rows == 0 || p.cols == 0) continue;
+      const uint64_t span = (uint64_t)(p.rows - 1) * p.out_pitch + p.cols;
+      const void *have[6] = {p.cls, p.n_out, p.status, p.z_out, p.dz_out, p.dexp_out};
+      const size_t width[6] = {1, 4, 1, 16, 16, 8};
+      for (int c = 0; c < 6; ++c)
+        if (!have[c]) {
+          need.push_back({k, c, (size_t)((span * width[c] + 255) & ~(uint64_t)255)});
+          total_bytes += need.back().bytes;
+        }
+    }
+    if (total_bytes) {
+      // from the context's pool: a film or tile service creating a batch per step reuses it
+      b->raw = pool_get(ctx, total_bytes);
+      if (!b->raw) {
+        free_batch(b);
+        return fail(ctx, FDC_DEVICE_ERROR, "device memory for the batch's raw-state scratch");
+      }
+      b->raw_bytes = total_bytes;
+      char *at = (char *)b->raw;
+      for (const Need &n : need) {
+        fdk::Params &p = params[n.k];
+        switch (n.col) {
+          case 0: p.cls = (uint8_t *)at; break;
+          case 1: p.n_out = (uint32_t *)at; break;
+          case 2: p.status = (uint8_t *)at; break;
+          case 3: p.z_out = (double2 *)at; break;
+          case 4: p.dz_out = (double2 *)at; break;
+          default: p.dexp_out = (int64_t *)at; break;
+        }
+        at += n.bytes;
+      }
+    }
+  }
   // group by kernel variant; within a group the deepest jobs first (their samples run
   // longest, so starting them first shortens the tail of the launch)
   std::map<int, std::vector<uint32_t>> by;
@@ -1256,6 +1308,9 @@ fdc_status fdc_batch_create(fdc_ctx *ctx, const fdc_job *jobs, const fdc_out *ou
       starts.push_back(total);
       gp.push_back(params[k]);
       total += params[k].total;
+      const fdk::Params &p = params[k];
+      if (g.bla && (p.nu || p.de || p.normal)) g.encode = true;
+      g.max_window = std::max<uint64_t>(g.max_window, (uint64_t)p.rows * p.cols);
     }
     starts.push_back(total);
     g.total = total;
@@ -1308,6 +1363,13 @@ fdc_status fdc_batch_create(fdc_ctx *ctx, const fdc_job *jobs, const fdc_out *ou
       e = cudaLaunchKernel(fn, dim3(grid_blocks(ctx, ctx->blocks_per_sm_batch[variant])), dim3(128), args, 0,
                            ctx->stream);
     }
+    if (e == cudaSuccess && g.encode) {  // the group's columns from the raw state
+      const unsigned per_job = std::max(1u, (unsigned)std::min<uint64_t>((g.max_window + 255) / 256, 64));
+      for (uint32_t off = 0; off < n && e == cudaSuccess; off += 65535u) {  // grid.y <= 65535
+        fdk::encode_jobs_kernel<0><<<dim3(per_job, std::min(n - off, 65535u)), 256, 0, ctx->stream>>>(g.jobs + off);
+        e = cudaGetLastError();
+      }
+    }
   }
   cudaError_t e2 = cudaStreamEndCapture(ctx->stream, &b->graph);
   if (e == cudaSuccess) e = e2;
@@ -1353,7 +1415,9 @@ fdc_status fdc_batch_run(fdc_ctx *ctx, fdc_batch *b, fdc_counters *total, fdc_co
       sum.closed_form_samples += one.closed_form_samples;
     }
   sum.kernel_ms = ms;
-  sum.launches = (uint32_t)b->groups.size();
+  sum.launches = 0;
+  for (auto &g : b->groups)
+    sum.launches += 1u + (g.encode ? ((uint32_t)g.order.size() + 65534u) / 65535u : 0u);
   if (total) *total = sum;
   return FDC_OK;
 }
@@ -1362,11 +1426,14 @@ void fdc_batch_free(fdc_ctx *ctx, fdc_batch *b) {
   if (ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
-    if (b)
+    if (b) {
       for (int32_t h : b->orbits) {
         auto it = ctx->orbits.find(h);
         if (it != ctx->orbits.end() && it->second.batch_refs) --it->second.batch_refs;
       }
+      pool_put(ctx, b->raw, b->raw_bytes);  // the stream is idle: the next user may take it
+      b->raw = nullptr;
+    }
   }
   free_batch(b);
 }

@@ -693,8 +693,9 @@ __global__ void __launch_bounds__(128, FDK_MIN_BLOCKS_F32)
   uint32_t job = 0, counted = 0xffffffffu;
   LaneCounters lc;
   lc.clear();
+  // as the plain batch kernel: the BLA variants store raw state for encode_jobs_kernel
   auto finish = [&](const Params &p, uint32_t idx, const Result &r, uint64_t nblocks, uint64_t nskipped) {
-    put(p, idx, r);
+    put<false, false, L>(p, idx, r);
     if (counted != job) {
       if (counted != 0xffffffffu) lc.flush(per_job + counted);
       counted = job;

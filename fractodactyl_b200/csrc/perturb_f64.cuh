@@ -1130,12 +1130,11 @@ __device__ __forceinline__ void put(const Params &p, uint32_t sample, const Resu
 }
 
 // The columns of the escaped samples of a window whose persistent kernel stored only their
-// raw state (put with R): one thread per sample, the same expressions as put. (A template,
-// so that every translation unit including this header may hold it.)
-template <int V = 0>
-__global__ void encode_kernel(Params p) {
+// raw state (put with R), samples t = start, start + stride, ... of the window: the same
+// expressions as put.
+__device__ __forceinline__ void encode_window(const Params &p, uint64_t start, uint64_t stride) {
   const uint64_t total = (uint64_t)p.rows * p.cols;
-  for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (uint64_t)gridDim.x * blockDim.x) {
+  for (uint64_t t = start; t < total; t += stride) {
     const uint64_t jj = t / p.cols, ii = t - jj * p.cols;
     const uint64_t idx = jj * p.out_pitch + ii;
     if (!p.status[idx] || p.cls[idx] != 0) continue;
@@ -1151,6 +1150,21 @@ __global__ void encode_kernel(Params p) {
     const double z2 = r.zr * r.zr + r.zi * r.zi;
     encode_columns(p, idx, r, z2, 0.5 * log2(z2), false, 0.0);
   }
+}
+
+// One thread per sample of a frame job's window. (Templates, so that every translation unit
+// including this header may hold them.)
+template <int V = 0>
+__global__ void encode_kernel(Params p) {
+  encode_window(p, (uint64_t)blockIdx.x * blockDim.x + threadIdx.x, (uint64_t)gridDim.x * blockDim.x);
+}
+
+// The same for the jobs of a batch group after its persistent kernel: job blockIdx.y.
+template <int V = 0>
+__global__ void encode_jobs_kernel(const Params *__restrict__ jobs) {
+  const Params &p = jobs[blockIdx.y];
+  if (!(p.nu || p.de || p.normal)) return;
+  encode_window(p, (uint64_t)blockIdx.x * blockDim.x + threadIdx.x, (uint64_t)gridDim.x * blockDim.x);
 }
 
 // S: the series-start variant (ordinary tiers, jobs with an admitted series); the others
@@ -1336,8 +1350,10 @@ __global__ void __launch_bounds__(128, Occupancy<EXT>::blocks)
   Reservation slots;
   LaneCounters lc;
   lc.clear();
+  // the BLA variants store a finished sample's raw state; encode_jobs_kernel computes the
+  // columns afterwards (every raw pointer present: fdc_batch_create provides scratch)
   auto finish = [&](const Params &p, uint32_t idx, const Result &r, uint64_t nblocks, uint64_t nskipped) {
-    put(p, idx, r);
+    put<false, false, L>(p, idx, r);
     if (counted != job) {
       if (counted != 0xffffffffu) lc.flush(per_job + counted);
       counted = job;

@@ -119,8 +119,8 @@ fdc_status fdc_upload_bla(fdc_ctx *ctx, int32_t orbit, const double *blocks7, co
                           uint32_t levels, double eps, double dc_max, int64_t dc_exp);
 
 /* Build that table on the device from the uploaded orbit instead of uploading it:
- * Bla::build_scaled(reference, eps, dc_max, dc_exp) (bla.rs:161-216, called by
- * frame.rs:119-140 before pack_bla), with the same blocks bit for bit and the same refusals
+ * Bla::build_scaled(reference, eps, dc_max, dc_exp) (bla.rs:161-216, which control.rs:359
+ * and film.rs:1321 call before rendering), with the same blocks bit for bit and the same refusals
  * as fdc_upload_bla. *levels (optional) receives the kept level count; export7 (optional,
  * host memory for len - 3 blocks) receives the kept levels in the export form above,
  * level i at offset sum_{j<i} (len - 2) >> (j + 1). Replaces the host build and the
@@ -210,10 +210,13 @@ fdc_status fdc_get_tuning(const fdc_ctx *ctx, fdc_tuning *tuning);
  * kernel variant from a single work queue over all jobs' tiles, deepest jobs first, the
  * whole run captured once in a CUDA graph and replayed by fdc_batch_run. Results equal
  * fdc_render's per job. Jobs need FDC_DEVICE_OUT, no mask/offsets/deadline/FDC_SERIES; orbits and
- * tables must stay uploaded while the batch exists: fdc_free_orbit and fdc_upload_bla refuse
- * (FDC_INVALID) an orbit that a live batch reads, until fdc_batch_free. Free batches before
- * fdc_close. per_job (optional) has njobs
- * entries; counters->kernel_ms is the device time of the whole replay. */
+ * tables must stay uploaded while the batch exists: fdc_free_orbit, fdc_upload_bla and
+ * fdc_build_bla refuse (FDC_INVALID) an orbit that a live batch reads, until fdc_batch_free.
+ * Free batches before fdc_close. BLA jobs store each finished sample's raw state (class,
+ * count, status, z, dz/dc, its exponent) and a second kernel per group encodes nu / de /
+ * normal from it: the batch holds device scratch for those the job's fdc_out leaves null
+ * (up to 46 bytes per sample of the window's rows at the output pitch). per_job (optional)
+ * has njobs entries; counters->kernel_ms is the device time of the whole replay. */
 typedef struct fdc_batch fdc_batch;
 fdc_status fdc_batch_create(fdc_ctx *ctx, const fdc_job *jobs, const fdc_out *outs, uint32_t njobs,
                             fdc_batch **batch);

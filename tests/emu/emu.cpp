@@ -82,6 +82,11 @@ struct Setup {
   std::vector<uint32_t> order;
   fdk::Params p{};
   bool ext = false, deriv = false, bla = false;
+  // raw-state scratch of a batch BLA job without those outputs (as fdc_batch_create gives)
+  std::vector<uint8_t> raw_cls, raw_status;
+  std::vector<uint32_t> raw_n;
+  std::vector<double2> raw_z, raw_dz;
+  std::vector<int64_t> raw_dexp;
 };
 
 template <bool EXT, bool D, bool L, bool S, bool B, bool T = false>
@@ -398,6 +403,16 @@ int emu_render_batch(EmuJob *jobs, uint32_t njobs) {
                      false))
       return -1;
     stage_outputs(s->p, j.cls, j.n, j.nu, j.de, j.normal, j.z, j.dz, j.dexp, j.status);
+    if (s->bla && s->p.rows && s->p.cols) {  // the BLA batch kernels store raw state: scratch where absent
+      fdk::Params &p = s->p;
+      const size_t span = (size_t)(p.rows - 1) * p.out_pitch + p.cols;
+      if (!p.cls) p.cls = (s->raw_cls.assign(span, 0), s->raw_cls.data());
+      if (!p.status) p.status = (s->raw_status.assign(span, 0), s->raw_status.data());
+      if (!p.n_out) p.n_out = (s->raw_n.assign(span, 0), s->raw_n.data());
+      if (!p.z_out) p.z_out = (s->raw_z.assign(span, double2{0, 0}), s->raw_z.data());
+      if (!p.dz_out) p.dz_out = (s->raw_dz.assign(span, double2{0, 0}), s->raw_dz.data());
+      if (!p.dexp_out) p.dexp_out = (s->raw_dexp.assign(span, 0), s->raw_dexp.data());
+    }
     by[((j.flags & 4) ? 8 : 0) | (s->ext ? 4 : 0) | (s->deriv ? 2 : 0) | (s->bla ? 1 : 0)].push_back(k);
     setups[k] = std::move(s);
   }
@@ -432,6 +447,9 @@ int emu_render_batch(EmuJob *jobs, uint32_t njobs) {
       else l ? launch_batch<false, false, true>(gp, starts, cnt.data(), defer)
              : launch_batch<false, false, false>(gp, starts, cnt.data(), defer);
     }
+    if (l)  // the columns from the raw state, as fdc_batch_create's encode pass does
+      for (const fdk::Params &p : gp)
+        if (p.nu || p.de || p.normal) fdk::encode_window(p, 0, 1);
     for (size_t i = 0; i < order.size(); ++i) copy_counters(cnt[i], jobs[order[i]].counters);
   }
   return 0;
