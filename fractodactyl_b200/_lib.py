@@ -113,7 +113,7 @@ FDC_SYMBOLS = ["fdc_abi_version", "fdc_open", "fdc_close", "fdc_last_error", "fd
                "fdc_render_noalloc", "fdc_set_tuning", "fdc_get_tuning"]
 FDH_SYMBOLS = ["fdh_last_error", "fdh_plane_new", "fdh_orbit_fixed", "fdh_orbit_fixed_threads", "fdh_orbit_f64",
                "fdh_nucleus_period",
-               "fdh_bla_build", "fdh_bla_build_into", "fdh_series_build", "fdh_error_radius", "fdh_dc_bound", "fdh_encode", "fdh_location"]
+               "fdh_bla_build", "fdh_bla_build_into", "fdh_guarded_bla_build", "fdh_external_escape_ok", "fdh_series_build", "fdh_error_radius", "fdh_dc_bound", "fdh_encode", "fdh_location"]
 
 _lib = None
 
@@ -165,6 +165,10 @@ def lib():
     L.fdh_series_build.argtypes = [P, P, U64, D, D, U64, U64, C.POINTER(SeriesInfo), P, U32]
     L.fdh_bla_build_into.restype = C.c_int
     L.fdh_bla_build_into.argtypes = [P, P, U64, D, D, I64, C.c_int, P, U64, P, U32, C.POINTER(U32), C.POINTER(U64)]
+    L.fdh_guarded_bla_build.restype = C.c_int
+    L.fdh_guarded_bla_build.argtypes = [P, P, P, U64, D, D, P, U64, P, U32, C.POINTER(U32), C.POINTER(U64)]
+    L.fdh_external_escape_ok.restype = C.c_int
+    L.fdh_external_escape_ok.argtypes = [U64, D, D, D, D, I64, D, D, D, I64]
     L.fdh_encode.argtypes = [C.POINTER(Plane), U32, U64, P, P, P, P, P, P, P, P, C.c_int]
     L.fdh_dc_bound.argtypes = [C.POINTER(Plane), I32, U32, U32, C.POINTER(D), C.POINTER(I64)]
     L.fdh_location.argtypes = [C.c_char_p, C.c_char_p, D, D, U64, U64, C.c_char_p, C.c_char_p, C.c_size_t,

@@ -565,6 +565,57 @@ Fix fe_to_fix(double m, int64_t e, size_t L) {
 
 }  // namespace
 
+// ------------------------------------------------------------------------------------
+// Guarded BLA (crates/fd-kernel/src/bla/guarded.rs:1-134): the BLA blocks with the
+// affine uncertainty envelopes of the approximate GPU route's admission (alpha / beta on
+// the state, derivative alpha / beta on dz/dc), built over the same reference with the
+// reference's radii q[k]. Stored as [f64; 9]: the block's seven fields, then the two
+// derivative envelopes.
+struct GBlk {
+  Blk b;
+  double da, db;
+};
+
+inline double l1(double re, double im) { return std::fabs(re) + std::fabs(im); }  // guarded.rs:8-10
+inline double up(double x) {  // guarded.rs:11-13
+  return x * (1.0 + 64.0 * std::numeric_limits<double>::epsilon()) + std::numeric_limits<double>::min();
+}
+
+inline GBlk gblk_single(double zr, double zi, double q, double eps) {  // guarded.rs:35-50
+  Blk b = blk_single(zr, zi, eps);
+  if (b.r == 0.0 || !std::isfinite(q) || q < 0.0 || l1(zr, zi) + q > 2.0) return GBlk{};
+  const double da = up(2.0 * b.r + 2.0 * q);
+  b.alpha = up(b.r + 2.0 * q);
+  return GBlk{b, da, 0.0};
+}
+
+inline GBlk gblk_merge(const GBlk &gx, const GBlk &gy, double c) {  // guarded.rs:51-98
+  const Blk &x = gx.b, &y = gy.b;
+  if (x.r == 0.0 || y.r == 0.0) return GBlk{};
+  const double eps64 = std::numeric_limits<double>::epsilon();
+  const double ax = l1(x.ar, x.ai), ay = l1(y.ar, y.ai), bx = l1(x.br, x.bi);
+  const double r = fmin_rust(x.r, (y.r - up((bx + x.beta) * c)) / up(ax + x.alpha)) * (1.0 - 64.0 * eps64);
+  GBlk z;
+  z.b.ar = y.ar * x.ar - y.ai * x.ai + 0.0 + 0.0;  // affine(x.a, y.a, 0) (bla.rs:124-129)
+  z.b.ai = y.ar * x.ai + y.ai * x.ar + 0.0 + 0.0;
+  z.b.br = y.ar * x.br - y.ai * x.bi + y.br + 0.0;  // affine(x.b, y.a, y.b)
+  z.b.bi = y.ar * x.bi + y.ai * x.br + y.bi + 0.0;
+  z.b.r = r;
+  const double ra = up(32.0 * eps64 * ay * ax);
+  const double rb = up(32.0 * eps64 * (ay * bx + l1(y.br, y.bi)));
+  // remainder(ay, ax, bx, xa, xb, ya, yb) (guarded.rs:14-19) for the state and derivative
+  auto rem_a = [&](double xa, double ya) { return up(ay * xa + ya * (ax + xa)); };
+  auto rem_b = [&](double xb, double ya, double yb) { return up(ay * xb + ya * (bx + xb) + yb); };
+  z.b.alpha = up(rem_a(x.alpha, y.alpha) + ra);
+  z.b.beta = up(rem_b(x.beta, y.alpha, y.beta) + rb);
+  z.da = up(rem_a(gx.da, gy.da) + ra);
+  z.db = up(rem_b(gx.db, gy.da, gy.db) + rb);
+  const double v[9] = {z.b.ar, z.b.ai, z.b.br, z.b.bi, z.b.r, z.b.alpha, z.b.beta, z.da, z.db};
+  bool fin = true;
+  for (double t : v) fin = fin && std::isfinite(t);
+  return (r > 0.0 && fin) ? z : GBlk{};
+}
+
 extern "C" {
 
 const char *fdh_last_error(void) { return g_err.c_str(); }
@@ -706,6 +757,99 @@ int fdh_bla_build_into(const double *re, const double *im, uint64_t len, double 
   }
   bla_offsets(len, lv, level_offsets);
   return 0;
+}
+
+// GuardedBla::build (guarded.rs:110-134): singles over Z_1..Z_{len-2} with their radii
+// q, pairwise merges level by level, the levels kept up to the first without a valid block;
+// level-major [f64; 9] blocks (level i: (len - 2) >> (i + 1) of them).
+int fdh_guarded_bla_build(const double *re, const double *im, const double *q, uint64_t len, double eps,
+                          double dc_max, double *blocks9, uint64_t cap_blocks, uint64_t *level_offsets,
+                          uint32_t cap_levels, uint32_t *levels, uint64_t *blocks) {
+  if (!(eps > 0.0 && eps <= 1.0 / (double)(1u << 24) && dc_max > 0.0 && std::isfinite(dc_max))) {
+    g_err = "BLA needs 0 < eps <= 2^-24 and a finite dc_max > 0";
+    return -1;
+  }
+  if (!re || !im || !q || !levels || !blocks || !level_offsets) {
+    g_err = "null guarded BLA argument";
+    return -1;
+  }
+  for (uint64_t k = 0; k < len; ++k)
+    if (!std::isfinite(q[k]) || q[k] < 0.0) {
+      g_err = "guarded BLA needs one finite nonnegative reference radius per point";
+      return -1;
+    }
+  std::vector<GBlk> next;
+  for (uint64_t k = 1; k + 1 < len; ++k) next.push_back(gblk_single(re[k], im[k], q[k], eps));
+  uint32_t lv = 0;
+  uint64_t total = 0;
+  std::vector<GBlk> kept;
+  std::vector<uint64_t> offs;
+  for (;;) {
+    std::vector<GBlk> merged(next.size() / 2);
+    bool any = false;
+    for (size_t t = 0; t < merged.size(); ++t) {
+      merged[t] = gblk_merge(next[2 * t], next[2 * t + 1], dc_max);
+      any = any || merged[t].b.r > 0.0;
+    }
+    next.swap(merged);
+    if (!any) break;
+    offs.push_back(total);
+    kept.insert(kept.end(), next.begin(), next.end());
+    total += next.size();
+    ++lv;
+  }
+  *levels = lv;
+  *blocks = total;
+  if (total > cap_blocks || lv + 1 > cap_levels || (total && !blocks9)) {
+    g_err = "guarded BLA table larger than the buffers given";
+    return -1;
+  }
+  for (uint64_t t = 0; t < total; ++t) {
+    const GBlk &g = kept[t];
+    const double v[9] = {g.b.ar, g.b.ai, g.b.br, g.b.bi, g.b.r, g.b.alpha, g.b.beta, g.da, g.db};
+    std::memcpy(blocks9 + 9 * t, v, sizeof v);
+  }
+  for (uint32_t i = 0; i < lv; ++i) level_offsets[i] = offs[i];
+  level_offsets[lv] = total;
+  return 0;
+}
+
+// external_escape_ok (crates/fd-kernel/src/store.rs:152-198): whether an externally
+// computed escaped state (n, z, dz/dc = (dr, di) 2^dexp) with error radii ez (z units)
+// and ed (derivative-mantissa units) encodes within half the comparison budget (1e-3 px,
+// 0.2% DE, 0.2 degrees) for the output pixel px_m 2^px_e; the Bounded evidence of
+// store.rs:115-151 and de_px of store.rs:153-160, with the host's libm. 1 or 0.
+int fdh_external_escape_ok(uint64_t n, double zr, double zi, double dr, double di, int64_t dexp, double ez, double ed,
+                           double px_m, int64_t px_e) {
+  const double U = std::numeric_limits<double>::epsilon() / 2.0;
+  const double LN_2 = 0.693147180559945309417232121458176568;
+  const double TAU = 6.28318530717958647692528676655900577;
+  const double az = std::hypot(zr, zi), ad = std::hypot(dr, di);
+  if (!(ez >= 0.0 && ed >= 0.0 && std::isfinite(ez) && std::isfinite(ed) && std::isfinite(az) && std::isfinite(ad)))
+    return 0;
+  // bounds (store.rs:115-151)
+  const double lo = az - ez;
+  if (!(lo > 2.0 && ed < 0.5 * ad)) return 0;
+  const double lnz = std::log(az), llo = std::log(lo), lhi = std::log(az + ez);
+  const double nu = std::log1p(-std::log1p(-ez / az) / llo) / LN_2 + 8.0 * U * ((double)n + 8.0);
+  const double g = lhi * std::exp2(-(double)n);
+  const double de_lo0 = (lo * llo) / (az * lnz) * ad / (ad + ed) * std::exp(-g) * (1.0 - 4.0 / (lo * lo)) * (1.0 - 1e-6);
+  const double de_hi0 = ((az + ez) * lhi) / (az * lnz) * ad / (ad - ed) * (1.0 + 1e-6);
+  const double blo = de_lo0, bound = nu * de_hi0 / de_lo0 * (1.0 + 1e-6);
+  // de_px (store.rs:153-160) at log2 |z|
+  const double lnz2 = std::log2(az) * LN_2;
+  const double base0 = 2.0 * az * lnz2 / (std::hypot(dr, di) * px_m);
+  int64_t kk = -(dexp + px_e);
+  kk = std::max<int64_t>(-4000, std::min<int64_t>(4000, kk));
+  const double de = (double)(float)(base0 * exp2i(kk / 2) * exp2i(kk - kk / 2));
+  const double displacement = bound * de * blo * LN_2 / 2.0;
+  const double base = az * std::log(az);
+  const double de_hi = (az + ez) * std::log(az + ez) / base * ad / (ad - ed);
+  const double de_lo = (az - ez) * std::log(az - ez) / base * ad / (ad + ed);
+  const double angle = std::asin(ez / az) + std::asin(ed / ad);
+  const double f32eps = (double)std::numeric_limits<float>::epsilon();
+  return std::isfinite(displacement) && displacement <= 5e-4 && std::isfinite(de) && de_hi - 1.0 + f32eps <= 1e-3 &&
+         1.0 - de_lo + f32eps <= 1e-3 && angle + TAU / 65536.0 <= 0.1 * (TAU / 360.0);
 }
 
 // Reference::error_radius (crates/fd-kernel/src/reference.rs:122-148): bounds

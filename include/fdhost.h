@@ -69,6 +69,25 @@ int fdh_bla_build_into(const double *re, const double *im, uint64_t len, double 
                        int threads, double *blocks7, uint64_t cap_blocks, uint64_t *level_offsets, uint32_t cap_levels,
                        uint32_t *levels, uint64_t *blocks);
 
+/* GuardedBla::build (crates/fd-kernel/src/bla/guarded.rs:110-134): the BLA blocks with
+ * the affine uncertainty envelopes that the reference's approximate GPU route admits its
+ * results by, over the orbit and its reference radii q[len] (Reference::error_radius):
+ * level-major [f64; 9] blocks (a.re, a.im, b.re, b.im, r, alpha, beta, derivative alpha,
+ * derivative beta), level i at blocks9[9 * level_offsets[i]...], levels + 1 offsets. The
+ * CUDA route runs the reference's algorithm exactly and needs no admission; this serves
+ * callers that keep the reference's guarded route. Refusals: bla.rs:27-33, a radius that
+ * is negative or not finite. */
+int fdh_guarded_bla_build(const double *re, const double *im, const double *q, uint64_t len, double eps,
+                          double dc_max, double *blocks9, uint64_t cap_blocks, uint64_t *level_offsets,
+                          uint32_t cap_levels, uint32_t *levels, uint64_t *blocks);
+
+/* external_escape_ok (crates/fd-kernel/src/store.rs:152-198): 1 when an externally
+ * computed escaped state (n, z, dz/dc = (dr, di) 2^dexp) with error radii ez on z and ed on
+ * the derivative mantissa encodes within half the comparison budget for the output pixel
+ * px_m 2^px_e (host libm, as the reference's Rust); 0 otherwise. */
+int fdh_external_escape_ok(uint64_t n, double zr, double zi, double dr, double di, int64_t dexp, double ez, double ed,
+                           double px_m, int64_t px_e);
+
 /* Reference::error_radius (crates/fd-kernel/src/reference.rs:122-148) into q (len
  * entries): bounds on each orbit point's distance from the exact orbit of the exact centre,
  * for the Bound column (fdc_upload_error_radius). bits >= 0: a fixed-point orbit of that
